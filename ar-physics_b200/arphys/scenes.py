@@ -1,0 +1,214 @@
+"""Scene descriptions and seeded synthetic scene generators.
+
+A `Scene` is everything `FluidSim::new` receives (src/soft_body/mod.rs:58-66)
+after the reference's regions have been seeded into particles: mobile and
+boundary particle records, the material table, an optional interaction table,
+the AABB, kernel radius, integrator, time step, subticks and gravity.
+
+Material constructors follow src/soft_body/material_region/material.rs:61-121
+and the TOML mapping of examples/test_mods/config.rs:351-391 (bulk_visc =
+alpha * h * c, state equation inferred from the keys given).  Masses follow
+the reference's rule (material_region/mod.rs:316-323): start density times
+the lattice cell volume.
+
+The benchmark workloads are the five configurations the benchmark is quoted
+on (2D dam break; 3D fluid + clamped elastic bar at 1,048,576 particles;
+batched scenes; elastic bar for differentiation; batched Rayleigh-Taylor).
+No dataset exists for them: every input is generated here from fixed seeds.
+"""
+from dataclasses import dataclass, field
+import math
+
+import numpy as np
+
+from .abi import (PARTICLE_DTYPE, MATERIAL_DTYPE, INTERACTION_DTYPE, INVALID, EOS_ZERO, EOS_TAIT,
+                  EOS_IDEAL_GAS)
+
+
+@dataclass
+class Scene:
+    particles: np.ndarray
+    boundary: np.ndarray
+    materials: np.ndarray
+    bounds_min: tuple
+    bounds_dim: tuple
+    h: float
+    integrator: str = "rk4"
+    dt: float = 1e-4
+    subticks: int = 1
+    gravity: float = 9.81
+    alpha: float = 0.0
+    interactions: np.ndarray = None
+    interaction_given: np.ndarray = None
+    name: str = ""
+    meta: dict = field(default_factory=dict)
+
+    @property
+    def n(self):
+        return len(self.particles)
+
+    @property
+    def nb(self):
+        return len(self.boundary)
+
+    @property
+    def dim(self):
+        return sum(1 for d in self.bounds_dim if d > 0)
+
+    def n_solids(self):
+        stiff = (self.materials["normal_stiffness"] != 0) | (self.materials["shear_stiffness"] != 0)
+        return int(np.count_nonzero(stiff[self.particles["mat"]]))
+
+
+def material(**kw):
+    m = np.zeros((), dtype=MATERIAL_DTYPE)
+    for k, v in kw.items():
+        m[k] = v
+    return m
+
+
+def liquid(density, sound_speed, h, alpha, visc=0.0, mass=0.0, state=EOS_TAIT, target=None):
+    """An `[objects]` fluid as config.rs:354-375 builds it (Tait unless told otherwise)."""
+    return material(start_den=density, target_den=density if target is None else target,
+                    sound_speed=sound_speed, visc=visc, bulk_visc=np.float32(alpha) * np.float32(h) *
+                    np.float32(sound_speed), state_eq=state, mass=mass, strain_order=2)
+
+
+def elastic_solid(density, lam, mu, mass, strain_order=2, normal_damp=0.0, shear_damp=0.0, plastic=None):
+    m = material(start_den=density, target_den=density, state_eq=EOS_ZERO, mass=mass,
+                 strain_order=strain_order, normal_stiffness=lam, shear_stiffness=mu,
+                 normal_damp=normal_damp, shear_damp=shear_damp)
+    if plastic:
+        m["plastic"] = 1
+        for k, v in plastic.items():
+            m[k] = v
+    return m
+
+
+def immobile(friction, mass):
+    """Material::new_immobile (material.rs:113-120); mass by the lattice rule."""
+    return material(immobile=1, visc=friction, start_den=1.0, target_den=1.0, mass=mass)
+
+
+def lame_from_young(E, nu):
+    """Lame parameters of (E, nu), negated: the reference's force convention
+    (solid.rs:366-368 with r = X_j - X_i and a negative-definite correction
+    matrix) is restoring only for negative stiffness, which is why every solid
+    scene it ships uses negative values (examples/metal_bar.toml:16-17)."""
+    lam = E * nu / ((1 + nu) * (1 - 2 * nu))
+    mu = E / (2 * (1 + nu))
+    return -lam, -mu
+
+
+def particles(pos, mat, den, vel=None):
+    n = len(pos)
+    p = np.zeros(n, dtype=PARTICLE_DTYPE)
+    p["den"] = den
+    p["mat"] = mat
+    p["solid_id"] = INVALID
+    p["pos"][:, :pos.shape[1]] = pos
+    if vel is not None:
+        p["vel"][:, :vel.shape[1]] = vel
+    return p
+
+
+def lattice(origin, counts, spacing):
+    """Cubic lattice points origin + spacing * index, x fastest."""
+    axes = [origin[a] + spacing * np.arange(counts[a], dtype=np.float64) for a in range(len(counts))]
+    grids = np.meshgrid(*axes[::-1], indexing="ij")
+    return np.stack([g.reshape(-1) for g in grids[::-1]], axis=1)
+
+
+def jitter(pos, amp, rng):
+    return pos + rng.uniform(-amp, amp, size=pos.shape)
+
+
+def dam_break_2d(nx=128, ny=128, spacing=0.01, seed=1, steps=1000, integrator="rk4", dt=1e-4,
+                 box=(2.56, 1.28), layers=3, c0=20.0, rho0=1000.0, alpha=0.1, visc=0.0):
+    """2D dam break: nx x ny fluid lattice (spacing 0.01, jitter +-1e-4) at the
+    left wall of a box, `layers` rows of static boundary particles outside the
+    box walls, h = 2 x spacing, Tait (rho0, c0), artificial viscosity alpha."""
+    rng = np.random.default_rng(seed)
+    s = spacing
+    h = 2.0 * s
+    fluid = jitter(lattice((0.5 * s, 0.5 * s), (nx, ny), s), 1e-4, rng)
+    bx, by = box
+    mx, my = int(round(bx / s)), int(round(by / s))
+    ring = lattice((-(layers - 0.5) * s, -(layers - 0.5) * s), (mx + 2 * layers, my + 2 * layers), s)
+    inside = (ring[:, 0] > 0) & (ring[:, 0] < bx) & (ring[:, 1] > 0) & (ring[:, 1] < by)
+    ring = ring[~inside]
+    mats = np.array([
+        immobile(0.0, mass=1.0 * s * s),
+        liquid(rho0, c0, h, alpha, visc=visc, mass=rho0 * s * s),
+    ])
+    return Scene(
+        particles=particles(fluid, 1, rho0), boundary=particles(ring, 0, 1.0), materials=mats,
+        bounds_min=(0.0, 0.0, 0.0, 0.0), bounds_dim=(bx, by, 0.0, 0.0), h=h, integrator=integrator, dt=dt,
+        subticks=1, gravity=9.81, alpha=alpha, name=f"dam_break_2d_{nx}x{ny}", meta={"steps": steps})
+
+
+def fluid_bar_3d(fluid_n=(96, 96, 96), bar_n=(32, 128, 32), floor_n=(256, 128), spacing=0.01, seed=2,
+                 clamp_layers=2, E=1e6, nu=0.3, c0=20.0, rho0=1000.0, alpha=0.1, integrator="rk2", dt=1e-4,
+                 fluid_speed=2.0, box=(2.56, 1.28, 1.28), steps=500):
+    """3D fluid block striking a vertical linear-elastic bar clamped at its
+    base.  Default sizes: 96^3 fluid + 32x128x32 bar (2 clamped layers made
+    immobile) + a 256x128 floor layer = 1,048,576 particles, h = 2 x spacing,
+    Tait fluid, E = 1e6 / nu = 0.3 bar (strain order 2), RK2.
+
+    The fluid starts 2.5 h from the bar moving towards it at `fluid_speed`.
+    """
+    rng = np.random.default_rng(seed)
+    s = spacing
+    h = 2.0 * s
+    bx, by, bz = box
+    fx, fy, fz = fluid_n
+    ax, ay, az = bar_n
+    # fluid block ends at 5/8 of the box; the bar (centred in z) starts 4
+    # spacings after the last fluid column
+    fluid_x0 = max(0.5 * s, 0.625 * bx - s * fx)
+    bar_x0 = fluid_x0 + s * (fx + 4)
+    zc = 0.5 * bz
+    fluid = jitter(lattice((fluid_x0, 0.5 * s, zc - 0.5 * s * fz + 0.5 * s), (fx, fy, fz), s), 1e-4, rng)
+    bar = lattice((bar_x0, 0.5 * s, zc - 0.5 * s * az + 0.5 * s), (ax, ay, az), s)
+    clamped = bar[:, 1] < (clamp_layers * s)
+    floor = lattice((0.5 * s, -0.5 * s, 0.5 * s), (floor_n[0], 1, floor_n[1]), s)
+    lam, mu = lame_from_young(E, nu)
+    mats = np.array([
+        immobile(0.0, mass=1.0 * s ** 3),                         # 0 floor
+        immobile(0.0, mass=1.0 * s ** 3),                         # 1 bar clamp
+        liquid(rho0, c0, h, alpha, mass=rho0 * s ** 3),           # 2 water
+        elastic_solid(rho0, lam, mu, mass=rho0 * s ** 3),         # 3 bar
+    ])
+    vel = np.zeros_like(fluid)
+    vel[:, 0] = fluid_speed
+    mobile = np.concatenate([particles(fluid, 2, rho0, vel), particles(bar[~clamped], 3, rho0)])
+    bnd = np.concatenate([particles(floor, 0, 1.0), particles(bar[clamped], 1, 1.0)])
+    return Scene(
+        particles=mobile, boundary=bnd, materials=mats, bounds_min=(0.0, 0.0, 0.0, 0.0),
+        bounds_dim=(bx, by, bz, 0.0), h=h, integrator=integrator, dt=dt, subticks=1, gravity=9.81, alpha=alpha,
+        name=f"fluid_bar_3d_{len(mobile) + len(bnd)}", meta={"steps": steps, "E": E, "nu": nu})
+
+
+def small_fluid_bar_3d(seed=5, integrator="rk2"):
+    """A few-thousand-particle version of `fluid_bar_3d` for parity tests."""
+    return fluid_bar_3d(fluid_n=(12, 12, 12), bar_n=(4, 16, 4), floor_n=(32, 16), spacing=0.01, seed=seed,
+                        box=(0.32, 0.2, 0.16), integrator=integrator, fluid_speed=2.0)
+
+
+def stretched_bar(n=(20, 4, 4), spacing=0.01, stretch=1.01, lam=-1e5, mu=-1e5, dim=3):
+    """An elastic bar with positions stretched along x from its reference
+    configuration (used to pin the sign of the elastic force)."""
+    s = spacing
+    h = 2.0 * s
+    counts = n[:dim]
+    ref = lattice(tuple(0.3 + 0.5 * s for _ in range(dim)), counts, s)
+    mats = np.array([elastic_solid(1000.0, lam, mu, mass=1000.0 * s ** dim)])
+    p = particles(ref, 0, 1000.0)
+    box_dim = tuple([1.0] * dim + [0.0] * (4 - dim))
+    sc = Scene(particles=p, boundary=np.zeros(0, dtype=PARTICLE_DTYPE), materials=mats,
+               bounds_min=(0.0, 0.0, 0.0, 0.0), bounds_dim=box_dim, h=h, integrator="euler", dt=1e-5,
+               gravity=0.0, name="stretched_bar")
+    stretched = ref.copy()
+    x0 = ref[:, 0].mean()
+    stretched[:, 0] = x0 + (ref[:, 0] - x0) * stretch
+    return sc, stretched

@@ -1,0 +1,179 @@
+"""`FluidSim` over the C ABI, with the reference's method names
+(src/soft_body/mod.rs:45-274): new, init, update, particles, time,
+kernel_radius, num_materials, add_particles.  Errors raise `ArpError`
+carrying the library's status code and message (the reference returns
+`GLError` from `new` and panics elsewhere)."""
+import ctypes
+
+import numpy as np
+
+from .abi import (PARTICLE_DTYPE, SOLID_DTYPE, MATERIAL_DTYPE, INTERACTION_DTYPE, ArpProfile, ArpStats,
+                  ArpDeviceView, check, load_library, ptr, scene_struct)
+
+
+class FluidSim:
+    def __init__(self, scene=None, _handle=None):
+        self._L = load_library()
+        if _handle is not None:
+            self._h = _handle
+        else:
+            sc, keep = scene_struct(scene)
+            h = ctypes.c_void_p()
+            check(self._L.arp_sim_create(ctypes.byref(sc), ctypes.byref(h)))
+            self._h = h
+        self._refresh_counts()
+
+    @classmethod
+    def new(cls, scene):
+        """FluidSim::new (mod.rs:58-166)."""
+        return cls(scene)
+
+    @classmethod
+    def from_toml(cls, path):
+        L = load_library()
+        h = ctypes.c_void_p()
+        check(L.arp_sim_create_from_toml(str(path).encode(), ctypes.byref(h)))
+        return cls(_handle=h)
+
+    def _refresh_counts(self):
+        n, nb, ns = ctypes.c_uint32(), ctypes.c_uint32(), ctypes.c_uint32()
+        check(self._L.arp_sim_counts(self._h, ctypes.byref(n), ctypes.byref(nb), ctypes.byref(ns)))
+        self.n, self.nb, self.ns = n.value, nb.value, ns.value
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._L.arp_sim_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def init(self):
+        """FluidSim::init (mod.rs:213-233)."""
+        check(self._L.arp_sim_init(self._h))
+
+    def update(self):
+        """FluidSim::update (mod.rs:235-274): `subticks` steps."""
+        check(self._L.arp_sim_update(self._h))
+
+    def step(self, n=1):
+        check(self._L.arp_sim_step(self._h, int(n)))
+
+    def time(self):
+        t = ctypes.c_float()
+        check(self._L.arp_sim_time(self._h, ctypes.byref(t)))
+        return t.value
+
+    def kernel_radius(self):
+        t = ctypes.c_float()
+        check(self._L.arp_sim_kernel_radius(self._h, ctypes.byref(t)))
+        return t.value
+
+    def num_materials(self):
+        t = ctypes.c_uint32()
+        check(self._L.arp_sim_num_materials(self._h, ctypes.byref(t)))
+        return t.value
+
+    def dim(self):
+        t = ctypes.c_uint32()
+        check(self._L.arp_sim_dim(self._h, ctypes.byref(t)))
+        return t.value
+
+    def particles(self, out=None):
+        """Mobile particle records in caller order (FluidSim::particles)."""
+        if out is None:
+            out = np.zeros(self.n, dtype=PARTICLE_DTYPE)
+        check(self._L.arp_sim_get_particles(self._h, ptr(out), len(out)))
+        return out
+
+    def solids(self):
+        out = np.zeros(self.ns, dtype=SOLID_DTYPE)
+        if self.ns:
+            check(self._L.arp_sim_get_solids(self._h, ptr(out), len(out)))
+        return out
+
+    def boundary(self):
+        out = np.zeros(self.nb, dtype=PARTICLE_DTYPE)
+        if self.nb:
+            check(self._L.arp_sim_get_boundary(self._h, ptr(out), len(out)))
+        return out
+
+    def materials(self):
+        out = np.zeros(self.num_materials(), dtype=MATERIAL_DTYPE)
+        check(self._L.arp_sim_get_materials(self._h, ptr(out), len(out)))
+        return out
+
+    def interactions(self):
+        m = self.num_materials()
+        out = np.zeros(m * m, dtype=INTERACTION_DTYPE)
+        check(self._L.arp_sim_get_interactions(self._h, ptr(out), len(out)))
+        return out.reshape(m, m)
+
+    def set_particles(self, p):
+        p = np.ascontiguousarray(p, dtype=PARTICLE_DTYPE)
+        check(self._L.arp_sim_set_particles(self._h, ptr(p), len(p)))
+
+    def add_particles(self, p, material, offset=None):
+        """FluidSim::add_particles (mod.rs:180-206); returns True when a
+        material entry was appended."""
+        p = np.ascontiguousarray(p, dtype=PARTICLE_DTYPE)
+        m = np.ascontiguousarray(np.asarray(material, dtype=MATERIAL_DTYPE).reshape(1))
+        off = None if offset is None else np.ascontiguousarray(offset, dtype=np.float32)
+        added = ctypes.c_int(0)
+        check(self._L.arp_sim_add_particles(self._h, ptr(p), len(p), ptr(m), ptr(off), ctypes.byref(added)))
+        self._refresh_counts()
+        return bool(added.value)
+
+    def grid(self):
+        sub = np.zeros(4, np.uint32)
+        nc = ctypes.c_uint32()
+        check(self._L.arp_sim_grid(self._h, ptr(sub), ctypes.byref(nc)))
+        return sub, nc.value
+
+    def neighbors(self):
+        _, nc = self.grid()
+        cell_of = np.zeros(self.n, np.uint32)
+        start = np.zeros(nc + 1, np.uint32)
+        members = np.zeros(max(self.n, 1), np.uint32)
+        nbr = np.zeros(self.n, np.uint32)
+        check(self._L.arp_sim_neighbors(self._h, ptr(cell_of), ptr(start), ptr(members), ptr(nbr)))
+        return dict(cell_of=cell_of, cell_start=start, members=members[:self.n], nbr_count=nbr)
+
+    def boundary_cells(self):
+        _, nc = self.grid()
+        start = np.zeros(nc + 1, np.uint32)
+        members = np.zeros(max(self.nb, 1), np.uint32)
+        check(self._L.arp_sim_boundary_cells(self._h, ptr(start), ptr(members)))
+        return start, members[:self.nb]
+
+    def set_stream(self, stream_handle):
+        check(self._L.arp_sim_set_stream(self._h, ctypes.c_void_p(stream_handle)))
+
+    def synchronize(self):
+        check(self._L.arp_sim_synchronize(self._h))
+
+    def profile_enable(self, on=True):
+        check(self._L.arp_sim_profile_enable(self._h, int(bool(on))))
+
+    def profile_read(self):
+        p = ArpProfile()
+        check(self._L.arp_sim_profile_read(self._h, ctypes.byref(p)))
+        return {k: getattr(p, k) for k, _ in ArpProfile._fields_}
+
+    def stats(self):
+        s = ArpStats()
+        check(self._L.arp_sim_stats(self._h, ctypes.byref(s)))
+        return {k: getattr(s, k) for k, _ in ArpStats._fields_}
+
+    def launch_count(self):
+        c = ctypes.c_uint64()
+        check(self._L.arp_sim_launch_count(self._h, ctypes.byref(c)))
+        return c.value
+
+    def device_state(self):
+        v = ArpDeviceView()
+        check(self._L.arp_sim_device_state(self._h, ctypes.byref(v)))
+        return dict(pos_den=v.pos_den, vel_mat=v.vel_mat, orig_id=v.orig_id, n=v.n)

@@ -1,0 +1,188 @@
+// arp_internal.h -- device-side data layout and kernel entry points of libarphys.
+//
+// State layout in HBM (structure of arrays, cell-sorted):
+//   pos_den  float4[N]  x, y, z, density          (the reference's pos.xyz + den)
+//   vel_mat  float4[N]  vx, vy, vz, material bits  (vel.xyz + mat)
+//   orig     uint32[N]  caller-order particle id of each slot
+//   sid      uint32[N]  solid id of each slot or ARP_INVALID_INDEX
+// Solid data stays in solid-id order (solid ids never change):
+//   ref      float4[Ns] reference position
+//   ep       float4[4*Ns] plastic strain mat4, column-major (SolidParticle.stress)
+//   L        float4[3*Ns] correction matrix columns (constant, built at init)
+// Particles are re-sorted by cell at the start of every integrator step; the
+// grid of each later RK stage is a permutation over those slots.
+#pragma once
+
+#include <cstdint>
+#include <cuda_runtime.h>
+
+#include "../../include/arphys.h"
+
+namespace arp {
+
+constexpr uint32_t kInvalid = 0xFFFFFFFFu;
+constexpr uint32_t kBucketSlots = 128;  // neighbor_list.rs:45
+constexpr int kMaxMaterials = 32;
+
+// Uniform grid of NeighborList::new (neighbor_list.rs:199-217).
+struct Grid {
+    float min[3];
+    float dim[3];
+    uint32_t sub[3];
+    uint32_t ncells;
+};
+
+// Per-material constants the kernels read (a subset of `Material`).
+struct DevMat {
+    float mass, start_den, sound_speed, target_den;
+    float visc, bulk_visc, lam, mu;
+    float lam_d, mu_d, yield_strength, work_hardening;
+    float work_hardening_exp, kinematic_hardening, relaxation_time, vol0;  // vol0 = mass / start_den
+    uint32_t state_eq, stiff, plastic;
+    int32_t strain_order;
+};
+
+struct DevInter {
+    uint32_t potential;
+    float strength, radius, dampening, friction;
+};
+
+// Scalars shared by the force kernels.  Products are rounded exactly as the
+// shaders group them (e.g. EPSILON*h*h = (0.1*h)*h).
+struct Params {
+    Grid grid;
+    uint32_t dim, nmat;
+    float h, h2, kconst, g;
+    float eps_hh;   // (0.1f * h) * h
+    float eps_h;    // 0.1f * h
+    float hg_h;     // (10 * 0.1f) * h
+    float rcut, rcut2, r_geom;  // 8h, (8h)^2, h*h/(8h)
+};
+
+// Health counters written by device code.
+struct DevStats {
+    uint32_t max_cell_occupancy;
+    uint32_t overflow_cells;
+    uint32_t nonfinite_positions;
+    uint32_t clamped_coordinates;
+};
+
+// One stage of the Runge-Kutta epilogue (fused into the fluid kernel).
+// y_next = y0 + sum_j c_next[j] * k_j (j <= stage), acc += c_acc * k_stage,
+// on the last stage y_new = y0 + acc.
+struct StageCoefs {
+    int stage;          // 0-based
+    int last;           // 1 when this stage ends the step
+    float c_next[4];    // a[stage+1][j] * dt, j <= stage (unused when last)
+    float c_acc;        // b[stage] * dt
+    int acc_first;      // 1 when no earlier stage contributed to acc
+    int store_k;        // 1 when k of this stage is read by a later stage
+};
+
+struct StageBuffers {
+    const float4* y0_pd;   // y0 (storage order)
+    const float4* y0_vm;
+    float4* next_pd;       // y_{s+1} or y_new (storage order)
+    float4* next_vm;
+    float4* acc_pd;        // b-weighted derivative accumulator
+    float4* acc_vm;
+    float4* kst_pd[4];     // stored stage derivatives (non-diagonal tableaus)
+    float4* kst_vm[4];
+};
+
+// ---- neighbor grid (neighbor.cu) -------------------------------------------
+struct GridBuffers {
+    uint32_t* key;         // [cap] cell id of each slot (ncells for non-finite)
+    uint32_t* rank;        // [cap] arrival rank inside the cell
+    uint32_t* count;       // [ncells + 1] occupancy (zeroed by the scan)
+    uint32_t* start;       // [ncells + 2] exclusive prefix of count
+    uint32_t* perm;        // [cap] sorted index -> slot
+    uint32_t* block_sums;  // scan partials
+    uint32_t block_sums_cap;
+};
+
+// Build cell_start / perm for `n` positions.  Counting sort: keys and
+// histogram, exclusive scan, scatter, then ascending slot order within each
+// cell.  Returns the number of kernel launches issued.
+int build_grid(const float4* pos, uint32_t n, const Grid& grid, GridBuffers& gb, DevStats* stats,
+               const uint32_t* boundary_start, cudaStream_t st);
+
+// Exclusive scan of `len` counts into out (len entries); clears `count`.
+int exclusive_scan(uint32_t* count, uint32_t len, uint32_t* out, uint32_t* block_sums, cudaStream_t st);
+// Scratch entries exclusive_scan needs for `len` items.
+uint32_t scan_block_sums_needed(uint32_t len);
+
+// out[k] = in[perm[k]] for float4 / uint32 arrays (nullptr entries skipped).
+int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* a_out, const float4* b_in,
+                  float4* b_out, const uint32_t* c_in, uint32_t* c_out, const uint32_t* d_in, uint32_t* d_out,
+                  cudaStream_t st);
+// slot_of[sid[k]] = k for solid slots.
+int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st);
+// Neighbor counts within h of each sorted particle (mobile + boundary),
+// computed with separately rounded float products for bit-exact output.
+int count_neighbors(const float4* xs, const uint32_t* start, uint32_t n, const float4* bxs,
+                    const uint32_t* bstart, const Params& P, uint32_t* out_sorted, cudaStream_t st);
+
+// ---- fluid forces + stage update (fluid.cu) ---------------------------------
+struct FluidArgs {
+    const float4* xs;        // sorted stage positions/density
+    const float4* vs;        // sorted stage velocity/material
+    const uint32_t* start;   // mobile cell start (ncells + 1)
+    const float4* bxs;       // boundary sorted
+    const float4* bvs;
+    const uint32_t* bstart;  // boundary cell start
+    const uint32_t* perm;    // sorted -> storage slot (nullptr = identity)
+    const uint32_t* sid;     // storage-order solid id
+    const uint32_t* sid_of_boundary_index;  // solid id of mobile particle with caller id == boundary caller id
+    const uint32_t* borig;   // boundary caller ids, sorted
+    const float4* ksol;      // per-solid solid-term acceleration (nullptr when the solid branch is off)
+    const DevMat* mats;
+    const DevInter* inter;
+    uint32_t n;
+    uint32_t n_mobile_total;  // particle count for the Q2 range check
+    int solid_branch;
+    int any_stiff_immobile;
+};
+int launch_fluid(const FluidArgs& a, const Params& P, const StageCoefs& c, const StageBuffers& b,
+                 cudaStream_t st);
+
+// ---- solids (solid.cu) ------------------------------------------------------
+struct SolidRefList {
+    uint32_t* off;   // [ns + 1]
+    uint32_t* nbr;   // [nnz] solid id | 0x80000000 when same material
+    float4* gw;      // [nnz] grad_w(X_j - X_i).xyz, w = vol0 of j
+    uint32_t nnz;
+};
+// Reference-neighbor lists: counts per solid (pass 1), then after an
+// exclusive scan of the counts into rl.off, the entries and L (pass 2).
+// `gb` holds a grid built over the reference positions.
+int ref_lists_count(const float4* ref, uint32_t ns, const GridBuffers& gb, const Params& P, uint32_t* count,
+                    cudaStream_t st);
+int ref_lists_fill(const float4* ref, const uint32_t* mat_of_solid, uint32_t ns, const GridBuffers& gb,
+                   const Params& P, const DevMat* mats, SolidRefList& rl, float4* L, cudaStream_t st);
+
+struct SolidArgs {
+    const float4* pd;         // stage state, storage order
+    const float4* vm;
+    const uint32_t* slot_of;  // solid id -> storage slot
+    const float4* ref;
+    const float4* L;
+    SolidRefList rl;
+    const float4* ep;         // stage plastic strain (4 per solid)
+    const float4* ep0;        // step-start plastic strain
+    float4* ep_next;          // stage / step output
+    float4* ep_acc;
+    float4* ep_kst[4];
+    float4* F;                // [3*ns] deformation gradient columns (stage scratch)
+    float4* A;                // [3*ns] sigma * L columns (stage scratch)
+    float4* ksol;             // [ns] solid-term acceleration
+    const float4* xs;         // sorted stage positions (current-neighbor loop)
+    const float4* vs;
+    const uint32_t* start;
+    const uint32_t* sid_sorted;
+    const DevMat* mats;
+    uint32_t ns;
+};
+int launch_solid(const SolidArgs& a, const Params& P, const StageCoefs& c, cudaStream_t st);
+
+}  // namespace arp

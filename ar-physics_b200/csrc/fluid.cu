@@ -1,0 +1,308 @@
+// fluid.cu -- fluid forces with the Runge-Kutta stage update fused at the tail.
+//
+// Replaces the reference's `fluid_forces` shader (src/soft_body/shaders/
+// fluid.rs:95-336) and the lin_comb stage arithmetic that follows it
+// (src/soft_body/particle_state/particles.rs:8-154).  The shader runs one
+// 81-invocation workgroup per particle (27 cells x 3 strided lanes) with a
+// shared-memory tree reduction; here one thread owns one cell-sorted particle
+// and walks the 3x3(x3) neighborhood as 3 (2D) or 9 (3D) contiguous row
+// ranges of the sorted arrays, so neighbor loads are coalesced across a warp
+// (consecutive threads sit in the same or adjacent cells).
+//
+// Per pair the math is the shader's, term by term: continuity density rate,
+// symmetric pressure force with the equation of state evaluated for both
+// particles, contact potential (with the shader's argument order) and
+// friction, physical viscosity and artificial viscosity.  Every term carries
+// grad_w, which is zero for |r| >= h, so pairs outside the kernel radius are
+// skipped before any of it is evaluated.
+//
+// Epilogue: k = (v, drho/dt, F/rho - g y) (+ the solid term for solid
+// particles) is combined into the next stage state y0 + sum c_j k_j and the
+// b-weighted accumulator with separately rounded products and sums, the same
+// order the oracle uses.
+#include "grid.cuh"
+
+namespace arp {
+
+namespace {
+
+struct FluidMat {
+    float mass, c, d0, visc, bulk;
+    uint32_t eos, stiff, pad;
+};
+
+__device__ __forceinline__ float pow7(float x) {
+    const float x2 = x * x;
+    const float x3 = x2 * x;
+    const float x6 = x3 * x3;
+    return x6 * x;
+}
+
+// fluid.rs:131-138
+__device__ __forceinline__ float eos_pressure(uint32_t eq, float density, float c, float d0) {
+    switch (eq) {
+        case ARP_EOS_CONSTANT: return c * c;
+        case ARP_EOS_IDEAL_GAS: return c * c * (density - d0);
+        case ARP_EOS_TAIT: return (c * c * d0 / 7.0f) * (pow7(density / d0) - 1.0f);
+        default: return 0.0f;
+    }
+}
+
+// fluid.rs:140-153 (called with radius and strength in the shader's order)
+__device__ __forceinline__ float contact_potential(uint32_t eq, float r, float strength, float r0) {
+    switch (eq) {
+        case ARP_CONTACT_CONSTANT: return r <= r0 ? strength : 0.0f;
+        case ARP_CONTACT_LINEAR: return strength * (r0 - r);
+        case ARP_CONTACT_TAIT: return (strength * r / 7.0f) * (pow7(r0 / r) - 1.0f);
+        case ARP_CONTACT_LENNARD_JONES: {
+            float f = r0 / r;
+            f *= f * f;
+            f *= f;
+            return strength * (f * f - 2.0f * f);
+        }
+        case ARP_CONTACT_HERTZ: return (strength * r0 / 7.0f) * (pow7(r / r0) - 1.0f);
+        default: return 0.0f;
+    }
+}
+
+struct Self {
+    float3 x, v;
+    float d1, m1, pterm1, f1, bf1;
+    uint32_t mat;
+    bool elastic;
+};
+
+struct Acc {
+    float den;
+    float3 f;
+};
+
+template <int DIM, bool BOUNDARY>
+__device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, uint32_t mat2, bool elastic2,
+                                     const FluidMat* __restrict__ sm, const DevInter* __restrict__ si,
+                                     uint32_t nmat, const Params& P, Acc& acc) {
+    const float rx = xj.x - s.x.x, ry = xj.y - s.x.y, rz = DIM == 3 ? xj.z - s.x.z : 0.0f;
+    const float r2 = DIM == 3 ? (rx * rx + ry * ry) + rz * rz : rx * rx + ry * ry;
+    const float diff = P.h2 - r2;
+    if (!(diff > 0.0f)) return;
+    const float gws = -6.0f * P.kconst * diff * diff;
+    const float gx = gws * rx, gy = gws * ry, gz = gws * rz;
+    const float vx = vj.x - s.v.x, vy = vj.y - s.v.y, vz = DIM == 3 ? vj.z - s.v.z : 0.0f;
+    const float d2 = xj.w;
+    const FluidMat m2 = sm[mat2];
+    const float p2 = eos_pressure(m2.eos, d2, m2.c, m2.d0);
+    const float vgw = DIM == 3 ? (vx * gx + vy * gy) + vz * gz : vx * gx + vy * gy;
+    if (!BOUNDARY) acc.den += m2.mass * vgw;
+    const float pf = s.m1 * m2.mass * (s.pterm1 + p2 / (d2 * d2));
+    acc.f.x += pf * gx;
+    acc.f.y += pf * gy;
+    acc.f.z += pf * gz;
+    const DevInter it = si[s.mat * nmat + mat2];
+    if (it.potential != ARP_CONTACT_ZERO) {
+        const float cp = contact_potential(it.potential, sqrtf(r2), it.radius, it.strength);
+        if (cp != 0.0f) {
+            const float cs = m2.mass * cp / d2;
+            const float cx = cs * gx, cy = cs * gy, cz = cs * gz;
+            if ((s.elastic || elastic2 || BOUNDARY) && s.mat != mat2) {
+                // fluid.rs:278-285: friction along the normalised tangential velocity
+                const float ix = rx / r2, iy = ry / r2, iz = rz / r2;
+                const float cr = DIM == 3 ? (cx * rx + cy * ry) + cz * rz : cx * rx + cy * ry;
+                const float nx = ix * cr, ny = iy * cr, nz = iz * cr;
+                const float vr = DIM == 3 ? (vx * rx + vy * ry) + vz * rz : vx * rx + vy * ry;
+                float tx = vx - ix * vr, ty = vy - iy * vr, tz = vz - iz * vr;
+                float tl = sqrtf(DIM == 3 ? (tx * tx + ty * ty) + tz * tz : tx * tx + ty * ty);
+                tx /= tl; ty /= tl; tz /= tl;
+                if (isfinite(tx) && isfinite(ty) && isfinite(tz)) {
+                    // normalize() applied a second time, as the shader does
+                    const float tl2 = sqrtf(DIM == 3 ? (tx * tx + ty * ty) + tz * tz : tx * tx + ty * ty);
+                    const float nl = sqrtf(DIM == 3 ? (nx * nx + ny * ny) + nz * nz : nx * nx + ny * ny);
+                    const float fr = it.friction * nl;
+                    acc.f.x += fr * (tx / tl2);
+                    acc.f.y += fr * (ty / tl2);
+                    acc.f.z += fr * (tz / tl2);
+                }
+            }
+            acc.f.x += cx;
+            acc.f.y += cy;
+            acc.f.z += cz;
+        }
+    }
+    if (!BOUNDARY) {
+        const float denom = r2 + P.eps_hh;
+        if (!s.elastic) {
+            const float fsum = s.f1 + m2.visc;
+            if (fsum != 0.0f) {
+                const float rgw = DIM == 3 ? (rx * gx + ry * gy) + rz * gz : rx * gx + ry * gy;
+                const float q = s.m1 * m2.mass * fsum * rgw;
+                const float dd = s.d1 * d2 * denom;
+                acc.f.x -= (q * vx) / dd;
+                acc.f.y -= (q * vy) / dd;
+                acc.f.z -= (q * vz) / dd;
+            }
+        }
+        const float f_ = s.mat == mat2 ? s.bf1 + m2.bulk : it.dampening;
+        if (f_ != 0.0f) {
+            const float vr = DIM == 3 ? (vx * rx + vy * ry) + vz * rz : vx * rx + vy * ry;
+            const float q = s.m1 * m2.mass * ((f_ * vr) / ((s.d1 + d2) * denom));
+            acc.f.x -= q * gx;
+            acc.f.y -= q * gy;
+            acc.f.z -= q * gz;
+        }
+    }
+}
+
+__device__ __forceinline__ float4 comb(float4 y0, float4 t, bool keep_w) {
+    float4 r;
+    r.x = __fadd_rn(y0.x, t.x);
+    r.y = __fadd_rn(y0.y, t.y);
+    r.z = __fadd_rn(y0.z, t.z);
+    r.w = keep_w ? y0.w : __fadd_rn(y0.w, t.w);
+    return r;
+}
+__device__ __forceinline__ float4 axpy(float c, float4 k, float4 t) {
+    return make_float4(__fadd_rn(t.x, __fmul_rn(c, k.x)), __fadd_rn(t.y, __fmul_rn(c, k.y)),
+                       __fadd_rn(t.z, __fmul_rn(c, k.z)), __fadd_rn(t.w, __fmul_rn(c, k.w)));
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(256) k_fluid(FluidArgs a, Params P, StageCoefs c, StageBuffers b) {
+    extern __shared__ unsigned char smem_raw[];
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw);
+    DevInter* si = reinterpret_cast<DevInter*>(smem_raw + sizeof(FluidMat) * P.nmat);
+    for (uint32_t i = threadIdx.x; i < P.nmat; i += blockDim.x) {
+        const DevMat m = a.mats[i];
+        sm[i] = FluidMat{m.mass, m.sound_speed, m.target_den, m.visc, m.bulk_visc, m.state_eq, m.stiff, 0u};
+    }
+    for (uint32_t i = threadIdx.x; i < P.nmat * P.nmat; i += blockDim.x) si[i] = a.inter[i];
+    __syncthreads();
+
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const float4 xi = a.xs[k];
+    const float4 vi = a.vs[k];
+    const uint32_t slot = a.perm ? a.perm[k] : k;
+    const uint32_t sid = a.sid[slot];
+    Self s;
+    s.x = make_float3(xi.x, xi.y, xi.z);
+    s.v = make_float3(vi.x, vi.y, vi.z);
+    s.mat = __float_as_uint(vi.w);
+    s.d1 = xi.w;
+    const FluidMat m1 = sm[s.mat];
+    s.m1 = m1.mass;
+    s.f1 = m1.visc;
+    s.bf1 = m1.bulk;
+    s.elastic = sid != kInvalid && m1.stiff;
+    const float p1 = eos_pressure(m1.eos, s.d1, m1.c, m1.d0);
+    s.pterm1 = p1 / (s.d1 * s.d1);
+
+    Acc acc;
+    acc.den = 0.0f;
+    acc.f = make_float3(0.0f, 0.0f, 0.0f);
+    if (finite3(xi)) {
+        const Grid& g = P.grid;
+        const CellCoord cc = cell_coord(xi, g);
+        const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
+        const int zlo = DIM == 3 ? -1 : 0, zhi = DIM == 3 ? 1 : 0;
+        for (int dz = zlo; dz <= zhi; ++dz) {
+            const int z = cc.z + dz;
+            if (z < 0 || z >= (int)g.sub[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = cc.y + dy;
+                if (y < 0 || y >= (int)g.sub[1]) continue;
+                const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
+                const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
+                for (uint32_t j = bb; j < be; ++j) {
+                    const float4 xj = a.bxs[j];
+                    const float4 vj = a.bvs[j];
+                    const uint32_t mat2 = __float_as_uint(vj.w);
+                    bool elastic2 = false;
+                    if (a.any_stiff_immobile && sm[mat2].stiff) {
+                        // fluid.rs:227: the boundary index reads the mobile array's solid id
+                        const uint32_t bi = a.borig[j];
+                        elastic2 = bi < a.n_mobile_total && a.sid_of_boundary_index[bi] != kInvalid;
+                    }
+                    pair<DIM, true>(s, xj, vj, mat2, elastic2, sm, si, P.nmat, P, acc);
+                }
+                const uint32_t jb = a.start[c0], je = a.start[c1];
+                for (uint32_t j = jb; j < je; ++j) {
+                    const float4 xj = a.xs[j];
+                    const float4 vj = a.vs[j];
+                    const uint32_t mat2 = __float_as_uint(vj.w);
+                    pair<DIM, false>(s, xj, vj, mat2, sm[mat2].stiff != 0u, sm, si, P.nmat, P, acc);
+                }
+            }
+        }
+    }
+
+    // derivative record (fluid.rs:329-333), plus the solid term when active
+    float4 kpd = make_float4(vi.x, vi.y, vi.z, acc.den);
+    float4 kvm = make_float4(__fdiv_rn(acc.f.x, s.d1), __fadd_rn(__fdiv_rn(acc.f.y, s.d1), -P.g),
+                             __fdiv_rn(acc.f.z, s.d1), 0.0f);
+    if (a.solid_branch && sid != kInvalid) {
+        const float4 ks = a.ksol[sid];
+        kpd.x = __fadd_rn(kpd.x, vi.x);
+        kpd.y = __fadd_rn(kpd.y, vi.y);
+        kpd.z = __fadd_rn(kpd.z, vi.z);
+        kvm.x = __fadd_rn(kvm.x, ks.x);
+        kvm.y = __fadd_rn(kvm.y, ks.y);
+        kvm.z = __fadd_rn(kvm.z, ks.z);
+    }
+
+    // Runge-Kutta stage epilogue
+    if (c.store_k) {
+        b.kst_pd[c.stage][slot] = kpd;
+        b.kst_vm[c.stage][slot] = kvm;
+    }
+    const float4 y0p = b.y0_pd[slot];
+    const float4 y0v = b.y0_vm[slot];
+    float4 accp = make_float4(0.f, 0.f, 0.f, 0.f), accv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c.c_acc != 0.0f) {
+        if (!c.acc_first) {
+            accp = b.acc_pd[slot];
+            accv = b.acc_vm[slot];
+        }
+        accp = axpy(c.c_acc, kpd, accp);
+        accv = axpy(c.c_acc, kvm, accv);
+        if (!c.last) {
+            b.acc_pd[slot] = accp;
+            b.acc_vm[slot] = accv;
+        }
+    } else if (c.last) {
+        accp = b.acc_pd[slot];
+        accv = b.acc_vm[slot];
+    }
+    if (c.last) {
+        b.next_pd[slot] = comb(y0p, accp, false);
+        b.next_vm[slot] = comb(y0v, accv, true);
+    } else {
+        float4 tp = make_float4(0.f, 0.f, 0.f, 0.f), tv = make_float4(0.f, 0.f, 0.f, 0.f);
+        for (int j = 0; j < c.stage; ++j) {
+            if (c.c_next[j] == 0.0f) continue;
+            tp = axpy(c.c_next[j], b.kst_pd[j][slot], tp);
+            tv = axpy(c.c_next[j], b.kst_vm[j][slot], tv);
+        }
+        if (c.c_next[c.stage] != 0.0f) {
+            tp = axpy(c.c_next[c.stage], kpd, tp);
+            tv = axpy(c.c_next[c.stage], kvm, tv);
+        }
+        b.next_pd[slot] = comb(y0p, tp, false);
+        b.next_vm[slot] = comb(y0v, tv, true);
+    }
+}
+
+}  // namespace
+
+int launch_fluid(const FluidArgs& a, const Params& P, const StageCoefs& c, const StageBuffers& b, cudaStream_t st) {
+    if (a.n == 0) return 0;
+    const int threads = 256;
+    const uint32_t blocks = (a.n + threads - 1) / threads;
+    const size_t smem = sizeof(FluidMat) * P.nmat + sizeof(DevInter) * P.nmat * P.nmat;
+    if (P.dim == 3)
+        k_fluid<3><<<blocks, threads, smem, st>>>(a, P, c, b);
+    else
+        k_fluid<2><<<blocks, threads, smem, st>>>(a, P, c, b);
+    return 1;
+}
+
+}  // namespace arp

@@ -1,0 +1,273 @@
+// neighbor.cu -- uniform-grid neighbor build (replaces reset_buckets +
+// fill_buckets, src/soft_body/neighbor_list.rs:37-143 and update_contents
+// :224-294).
+//
+// The reference appends each particle into a fixed 128-slot bucket with
+// atomics, so slot order is nondeterministic on a GPU and particles past 128
+// are dropped.  Here the grid is a counting sort with no capacity limit:
+//   1. cell key + histogram (one atomic per particle; the returned value is
+//      the particle's arrival rank inside its cell);
+//   2. exclusive scan of the histogram (warp-shuffle block scan, block sums,
+//      offsets), which also clears the histogram for the next build;
+//   3. scatter to perm[start[key] + rank];
+//   4. sort each cell's run by slot so the order is deterministic; this also
+//      records the largest occupancy and cells over the reference's 128.
+// Memory traffic per particle: 16 B position read, 4+4 B key/rank write and
+// read, 4 B perm write, 4+4 B perm read/write in the run sort.
+#include <cstdio>
+
+#include "grid.cuh"
+
+namespace arp {
+
+namespace {
+
+constexpr int kThreads = 256;
+constexpr int kScanThreads = 1024;
+constexpr int kScanItems = 4;  // per thread
+constexpr int kScanTile = kScanThreads * kScanItems;
+
+__global__ void k_cell_keys(const float4* __restrict__ pos, uint32_t n, Grid grid, uint32_t* __restrict__ key,
+                            uint32_t* __restrict__ rank, uint32_t* __restrict__ count, DevStats* stats) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    float4 p = pos[i];
+    uint32_t k;
+    if (!finite3(p)) {
+        k = grid.ncells;
+        if (stats) atomicAdd(&stats->nonfinite_positions, 1u);
+    } else {
+        k = cell_id(cell_coord(p, grid), grid);
+        if (stats) {
+            // a coordinate on the upper face would hash one past the last cell
+            bool face = (grid.dim[0] != 0.0f && p.x == grid.min[0] + grid.dim[0]) ||
+                        (grid.dim[1] != 0.0f && p.y == grid.min[1] + grid.dim[1]) ||
+                        (grid.dim[2] != 0.0f && p.z == grid.min[2] + grid.dim[2]);
+            if (face) atomicAdd(&stats->clamped_coordinates, 1u);
+        }
+    }
+    key[i] = k;
+    rank[i] = atomicAdd(&count[k], 1u);
+}
+
+__device__ __forceinline__ uint32_t warp_incl_scan(uint32_t v) {
+    const int lane = threadIdx.x & 31;
+#pragma unroll
+    for (int o = 1; o < 32; o <<= 1) {
+        uint32_t t = __shfl_up_sync(0xffffffffu, v, o);
+        if (lane >= o) v += t;
+    }
+    return v;
+}
+
+// Block-wide exclusive scan of one value per thread (blockDim.x a multiple
+// of 32, at most 1024).  The block total is excl + v of the last thread.
+__device__ __forceinline__ void block_excl_scan(uint32_t v, uint32_t& excl) {
+    __shared__ uint32_t warp_tot[kScanThreads / 32];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const int nwarps = (int)(blockDim.x >> 5);
+    uint32_t inc = warp_incl_scan(v);
+    if (lane == 31) warp_tot[warp] = inc;
+    __syncthreads();
+    if (warp == 0) {
+        uint32_t w = lane < nwarps ? warp_tot[lane] : 0u;
+        uint32_t wi = warp_incl_scan(w);
+        if (lane < nwarps) warp_tot[lane] = wi - w;
+    }
+    __syncthreads();
+    excl = warp_tot[warp] + inc - v;
+}
+
+__global__ void k_scan_tiles(uint32_t* __restrict__ count, uint32_t len, uint32_t* __restrict__ out,
+                             uint32_t* __restrict__ block_sums) {
+    __shared__ uint32_t last_total;
+    const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
+    uint32_t v[kScanItems];
+    uint32_t s = 0;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        uint32_t idx = base + j;
+        v[j] = idx < len ? count[idx] : 0u;
+        if (idx < len) count[idx] = 0u;  // ready for the next histogram
+        s += v[j];
+    }
+    uint32_t excl;
+    block_excl_scan(s, excl);
+    if (threadIdx.x == blockDim.x - 1) last_total = excl + s;
+    uint32_t run = excl;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        uint32_t idx = base + j;
+        if (idx < len) out[idx] = run;
+        run += v[j];
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) block_sums[blockIdx.x] = last_total;
+}
+
+// One block: exclusive scan of the tile totals in chunks, carrying the sum.
+__global__ void k_scan_sums(uint32_t* __restrict__ sums, uint32_t nb) {
+    __shared__ uint32_t carry;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (uint32_t base = 0; base < nb; base += blockDim.x) {
+        uint32_t idx = base + threadIdx.x;
+        uint32_t v = idx < nb ? sums[idx] : 0u;
+        uint32_t excl;
+        block_excl_scan(v, excl);
+        __shared__ uint32_t chunk_total;
+        if (threadIdx.x == blockDim.x - 1) chunk_total = excl + v;
+        if (idx < nb) sums[idx] = carry + excl;
+        __syncthreads();
+        if (threadIdx.x == 0) carry += chunk_total;
+        __syncthreads();
+    }
+}
+
+__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t len, const uint32_t* __restrict__ sums) {
+    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
+    if (idx < len) out[idx] += sums[idx / kScanTile];
+}
+
+__global__ void k_scatter(const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank, uint32_t n,
+                          const uint32_t* __restrict__ start, uint32_t* __restrict__ perm) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    perm[start[key[i]] + rank[i]] = i;
+}
+
+// Sort each cell's run ascending (insertion sort; runs longer than 256 are
+// left in arrival order, which is still a valid grid).
+__global__ void k_sort_runs(const uint32_t* __restrict__ start, uint32_t ncells, uint32_t* __restrict__ perm,
+                            const uint32_t* __restrict__ boundary_start, DevStats* stats) {
+    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c > ncells) return;  // includes the non-finite bucket at index ncells
+    const uint32_t b = start[c], e = start[c + 1];
+    const uint32_t len = e - b;
+    if (stats && c < ncells) {
+        uint32_t occ = len + (boundary_start ? boundary_start[c + 1] - boundary_start[c] : 0u);
+        if (occ > 0) atomicMax(&stats->max_cell_occupancy, occ);
+        if (occ > kBucketSlots) atomicAdd(&stats->overflow_cells, 1u);
+    }
+    if (len < 2 || len > 256) return;
+    for (uint32_t i = b + 1; i < e; ++i) {
+        uint32_t v = perm[i];
+        uint32_t j = i;
+        while (j > b && perm[j - 1] > v) {
+            perm[j] = perm[j - 1];
+            --j;
+        }
+        perm[j] = v;
+    }
+}
+
+__global__ void k_gather(const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ a_in,
+                         float4* __restrict__ a_out, const float4* __restrict__ b_in, float4* __restrict__ b_out,
+                         const uint32_t* __restrict__ c_in, uint32_t* __restrict__ c_out,
+                         const uint32_t* __restrict__ d_in, uint32_t* __restrict__ d_out) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t s = perm[k];
+    if (a_out) a_out[k] = a_in[s];
+    if (b_out) b_out[k] = b_in[s];
+    if (c_out) c_out[k] = c_in[s];
+    if (d_out) d_out[k] = d_in[s];
+}
+
+__global__ void k_index_solids(const uint32_t* __restrict__ sid, uint32_t n, uint32_t* __restrict__ slot_of) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t s = sid[k];
+    if (s != kInvalid) slot_of[s] = k;
+}
+
+__device__ __forceinline__ bool within_h_exact(float4 q, float4 p, float h2) {
+    const float rx = __fsub_rn(q.x, p.x), ry = __fsub_rn(q.y, p.y), rz = __fsub_rn(q.z, p.z);
+    const float d = __fadd_rn(__fadd_rn(__fmul_rn(rx, rx), __fmul_rn(ry, ry)), __fmul_rn(rz, rz));
+    return __fsub_rn(h2, d) > 0.0f;
+}
+
+__global__ void k_count_neighbors(const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t n,
+                                  const float4* __restrict__ bxs, const uint32_t* __restrict__ bstart, Params P,
+                                  uint32_t* __restrict__ out) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 p = xs[k];
+    uint32_t cnt = 0;
+    if (finite3(p)) {
+        const Grid& g = P.grid;
+        const CellCoord c = cell_coord(p, g);
+        const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, (int)g.sub[0] - 1);
+        for (int dz = -1; dz <= 1; ++dz) {
+            const int z = c.z + dz;
+            if (z < 0 || z >= (int)g.sub[2]) continue;
+            for (int dy = -1; dy <= 1; ++dy) {
+                const int y = c.y + dy;
+                if (y < 0 || y >= (int)g.sub[1]) continue;
+                const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
+                if (bstart)
+                    for (uint32_t j = bstart[c0]; j < bstart[c1]; ++j) cnt += within_h_exact(bxs[j], p, P.h2);
+                for (uint32_t j = start[c0]; j < start[c1]; ++j) cnt += within_h_exact(xs[j], p, P.h2);
+            }
+        }
+    }
+    out[k] = cnt;
+}
+
+inline uint32_t blocks_for(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / (uint32_t)t; }
+
+}  // namespace
+
+int build_grid(const float4* pos, uint32_t n, const Grid& grid, GridBuffers& gb, DevStats* stats,
+               const uint32_t* boundary_start, cudaStream_t st) {
+    int launches = 0;
+    if (n > 0) {
+        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, grid, gb.key, gb.rank, gb.count, stats);
+        ++launches;
+    }
+    // cells, the non-finite bucket, and the total
+    launches += exclusive_scan(gb.count, grid.ncells + 2, gb.start, gb.block_sums, st);
+    if (n > 0) {
+        k_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>(gb.key, gb.rank, n, gb.start, gb.perm);
+        ++launches;
+    }
+    k_sort_runs<<<blocks_for(grid.ncells + 1, kThreads), kThreads, 0, st>>>(gb.start, grid.ncells, gb.perm,
+                                                                            boundary_start, stats);
+    ++launches;
+    return launches;
+}
+
+uint32_t scan_block_sums_needed(uint32_t len) { return blocks_for(len, kScanTile) + 1; }
+
+int exclusive_scan(uint32_t* count, uint32_t len, uint32_t* out, uint32_t* block_sums, cudaStream_t st) {
+    const uint32_t tiles = blocks_for(len, kScanTile);
+    k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(count, len, out, block_sums);
+    k_scan_sums<<<1, kScanThreads, 0, st>>>(block_sums, tiles);
+    k_scan_add<<<blocks_for(len, kThreads), kThreads, 0, st>>>(out, len, block_sums);
+    return 3;
+}
+
+int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* a_out, const float4* b_in,
+                  float4* b_out, const uint32_t* c_in, uint32_t* c_out, const uint32_t* d_in, uint32_t* d_out,
+                  cudaStream_t st) {
+    if (n == 0) return 0;
+    k_gather<<<blocks_for(n, kThreads), kThreads, 0, st>>>(perm, n, a_in, a_out, b_in, b_out, c_in, c_out, d_in,
+                                                           d_out);
+    return 1;
+}
+
+int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_index_solids<<<blocks_for(n, kThreads), kThreads, 0, st>>>(sid, n, slot_of);
+    return 1;
+}
+
+int count_neighbors(const float4* xs, const uint32_t* start, uint32_t n, const float4* bxs, const uint32_t* bstart,
+                    const Params& P, uint32_t* out_sorted, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_count_neighbors<<<blocks_for(n, kThreads), kThreads, 0, st>>>(xs, start, n, bxs, bstart, P, out_sorted);
+    return 1;
+}
+
+}  // namespace arp

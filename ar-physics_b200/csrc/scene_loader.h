@@ -1,0 +1,48 @@
+// scene_loader.h -- TOML scene files (the reference's examples/*.toml schema)
+// turned into an arp_scene.
+#pragma once
+
+#include <string>
+#include <vector>
+
+#include "../../include/arphys.h"
+
+namespace arp {
+
+struct LoadedScene {
+    std::vector<arp_particle> particles, boundary;
+    std::vector<arp_material> materials;
+    std::vector<arp_interaction> interactions;
+    std::vector<uint8_t> given;
+    arp_aabb bounds{};
+    float h = 1.0f / 64.0f, dt = 0.01f, gravity = 1.0f, alpha = 50.0f;
+    uint32_t subticks = 1;
+    int integrator = ARP_INT_VERLET;
+    std::string name;
+
+    arp_scene as_scene() const {
+        arp_scene s{};
+        s.particles = particles.data();
+        s.n_particles = (uint32_t)particles.size();
+        s.boundary = boundary.data();
+        s.n_boundary = (uint32_t)boundary.size();
+        s.materials = materials.data();
+        s.n_materials = (uint32_t)materials.size();
+        s.interactions = interactions.empty() ? nullptr : interactions.data();
+        s.interaction_given = given.empty() ? nullptr : given.data();
+        s.bounds = bounds;
+        s.kernel_radius = h;
+        s.integrator = integrator;
+        s.timestep = dt;
+        s.subticks = subticks;
+        s.gravity = gravity;
+        s.artificial_viscocity = alpha;
+        return s;
+    }
+};
+
+// Parse `path` and seed its regions.  Returns ARP_OK or an error code with a
+// message in `err`.
+arp_status load_scene_toml(const char* path, LoadedScene& out, std::string& err);
+
+}  // namespace arp

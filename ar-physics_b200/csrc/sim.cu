@@ -1,0 +1,1091 @@
+// sim.cu -- host side of libarphys: the FluidSim equivalent behind the C ABI.
+//
+// Mirrors src/soft_body/mod.rs (FluidSim::new / init / update / accessors)
+// with device state owned by an `arp_sim` handle.  One integrator step:
+//   1. grid over y0 positions; y0 (and caller ids, solid ids) gathered into
+//      cell order, so stage 0 reads the state in place;
+//   2. for each RK stage s: (s > 0) grid over the stage positions and sorted
+//      copies; solid kernels when the scene has more than one solid
+//      (src/soft_body/shaders/mod.rs:51); fluid kernel with the fused stage
+//      update writing y_{s+1} (or y_new) in storage order.
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <new>
+#include <string>
+#include <vector>
+
+#include "arp_internal.h"
+#include "grid.cuh"
+#include "scene_loader.h"
+
+using namespace arp;
+
+namespace {
+
+thread_local std::string g_last_error;
+
+arp_status fail(arp_status code, const std::string& msg) {
+    g_last_error = msg;
+    return code;
+}
+
+#define CUDA_TRY(expr)                                                                          \
+    do {                                                                                        \
+        cudaError_t e_ = (expr);                                                                \
+        if (e_ != cudaSuccess) {                                                                \
+            return fail(e_ == cudaErrorMemoryAllocation ? ARP_ERR_OUT_OF_MEMORY : ARP_ERR_CUDA, \
+                        std::string(#expr) + ": " + cudaGetErrorString(e_));                    \
+        }                                                                                       \
+    } while (0)
+
+#define ARP_TRY(expr)                   \
+    do {                                \
+        arp_status s_ = (expr);         \
+        if (s_ != ARP_OK) return s_;    \
+    } while (0)
+
+struct Tableau {
+    int stages;
+    double a[4][4];
+    double b[4];
+};
+
+bool make_tableau(int id, Tableau& t) {
+    std::memset(&t, 0, sizeof(t));
+    switch (id) {
+        case ARP_INT_EULER: t.stages = 1; t.b[0] = 1; return true;
+        case ARP_INT_MIDPOINT: t.stages = 2; t.a[1][0] = 0.5; t.b[1] = 1; return true;
+        case ARP_INT_HEUN2: t.stages = 2; t.a[1][0] = 1; t.b[0] = 0.5; t.b[1] = 0.5; return true;
+        case ARP_INT_RALSTON: t.stages = 2; t.a[1][0] = 2.0 / 3.0; t.b[0] = 0.25; t.b[1] = 0.75; return true;
+        case ARP_INT_RK3:
+            t.stages = 3; t.a[1][0] = 0.5; t.a[2][0] = -1; t.a[2][1] = 2;
+            t.b[0] = 1.0 / 6.0; t.b[1] = 2.0 / 3.0; t.b[2] = 1.0 / 6.0; return true;
+        case ARP_INT_HEUN3:
+            t.stages = 3; t.a[1][0] = 1.0 / 3.0; t.a[2][1] = 2.0 / 3.0; t.b[0] = 0.25; t.b[2] = 0.75; return true;
+        case ARP_INT_RK4:
+            t.stages = 4; t.a[1][0] = 0.5; t.a[2][1] = 0.5; t.a[3][2] = 1;
+            t.b[0] = 1.0 / 6.0; t.b[1] = 1.0 / 3.0; t.b[2] = 1.0 / 3.0; t.b[3] = 1.0 / 6.0; return true;
+        case ARP_INT_RK_3_8:
+            t.stages = 4; t.a[1][0] = 1.0 / 3.0; t.a[2][0] = -1.0 / 3.0; t.a[2][1] = 1;
+            t.a[3][0] = 1; t.a[3][1] = -1; t.a[3][2] = 1;
+            t.b[0] = 0.125; t.b[1] = 0.375; t.b[2] = 0.375; t.b[3] = 0.125; return true;
+        default: return false;
+    }
+}
+
+// kernel.rs:280-286 and :335-338, in f32 as the Rust code evaluates them
+float volume_nball_f32(uint32_t n, float r) {
+    if (n == 0) return 1.0f;
+    if (n == 1) return 2.0f * r;
+    const float pi = 3.14159265358979323846f;
+    volatile float t = 2.0f * pi;
+    t = t * r;
+    t = t * r;
+    t = t * volume_nball_f32(n - 2, r);
+    return t / (float)n;
+}
+float norm_const_f32(uint32_t n, float h) {
+    const float pi = 3.14159265358979323846f;
+    volatile float p3 = pi * pi;
+    p3 = p3 * pi;
+    volatile float d = 6.0f * volume_nball_f32(n + 6, h);
+    return p3 / d;
+}
+
+bool is_stiff(const arp_material& m) { return m.normal_stiffness != 0.0f || m.shear_stiffness != 0.0f; }
+
+// Owning device allocation (move-only).
+template <class T>
+struct DevBuf {
+    T* p = nullptr;
+    size_t n = 0;
+    DevBuf() = default;
+    DevBuf(const DevBuf&) = delete;
+    DevBuf& operator=(const DevBuf&) = delete;
+    DevBuf(DevBuf&& o) noexcept : p(o.p), n(o.n) {
+        o.p = nullptr;
+        o.n = 0;
+    }
+    DevBuf& operator=(DevBuf&& o) noexcept {
+        if (this != &o) {
+            release();
+            p = o.p;
+            n = o.n;
+            o.p = nullptr;
+            o.n = 0;
+        }
+        return *this;
+    }
+    ~DevBuf() { release(); }
+    cudaError_t alloc(size_t count) {
+        release();
+        if (count == 0) count = 1;
+        cudaError_t e = cudaMalloc(&p, count * sizeof(T));
+        if (e == cudaSuccess) n = count;
+        else p = nullptr;
+        return e;
+    }
+    void release() {
+        if (p) cudaFree(p);
+        p = nullptr;
+        n = 0;
+    }
+};
+
+struct StateBuf {
+    DevBuf<float4> pd, vm;
+};
+
+// Page-locked host staging for state uploads and downloads.
+struct HostStage {
+    float4* pd = nullptr;
+    float4* vm = nullptr;
+    uint32_t* orig = nullptr;
+    uint32_t* sid = nullptr;
+    size_t cap = 0;
+    cudaError_t ensure(size_t n) {
+        if (cap >= n && pd) return cudaSuccess;
+        release();
+        n = n ? n : 1;
+        cudaError_t e;
+        if ((e = cudaMallocHost(&pd, n * sizeof(float4))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&vm, n * sizeof(float4))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&orig, n * sizeof(uint32_t))) != cudaSuccess) return e;
+        if ((e = cudaMallocHost(&sid, n * sizeof(uint32_t))) != cudaSuccess) return e;
+        cap = n;
+        return cudaSuccess;
+    }
+    void release() {
+        if (pd) cudaFreeHost(pd);
+        if (vm) cudaFreeHost(vm);
+        if (orig) cudaFreeHost(orig);
+        if (sid) cudaFreeHost(sid);
+        pd = vm = nullptr;
+        orig = sid = nullptr;
+        cap = 0;
+    }
+};
+
+}  // namespace
+
+struct arp_sim {
+    // scene
+    uint32_t n = 0, nb = 0, ns = 0, M = 0;
+    uint32_t dim = 0;      // the reference's count of non-zero box axes
+    int kdim = 3;          // 2 when every particle shares one z and z has no extent
+    float pos_w = 0.0f;    // common w coordinate of all positions
+    std::vector<arp_material> mats;
+    std::vector<arp_interaction> inter;
+    arp_aabb bounds{};
+    float h = 0, timestep = 0, dt_sub = 0, gravity = 0, alpha = 0;
+    uint32_t subticks = 1;
+    int integrator = 0;
+    Tableau tab{};
+    float time = 0;
+    bool initialized = false;
+    bool any_stiff_immobile = false;
+    Params P{};
+
+    std::vector<arp_particle> host_particles;  // caller order (initial state)
+    std::vector<arp_particle> host_boundary;
+    std::vector<uint32_t> sid_of_caller;       // caller id -> solid id
+    std::vector<uint32_t> part_of_solid;       // solid id -> caller id
+
+    cudaStream_t own_stream = nullptr, stream = nullptr;
+    uint64_t launches = 0;
+    HostStage stage;
+
+    // device: materials
+    DevBuf<DevMat> d_mats;
+    DevBuf<DevInter> d_inter;
+    // mobile state: Y (y0), T (reorder target / y_new), S[2] (stage states)
+    StateBuf Y, T, S[2], X, acc, kst[4];
+    DevBuf<uint32_t> orig, orig_r, sid, sid_r, sid_sorted, slot_of;
+    // boundary (cell-sorted)
+    DevBuf<float4> b_pd, b_vm;
+    DevBuf<uint32_t> b_orig, b_start, sid_of_bidx;
+    // grid scratch
+    GridBuffers gb{};
+    DevBuf<uint32_t> g_key, g_rank, g_count, g_start, g_perm, g_bsums;
+    uint32_t grid_cap = 0;
+    // solids
+    DevBuf<float4> ref, L, F, A, ksol;
+    DevBuf<float4> ep, ep_t, ep_s[2], ep_acc, ep_kst[4];
+    DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
+    DevBuf<float4> rl_gw;
+    uint32_t rl_nnz = 0;
+    DevBuf<DevStats> d_stats;
+
+    // profiling
+    bool profiling = false;
+    std::vector<cudaEvent_t> ev_free;
+    struct Mark {
+        cudaEvent_t e[4];
+    };
+    std::vector<Mark> marks;
+    double acc_ms[3] = {0, 0, 0};  // neighbor, solid, fluid
+    uint64_t prof_steps = 0, prof_launches = 0, prof_l[3] = {0, 0, 0};
+
+    ~arp_sim() {
+        for (auto& m : marks)
+            for (auto e : m.e) ev_free.push_back(e);
+        for (auto e : ev_free) cudaEventDestroy(e);
+        if (own_stream) cudaStreamDestroy(own_stream);
+        stage.release();
+    }
+
+    bool solid_branch() const { return ns > 1; }  // shaders/mod.rs:51: solids.len() > 1
+};
+
+namespace {
+
+arp_status alloc_state(StateBuf& s, size_t n) {
+    CUDA_TRY(s.pd.alloc(n));
+    CUDA_TRY(s.vm.alloc(n));
+    return ARP_OK;
+}
+
+arp_status ensure_grid(arp_sim* S, uint32_t cap) {
+    const uint32_t nc = S->P.grid.ncells;
+    if (S->grid_cap >= cap && S->g_start.p) return ARP_OK;
+    cap = std::max(cap, 1u);
+    CUDA_TRY(S->g_key.alloc(cap));
+    CUDA_TRY(S->g_rank.alloc(cap));
+    CUDA_TRY(S->g_perm.alloc(cap));
+    if (!S->g_start.p) {
+        CUDA_TRY(S->g_count.alloc(size_t(nc) + 2));
+        CUDA_TRY(S->g_start.alloc(size_t(nc) + 2));
+        CUDA_TRY(cudaMemset(S->g_count.p, 0, (size_t(nc) + 2) * sizeof(uint32_t)));
+    }
+    const uint32_t bs = std::max(scan_block_sums_needed(nc + 2), scan_block_sums_needed(cap + 1));
+    if (S->g_bsums.n < bs) CUDA_TRY(S->g_bsums.alloc(bs));
+    S->grid_cap = cap;
+    S->gb.key = S->g_key.p;
+    S->gb.rank = S->g_rank.p;
+    S->gb.count = S->g_count.p;
+    S->gb.start = S->g_start.p;
+    S->gb.perm = S->g_perm.p;
+    S->gb.block_sums = S->g_bsums.p;
+    S->gb.block_sums_cap = (uint32_t)S->g_bsums.n;
+    return ARP_OK;
+}
+
+arp_status check_launch(const char* what) {
+    cudaError_t e = cudaGetLastError();
+    if (e != cudaSuccess) return fail(ARP_ERR_CUDA, std::string(what) + ": " + cudaGetErrorString(e));
+    return ARP_OK;
+}
+
+cudaEvent_t take_event(arp_sim* S) {
+    if (!S->ev_free.empty()) {
+        cudaEvent_t e = S->ev_free.back();
+        S->ev_free.pop_back();
+        return e;
+    }
+    cudaEvent_t e = nullptr;
+    cudaEventCreate(&e);
+    return e;
+}
+
+void harvest_marks(arp_sim* S) {
+    if (S->marks.empty()) return;
+    cudaEventSynchronize(S->marks.back().e[3]);
+    for (auto& m : S->marks) {
+        for (int k = 0; k < 3; ++k) {
+            float ms = 0;
+            if (cudaEventElapsedTime(&ms, m.e[k], m.e[k + 1]) == cudaSuccess) S->acc_ms[k] += ms;
+        }
+        for (auto e : m.e) S->ev_free.push_back(e);
+    }
+    S->marks.clear();
+}
+
+void upload_params(arp_sim* S) {
+    Params& P = S->P;
+    for (int a = 0; a < 3; ++a) {
+        P.grid.min[a] = S->bounds.min[a];
+        P.grid.dim[a] = S->bounds.dim[a];
+    }
+    uint64_t nc = 1;
+    for (int a = 0; a < 4; ++a) {
+        const float q = std::max(1.0f, S->bounds.dim[a] / S->h);  // neighbor_list.rs:201-206
+        const uint32_t s = (uint32_t)q;
+        if (a < 3) P.grid.sub[a] = s;
+        nc *= s;
+    }
+    P.grid.ncells = (uint32_t)nc;
+    P.dim = S->dim;
+    P.nmat = S->M;
+    P.h = S->h;
+    P.h2 = S->h * S->h;
+    P.kconst = norm_const_f32(S->dim, S->h);
+    P.g = S->gravity;
+    const float eps = 0.1f;
+    volatile float t = eps * S->h;
+    P.eps_h = t;
+    P.eps_hh = t * S->h;
+    volatile float ten_eps = 10.0f * eps;
+    P.hg_h = ten_eps * S->h;
+    P.rcut = 8.0f * S->h;
+    P.rcut2 = P.rcut * P.rcut;
+    volatile float hh = S->h * S->h;
+    P.r_geom = hh / P.rcut;
+}
+
+// Solid data, boundary grid, reference neighbor lists (FluidSim::init).
+arp_status do_init(arp_sim* S) {
+    cudaStream_t st = S->stream;
+    const uint32_t n = S->n, nb = S->nb, ns = S->ns;
+    const uint32_t nc = S->P.grid.ncells;
+    ARP_TRY(ensure_grid(S, std::max({n, nb, ns, 1u})));
+
+    // mobile state in caller order
+    std::vector<float4> pd(n), vm(n);
+    std::vector<uint32_t> orig(n), sid(n);
+    for (uint32_t i = 0; i < n; ++i) {
+        const arp_particle& p = S->host_particles[i];
+        pd[i] = make_float4(p.pos[0], p.pos[1], p.pos[2], p.den);
+        uint32_t mbits = p.mat;
+        float mf;
+        std::memcpy(&mf, &mbits, 4);
+        vm[i] = make_float4(p.vel[0], p.vel[1], p.vel[2], mf);
+        orig[i] = i;
+        sid[i] = S->sid_of_caller[i];
+    }
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(S->Y.pd.p, pd.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(S->Y.vm.p, vm.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(S->orig.p, orig.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(S->sid.p, sid.data(), n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+    }
+
+    // boundary grid: filled once (neighbor_list.rs:247-264)
+    {
+        std::vector<float4> bpd(nb), bvm(nb);
+        std::vector<uint32_t> bo(nb);
+        for (uint32_t i = 0; i < nb; ++i) {
+            const arp_particle& p = S->host_boundary[i];
+            bpd[i] = make_float4(p.pos[0], p.pos[1], p.pos[2], p.den);
+            uint32_t mbits = p.mat;
+            float mf;
+            std::memcpy(&mf, &mbits, 4);
+            bvm[i] = make_float4(p.vel[0], p.vel[1], p.vel[2], mf);
+            bo[i] = i;
+        }
+        DevBuf<float4> tmp_pd, tmp_vm;
+        DevBuf<uint32_t> tmp_o;
+        CUDA_TRY(tmp_pd.alloc(nb));
+        CUDA_TRY(tmp_vm.alloc(nb));
+        CUDA_TRY(tmp_o.alloc(nb));
+        if (nb) {
+            CUDA_TRY(cudaMemcpyAsync(tmp_pd.p, bpd.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(tmp_vm.p, bvm.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(tmp_o.p, bo.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        }
+        S->launches += build_grid(tmp_pd.p, nb, S->P.grid, S->gb, nullptr, nullptr, st);
+        S->launches += gather_sorted(S->gb.perm, nb, tmp_pd.p, S->b_pd.p, tmp_vm.p, S->b_vm.p, tmp_o.p,
+                                     S->b_orig.p, nullptr, nullptr, st);
+        CUDA_TRY(cudaMemcpyAsync(S->b_start.p, S->gb.start, (size_t(nc) + 2) * sizeof(uint32_t),
+                                 cudaMemcpyDeviceToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        ARP_TRY(check_launch("boundary grid"));
+    }
+    if (S->any_stiff_immobile) {
+        std::vector<uint32_t> sb(std::max(nb, 1u), kInvalid);
+        for (uint32_t b = 0; b < nb; ++b) sb[b] = b < n ? S->sid_of_caller[b] : kInvalid;
+        CUDA_TRY(cudaMemcpy(S->sid_of_bidx.p, sb.data(), sb.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+
+    // solids: reference positions, plastic strain = 0, neighbor lists, L
+    if (ns > 0) {
+        std::vector<float4> refh(ns);
+        std::vector<uint32_t> mos(ns);
+        for (uint32_t s = 0; s < ns; ++s) {
+            const arp_particle& p = S->host_particles[S->part_of_solid[s]];
+            refh[s] = make_float4(p.pos[0], p.pos[1], p.pos[2], 0.0f);
+            mos[s] = p.mat;
+        }
+        CUDA_TRY(cudaMemcpyAsync(S->ref.p, refh.data(), ns * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(S->mat_of_solid.p, mos.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemsetAsync(S->ep.p, 0, size_t(ns) * 4 * sizeof(float4), st));
+        // grid over reference positions (neighbor_list.rs:266-275, mode 1)
+        S->launches += build_grid(S->ref.p, ns, S->P.grid, S->gb, nullptr, nullptr, st);
+        DevBuf<uint32_t> cnt;
+        CUDA_TRY(cnt.alloc(size_t(ns) + 1));
+        CUDA_TRY(cudaMemsetAsync(cnt.p, 0, (size_t(ns) + 1) * sizeof(uint32_t), st));
+        S->launches += ref_lists_count(S->ref.p, ns, S->gb, S->P, cnt.p, st);
+        CUDA_TRY(S->rl_off.alloc(size_t(ns) + 1));
+        S->launches += exclusive_scan(cnt.p, ns + 1, S->rl_off.p, S->gb.block_sums, st);
+        uint32_t nnz = 0;
+        CUDA_TRY(cudaMemcpyAsync(&nnz, S->rl_off.p + ns, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        CUDA_TRY(S->rl_nbr.alloc(std::max(nnz, 1u)));
+        CUDA_TRY(S->rl_gw.alloc(std::max(nnz, 1u)));
+        S->rl_nnz = nnz;
+        SolidRefList rl{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, nnz};
+        S->launches += ref_lists_fill(S->ref.p, S->mat_of_solid.p, ns, S->gb, S->P, S->d_mats.p, rl, S->L.p, st);
+        CUDA_TRY(cudaStreamSynchronize(st));
+        ARP_TRY(check_launch("reference neighbor lists"));
+    }
+    CUDA_TRY(cudaMemsetAsync(S->d_stats.p, 0, sizeof(DevStats), st));
+    S->initialized = true;
+    return ARP_OK;
+}
+
+void mark(arp_sim* S, arp_sim::Mark& m, int k) {
+    if (!S->profiling) return;
+    m.e[k] = take_event(S);
+    cudaEventRecord(m.e[k], S->stream);
+}
+
+arp_status do_step(arp_sim* S) {
+    cudaStream_t st = S->stream;
+    const uint32_t n = S->n, ns = S->ns;
+    const Tableau& tab = S->tab;
+    const bool sb = S->solid_branch();
+    S->time += S->dt_sub;
+    const uint32_t* bstart = S->b_start.p;
+    uint64_t l0 = S->launches;
+
+    // 1. sort y0 into cell order
+    arp_sim::Mark mk{};
+    mark(S, mk, 0);
+    S->launches += build_grid(S->Y.pd.p, n, S->P.grid, S->gb, S->d_stats.p, bstart, st);
+    S->launches += gather_sorted(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
+                                 S->orig_r.p, S->sid.p, S->sid_r.p, st);
+    std::swap(S->Y, S->T);
+    std::swap(S->orig, S->orig_r);
+    std::swap(S->sid, S->sid_r);
+    if (ns) S->launches += index_solids(S->sid.p, n, S->slot_of.p, st);
+    uint64_t nl = S->launches - l0;
+
+    StageBuffers B{};
+    B.y0_pd = S->Y.pd.p;
+    B.y0_vm = S->Y.vm.p;
+    B.acc_pd = S->acc.pd.p;
+    B.acc_vm = S->acc.vm.p;
+    for (int j = 0; j < 4; ++j) {
+        B.kst_pd[j] = S->kst[j].pd.p;
+        B.kst_vm[j] = S->kst[j].vm.p;
+    }
+    bool acc_started = false;
+    const float4* cur_pd = S->Y.pd.p;
+    const float4* cur_vm = S->Y.vm.p;
+    const float4* cur_ep = S->ep.p;
+    for (int s = 0; s < tab.stages; ++s) {
+        const bool last = s == tab.stages - 1;
+        StageCoefs c{};
+        c.stage = s;
+        c.last = last ? 1 : 0;
+        if (!last)
+            for (int j = 0; j <= s; ++j) c.c_next[j] = (float)(tab.a[s + 1][j] * (double)S->dt_sub);
+        c.c_acc = (float)(tab.b[s] * (double)S->dt_sub);
+        c.acc_first = acc_started ? 0 : 1;
+        if (c.c_acc != 0.0f) acc_started = true;
+        c.store_k = 0;
+        for (int t = s + 2; t < tab.stages; ++t)
+            if (tab.a[t][s] != 0.0) c.store_k = 1;
+
+        if (s > 0) {
+            if (S->profiling && s > 0) mark(S, mk, 0);
+            l0 = S->launches;
+            S->launches += build_grid(cur_pd, n, S->P.grid, S->gb, S->d_stats.p, bstart, st);
+            S->launches += gather_sorted(S->gb.perm, n, cur_pd, S->X.pd.p, cur_vm, S->X.vm.p, sb ? S->sid.p : nullptr,
+                                         sb ? S->sid_sorted.p : nullptr, nullptr, nullptr, st);
+            nl += S->launches - l0;
+        }
+        const float4* xs = s == 0 ? S->Y.pd.p : S->X.pd.p;
+        const float4* vs = s == 0 ? S->Y.vm.p : S->X.vm.p;
+        const uint32_t* perm = s == 0 ? nullptr : S->gb.perm;
+        const uint32_t* sid_sorted = s == 0 ? S->sid.p : S->sid_sorted.p;
+        float4* next_pd = last ? S->T.pd.p : S->S[s % 2].pd.p;
+        float4* next_vm = last ? S->T.vm.p : S->S[s % 2].vm.p;
+        mark(S, mk, 1);
+
+        uint64_t sl = 0;
+        if (sb) {
+            SolidArgs a{};
+            a.pd = cur_pd;
+            a.vm = cur_vm;
+            a.slot_of = S->slot_of.p;
+            a.ref = S->ref.p;
+            a.L = S->L.p;
+            a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz};
+            a.ep = cur_ep;
+            a.ep0 = S->ep.p;
+            a.ep_next = last ? S->ep_t.p : S->ep_s[s % 2].p;
+            a.ep_acc = S->ep_acc.p;
+            for (int j = 0; j < 4; ++j) a.ep_kst[j] = S->ep_kst[j].p;
+            a.F = S->F.p;
+            a.A = S->A.p;
+            a.ksol = S->ksol.p;
+            a.xs = xs;
+            a.vs = vs;
+            a.start = S->gb.start;
+            a.sid_sorted = sid_sorted;
+            a.mats = S->d_mats.p;
+            a.ns = ns;
+            sl = launch_solid(a, S->P, c, st);
+            S->launches += sl;
+            cur_ep = a.ep_next;
+        }
+        mark(S, mk, 2);
+
+        FluidArgs f{};
+        f.xs = xs;
+        f.vs = vs;
+        f.start = S->gb.start;
+        f.bxs = S->b_pd.p;
+        f.bvs = S->b_vm.p;
+        f.bstart = bstart;
+        f.perm = perm;
+        f.sid = S->sid.p;
+        f.sid_of_boundary_index = S->sid_of_bidx.p;
+        f.borig = S->b_orig.p;
+        f.ksol = sb ? S->ksol.p : nullptr;
+        f.mats = S->d_mats.p;
+        f.inter = S->d_inter.p;
+        f.n = n;
+        f.n_mobile_total = n;
+        f.solid_branch = sb ? 1 : 0;
+        f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
+        B.next_pd = next_pd;
+        B.next_vm = next_vm;
+        S->launches += launch_fluid(f, S->P, c, B, st);
+        mark(S, mk, 3);
+        if (S->profiling) {
+            S->marks.push_back(mk);
+            S->prof_l[0] += nl;
+            S->prof_l[1] += sl;
+            S->prof_l[2] += 1;
+            nl = 0;
+            mk = arp_sim::Mark{};
+            if (S->marks.size() > 256) harvest_marks(S);
+        }
+        cur_pd = next_pd;
+        cur_vm = next_vm;
+    }
+    std::swap(S->Y, S->T);
+    if (sb) std::swap(S->ep, S->ep_t);
+    if (S->profiling) S->prof_steps++;
+    return check_launch("step");
+}
+
+arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
+    if (!sc) return fail(ARP_ERR_INVALID_ARG, "scene is null");
+    if (sc->n_materials == 0 || !sc->materials) return fail(ARP_ERR_INVALID_ARG, "scene has no materials");
+    if (sc->n_materials > (uint32_t)kMaxMaterials)
+        return fail(ARP_ERR_UNSUPPORTED, "more than 32 materials");
+    if (sc->n_particles && !sc->particles) return fail(ARP_ERR_INVALID_ARG, "particles is null");
+    if (sc->n_boundary && !sc->boundary) return fail(ARP_ERR_INVALID_ARG, "boundary is null");
+    if (!(sc->kernel_radius > 0.0f) || !std::isfinite(sc->kernel_radius))
+        return fail(ARP_ERR_INVALID_ARG, "kernel_radius must be positive");
+    if (!std::isfinite(sc->timestep)) return fail(ARP_ERR_INVALID_ARG, "timestep must be finite");
+    if (sc->integrator == ARP_INT_VERLET)
+        return fail(ARP_ERR_UNSUPPORTED, "the velocity-Verlet integrator is not implemented; use an RK tableau");
+    if (!make_tableau(sc->integrator, S->tab)) return fail(ARP_ERR_INVALID_ARG, "unknown integrator id");
+    if (sc->bounds.dim[3] > 0.0f) return fail(ARP_ERR_UNSUPPORTED, "4-dimensional boxes are not supported");
+    for (int a = 0; a < 4; ++a)
+        if (!std::isfinite(sc->bounds.min[a]) || !std::isfinite(sc->bounds.dim[a]) || sc->bounds.dim[a] < 0.0f)
+            return fail(ARP_ERR_INVALID_ARG, "bounds must be finite with non-negative extent");
+    S->M = sc->n_materials;
+    S->mats.assign(sc->materials, sc->materials + S->M);
+    S->n = sc->n_particles;
+    S->nb = sc->n_boundary;
+    S->host_particles.assign(sc->particles, sc->particles + S->n);
+    S->host_boundary.assign(sc->boundary, sc->boundary + S->nb);
+    bool have_w = false;
+    bool flat_z = sc->bounds.dim[2] == 0.0f;
+    float z0 = 0.0f;
+    bool have_z = false;
+    auto check_p = [&](const arp_particle& p, bool boundary) -> arp_status {
+        if (p.mat >= S->M) return fail(ARP_ERR_INVALID_ARG, "particle material index out of range");
+        const bool imm = S->mats[p.mat].immobile != 0;
+        if (imm != boundary)
+            return fail(ARP_ERR_INVALID_ARG, boundary ? "boundary particle uses a mobile material"
+                                                      : "mobile particle uses an immobile material");
+        if (!std::isfinite(p.pos[3])) return fail(ARP_ERR_INVALID_ARG, "non-finite w coordinate");
+        if (!have_w) {
+            S->pos_w = p.pos[3];
+            have_w = true;
+        } else if (p.pos[3] != S->pos_w) {
+            return fail(ARP_ERR_UNSUPPORTED, "positions must share one w coordinate (4D motion is not supported)");
+        }
+        if (p.vel[3] != 0.0f) return fail(ARP_ERR_UNSUPPORTED, "velocities must have zero w component");
+        if (!have_z) {
+            z0 = p.pos[2];
+            have_z = true;
+        } else if (p.pos[2] != z0) {
+            flat_z = false;
+        }
+        if (p.vel[2] != 0.0f) flat_z = false;
+        return ARP_OK;
+    };
+    for (uint32_t i = 0; i < S->n; ++i) ARP_TRY(check_p(S->host_particles[i], false));
+    for (uint32_t i = 0; i < S->nb; ++i) ARP_TRY(check_p(S->host_boundary[i], true));
+    S->kdim = flat_z ? 2 : 3;
+    // mod.rs:93-111 interaction matrix
+    const uint32_t M = S->M;
+    S->inter.assign(size_t(M) * M, arp_interaction{0, 0, 0, 0, 0});
+    auto given = [&](uint32_t i, uint32_t j) -> bool {
+        if (!sc->interactions) return false;
+        if (!sc->interaction_given) return true;
+        return sc->interaction_given[size_t(i) * M + j] != 0;
+    };
+    for (uint32_t i = 0; i < M; ++i)
+        for (uint32_t j = i; j < M; ++j) {
+            arp_interaction x{0, 0, 0, 0, 0};
+            if (given(i, j)) x = sc->interactions[size_t(i) * M + j];
+            else if (given(j, i)) x = sc->interactions[size_t(j) * M + i];
+            else if (i != j) {
+                const arp_material& a = S->mats[i];
+                const arp_material& b = S->mats[j];
+                if (a.state_eq != ARP_EOS_ZERO && b.state_eq != ARP_EOS_ZERO) x = arp_interaction{0, 0, 0, 0, 0};
+                else x = arp_interaction{ARP_CONTACT_LINEAR, 10000.0f, sc->kernel_radius * 2.0f, 0.0f, a.visc + b.visc};
+            }
+            S->inter[size_t(i) * M + j] = x;
+            S->inter[size_t(j) * M + i] = x;
+        }
+    for (const auto& m : S->mats)
+        if (m.immobile && is_stiff(m)) S->any_stiff_immobile = true;
+    S->bounds = sc->bounds;
+    S->dim = 0;
+    for (int a = 0; a < 4; ++a)
+        if (sc->bounds.dim[a] > 0.0f) S->dim++;
+    if (S->dim == 0) return fail(ARP_ERR_INVALID_ARG, "bounds have no extent");
+    S->h = sc->kernel_radius;
+    S->timestep = sc->timestep;
+    S->subticks = sc->subticks ? sc->subticks : 1;
+    S->dt_sub = sc->timestep / (float)S->subticks;
+    S->gravity = sc->gravity;
+    S->alpha = sc->artificial_viscocity;
+    S->integrator = sc->integrator;
+    // particles.rs:488-506: solid ids in particle order for stiff materials
+    S->sid_of_caller.assign(S->n, kInvalid);
+    S->part_of_solid.clear();
+    for (uint32_t i = 0; i < S->n; ++i)
+        if (is_stiff(S->mats[S->host_particles[i].mat])) {
+            S->sid_of_caller[i] = (uint32_t)S->part_of_solid.size();
+            S->part_of_solid.push_back(i);
+        }
+    S->ns = (uint32_t)S->part_of_solid.size();
+    upload_params(S);
+    if ((uint64_t)S->P.grid.ncells * 1 > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "grid has more than 2^31 cells");
+    uint64_t nc = 1;
+    for (int a = 0; a < 4; ++a) nc *= std::max<uint64_t>(1, (uint64_t)std::max(1.0f, S->bounds.dim[a] / S->h));
+    if (nc > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "grid has more than 2^31 cells");
+    return ARP_OK;
+}
+
+arp_status allocate(arp_sim* S) {
+    const size_t n = std::max(S->n, 1u), nb = std::max(S->nb, 1u), ns = std::max(S->ns, 1u);
+    const size_t nc = S->P.grid.ncells;
+    ARP_TRY(alloc_state(S->Y, n));
+    ARP_TRY(alloc_state(S->T, n));
+    ARP_TRY(alloc_state(S->S[0], n));
+    if (S->tab.stages > 2) ARP_TRY(alloc_state(S->S[1], n));
+    ARP_TRY(alloc_state(S->X, n));
+    ARP_TRY(alloc_state(S->acc, n));
+    for (int j = 0; j < S->tab.stages; ++j) {
+        bool needed = false;
+        for (int t = j + 2; t < S->tab.stages; ++t)
+            if (S->tab.a[t][j] != 0.0) needed = true;
+        if (needed) ARP_TRY(alloc_state(S->kst[j], n));
+    }
+    CUDA_TRY(S->orig.alloc(n));
+    CUDA_TRY(S->orig_r.alloc(n));
+    CUDA_TRY(S->sid.alloc(n));
+    CUDA_TRY(S->sid_r.alloc(n));
+    CUDA_TRY(S->sid_sorted.alloc(n));
+    CUDA_TRY(S->slot_of.alloc(ns));
+    CUDA_TRY(S->b_pd.alloc(nb));
+    CUDA_TRY(S->b_vm.alloc(nb));
+    CUDA_TRY(S->b_orig.alloc(nb));
+    CUDA_TRY(S->b_start.alloc(nc + 2));
+    CUDA_TRY(S->sid_of_bidx.alloc(nb));
+    CUDA_TRY(S->ref.alloc(ns));
+    CUDA_TRY(S->mat_of_solid.alloc(ns));
+    CUDA_TRY(S->L.alloc(3 * ns));
+    CUDA_TRY(S->F.alloc(3 * ns));
+    CUDA_TRY(S->A.alloc(3 * ns));
+    CUDA_TRY(S->ksol.alloc(ns));
+    CUDA_TRY(S->ep.alloc(4 * ns));
+    CUDA_TRY(S->ep_t.alloc(4 * ns));
+    CUDA_TRY(S->ep_s[0].alloc(4 * ns));
+    CUDA_TRY(S->ep_s[1].alloc(4 * ns));
+    CUDA_TRY(S->ep_acc.alloc(4 * ns));
+    for (int j = 0; j < 4; ++j)
+        if (S->kst[j].pd.p) CUDA_TRY(S->ep_kst[j].alloc(4 * ns));
+    CUDA_TRY(S->d_stats.alloc(1));
+    CUDA_TRY(cudaMemset(S->d_stats.p, 0, sizeof(DevStats)));
+    // materials
+    std::vector<DevMat> dm(S->M);
+    for (uint32_t i = 0; i < S->M; ++i) {
+        const arp_material& m = S->mats[i];
+        DevMat d{};
+        d.mass = m.mass; d.start_den = m.start_den; d.sound_speed = m.sound_speed; d.target_den = m.target_den;
+        d.visc = m.visc; d.bulk_visc = m.bulk_visc; d.lam = m.normal_stiffness; d.mu = m.shear_stiffness;
+        d.lam_d = m.normal_damp; d.mu_d = m.shear_damp; d.yield_strength = m.yield_strength;
+        d.work_hardening = m.work_hardening; d.work_hardening_exp = m.work_hardening_exp;
+        d.kinematic_hardening = m.kinematic_hardening; d.relaxation_time = m.relaxation_time;
+        d.vol0 = m.mass / m.start_den;
+        d.state_eq = m.state_eq; d.stiff = is_stiff(m) ? 1u : 0u; d.plastic = m.plastic ? 1u : 0u;
+        d.strain_order = m.strain_order;
+        dm[i] = d;
+    }
+    CUDA_TRY(S->d_mats.alloc(S->M));
+    CUDA_TRY(cudaMemcpy(S->d_mats.p, dm.data(), S->M * sizeof(DevMat), cudaMemcpyHostToDevice));
+    std::vector<DevInter> di(size_t(S->M) * S->M);
+    for (size_t i = 0; i < di.size(); ++i) {
+        const arp_interaction& x = S->inter[i];
+        di[i] = DevInter{x.potential, x.strength, x.radius, x.dampening, x.friction};
+    }
+    CUDA_TRY(S->d_inter.alloc(di.size()));
+    CUDA_TRY(cudaMemcpy(S->d_inter.p, di.data(), di.size() * sizeof(DevInter), cudaMemcpyHostToDevice));
+    return ARP_OK;
+}
+
+// Download the state into the pinned staging buffers (cell order).
+arp_status download(arp_sim* S) {
+    const uint32_t n = S->n;
+    CUDA_TRY(S->stage.ensure(n));
+    if (!n) return ARP_OK;
+    cudaStream_t st = S->stream;
+    CUDA_TRY(cudaMemcpyAsync(S->stage.pd, S->Y.pd.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(S->stage.vm, S->Y.vm.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(S->stage.orig, S->orig.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(S->stage.sid, S->sid.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return ARP_OK;
+}
+
+arp_status need_init(const arp_sim* S) {
+    if (!S) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (!S->initialized) return fail(ARP_ERR_INVALID_ARG, "arp_sim_init must be called first");
+    return ARP_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+const char* arp_last_error(void) { return g_last_error.c_str(); }
+uint32_t arp_abi_version(void) { return ARP_ABI_VERSION; }
+
+arp_status arp_sim_create(const arp_scene* scene, arp_sim** out) {
+    g_last_error.clear();
+    if (!out) return fail(ARP_ERR_INVALID_ARG, "out is null");
+    *out = nullptr;
+    arp_sim* S = new (std::nothrow) arp_sim();
+    if (!S) return fail(ARP_ERR_OUT_OF_MEMORY, "host allocation failed");
+    arp_status s = validate_and_copy(scene, S);
+    if (s == ARP_OK) {
+        cudaError_t e = cudaStreamCreateWithFlags(&S->own_stream, cudaStreamNonBlocking);
+        if (e != cudaSuccess) s = fail(ARP_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
+        S->stream = S->own_stream;
+    }
+    if (s == ARP_OK) s = allocate(S);
+    if (s != ARP_OK) {
+        delete S;
+        return s;
+    }
+    *out = S;
+    return ARP_OK;
+}
+
+arp_status arp_sim_create_from_toml(const char* path, arp_sim** out) {
+    g_last_error.clear();
+    if (!path || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    arp::LoadedScene ls;
+    std::string err;
+    arp_status s = arp::load_scene_toml(path, ls, err);
+    if (s != ARP_OK) return fail(s, err);
+    arp_scene sc = ls.as_scene();
+    return arp_sim_create(&sc, out);
+}
+
+arp_status arp_sim_destroy(arp_sim* sim) {
+    if (!sim) return ARP_OK;
+    if (sim->stream) cudaStreamSynchronize(sim->stream);
+    delete sim;
+    return ARP_OK;
+}
+
+arp_status arp_sim_init(arp_sim* sim) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    return do_init(sim);
+}
+
+arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
+    ARP_TRY(need_init(sim));
+    for (uint32_t i = 0; i < nsteps; ++i) ARP_TRY(do_step(sim));
+    return ARP_OK;
+}
+
+arp_status arp_sim_update(arp_sim* sim) {
+    ARP_TRY(need_init(sim));
+    return arp_sim_step(sim, sim->subticks);
+}
+
+arp_status arp_sim_time(const arp_sim* sim, float* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = sim->time;
+    return ARP_OK;
+}
+arp_status arp_sim_kernel_radius(const arp_sim* sim, float* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = sim->h;
+    return ARP_OK;
+}
+arp_status arp_sim_num_materials(const arp_sim* sim, uint32_t* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = sim->M;
+    return ARP_OK;
+}
+arp_status arp_sim_counts(const arp_sim* sim, uint32_t* n, uint32_t* nb, uint32_t* ns) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (n) *n = sim->n;
+    if (nb) *nb = sim->nb;
+    if (ns) *ns = sim->ns;
+    return ARP_OK;
+}
+arp_status arp_sim_dim(const arp_sim* sim, uint32_t* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = sim->dim;
+    return ARP_OK;
+}
+
+arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap) {
+    if (!sim || (!out && sim->n)) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (cap < sim->n) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_particles");
+    if (!sim->initialized) {
+        std::memcpy(out, sim->host_particles.data(), sim->n * sizeof(arp_particle));
+        for (uint32_t i = 0; i < sim->n; ++i) out[i].solid_id = sim->sid_of_caller[i];
+        return ARP_OK;
+    }
+    ARP_TRY(download(sim));
+    const float4* pd = sim->stage.pd;
+    const float4* vm = sim->stage.vm;
+    const uint32_t* orig = sim->stage.orig;
+    const uint32_t* sid = sim->stage.sid;
+    for (uint32_t k = 0; k < sim->n; ++k) {
+        arp_particle& p = out[orig[k]];
+        p.den = pd[k].w;
+        std::memcpy(&p.mat, &vm[k].w, 4);
+        p.solid_id = sid[k];
+        p._pad0 = 0;
+        p.pos[0] = pd[k].x; p.pos[1] = pd[k].y; p.pos[2] = pd[k].z; p.pos[3] = sim->pos_w;
+        p.vel[0] = vm[k].x; p.vel[1] = vm[k].y; p.vel[2] = vm[k].z; p.vel[3] = 0.0f;
+    }
+    return ARP_OK;
+}
+
+arp_status arp_sim_get_solids(arp_sim* sim, arp_solid_particle* out, uint32_t cap) {
+    if (!sim || (!out && sim->ns)) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (cap < sim->ns) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_solids");
+    const uint32_t ns = sim->ns;
+    std::vector<float4> ep(4 * size_t(ns));
+    if (sim->initialized && ns) {
+        CUDA_TRY(cudaMemcpyAsync(ep.data(), sim->ep.p, 4 * ns * sizeof(float4), cudaMemcpyDeviceToHost, sim->stream));
+        CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    }
+    for (uint32_t s = 0; s < ns; ++s) {
+        arp_solid_particle& r = out[s];
+        std::memset(&r, 0, sizeof(r));
+        r.part_id = sim->part_of_solid[s];
+        const arp_particle& p = sim->host_particles[r.part_id];
+        for (int a = 0; a < 3; ++a) r.ref_pos[a] = p.pos[a];
+        r.ref_pos[3] = sim->pos_w;
+        for (int c = 0; c < 4; ++c) {
+            r.stress[4 * c + 0] = ep[4 * s + c].x;
+            r.stress[4 * c + 1] = ep[4 * s + c].y;
+            r.stress[4 * c + 2] = ep[4 * s + c].z;
+            r.stress[4 * c + 3] = ep[4 * s + c].w;
+        }
+    }
+    return ARP_OK;
+}
+
+arp_status arp_sim_get_boundary(arp_sim* sim, arp_particle* out, uint32_t cap) {
+    if (!sim || (!out && sim->nb)) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (cap < sim->nb) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_boundary");
+    std::memcpy(out, sim->host_boundary.data(), sim->nb * sizeof(arp_particle));
+    for (uint32_t i = 0; i < sim->nb; ++i) out[i].solid_id = kInvalid;
+    return ARP_OK;
+}
+
+arp_status arp_sim_get_materials(const arp_sim* sim, arp_material* out, uint32_t cap) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (cap < sim->M) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_materials");
+    std::memcpy(out, sim->mats.data(), sim->M * sizeof(arp_material));
+    return ARP_OK;
+}
+
+arp_status arp_sim_get_interactions(const arp_sim* sim, arp_interaction* out, uint32_t cap) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (cap < sim->M * sim->M) return fail(ARP_ERR_CAPACITY, "output holds fewer than n_materials^2 records");
+    std::memcpy(out, sim->inter.data(), sim->inter.size() * sizeof(arp_interaction));
+    return ARP_OK;
+}
+
+arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t n) {
+    ARP_TRY(need_init(sim));
+    if (!in && n) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (n != sim->n) return fail(ARP_ERR_INVALID_ARG, "particle count differs from the handle's");
+    CUDA_TRY(sim->stage.ensure(n));
+    float4* pd = sim->stage.pd;
+    float4* vm = sim->stage.vm;
+    uint32_t* orig = sim->stage.orig;
+    uint32_t* sid = sim->stage.sid;
+    for (uint32_t i = 0; i < n; ++i) {
+        const arp_particle& p = in[i];
+        if (p.mat != sim->host_particles[i].mat) return fail(ARP_ERR_INVALID_ARG, "material of a particle changed");
+        if (p.pos[3] != sim->pos_w || p.vel[3] != 0.0f)
+            return fail(ARP_ERR_UNSUPPORTED, "w components must keep their values");
+        pd[i] = make_float4(p.pos[0], p.pos[1], p.pos[2], p.den);
+        float mf;
+        std::memcpy(&mf, &p.mat, 4);
+        vm[i] = make_float4(p.vel[0], p.vel[1], p.vel[2], mf);
+        orig[i] = i;
+        sid[i] = sim->sid_of_caller[i];
+    }
+    cudaStream_t st = sim->stream;
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(sim->Y.pd.p, pd, n * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(sim->Y.vm.p, vm, n * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(sim->orig.p, orig, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(sim->sid.p, sid, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    return ARP_OK;
+}
+
+arp_status arp_sim_device_state(arp_sim* sim, arp_device_view* out) {
+    ARP_TRY(need_init(sim));
+    if (!out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    out->pos_den = sim->Y.pd.p;
+    out->vel_mat = sim->Y.vm.p;
+    out->orig_id = sim->orig.p;
+    out->n = sim->n;
+    return ARP_OK;
+}
+
+arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n, const arp_material* material,
+                                 const float* offset, int* material_added) {
+    (void)p; (void)n; (void)material; (void)offset; (void)material_added;
+    ARP_TRY(need_init(sim));
+    return fail(ARP_ERR_UNSUPPORTED, "add_particles is not implemented in this build");
+}
+
+arp_status arp_sim_grid(const arp_sim* sim, uint32_t subdivisions[4], uint32_t* n_cells) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (subdivisions) {
+        for (int a = 0; a < 3; ++a) subdivisions[a] = sim->P.grid.sub[a];
+        subdivisions[3] = 1;
+    }
+    if (n_cells) *n_cells = sim->P.grid.ncells;
+    return ARP_OK;
+}
+
+arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_start, uint32_t* members,
+                             uint32_t* nbr_count) {
+    ARP_TRY(need_init(sim));
+    const uint32_t n = sim->n, nc = sim->P.grid.ncells;
+    cudaStream_t st = sim->stream;
+    sim->launches += build_grid(sim->Y.pd.p, n, sim->P.grid, sim->gb, nullptr, nullptr, st);
+    sim->launches += gather_sorted(sim->gb.perm, n, sim->Y.pd.p, sim->X.pd.p, nullptr, nullptr, nullptr, nullptr,
+                                   nullptr, nullptr, st);
+    DevBuf<uint32_t> cnt;
+    CUDA_TRY(cnt.alloc(n));
+    sim->launches += count_neighbors(sim->X.pd.p, sim->gb.start, n, sim->b_pd.p, sim->b_start.p, sim->P, cnt.p, st);
+    std::vector<uint32_t> key(n), perm(n), start(size_t(nc) + 2), orig(n), c(n);
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(key.data(), sim->gb.key, n * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(perm.data(), sim->gb.perm, n * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(orig.data(), sim->orig.p, n * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(c.data(), cnt.p, n * 4, cudaMemcpyDeviceToHost, st));
+    }
+    CUDA_TRY(cudaMemcpyAsync(start.data(), sim->gb.start, (size_t(nc) + 2) * 4, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    ARP_TRY(check_launch("neighbors"));
+    if (cell_of)
+        for (uint32_t k = 0; k < n; ++k) cell_of[orig[k]] = key[k] >= nc ? kInvalid : key[k];
+    if (cell_start) std::memcpy(cell_start, start.data(), (size_t(nc) + 1) * 4);
+    if (members) {
+        for (uint32_t k = 0; k < n; ++k) members[k] = orig[perm[k]];
+        for (uint32_t cc = 0; cc <= nc; ++cc) std::sort(members + start[cc], members + start[cc + 1]);
+    }
+    if (nbr_count)
+        for (uint32_t k = 0; k < n; ++k) nbr_count[orig[perm[k]]] = c[k];
+    return ARP_OK;
+}
+
+arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* members) {
+    ARP_TRY(need_init(sim));
+    const uint32_t nb = sim->nb, nc = sim->P.grid.ncells;
+    if (cell_start)
+        CUDA_TRY(cudaMemcpy(cell_start, sim->b_start.p, (size_t(nc) + 1) * 4, cudaMemcpyDeviceToHost));
+    if (members && nb) CUDA_TRY(cudaMemcpy(members, sim->b_orig.p, size_t(nb) * 4, cudaMemcpyDeviceToHost));
+    return ARP_OK;
+}
+
+arp_status arp_sim_set_stream(arp_sim* sim, void* stream) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    sim->stream = stream ? (cudaStream_t)stream : sim->own_stream;
+    return ARP_OK;
+}
+
+arp_status arp_sim_synchronize(arp_sim* sim) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    return check_launch("synchronize");
+}
+
+arp_status arp_sim_profile_enable(arp_sim* sim, int enable) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (!enable) harvest_marks(sim);
+    sim->profiling = enable != 0;
+    return ARP_OK;
+}
+
+arp_status arp_sim_profile_read(arp_sim* sim, arp_profile* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    harvest_marks(sim);
+    out->steps = sim->prof_steps;
+    out->launches = sim->prof_l[0] + sim->prof_l[1] + sim->prof_l[2];
+    out->neighbor_ms = sim->acc_ms[0];
+    out->solid_ms = sim->acc_ms[1];
+    out->fluid_ms = sim->acc_ms[2];
+    out->integrate_ms = 0.0;
+    out->neighbor_launches = sim->prof_l[0];
+    out->solid_launches = sim->prof_l[1];
+    out->fluid_launches = sim->prof_l[2];
+    for (double& x : sim->acc_ms) x = 0;
+    for (auto& x : sim->prof_l) x = 0;
+    sim->prof_steps = 0;
+    return ARP_OK;
+}
+
+arp_status arp_sim_stats(arp_sim* sim, arp_stats* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    DevStats d{};
+    CUDA_TRY(cudaMemcpyAsync(&d, sim->d_stats.p, sizeof(d), cudaMemcpyDeviceToHost, sim->stream));
+    CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    out->max_cell_occupancy = d.max_cell_occupancy;
+    out->overflow_cells = d.overflow_cells;
+    out->nonfinite_positions = d.nonfinite_positions;
+    out->clamped_coordinates = d.clamped_coordinates;
+    return ARP_OK;
+}
+
+arp_status arp_sim_launch_count(const arp_sim* sim, uint64_t* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = sim->launches;
+    return ARP_OK;
+}
+
+}  // extern "C"

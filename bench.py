@@ -1,0 +1,306 @@
+#!/usr/bin/env python
+"""Benchmark of the SPH time step (particle-steps/s).
+
+Workload (default): the 3D fluid + clamped elastic bar scene at 1,048,576
+particles (96^3 Tait fluid, 32x128x32 bar with 2 clamped layers, 256x128
+floor), RK2, dt = 1e-4, synthetic seeded inputs.  One "step" is one RK2
+integrator step of the whole scene through the C ABI.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+`value` is device-timed (CUDA events on the stream the library launches on,
+L2 flushed between timed steps, max over ranks); `e2e` is the same metric
+through the C ABI with host records copied in and out every step;
+`roofline` covers the dominant kernel (fused fluid forces + stage update);
+`cpu_baseline` is the CPU oracle (the restatement of the reference shaders)
+on the host cores.  With N > 1 each rank runs an independent replica (the
+plain step does not shard; scene-parallel replicas, weak scaling).
+"""
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, os.path.join(ROOT, "ar-physics_b200"))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s at 1M (vs HBM roofline); batched scenes/s; adjoint/fwd ratio"
+UNIT = "particle-steps/s"
+L2_FLUSH_BYTES = 256 << 20
+
+
+def load_peaks():
+    p = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(p) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic():
+    """Per-launch DRAM bytes of the fluid kernel from the committed ncu summary."""
+    p = os.path.join(ROOT, "profiles", "ncu_traffic.txt")
+    out = {}
+    try:
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 3 and not line.startswith("#"):
+                out[parts[0]] = float(parts[2])
+    except OSError:
+        pass
+    return out
+
+
+class ClockSampler:
+    """nvidia-smi samples during the timed region (SM clock, reasons)."""
+
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        try:
+            fd, self.path = tempfile.mkstemp(suffix=".csv")
+            os.close(fd)
+            self.f = open(self.path, "w")
+            self.proc = subprocess.Popen(["nvidia-smi", "-i", str(self.gpu), f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"], stdout=self.f,
+                                         stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if not self.proc:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.f.close()
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for line in open(self.path):
+            c = [x.strip() for x in line.split(",")]
+            if len(c) < 9:
+                continue
+            try:
+                sm.append(float(c[1]))
+                mx.append(float(c[2]))
+            except ValueError:
+                continue
+            for nm, v in zip(names, c[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(nm)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(mx) if mx else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_scene(name):
+    from arphys import scenes
+    if name == "c1":
+        return scenes.dam_break_2d()
+    return scenes.fluid_bar_3d()
+
+
+def config_of(sc, name):
+    ns = sc.n_solids()
+    return {
+        "workload": ("fluid_bar_3d: 96^3 Tait fluid striking a 32x128x32 elastic bar (E=1e6, nu=0.3, 2 clamped "
+                     "layers) on a 256x128 floor, h=2x spacing, RK2, dt=1e-4" if name == "c2" else
+                     "dam_break_2d: 128x128 Tait fluid, 2340 boundary particles, h=2x spacing, RK4, dt=1e-4"),
+        "particles": int(sc.n + sc.nb), "mobile": int(sc.n), "solids": ns, "boundary": int(sc.nb),
+        "integrator": sc.integrator, "l2": "flushed between timed steps (256 MiB write)",
+    }
+
+
+def cpu_baseline(sc, max_seconds=20.0, max_steps=5):
+    """The CPU oracle on all host cores: full-size steps until ~max_seconds."""
+    from oracle import oracle as orc
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    o = orc.Oracle(sc, 32)
+    o.step(1)  # first step fills the boundary and reference buckets
+    t0 = time.perf_counter()
+    steps = 0
+    while steps < max_steps and time.perf_counter() - t0 < max_seconds:
+        o.step(1)
+        steps += 1
+    dt = time.perf_counter() - t0
+    parts = sc.n + sc.nb
+    return {"value": parts * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{steps} full RK steps of the {parts}-particle scene after 1 untimed step "
+                      f"(C++ oracle, float, OpenMP x{cores})", "seconds": dt}
+
+
+def run_reference(args, rank, world):
+    """The reference arm: the reference's path cannot run here (Rust + OpenGL
+    compute shaders, no GL stack), so the CPU restatement of its shaders is
+    timed on the host cores, rank 0 only."""
+    if rank != 0:
+        return
+    sc = make_scene(args.config)
+    from oracle import oracle as orc
+    cores = os.cpu_count() or 1
+    orc.set_threads(cores)
+    o = orc.Oracle(sc, 32)
+    for _ in range(args.warmup):
+        o.step(1)
+    t0 = time.perf_counter()
+    o.step(args.steps)
+    dt = time.perf_counter() - t0
+    parts = sc.n + sc.nb
+    v = parts * args.steps / dt
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": config_of(sc, args.config),
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
+                         "sample": f"{args.steps} full RK steps after {args.warmup} warm-up steps (C++ oracle, "
+                                   f"float, OpenMP x{cores}); the reference's Rust/OpenGL path cannot run here"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def run_ours(args, rank, world, local_rank):
+    import numpy as np
+    import torch
+    from arphys import FluidSim
+
+    torch.cuda.set_device(local_rank)
+    dist = world > 1
+    sc = make_scene(args.config)
+    sim = FluidSim(sc)
+    sim.init()
+    stream = torch.cuda.current_stream()
+    sim.set_stream(stream.cuda_stream)
+    flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
+    for _ in range(args.warmup):
+        sim.step(1)
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    sim.profile_enable(True)
+    sim.profile_read()
+    l0 = sim.launch_count()
+    clk = ClockSampler(local_rank)
+    clk.start()
+    evs = []
+    for _ in range(args.steps):
+        flush.zero_()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        sim.step(1)
+        e1.record(stream)
+        evs.append((e0, e1))
+    torch.cuda.synchronize()
+    if dist:
+        torch.distributed.barrier()
+    torch.cuda.synchronize()
+    clocks = clk.stop()
+    launches = sim.launch_count() - l0
+    prof = sim.profile_read()
+    sim.profile_enable(False)
+    total_ms = sum(a.elapsed_time(b) for a, b in evs)
+    if dist:
+        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        total_ms = float(t.item())
+    parts = sc.n + sc.nb
+    value = parts * args.steps * world / (total_ms / 1000.0)
+
+    # end to end through the C ABI: host records in, one step, host records out
+    host = sim.particles()
+    e2e_ms = []
+    for i in range(max(3, min(args.steps, 10))):
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        sim.set_particles(host)
+        sim.step(1)
+        sim.particles(out=host)
+        e2e_ms.append((time.perf_counter() - t0) * 1000)
+    e2e_step_ms = statistics.median(e2e_ms)
+    if dist:
+        t = torch.tensor([e2e_step_ms], device="cuda", dtype=torch.float64)
+        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+        e2e_step_ms = float(t.item())
+    bytes_per_slot = 16 + 16 + 4 + 4  # float4 pos/den + float4 vel/mat + caller id + solid id
+    e2e = {"value": parts * world / (e2e_step_ms / 1000.0), "unit": UNIT,
+           "h2d_bytes_per_step": sc.n * bytes_per_slot, "d2h_bytes_per_step": sc.n * bytes_per_slot,
+           "ms_per_step": e2e_step_ms,
+           "path": "arp_sim_set_particles (host Particle records) + arp_sim_step(1) + arp_sim_get_particles"}
+
+    peak, peak_kind = load_peaks()
+    fl = prof["fluid_launches"]
+    fluid_ms = prof["fluid_ms"] / fl if fl else float("nan")
+    alg_bytes = 96.0 * sc.n  # per stage: read y_s 32 B + read y0 32 B + write y_{s+1} 32 B per particle
+    achieved = alg_bytes / (fluid_ms / 1000.0) / 1e9
+    traffic = load_traffic().get(f"fluid_{args.config}")
+    roofline = {"bound": "hbm", "kernel": "k_fluid (fused fluid forces + RK stage update)",
+                "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                "peak_kind": peak_kind, "traffic": traffic, "alg_bytes_per_launch": alg_bytes,
+                "avg_launch_ms": fluid_ms,
+                "segments_ms_per_step": {k: prof[k] / max(prof["steps"], 1) for k in
+                                         ("neighbor_ms", "solid_ms", "fluid_ms")}}
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
+        "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
+        "config": dict(config_of(sc, args.config), parallelism=f"replicas x{world}"),
+        "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
+    }
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        line["cpu_baseline"] = cpu_baseline(sc)
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    sim.close()
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--config", default="c2", choices=["c1", "c2"])
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.impl == "reference":
+        run_reference(args, rank, world)
+        return
+    if world > 1:
+        import datetime
+        import torch
+        torch.cuda.set_device(local_rank)
+        torch.distributed.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    try:
+        run_ours(args, rank, world, local_rank)
+    finally:
+        if world > 1:
+            import torch
+            torch.distributed.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -1,0 +1,284 @@
+/*
+ * arphys.h -- C ABI of the B200-native SPH time step.
+ *
+ * This is the drop-in boundary for the simulation-step interface of
+ * jsmith628/ar-physics, `FluidSim` (src/soft_body/mod.rs:23-275).  Each entry
+ * point names the reference method it replaces.  The reference binds its GPU
+ * work through OpenGL buffers; here the state lives in CUDA device memory
+ * owned by an opaque `arp_sim` handle, and the host exchanges particles in the
+ * reference's own std430 record layouts (`Particle`, `SolidParticle`,
+ * `Material`, `MatInteraction`), so a caller that already builds those records
+ * passes them unchanged.
+ *
+ * Rules shared by every call:
+ *   - every call returns an `arp_status`; ARP_OK is 0.  No call aborts the
+ *     process.  `arp_last_error()` gives a message for the calling thread's
+ *     last failure.
+ *   - a handle is used by one host thread at a time; different handles are
+ *     independent and may be driven from different threads.
+ *   - each handle owns a CUDA stream (or uses the one given by
+ *     `arp_sim_set_stream`); device work of a call is ordered on that stream.
+ *   - host buffers passed in are only read during the call; host buffers
+ *     passed out are written before the call returns.
+ */
+#ifndef ARPHYS_H
+#define ARPHYS_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define ARP_ABI_VERSION 1u
+#define ARP_INVALID_INDEX 0xFFFFFFFFu
+
+typedef enum arp_status {
+    ARP_OK = 0,
+    ARP_ERR_INVALID_ARG = 1,  /* null pointer, bad count, bad enum, init order */
+    ARP_ERR_CUDA = 2,         /* a CUDA runtime call failed (message has the name) */
+    ARP_ERR_NAN_STATE = 3,    /* a non-finite position reached the neighbor build */
+    ARP_ERR_CELL_OVERFLOW = 4,/* strict mode only: a cell held more than 128 entries */
+    ARP_ERR_TIMEOUT = 5,      /* a bounded device-side wait gave up */
+    ARP_ERR_UNSUPPORTED = 6,  /* a scene feature this build does not implement */
+    ARP_ERR_OUT_OF_MEMORY = 7,
+    ARP_ERR_PARSE = 8,        /* scene file syntax or schema error */
+    ARP_ERR_IO = 9,           /* scene file could not be read */
+    ARP_ERR_CAPACITY = 10     /* a caller-provided output buffer is too small */
+} arp_status;
+
+/* Equation of state ids, src/soft_body/material_region/material.rs:54-59 and
+ * the shader switch in src/soft_body/shaders/fluid.rs:45-52. */
+enum { ARP_EOS_ZERO = 0, ARP_EOS_CONSTANT = 1, ARP_EOS_IDEAL_GAS = 2, ARP_EOS_TAIT = 3 };
+
+/* Contact potential ids, src/soft_body/material_region/interaction.rs:21-28. */
+enum {
+    ARP_CONTACT_ZERO = 0, ARP_CONTACT_CONSTANT = 1, ARP_CONTACT_LINEAR = 2,
+    ARP_CONTACT_TAIT = 3, ARP_CONTACT_LENNARD_JONES = 4, ARP_CONTACT_HERTZ = 5
+};
+
+/* Explicit integrators named by the reference's scene loader
+ * (examples/test.rs:165-180).  The tableaus are the textbook ones; the
+ * reference takes them from the un-vendored crate numerical-integration
+ * 0.0.1, so the exact stage arithmetic there is not observable. */
+typedef enum arp_integrator {
+    ARP_INT_EULER = 0,     /* "euler", "rk1" */
+    ARP_INT_MIDPOINT = 1,  /* "midpoint", "rk2" */
+    ARP_INT_HEUN2 = 2,     /* "heun2", "heun" */
+    ARP_INT_RALSTON = 3,   /* "ralston" */
+    ARP_INT_RK3 = 4,       /* "rk3" (Kutta's third-order method) */
+    ARP_INT_HEUN3 = 5,     /* "heun3" */
+    ARP_INT_RK4 = 6,       /* "rk4" */
+    ARP_INT_RK_3_8 = 7,    /* "rk_3_8" */
+    ARP_INT_VERLET = 8     /* "verlet": not implemented, rejected with ARP_ERR_UNSUPPORTED */
+} arp_integrator;
+
+/* `Material`, std430, 80 bytes (src/soft_body/material_region/material.rs:11-28).
+ * GLSL `bool` fields are 4-byte integers. */
+typedef struct arp_material {
+    uint32_t immobile;
+    float mass, start_den;
+    uint32_t state_eq;
+    float sound_speed, target_den, visc, bulk_visc;
+    int32_t strain_order;
+    float normal_stiffness, shear_stiffness, normal_damp, shear_damp;
+    uint32_t plastic;
+    float yield_strength, work_hardening, work_hardening_exp, kinematic_hardening, thermal_softening;
+    float relaxation_time;
+} arp_material;
+
+/* `MatInteraction`, std430, 20 bytes (src/soft_body/material_region/interaction.rs:10-14). */
+typedef struct arp_interaction {
+    uint32_t potential;
+    float strength, radius;
+    float dampening, friction;
+} arp_interaction;
+
+/* `Particle`, std430, 48 bytes (src/soft_body/particle_state/mod.rs:24-29):
+ * den@0 mat@4 solid_id@8 pos@16 vel@32.  The same record carries time
+ * derivatives where the reference uses it as a derivative container. */
+typedef struct arp_particle {
+    float den;
+    uint32_t mat;
+    uint32_t solid_id;
+    uint32_t _pad0;
+    float pos[4];
+    float vel[4];
+} arp_particle;
+
+/* `SolidParticle`, std430, 96 bytes (src/soft_body/particle_state/mod.rs:31-35).
+ * `stress` is the accumulated plastic strain, column-major mat4. */
+typedef struct arp_solid_particle {
+    uint32_t part_id;
+    uint32_t _pad0[3];
+    float ref_pos[4];
+    float stress[16];
+} arp_solid_particle;
+
+/* `AABB` (src/soft_body/material_region/region.rs:11-14). */
+typedef struct arp_aabb {
+    float min[4];
+    float dim[4];
+} arp_aabb;
+
+/* Everything `FluidSim::new` receives (src/soft_body/mod.rs:58-66), after the
+ * regions have been turned into particles (the reference does that inside
+ * `new` with `MaterialRegion::gen_particles`; `arp_sim_create_from_toml`
+ * does it here).  Particle `mat` fields index `materials`.  Mobile particles
+ * must use materials with immobile == 0, boundary particles materials with
+ * immobile != 0.  `solid_id` fields of the input are ignored: solid ids are
+ * assigned in particle order to particles whose material has non-zero
+ * stiffness, as `Particles::init_solid_particles` does
+ * (src/soft_body/particle_state/particles.rs:488-506). */
+typedef struct arp_scene {
+    const arp_particle* particles;     /* mobile particles, n_particles */
+    uint32_t n_particles;
+    const arp_particle* boundary;      /* immobile particles, n_boundary (may be 0) */
+    uint32_t n_boundary;
+    const arp_material* materials;     /* n_materials */
+    uint32_t n_materials;
+    /* Optional n_materials x n_materials interaction table (row-major) and
+     * matching "given" flags.  Pairs not given are resolved exactly as
+     * src/soft_body/mod.rs:93-111 does (symmetric copy, else
+     * MatInteraction::default_between for i != j, else zero).  With
+     * interactions == NULL every pair is resolved by default; with
+     * interaction_given == NULL every entry of `interactions` is used. */
+    const arp_interaction* interactions;
+    const uint8_t* interaction_given;
+    arp_aabb bounds;
+    float kernel_radius;
+    int32_t integrator;                /* arp_integrator */
+    float timestep;
+    uint32_t subticks;
+    float gravity;
+    float artificial_viscocity;        /* kept for the record: the step reads bulk_visc */
+} arp_scene;
+
+typedef struct arp_sim arp_sim;
+
+/* Per-segment device time, the reference's profiler segments
+ * (src/profiler.rs:10-81; "Bucketting", "Forces", "Arith").  Filled from CUDA
+ * events when profiling is enabled; reading resets the accumulators. */
+typedef struct arp_profile {
+    uint64_t steps;              /* integrator steps since the last read */
+    uint64_t launches;           /* kernels launched by the handle since the last read */
+    double neighbor_ms;          /* grid build: keys, histogram, scan, scatter, reorder */
+    double solid_ms;             /* deformation gradient, stress, solid forces */
+    double fluid_ms;             /* fluid forces + fused stage update */
+    double integrate_ms;         /* stand-alone stage arithmetic (non-fused paths) */
+    uint64_t fluid_launches;
+    uint64_t neighbor_launches;
+    uint64_t solid_launches;
+} arp_profile;
+
+/* Health counters collected on the device during steps. */
+typedef struct arp_stats {
+    uint32_t max_cell_occupancy;   /* largest mobile+boundary count of one cell seen */
+    uint32_t overflow_cells;       /* cells seen above the reference's 128-slot bucket */
+    uint32_t nonfinite_positions;  /* positions the grid build found NaN/Inf */
+    uint32_t clamped_coordinates;  /* coordinates exactly on the upper box face */
+} arp_stats;
+
+/* Device view of the current state (the headless stand-in for the GL buffers
+ * that `FluidSim::particles()` hands to the renderer,
+ * src/soft_body/mod.rs:172-174).  Pointers are owned by the handle and valid
+ * until the next call that steps or changes the particle set.  Particles are
+ * stored in cell order; `orig_id[k]` gives the caller-order index of slot k. */
+typedef struct arp_device_view {
+    const void* pos_den;   /* float4[n]: x, y, z, density */
+    const void* vel_mat;   /* float4[n]: vx, vy, vz, material id as uint32 bits */
+    const void* orig_id;   /* uint32[n] */
+    uint32_t n;
+} arp_device_view;
+
+/* ---- lifecycle (FluidSim::new / init / drop) ------------------------------ */
+
+/* FluidSim::new, src/soft_body/mod.rs:58-166. */
+arp_status arp_sim_create(const arp_scene* scene, arp_sim** out);
+/* FluidSim::new after examples/test_mods/config.rs:298-474 parses a scene
+ * file and src/soft_body/material_region/mod.rs:56-155 seeds its regions. */
+arp_status arp_sim_create_from_toml(const char* path, arp_sim** out);
+/* FluidSim::init, src/soft_body/mod.rs:213-233. */
+arp_status arp_sim_init(arp_sim* sim);
+/* Drop of FluidSim. */
+arp_status arp_sim_destroy(arp_sim* sim);
+
+/* ---- stepping -------------------------------------------------------------- */
+
+/* FluidSim::update, src/soft_body/mod.rs:235-274: `subticks` integrator steps
+ * of timestep/subticks. */
+arp_status arp_sim_update(arp_sim* sim);
+/* `nsteps` integrator steps of timestep/subticks (update() without the
+ * subtick grouping). */
+arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps);
+
+/* ---- queries (FluidSim accessors, src/soft_body/mod.rs:168-178) ------------ */
+
+arp_status arp_sim_time(const arp_sim* sim, float* out);
+arp_status arp_sim_kernel_radius(const arp_sim* sim, float* out);
+arp_status arp_sim_num_materials(const arp_sim* sim, uint32_t* out);
+arp_status arp_sim_counts(const arp_sim* sim, uint32_t* n_particles, uint32_t* n_boundary,
+                          uint32_t* n_solids);
+arp_status arp_sim_dim(const arp_sim* sim, uint32_t* out);
+
+/* FluidSim::particles() read back, src/soft_body/particle_state/particles.rs:534-541:
+ * mobile particles in caller order (`cap` >= n_particles). */
+arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap);
+/* Solid records in solid-id order (`cap` >= n_solids). */
+arp_status arp_sim_get_solids(arp_sim* sim, arp_solid_particle* out, uint32_t cap);
+arp_status arp_sim_get_boundary(arp_sim* sim, arp_particle* out, uint32_t cap);
+arp_status arp_sim_get_materials(const arp_sim* sim, arp_material* out, uint32_t cap);
+/* The resolved n_materials^2 interaction table (src/soft_body/mod.rs:93-111). */
+arp_status arp_sim_get_interactions(const arp_sim* sim, arp_interaction* out, uint32_t cap);
+/* Replace the mobile state (den, pos, vel) of all particles, caller order;
+ * mat and solid_id of the input must match the handle's. */
+arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t n);
+arp_status arp_sim_device_state(arp_sim* sim, arp_device_view* out);
+
+/* FluidSim::add_particles, src/soft_body/mod.rs:180-206 with
+ * Particles::add_particles, src/soft_body/particle_state/particles.rs:547-631.
+ * `p` holds particles already seeded for `material`; `offset` (4 floats, may
+ * be NULL) is added to their positions.  `*material_added` receives 1 when a
+ * new material entry was appended. */
+arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n,
+                                 const arp_material* material, const float* offset,
+                                 int* material_added);
+
+/* ---- neighbor grid (src/soft_body/neighbor_list.rs) ------------------------ */
+
+/* Grid shape: subdivisions as NeighborList::new computes them (:199-217). */
+arp_status arp_sim_grid(const arp_sim* sim, uint32_t subdivisions[4], uint32_t* n_cells);
+/* Build the grid for the current positions and copy it out in the reference's
+ * terms: `cell_of[i]` = bucket of mobile particle i (caller order), or
+ * ARP_INVALID_INDEX for a non-finite position; `cell_start` (n_cells+1) and
+ * `members` (n_particles) = mobile particles of each cell in ascending caller
+ * id; `nbr_count[i]` = mobile + boundary particles within the kernel radius
+ * among the 27 cells around i (i itself included).  Any output may be NULL. */
+arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_start,
+                             uint32_t* members, uint32_t* nbr_count);
+/* Boundary section of the grid: `cell_start` (n_cells+1), `members`
+ * (n_boundary) in ascending boundary id. */
+arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* members);
+
+/* ---- streams, profiling, health ------------------------------------------- */
+
+/* Use a caller-owned CUDA stream (cudaStream_t passed as void*); NULL returns
+ * to the handle's own stream. */
+arp_status arp_sim_set_stream(arp_sim* sim, void* stream);
+arp_status arp_sim_synchronize(arp_sim* sim);
+arp_status arp_sim_profile_enable(arp_sim* sim, int enable);
+arp_status arp_sim_profile_read(arp_sim* sim, arp_profile* out);
+arp_status arp_sim_stats(arp_sim* sim, arp_stats* out);
+/* Kernels launched by this handle since creation. */
+arp_status arp_sim_launch_count(const arp_sim* sim, uint64_t* out);
+
+/* Thread-local message of the last failing call ("" when none). */
+const char* arp_last_error(void);
+uint32_t arp_abi_version(void);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* ARPHYS_H */

@@ -1,0 +1,88 @@
+"""CPU checks of the C ABI: the in-tree library loads, exports every entry
+point include/arphys.h declares, and rejects bad scenes before touching a
+GPU."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+from arphys import scenes
+from arphys.abi import (PARTICLE_DTYPE, SOLID_DTYPE, MATERIAL_DTYPE, INTERACTION_DTYPE, ArpScene, scene_struct,
+                        load_library)
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def declared_functions():
+    txt = open(os.path.join(ROOT, "include", "arphys.h")).read()
+    txt = re.sub(r"/\*.*?\*/", "", txt, flags=re.S)
+    return sorted(set(re.findall(r"\b(arp_[a-z0-9_]+)\s*\(", txt)))
+
+
+def test_library_exports_every_declared_symbol(lib):
+    names = declared_functions()
+    assert len(names) > 25
+    missing = [n for n in names if not hasattr(lib, n)]
+    assert not missing, missing
+
+
+def test_record_layouts_match_std430():
+    assert PARTICLE_DTYPE.itemsize == 48 and PARTICLE_DTYPE.fields["pos"][1] == 16
+    assert PARTICLE_DTYPE.fields["vel"][1] == 32
+    assert SOLID_DTYPE.itemsize == 96 and SOLID_DTYPE.fields["ref_pos"][1] == 16
+    assert MATERIAL_DTYPE.itemsize == 80 and INTERACTION_DTYPE.itemsize == 20
+
+
+def test_abi_version_and_error_string(lib):
+    assert lib.arp_abi_version() == 1
+    assert isinstance(lib.arp_last_error(), bytes)
+
+
+def _create(lib, scene):
+    sc, keep = scene_struct(scene)
+    h = ctypes.c_void_p()
+    code = lib.arp_sim_create(ctypes.byref(sc), ctypes.byref(h))
+    return code, h, lib.arp_last_error().decode()
+
+
+def test_null_scene_is_rejected(lib):
+    h = ctypes.c_void_p()
+    assert lib.arp_sim_create(None, ctypes.byref(h)) == 1
+    assert b"null" in lib.arp_last_error()
+
+
+def test_verlet_is_reported_unsupported(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.integrator = "verlet"
+    code, _, msg = _create(lib, sc)
+    assert code == 6 and "Verlet" in msg
+
+
+def test_four_dimensional_box_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.bounds_dim = (0.2, 0.2, 0.0, 0.1)
+    code, _, msg = _create(lib, sc)
+    assert code == 6 and "4-dimensional" in msg
+
+
+def test_mobile_particle_with_immobile_material_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.particles["mat"][0] = 0
+    code, _, msg = _create(lib, sc)
+    assert code == 1 and "immobile" in msg
+
+
+def test_material_index_out_of_range_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.particles["mat"][1] = 7
+    code, _, _ = _create(lib, sc)
+    assert code == 1
+
+
+def test_null_handle_calls_fail_cleanly(lib):
+    t = ctypes.c_float()
+    assert lib.arp_sim_time(None, ctypes.byref(t)) == 1
+    assert lib.arp_sim_step(None, 1) == 1
+    assert lib.arp_sim_destroy(None) == 0

@@ -1,0 +1,172 @@
+"""CPU tests of the oracle (the CPU restatement of the reference shaders).
+
+The reference ships no golden vectors, so the oracle is pinned by analytic
+known-answer tests: kernel normalisation and gradient, the correction matrix
+identity on a lattice, the sign of the elastic force on a stretched bar,
+momentum balance of the pair terms, brute-force neighbor sets, and exact
+integration of free fall by the Runge-Kutta tableaus.
+"""
+import numpy as np
+import pytest
+
+from arphys import scenes
+from arphys.abi import INVALID, PARTICLE_DTYPE, MATERIAL_DTYPE
+from oracle.oracle import Oracle, poly6, norm_const_f32
+
+
+@pytest.mark.parametrize("dim", [2, 3])
+def test_poly6_integrates_to_one(dim):
+    h = 0.02
+    m = 80 if dim == 3 else 400
+    ax = (np.arange(m) + 0.5) / m * 2 * h - h
+    grids = np.meshgrid(*([ax] * dim), indexing="ij")
+    r = np.zeros((ax.size ** dim, 4))
+    for a in range(dim):
+        r[:, a] = grids[a].reshape(-1)
+    w, _, _ = poly6(dim, h, r)
+    cell = (2 * h / m) ** dim
+    assert abs(w.sum() * cell - 1.0) < 2e-3
+
+
+def test_poly6_gradient_matches_finite_difference():
+    h = 0.02
+    rng = np.random.default_rng(0)
+    r = np.zeros((50, 4))
+    r[:, :3] = rng.uniform(-0.6 * h, 0.6 * h, size=(50, 3))
+    _, gw, _ = poly6(3, h, r)
+    eps = 1e-7
+    for a in range(3):
+        rp, rm = r.copy(), r.copy()
+        rp[:, a] += eps
+        rm[:, a] -= eps
+        fd = (poly6(3, h, rp)[0] - poly6(3, h, rm)[0]) / (2 * eps)
+        np.testing.assert_allclose(gw[:, a], fd, rtol=1e-5, atol=1e-3 * np.abs(gw).max())
+
+
+def test_norm_const_matches_closed_form():
+    # poly6: 4/(pi h^8) in 2D, 315/(64 pi h^9) in 3D
+    h = 0.02
+    assert abs(norm_const_f32(2, h) / (4 / (np.pi * h ** 8)) - 1) < 1e-6
+    assert abs(norm_const_f32(3, h) / (315 / (64 * np.pi * h ** 9)) - 1) < 1e-6
+
+
+def test_deformation_gradient_is_identity_in_reference_configuration():
+    sc, _ = scenes.stretched_bar(n=(8, 6, 6))
+    o = Oracle(sc, precision=64)
+    st = o.strains()
+    F = st[:, 1].reshape(-1, 4, 4)  # column-major per solid
+    for i in range(len(F)):
+        np.testing.assert_allclose(F[i][:3, :3], np.eye(3), atol=1e-9)
+
+
+@pytest.mark.parametrize("sign", [-1.0, 1.0])
+def test_stretched_bar_force_sign(sign):
+    """With the reference's convention (r = X_j - X_i, negative-definite L),
+    negative stiffness is restoring and positive stiffness is not."""
+    sc, stretched = scenes.stretched_bar(n=(20, 4, 4), lam=sign * 1e5, mu=sign * 1e5)
+    o = Oracle(sc, precision=64)
+    pos = o.state()["pos"]
+    pos[:, :3] = stretched
+    o.set_state(pos=pos)
+    acc = o.derivative()["vel"][:, 0]
+    x = stretched[:, 0]
+    right = x > x.max() - 1e-9
+    left = x < x.min() + 1e-9
+    restoring = acc[right].mean() < 0 and acc[left].mean() > 0
+    assert restoring == (sign < 0)
+
+
+def test_fluid_pair_terms_conserve_momentum():
+    """sum_i rho_i (dv_i/dt + g) = sum of antisymmetric pair terms = 0 for a
+    fluid without boundary."""
+    sc = scenes.dam_break_2d(nx=24, ny=24, box=(0.64, 0.64), alpha=0.5, visc=0.01)
+    sc.boundary = sc.boundary[:0]
+    rng = np.random.default_rng(3)
+    o = Oracle(sc, precision=64)
+    st = o.state()
+    vel = st["vel"].copy()
+    vel[:, :2] = rng.normal(size=(len(vel), 2)) * 0.1
+    den = st["den"] * (1 + 0.01 * rng.normal(size=len(vel)))
+    o.set_state(den=den, vel=vel)
+    d = o.derivative()
+    a = d["vel"][:, :2].copy()
+    a[:, 1] += float(np.float32(sc.gravity))
+    tot = (den[:, None] * a).sum(axis=0)
+    scale = np.abs(den[:, None] * a).sum(axis=0)
+    assert np.all(np.abs(tot) <= 1e-9 * scale)
+
+
+def test_neighbor_buckets_match_brute_force():
+    sc = scenes.dam_break_2d(nx=20, ny=24, box=(0.4, 0.4))
+    o = Oracle(sc)
+    b = o.buckets()
+    pos = sc.particles["pos"][:, :2].astype(np.float32)
+    bpos = sc.boundary["pos"][:, :2].astype(np.float32)
+    h2 = np.float32(sc.h) * np.float32(sc.h)
+    allpos = np.concatenate([pos, bpos])
+    d = allpos[None, :, :] - pos[:, None, :]
+    r2 = (d[..., 0] * d[..., 0] + d[..., 1] * d[..., 1]).astype(np.float32)
+    brute = (h2 - r2 > 0).sum(axis=1)
+    np.testing.assert_array_equal(b["nbr_count"], brute)
+    assert np.all(b["pos_index"] != INVALID)
+    # every particle is listed exactly once in the position sections
+    cnt = b["counts"][:, 2].sum()
+    assert cnt == sc.n
+
+
+@pytest.mark.parametrize("integ", ["euler", "midpoint", "heun2", "ralston", "rk3", "heun3", "rk4", "rk_3_8"])
+def test_free_fall_is_integrated_exactly(integ):
+    """An isolated particle feels only gravity; any consistent tableau
+    integrates x(t) = x0 + v0 t - g t^2 / 2 exactly for order >= 2."""
+    mats = np.array([scenes.liquid(1000.0, 20.0, 0.02, 0.0, mass=0.1)])
+    p = np.zeros(1, dtype=PARTICLE_DTYPE)
+    p["den"] = 1000.0
+    p["mat"] = 0
+    p["pos"][0, :2] = (0.5, 0.5)
+    p["vel"][0, :2] = (0.3, 1.0)
+    sc = scenes.Scene(particles=p, boundary=np.zeros(0, PARTICLE_DTYPE), materials=mats,
+                      bounds_min=(0, 0, 0, 0), bounds_dim=(1, 1, 0, 0), h=0.02, integrator=integ, dt=1e-3,
+                      gravity=9.81)
+    o = Oracle(sc, precision=64)
+    o.step(10)
+    dt = float(np.float32(1e-3))
+    t = 10 * dt
+    assert abs(o.time - t) < 1e-8
+    s = o.state()
+    g = float(np.float32(9.81))
+    if integ == "euler":
+        y = 0.5 + 1.0 * t - g * dt * dt * 10 * 9 / 2  # sum of v_k dt
+    else:
+        y = 0.5 + 1.0 * t - g * t * t / 2
+    assert abs(s["pos"][0, 1] - y) < 1e-9
+    assert abs(s["vel"][0, 1] - (1.0 - g * t)) < 1e-9
+    assert abs(s["pos"][0, 0] - (0.5 + 0.3 * t)) < 1e-9
+
+
+def test_float_and_double_oracles_agree_over_steps():
+    sc = scenes.dam_break_2d(nx=24, ny=24, box=(0.48, 0.48))
+    a, b = Oracle(sc, 32), Oracle(sc, 64)
+    a.step(20)
+    b.step(20)
+    sa, sb = a.state(), b.state()
+    assert np.abs(sa["pos"] - sb["pos"]).max() < 1e-6
+    assert np.abs(sa["den"] - sb["den"]).max() / 1000 < 1e-5
+
+
+def test_literal_and_cutoff_evaluations_agree():
+    sc = scenes.small_fluid_bar_3d()
+    a, b = Oracle(sc, 32), Oracle(sc, 32, literal=True)
+    a.step(2)
+    b.step(2)
+    sa, sb = a.state(), b.state()
+    for k in ("pos", "vel", "den", "plastic"):
+        np.testing.assert_array_equal(sa[k], sb[k])
+
+
+def test_solid_scene_runs_and_stays_finite():
+    sc = scenes.small_fluid_bar_3d()
+    o = Oracle(sc)
+    assert o.ns == sc.n_solids() > 1
+    o.step(5)
+    s = o.state()
+    assert np.isfinite(s["pos"]).all() and np.isfinite(s["vel"]).all()
