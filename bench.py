@@ -188,7 +188,11 @@ def run_ours(args, rank, world, local_rank):
     sc = make_scene(args.config)
     sim = FluidSim(sc)
     sim.init()
-    stream = torch.cuda.current_stream()
+    # a dedicated stream: the library launches on it and the events below are
+    # recorded on it (torch's default stream is the legacy NULL stream, which
+    # the library's own non-blocking stream does not order against)
+    stream = torch.cuda.Stream()
+    torch.cuda.set_stream(stream)
     sim.set_stream(stream.cuda_stream)
     flush = torch.empty(L2_FLUSH_BYTES, dtype=torch.uint8, device="cuda")
     for _ in range(args.warmup):

@@ -123,7 +123,7 @@ def test_accessors_mirror_the_reference_interface():
     sim = make(sc)
     o = Oracle(sc)
     assert sim.num_materials() == len(sc.materials)
-    assert abs(sim.kernel_radius() - sc.h) == 0
+    assert sim.kernel_radius() == np.float32(sc.h)
     assert sim.ns == o.ns and sim.n == sc.n and sim.nb == sc.nb
     sim.update()
     assert abs(sim.time() - np.float32(sc.dt)) == 0
@@ -146,6 +146,6 @@ def test_profile_and_launch_counters():
     assert prof["steps"] == 3
     assert prof["fluid_launches"] == 12  # RK4: one fused fluid kernel per stage
     assert prof["fluid_ms"] > 0 and prof["neighbor_ms"] > 0
-    assert sim.launch_count() - before == prof["launches"] + 0 or sim.launch_count() > before
+    assert sim.launch_count() - before == prof["launches"]
     st = sim.stats()
     assert st["nonfinite_positions"] == 0 and st["max_cell_occupancy"] > 0
