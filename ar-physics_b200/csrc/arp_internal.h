@@ -68,15 +68,17 @@ struct DevStats {
 };
 
 // One stage of the Runge-Kutta epilogue (fused into the fluid kernel).
-// y_next = y0 + sum_j c_next[j] * k_j (j <= stage), acc += c_acc * k_stage,
-// on the last stage y_new = y0 + acc.
+// y_next = y0 + (c_prev0 k_0 + c_prev1 k_1 + c_prev2 k_2 + c_self k_stage)
+// (terms with a zero coefficient skipped, in stage order), acc += c_acc *
+// k_stage, and on the last stage y_new = y0 + acc.  Stage derivatives that a
+// later stage reads are stored (non-diagonal tableaus only).
 struct StageCoefs {
     int stage;          // 0-based
     int last;           // 1 when this stage ends the step
-    float c_next[4];    // a[stage+1][j] * dt, j <= stage (unused when last)
+    float c_prev0, c_prev1, c_prev2;  // a[stage+1][j] * dt for j < stage
+    float c_self;       // a[stage+1][stage] * dt (unused when last)
     float c_acc;        // b[stage] * dt
     int acc_first;      // 1 when no earlier stage contributed to acc
-    int store_k;        // 1 when k of this stage is read by a later stage
 };
 
 struct StageBuffers {
@@ -86,8 +88,14 @@ struct StageBuffers {
     float4* next_vm;
     float4* acc_pd;        // b-weighted derivative accumulator
     float4* acc_vm;
-    float4* kst_pd[4];     // stored stage derivatives (non-diagonal tableaus)
-    float4* kst_vm[4];
+    float4* store_pd;      // where k of this stage is kept, or null
+    float4* store_vm;
+    const float4* prev0_pd;  // stored k_0, k_1, k_2 (null when not read)
+    const float4* prev0_vm;
+    const float4* prev1_pd;
+    const float4* prev1_vm;
+    const float4* prev2_pd;
+    const float4* prev2_vm;
 };
 
 // ---- neighbor grid (neighbor.cu) -------------------------------------------
@@ -97,6 +105,7 @@ struct GridBuffers {
     uint32_t* count;       // [ncells + 1] occupancy (zeroed by the scan)
     uint32_t* start;       // [ncells + 2] exclusive prefix of count
     uint32_t* perm;        // [cap] sorted index -> slot
+    uint2* coord;          // [cap] packed cell coordinates of each slot: x | y << 16, z
     uint32_t* block_sums;  // scan partials
     uint32_t block_sums_cap;
 };
@@ -116,6 +125,13 @@ uint32_t scan_block_sums_needed(uint32_t len);
 int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* a_out, const float4* b_in,
                   float4* b_out, const uint32_t* c_in, uint32_t* c_out, const uint32_t* d_in, uint32_t* d_out,
                   cudaStream_t st);
+// Gather a state into sorted order (out[k] = in[perm[k]]) and evaluate the
+// pressure term p / rho^2 of every gathered particle (fluid.rs:131-138,
+// :270-271).  Any pointer pair may be null.
+int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* pd_out, const float4* vm_in,
+                 float4* vm_out, const uint32_t* a_in, uint32_t* a_out, const uint32_t* b_in, uint32_t* b_out,
+                 const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st);
+
 // slot_of[sid[k]] = k for solid slots.
 int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st);
 // Neighbor counts within h of each sorted particle (mobile + boundary),
@@ -135,6 +151,8 @@ struct FluidArgs {
     const uint32_t* sid;     // storage-order solid id
     const uint32_t* sid_of_boundary_index;  // solid id of mobile particle with caller id == boundary caller id
     const uint32_t* borig;   // boundary caller ids, sorted
+    const float* ps;         // p / rho^2 of each sorted particle
+    const float* bps;        // p / rho^2 of each sorted boundary particle
     const float4* ksol;      // per-solid solid-term acceleration (nullptr when the solid branch is off)
     const DevMat* mats;
     const DevInter* inter;
@@ -172,10 +190,16 @@ struct SolidArgs {
     const float4* ep0;        // step-start plastic strain
     float4* ep_next;          // stage / step output
     float4* ep_acc;
-    float4* ep_kst[4];
+    float4* ep_store;         // k of this stage, or null
+    const float4* ep_prev0;   // stored k_0, k_1, k_2
+    const float4* ep_prev1;
+    const float4* ep_prev2;
     float4* F;                // [3*ns] deformation gradient columns (stage scratch)
     float4* A;                // [3*ns] sigma * L columns (stage scratch)
     float4* ksol;             // [ns] solid-term acceleration
+    const uint2* coord;       // storage-order packed cell coordinates of the stage grid
+    uint32_t* contact_bound;  // [2] max |u_i - u_0| bits, outside-box flag (cleared per stage)
+    float contact_slack;      // r_cut - (largest in-stencil |dx|), 0 when no bound applies
     const float4* xs;         // sorted stage positions (current-neighbor loop)
     const float4* vs;
     const uint32_t* start;

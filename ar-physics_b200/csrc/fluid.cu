@@ -38,16 +38,6 @@ __device__ __forceinline__ float pow7(float x) {
     return x6 * x;
 }
 
-// fluid.rs:131-138
-__device__ __forceinline__ float eos_pressure(uint32_t eq, float density, float c, float d0) {
-    switch (eq) {
-        case ARP_EOS_CONSTANT: return c * c;
-        case ARP_EOS_IDEAL_GAS: return c * c * (density - d0);
-        case ARP_EOS_TAIT: return (c * c * d0 / 7.0f) * (pow7(density / d0) - 1.0f);
-        default: return 0.0f;
-    }
-}
-
 // fluid.rs:140-153 (called with radius and strength in the shader's order)
 __device__ __forceinline__ float contact_potential(uint32_t eq, float r, float strength, float r0) {
     switch (eq) {
@@ -77,23 +67,23 @@ struct Acc {
     float3 f;
 };
 
+// One neighbor pair inside the kernel radius (the caller has tested it).
+// `ptj` is p_j / rho_j^2 of the neighbor, precomputed per particle.
 template <int DIM, bool BOUNDARY>
-__device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, uint32_t mat2, bool elastic2,
+__device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, float ptj, uint32_t mat2, bool elastic2,
                                      const FluidMat* __restrict__ sm, const DevInter* __restrict__ si,
                                      uint32_t nmat, const Params& P, Acc& acc) {
     const float rx = xj.x - s.x.x, ry = xj.y - s.x.y, rz = DIM == 3 ? xj.z - s.x.z : 0.0f;
     const float r2 = DIM == 3 ? (rx * rx + ry * ry) + rz * rz : rx * rx + ry * ry;
-    const float diff = P.h2 - r2;
-    if (!(diff > 0.0f)) return;
+    const float diff = fmaxf(P.h2 - r2, 0.0f);
     const float gws = -6.0f * P.kconst * diff * diff;
     const float gx = gws * rx, gy = gws * ry, gz = gws * rz;
     const float vx = vj.x - s.v.x, vy = vj.y - s.v.y, vz = DIM == 3 ? vj.z - s.v.z : 0.0f;
     const float d2 = xj.w;
     const FluidMat m2 = sm[mat2];
-    const float p2 = eos_pressure(m2.eos, d2, m2.c, m2.d0);
     const float vgw = DIM == 3 ? (vx * gx + vy * gy) + vz * gz : vx * gx + vy * gy;
     if (!BOUNDARY) acc.den += m2.mass * vgw;
-    const float pf = s.m1 * m2.mass * (s.pterm1 + p2 / (d2 * d2));
+    const float pf = s.m1 * m2.mass * (s.pterm1 + ptj);
     acc.f.x += pf * gx;
     acc.f.y += pf * gy;
     acc.f.z += pf * gz;
@@ -164,11 +154,16 @@ __device__ __forceinline__ float4 axpy(float c, float4 k, float4 t) {
                        __fadd_rn(t.z, __fmul_rn(c, k.z)), __fadd_rn(t.w, __fmul_rn(c, k.w)));
 }
 
+constexpr int kFluidThreads = 128;
+constexpr int kListCap = 48;                  // hits held per thread before they are consumed
+constexpr uint32_t kBoundaryBit = 0x80000000u;
+
 template <int DIM>
-__global__ void __launch_bounds__(256) k_fluid(FluidArgs a, Params P, StageCoefs c, StageBuffers b) {
-    extern __shared__ unsigned char smem_raw[];
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw);
-    DevInter* si = reinterpret_cast<DevInter*>(smem_raw + sizeof(FluidMat) * P.nmat);
+__global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, StageCoefs c, StageBuffers b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);  // [kListCap][blockDim]
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * kFluidThreads);
+    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * P.nmat);
     for (uint32_t i = threadIdx.x; i < P.nmat; i += blockDim.x) {
         const DevMat m = a.mats[i];
         sm[i] = FluidMat{m.mass, m.sound_speed, m.target_den, m.visc, m.bulk_visc, m.state_eq, m.stiff, 0u};
@@ -192,46 +187,70 @@ __global__ void __launch_bounds__(256) k_fluid(FluidArgs a, Params P, StageCoefs
     s.f1 = m1.visc;
     s.bf1 = m1.bulk;
     s.elastic = sid != kInvalid && m1.stiff;
-    const float p1 = eos_pressure(m1.eos, s.d1, m1.c, m1.d0);
-    s.pterm1 = p1 / (s.d1 * s.d1);
+    s.pterm1 = a.ps[k];
 
     Acc acc;
     acc.den = 0.0f;
     acc.f = make_float3(0.0f, 0.0f, 0.0f);
+    uint32_t* my = lst + threadIdx.x;
+    uint32_t cnt = 0;
+    auto boundary_pair = [&](uint32_t jb) {
+        const float4 xj = a.bxs[jb];
+        const float4 vj = a.bvs[jb];
+        const uint32_t mat2 = __float_as_uint(vj.w);
+        bool elastic2 = false;
+        if (a.any_stiff_immobile && sm[mat2].stiff) {
+            // fluid.rs:227: the boundary index reads the mobile array's solid id
+            const uint32_t bi = a.borig[jb];
+            elastic2 = bi < a.n_mobile_total && a.sid_of_boundary_index[bi] != kInvalid;
+        }
+        pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, sm, si, P.nmat, P, acc);
+    };
+    auto mobile_pair = [&](uint32_t j) {
+        const float4 xj = a.xs[j];
+        const float4 vj = a.vs[j];
+        const uint32_t mat2 = __float_as_uint(vj.w);
+        pair<DIM, false>(s, xj, vj, a.ps[j], mat2, sm[mat2].stiff != 0u, sm, si, P.nmat, P, acc);
+    };
+    // pass 1: candidates of the 3x3(x3) cells whose squared distance is
+    // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0)) go to
+    // the thread's list; hits past its capacity are evaluated on the spot
+    auto hit = [&](float4 q) {
+        const float rx = q.x - xi.x, ry = q.y - xi.y;
+        const float r2 = DIM == 3 ? (rx * rx + ry * ry) + (q.z - xi.z) * (q.z - xi.z) : rx * rx + ry * ry;
+        return P.h2 - r2 > 0.0f;
+    };
     if (finite3(xi)) {
         const Grid& g = P.grid;
         const CellCoord cc = cell_coord(xi, g);
         const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
-        const int zlo = DIM == 3 ? -1 : 0, zhi = DIM == 3 ? 1 : 0;
-        for (int dz = zlo; dz <= zhi; ++dz) {
-            const int z = cc.z + dz;
-            if (z < 0 || z >= (int)g.sub[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = cc.y + dy;
-                if (y < 0 || y >= (int)g.sub[1]) continue;
+        const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
+        const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
+        for (int z = zlo; z <= zhi; ++z) {
+            for (int y = ylo; y <= yhi; ++y) {
                 const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
                 const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
                 const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
                 for (uint32_t j = bb; j < be; ++j) {
-                    const float4 xj = a.bxs[j];
-                    const float4 vj = a.bvs[j];
-                    const uint32_t mat2 = __float_as_uint(vj.w);
-                    bool elastic2 = false;
-                    if (a.any_stiff_immobile && sm[mat2].stiff) {
-                        // fluid.rs:227: the boundary index reads the mobile array's solid id
-                        const uint32_t bi = a.borig[j];
-                        elastic2 = bi < a.n_mobile_total && a.sid_of_boundary_index[bi] != kInvalid;
+                    if (hit(a.bxs[j])) {
+                        if (cnt < kListCap) my[cnt++ * kFluidThreads] = j | kBoundaryBit;
+                        else boundary_pair(j);
                     }
-                    pair<DIM, true>(s, xj, vj, mat2, elastic2, sm, si, P.nmat, P, acc);
                 }
                 const uint32_t jb = a.start[c0], je = a.start[c1];
                 for (uint32_t j = jb; j < je; ++j) {
-                    const float4 xj = a.xs[j];
-                    const float4 vj = a.vs[j];
-                    const uint32_t mat2 = __float_as_uint(vj.w);
-                    pair<DIM, false>(s, xj, vj, mat2, sm[mat2].stiff != 0u, sm, si, P.nmat, P, acc);
+                    if (j != k && hit(a.xs[j])) {  // the particle itself contributes exactly zero
+                        if (cnt < kListCap) my[cnt++ * kFluidThreads] = j;
+                        else mobile_pair(j);
+                    }
                 }
             }
+        }
+        // pass 2: pair math over the collected hits
+        for (uint32_t e = 0; e < cnt; ++e) {
+            const uint32_t j = my[e * kFluidThreads];
+            if (j & kBoundaryBit) boundary_pair(j & ~kBoundaryBit);
+            else mobile_pair(j);
         }
     }
 
@@ -250,9 +269,9 @@ __global__ void __launch_bounds__(256) k_fluid(FluidArgs a, Params P, StageCoefs
     }
 
     // Runge-Kutta stage epilogue
-    if (c.store_k) {
-        b.kst_pd[c.stage][slot] = kpd;
-        b.kst_vm[c.stage][slot] = kvm;
+    if (b.store_pd) {
+        b.store_pd[slot] = kpd;
+        b.store_vm[slot] = kvm;
     }
     const float4 y0p = b.y0_pd[slot];
     const float4 y0v = b.y0_vm[slot];
@@ -277,14 +296,21 @@ __global__ void __launch_bounds__(256) k_fluid(FluidArgs a, Params P, StageCoefs
         b.next_vm[slot] = comb(y0v, accv, true);
     } else {
         float4 tp = make_float4(0.f, 0.f, 0.f, 0.f), tv = make_float4(0.f, 0.f, 0.f, 0.f);
-        for (int j = 0; j < c.stage; ++j) {
-            if (c.c_next[j] == 0.0f) continue;
-            tp = axpy(c.c_next[j], b.kst_pd[j][slot], tp);
-            tv = axpy(c.c_next[j], b.kst_vm[j][slot], tv);
+        if (c.c_prev0 != 0.0f) {
+            tp = axpy(c.c_prev0, b.prev0_pd[slot], tp);
+            tv = axpy(c.c_prev0, b.prev0_vm[slot], tv);
         }
-        if (c.c_next[c.stage] != 0.0f) {
-            tp = axpy(c.c_next[c.stage], kpd, tp);
-            tv = axpy(c.c_next[c.stage], kvm, tv);
+        if (c.c_prev1 != 0.0f) {
+            tp = axpy(c.c_prev1, b.prev1_pd[slot], tp);
+            tv = axpy(c.c_prev1, b.prev1_vm[slot], tv);
+        }
+        if (c.c_prev2 != 0.0f) {
+            tp = axpy(c.c_prev2, b.prev2_pd[slot], tp);
+            tv = axpy(c.c_prev2, b.prev2_vm[slot], tv);
+        }
+        if (c.c_self != 0.0f) {
+            tp = axpy(c.c_self, kpd, tp);
+            tv = axpy(c.c_self, kvm, tv);
         }
         b.next_pd[slot] = comb(y0p, tp, false);
         b.next_vm[slot] = comb(y0v, tv, true);
@@ -295,9 +321,10 @@ __global__ void __launch_bounds__(256) k_fluid(FluidArgs a, Params P, StageCoefs
 
 int launch_fluid(const FluidArgs& a, const Params& P, const StageCoefs& c, const StageBuffers& b, cudaStream_t st) {
     if (a.n == 0) return 0;
-    const int threads = 256;
+    const int threads = kFluidThreads;
     const uint32_t blocks = (a.n + threads - 1) / threads;
-    const size_t smem = sizeof(FluidMat) * P.nmat + sizeof(DevInter) * P.nmat * P.nmat;
+    const size_t smem = sizeof(uint32_t) * kListCap * kFluidThreads + sizeof(FluidMat) * P.nmat +
+                        sizeof(DevInter) * P.nmat * P.nmat;
     if (P.dim == 3)
         k_fluid<3><<<blocks, threads, smem, st>>>(a, P, c, b);
     else

@@ -28,16 +28,20 @@ constexpr int kScanItems = 4;  // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 
 __global__ void k_cell_keys(const float4* __restrict__ pos, uint32_t n, Grid grid, uint32_t* __restrict__ key,
-                            uint32_t* __restrict__ rank, uint32_t* __restrict__ count, DevStats* stats) {
+                            uint32_t* __restrict__ rank, uint32_t* __restrict__ count, uint2* __restrict__ coord,
+                            DevStats* stats) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     float4 p = pos[i];
     uint32_t k;
     if (!finite3(p)) {
         k = grid.ncells;
+        if (coord) coord[i] = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         if (stats) atomicAdd(&stats->nonfinite_positions, 1u);
     } else {
-        k = cell_id(cell_coord(p, grid), grid);
+        const CellCoord cc = cell_coord(p, grid);
+        k = cell_id(cc, grid);
+        if (coord) coord[i] = make_uint2((uint32_t)cc.x | ((uint32_t)cc.y << 16), (uint32_t)cc.z);
         if (stats) {
             // a coordinate on the upper face would hash one past the last cell
             bool face = (grid.dim[0] != 0.0f && p.x == grid.min[0] + grid.dim[0]) ||
@@ -174,6 +178,45 @@ __global__ void k_gather(const uint32_t* __restrict__ perm, uint32_t n, const fl
     if (d_out) d_out[k] = d_in[s];
 }
 
+__device__ __forceinline__ float eos_pressure(uint32_t eq, float density, float c, float d0) {
+    switch (eq) {  // fluid.rs:131-138, x^7 by products
+        case ARP_EOS_CONSTANT: return c * c;
+        case ARP_EOS_IDEAL_GAS: return c * c * (density - d0);
+        case ARP_EOS_TAIT: {
+            const float x = density / d0;
+            const float x2 = x * x;
+            const float x3 = x2 * x;
+            const float x6 = x3 * x3;
+            return (c * c * d0 / 7.0f) * (x6 * x - 1.0f);
+        }
+        default: return 0.0f;
+    }
+}
+
+__global__ void k_gather_state(const uint32_t* __restrict__ perm, uint32_t n, const float4* __restrict__ pd_in,
+                               float4* __restrict__ pd_out, const float4* __restrict__ vm_in,
+                               float4* __restrict__ vm_out, const uint32_t* __restrict__ a_in,
+                               uint32_t* __restrict__ a_out, const uint32_t* __restrict__ b_in,
+                               uint32_t* __restrict__ b_out, const uint2* __restrict__ c_in,
+                               uint2* __restrict__ c_out, float* __restrict__ ps_out,
+                               const DevMat* __restrict__ mats) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t s = perm ? perm[k] : k;
+    const float4 pd = pd_in[s];
+    const float4 vm = vm_in[s];
+    if (pd_out) pd_out[k] = pd;
+    if (vm_out) vm_out[k] = vm;
+    if (a_out) a_out[k] = a_in[s];
+    if (b_out) b_out[k] = b_in[s];
+    if (c_out) c_out[k] = c_in[s];
+    if (ps_out) {
+        const DevMat& m = mats[__float_as_uint(vm.w)];
+        const float p = eos_pressure(m.state_eq, pd.w, m.sound_speed, m.target_den);
+        ps_out[k] = p / (pd.w * pd.w);
+    }
+}
+
 __global__ void k_index_solids(const uint32_t* __restrict__ sid, uint32_t n, uint32_t* __restrict__ slot_of) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -223,7 +266,8 @@ int build_grid(const float4* pos, uint32_t n, const Grid& grid, GridBuffers& gb,
                const uint32_t* boundary_start, cudaStream_t st) {
     int launches = 0;
     if (n > 0) {
-        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, grid, gb.key, gb.rank, gb.count, stats);
+        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, grid, gb.key, gb.rank, gb.count, gb.coord,
+                                                                  stats);
         ++launches;
     }
     // cells, the non-finite bucket, and the total
@@ -254,6 +298,15 @@ int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* 
     if (n == 0) return 0;
     k_gather<<<blocks_for(n, kThreads), kThreads, 0, st>>>(perm, n, a_in, a_out, b_in, b_out, c_in, c_out, d_in,
                                                            d_out);
+    return 1;
+}
+
+int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* pd_out, const float4* vm_in,
+                 float4* vm_out, const uint32_t* a_in, uint32_t* a_out, const uint32_t* b_in, uint32_t* b_out,
+                 const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_gather_state<<<blocks_for(n, kThreads), kThreads, 0, st>>>(perm, n, pd_in, pd_out, vm_in, vm_out, a_in, a_out,
+                                                                 b_in, b_out, c_in, c_out, ps_out, mats);
     return 1;
 }
 

@@ -203,12 +203,16 @@ struct arp_sim {
     // mobile state: Y (y0), T (reorder target / y_new), S[2] (stage states)
     StateBuf Y, T, S[2], X, acc, kst[4];
     DevBuf<uint32_t> orig, orig_r, sid, sid_r, sid_sorted, slot_of;
+    DevBuf<float> ps, bps;  // p / rho^2 of sorted particles / boundary particles
     // boundary (cell-sorted)
     DevBuf<float4> b_pd, b_vm;
     DevBuf<uint32_t> b_orig, b_start, sid_of_bidx;
     // grid scratch
     GridBuffers gb{};
     DevBuf<uint32_t> g_key, g_rank, g_count, g_start, g_perm, g_bsums;
+    DevBuf<uint2> g_coord, coord_s;  // grid coordinates per slot; storage-order copy for stage 0
+    DevBuf<uint32_t> contact_bound;
+    float contact_slack = 0.0f;
     uint32_t grid_cap = 0;
     // solids
     DevBuf<float4> ref, L, F, A, ksol;
@@ -254,6 +258,7 @@ arp_status ensure_grid(arp_sim* S, uint32_t cap) {
     CUDA_TRY(S->g_key.alloc(cap));
     CUDA_TRY(S->g_rank.alloc(cap));
     CUDA_TRY(S->g_perm.alloc(cap));
+    CUDA_TRY(S->g_coord.alloc(cap));
     if (!S->g_start.p) {
         CUDA_TRY(S->g_count.alloc(size_t(nc) + 2));
         CUDA_TRY(S->g_start.alloc(size_t(nc) + 2));
@@ -267,6 +272,7 @@ arp_status ensure_grid(arp_sim* S, uint32_t cap) {
     S->gb.count = S->g_count.p;
     S->gb.start = S->g_start.p;
     S->gb.perm = S->g_perm.p;
+    S->gb.coord = S->g_coord.p;
     S->gb.block_sums = S->g_bsums.p;
     S->gb.block_sums_cap = (uint32_t)S->g_bsums.n;
     return ARP_OK;
@@ -332,6 +338,21 @@ void upload_params(arp_sim* S) {
     P.rcut2 = P.rcut * P.rcut;
     volatile float hh = S->h * S->h;
     P.r_geom = hh / P.rcut;
+    // Largest |dx| between particles inside the box whose cells are within one
+    // cell per axis: 2 * |cell diagonal|.  An axis of zero extent contributes
+    // nothing only when every particle shares its coordinate (flat z).
+    double cs2 = 0.0;
+    bool bounded = true;
+    for (int a = 0; a < 3; ++a) {
+        if (S->bounds.dim[a] > 0.0f) {
+            const double cs = (double)S->bounds.dim[a] / (double)P.grid.sub[a];
+            cs2 += cs * cs;
+        } else if (!(a == 2 && S->kdim == 2)) {
+            bounded = false;
+        }
+    }
+    const double slack = 0.999 * (double)P.rcut - 2.0 * std::sqrt(cs2);
+    S->contact_slack = bounded && slack > 0.0 ? (float)slack : 0.0f;
 }
 
 // Solid data, boundary grid, reference neighbor lists (FluidSim::init).
@@ -385,8 +406,8 @@ arp_status do_init(arp_sim* S) {
             CUDA_TRY(cudaMemcpyAsync(tmp_o.p, bo.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         }
         S->launches += build_grid(tmp_pd.p, nb, S->P.grid, S->gb, nullptr, nullptr, st);
-        S->launches += gather_sorted(S->gb.perm, nb, tmp_pd.p, S->b_pd.p, tmp_vm.p, S->b_vm.p, tmp_o.p,
-                                     S->b_orig.p, nullptr, nullptr, st);
+        S->launches += gather_state(S->gb.perm, nb, tmp_pd.p, S->b_pd.p, tmp_vm.p, S->b_vm.p, tmp_o.p,
+                                    S->b_orig.p, nullptr, nullptr, nullptr, nullptr, S->bps.p, S->d_mats.p, st);
         CUDA_TRY(cudaMemcpyAsync(S->b_start.p, S->gb.start, (size_t(nc) + 2) * sizeof(uint32_t),
                                  cudaMemcpyDeviceToDevice, st));
         CUDA_TRY(cudaStreamSynchronize(st));
@@ -453,8 +474,9 @@ arp_status do_step(arp_sim* S) {
     arp_sim::Mark mk{};
     mark(S, mk, 0);
     S->launches += build_grid(S->Y.pd.p, n, S->P.grid, S->gb, S->d_stats.p, bstart, st);
-    S->launches += gather_sorted(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
-                                 S->orig_r.p, S->sid.p, S->sid_r.p, st);
+    S->launches += gather_state(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
+                                S->orig_r.p, S->sid.p, S->sid_r.p, ns > 1 ? S->gb.coord : nullptr,
+                                ns > 1 ? S->coord_s.p : nullptr, S->ps.p, S->d_mats.p, st);
     std::swap(S->Y, S->T);
     std::swap(S->orig, S->orig_r);
     std::swap(S->sid, S->sid_r);
@@ -466,10 +488,6 @@ arp_status do_step(arp_sim* S) {
     B.y0_vm = S->Y.vm.p;
     B.acc_pd = S->acc.pd.p;
     B.acc_vm = S->acc.vm.p;
-    for (int j = 0; j < 4; ++j) {
-        B.kst_pd[j] = S->kst[j].pd.p;
-        B.kst_vm[j] = S->kst[j].vm.p;
-    }
     bool acc_started = false;
     const float4* cur_pd = S->Y.pd.p;
     const float4* cur_vm = S->Y.vm.p;
@@ -479,21 +497,36 @@ arp_status do_step(arp_sim* S) {
         StageCoefs c{};
         c.stage = s;
         c.last = last ? 1 : 0;
-        if (!last)
-            for (int j = 0; j <= s; ++j) c.c_next[j] = (float)(tab.a[s + 1][j] * (double)S->dt_sub);
+        float cp[3] = {0.f, 0.f, 0.f};
+        if (!last) {
+            for (int j = 0; j < s && j < 3; ++j) cp[j] = (float)(tab.a[s + 1][j] * (double)S->dt_sub);
+            c.c_self = (float)(tab.a[s + 1][s] * (double)S->dt_sub);
+        }
+        c.c_prev0 = cp[0];
+        c.c_prev1 = cp[1];
+        c.c_prev2 = cp[2];
         c.c_acc = (float)(tab.b[s] * (double)S->dt_sub);
         c.acc_first = acc_started ? 0 : 1;
         if (c.c_acc != 0.0f) acc_started = true;
-        c.store_k = 0;
+        bool store_k = false;
         for (int t = s + 2; t < tab.stages; ++t)
-            if (tab.a[t][s] != 0.0) c.store_k = 1;
+            if (tab.a[t][s] != 0.0) store_k = true;
+        B.store_pd = store_k ? S->kst[s].pd.p : nullptr;
+        B.store_vm = store_k ? S->kst[s].vm.p : nullptr;
+        B.prev0_pd = cp[0] != 0.f ? S->kst[0].pd.p : nullptr;
+        B.prev0_vm = cp[0] != 0.f ? S->kst[0].vm.p : nullptr;
+        B.prev1_pd = cp[1] != 0.f ? S->kst[1].pd.p : nullptr;
+        B.prev1_vm = cp[1] != 0.f ? S->kst[1].vm.p : nullptr;
+        B.prev2_pd = cp[2] != 0.f ? S->kst[2].pd.p : nullptr;
+        B.prev2_vm = cp[2] != 0.f ? S->kst[2].vm.p : nullptr;
 
         if (s > 0) {
             if (S->profiling && s > 0) mark(S, mk, 0);
             l0 = S->launches;
             S->launches += build_grid(cur_pd, n, S->P.grid, S->gb, S->d_stats.p, bstart, st);
-            S->launches += gather_sorted(S->gb.perm, n, cur_pd, S->X.pd.p, cur_vm, S->X.vm.p, sb ? S->sid.p : nullptr,
-                                         sb ? S->sid_sorted.p : nullptr, nullptr, nullptr, st);
+            S->launches += gather_state(S->gb.perm, n, cur_pd, S->X.pd.p, cur_vm, S->X.vm.p, sb ? S->sid.p : nullptr,
+                                        sb ? S->sid_sorted.p : nullptr, nullptr, nullptr, nullptr, nullptr, S->ps.p,
+                                        S->d_mats.p, st);
             nl += S->launches - l0;
         }
         const float4* xs = s == 0 ? S->Y.pd.p : S->X.pd.p;
@@ -517,10 +550,16 @@ arp_status do_step(arp_sim* S) {
             a.ep0 = S->ep.p;
             a.ep_next = last ? S->ep_t.p : S->ep_s[s % 2].p;
             a.ep_acc = S->ep_acc.p;
-            for (int j = 0; j < 4; ++j) a.ep_kst[j] = S->ep_kst[j].p;
+            a.ep_store = store_k ? S->ep_kst[s].p : nullptr;
+            a.ep_prev0 = cp[0] != 0.f ? S->ep_kst[0].p : nullptr;
+            a.ep_prev1 = cp[1] != 0.f ? S->ep_kst[1].p : nullptr;
+            a.ep_prev2 = cp[2] != 0.f ? S->ep_kst[2].p : nullptr;
             a.F = S->F.p;
             a.A = S->A.p;
             a.ksol = S->ksol.p;
+            a.coord = s == 0 ? S->coord_s.p : S->gb.coord;  // storage-order coordinates of this stage's grid
+            a.contact_bound = S->contact_bound.p;
+            a.contact_slack = S->contact_slack;
             a.xs = xs;
             a.vs = vs;
             a.start = S->gb.start;
@@ -544,6 +583,8 @@ arp_status do_step(arp_sim* S) {
         f.sid = S->sid.p;
         f.sid_of_boundary_index = S->sid_of_bidx.p;
         f.borig = S->b_orig.p;
+        f.ps = S->ps.p;
+        f.bps = S->bps.p;
         f.ksol = sb ? S->ksol.p : nullptr;
         f.mats = S->d_mats.p;
         f.inter = S->d_inter.p;
@@ -700,6 +741,8 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->sid_r.alloc(n));
     CUDA_TRY(S->sid_sorted.alloc(n));
     CUDA_TRY(S->slot_of.alloc(ns));
+    CUDA_TRY(S->ps.alloc(n));
+    CUDA_TRY(S->bps.alloc(nb));
     CUDA_TRY(S->b_pd.alloc(nb));
     CUDA_TRY(S->b_vm.alloc(nb));
     CUDA_TRY(S->b_orig.alloc(nb));
@@ -711,6 +754,8 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->F.alloc(3 * ns));
     CUDA_TRY(S->A.alloc(3 * ns));
     CUDA_TRY(S->ksol.alloc(ns));
+    CUDA_TRY(S->coord_s.alloc(S->ns > 1 ? n : 1));
+    CUDA_TRY(S->contact_bound.alloc(2));
     CUDA_TRY(S->ep.alloc(4 * ns));
     CUDA_TRY(S->ep_t.alloc(4 * ns));
     CUDA_TRY(S->ep_s[0].alloc(4 * ns));

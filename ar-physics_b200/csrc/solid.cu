@@ -33,6 +33,13 @@ inline uint32_t blocks_for(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / 
 __device__ __forceinline__ float3 sub3(float4 a, float4 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
 __device__ __forceinline__ float dot3(float3 a, float3 b) { return (a.x * b.x + a.y * b.y) + a.z * b.z; }
 
+// unit diagonal on the axes at or above dim (solid.rs:149, :175, :227)
+__device__ __forceinline__ void pad_unit(M4& C, uint32_t dim) {
+#pragma unroll
+    for (uint32_t i = 0; i < 4; ++i)
+        if (i >= dim) C.m[i][i] = 1.0f;
+}
+
 // Walk the 27 reference cells around solid i (ascending cell, ascending
 // solid id inside a cell) and call f(j, dX, diff) for each other solid with
 // h^2 - |dX|^2 > 0.
@@ -109,7 +116,7 @@ __global__ void k_ref_L(const float4* __restrict__ ref, uint32_t ns, const uint3
 #pragma unroll
             for (int r = 0; r < 3; ++r) C.m[c][r] += g.w * (gg[r] * d[c]);
     }
-    for (uint32_t a = P.dim; a < 4; ++a) C.m[a][a] = 1.0f;
+    pad_unit(C, P.dim);
     const M4 Li = m4_inverse(C);
 #pragma unroll
     for (int c = 0; c < 3; ++c) L[3 * i + c] = make_float4(Li.m[c][0], Li.m[c][1], Li.m[c][2], Li.m[c][3]);
@@ -119,7 +126,9 @@ __global__ void k_ref_L(const float4* __restrict__ ref, uint32_t ns, const uint3
 
 __device__ __forceinline__ float trace_dim(const M4& A, uint32_t dim) {
     float t = A.m[0][0];
-    for (uint32_t i = 1; i < dim; ++i) t += A.m[i][i];
+#pragma unroll
+    for (uint32_t i = 1; i < 4; ++i)
+        if (i < dim) t += A.m[i][i];
     return t;
 }
 __device__ inline M4 mat_log5(const M4& A) {  // solid.rs:105-116
@@ -144,7 +153,7 @@ __device__ inline M4 mat_sqrt_db(const M4& Xm) {  // Denman-Beavers, solid.rs:11
 }
 __device__ inline M4 seth_hill(const M4& F, int two_m, uint32_t dim) {  // solid.rs:147-168
     M4 C = m4_mul(m4_transpose(F), F);
-    for (uint32_t i = dim; i < 4; ++i) C.m[i][i] = 1.0f;
+    pad_unit(C, dim);
     if (two_m == 0) return m4_scale(0.5f, mat_log5(C));
     const int a = two_m < 0 ? -two_m : two_m;
     const int m = a >> 1;
@@ -158,7 +167,7 @@ __device__ inline M4 seth_hill_rate(const M4& F, const M4& Fd, int two_m, uint32
     M4 dC = m4_mul(m4_transpose(Fd), F);
     dC = m4_add(dC, m4_transpose(dC));
     M4 C = m4_mul(m4_transpose(F), F);
-    for (uint32_t i = dim; i < 4; ++i) C.m[i][i] = 1.0f;
+    pad_unit(C, dim);
     if (two_m == 0) return m4_mul(m4_scale(0.5f, dC), m4_inverse(C));
     const int a = two_m < 0 ? -two_m : two_m;
     const int m = a >> 1;
@@ -241,6 +250,32 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P
         EP.m[cc][2] = e.z;
         EP.m[cc][3] = e.w;
     }
+    // Bound used to skip the self-contact scan: max |u_i - u_0| over solids
+    // (u = x - X) and whether any solid left the box.
+    {
+        const float4 X0 = a.ref[0];
+        const float4 x0 = a.pd[a.slot_of[0]];
+        const float4 Xi = a.ref[i];
+        const float ux = (xi.x - Xi.x) - (x0.x - X0.x), uy = (xi.y - Xi.y) - (x0.y - X0.y),
+                    uz = (xi.z - Xi.z) - (x0.z - X0.z);
+        const float du = sqrtf((ux * ux + uy * uy) + uz * uz);
+        bool outside = !finite3(xi) || !(du == du);
+        const float pc[3] = {xi.x, xi.y, xi.z};
+#pragma unroll
+        for (int ax = 0; ax < 3; ++ax) {
+            const float d = P.grid.dim[ax];
+            if (d != 0.0f) {
+                const float t = (pc[ax] - P.grid.min[ax]) / d;
+                outside = outside || !(t >= 0.0f && t < 1.0f);
+            }
+        }
+        const uint32_t mx = __reduce_max_sync(__activemask(), outside ? 0x7F800000u : __float_as_uint(du));
+        const uint32_t any_out = __reduce_or_sync(__activemask(), outside ? 1u : 0u);
+        if ((threadIdx.x & 31) == __ffs(__activemask()) - 1) {
+            atomicMax(&a.contact_bound[0], mx);
+            if (any_out) atomicOr(&a.contact_bound[1], 1u);
+        }
+    }
     // solid.rs:334-341
     const M4 strain = m4_add(seth_hill(Fm, mm.strain_order, P.dim), EP);
     const M4 rate = seth_hill_rate(Fm, Fdm, mm.strain_order, P.dim);
@@ -275,7 +310,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P
 #pragma unroll
     for (int cc = 0; cc < 4; ++cc) {
         const uint32_t o = 4 * i + cc;
-        if (c.store_k) a.ep_kst[c.stage][o] = kv[cc];
+        if (a.ep_store) a.ep_store[o] = kv[cc];
         const float4 y0 = a.ep0[o];
         float4 acc = make_float4(0.f, 0.f, 0.f, 0.f);
         if (c.c_acc != 0.0f) {
@@ -289,12 +324,21 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P
             a.ep_next[o] = add4(y0, acc);
         } else {
             float4 t = make_float4(0.f, 0.f, 0.f, 0.f);
-            for (int j = 0; j < c.stage; ++j)
-                if (c.c_next[j] != 0.0f) t = lin4(c.c_next[j], a.ep_kst[j][o], t);
-            if (c.c_next[c.stage] != 0.0f) t = lin4(c.c_next[c.stage], kv[cc], t);
+            if (c.c_prev0 != 0.0f) t = lin4(c.c_prev0, a.ep_prev0[o], t);
+            if (c.c_prev1 != 0.0f) t = lin4(c.c_prev1, a.ep_prev1[o], t);
+            if (c.c_prev2 != 0.0f) t = lin4(c.c_prev2, a.ep_prev2[o], t);
+            if (c.c_self != 0.0f) t = lin4(c.c_self, kv[cc], t);
             a.ep_next[o] = add4(y0, t);
         }
     }
+}
+
+__device__ __forceinline__ bool in_stencil(uint2 a, uint2 b) {
+    const int dx = (int)(a.x & 0xFFFFu) - (int)(b.x & 0xFFFFu);
+    const int dy = (int)(a.x >> 16) - (int)(b.x >> 16);
+    const int dz = (int)a.y - (int)b.y;
+    return a.y != 0xFFFFFFFFu && b.y != 0xFFFFFFFFu && dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 &&
+           dz <= 1;
 }
 
 __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P) {
@@ -307,14 +351,23 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
     const float m1 = mm.mass, d1 = xi.w;
     const float V1 = m1 / d1;
     const float4 Ai0 = a.A[3 * i], Ai1 = a.A[3 * i + 1], Ai2 = a.A[3 * i + 2];
+    const float4 Xi = a.ref[i];
+    const float4 Fi0 = a.F[3 * i], Fi1 = a.F[3 * i + 1], Fi2 = a.F[3 * i + 2];
+    const uint2 ci = a.coord[slot];
     float fx = 0.f, fy = 0.f, fz = 0.f;
-    // solid.rs:343-374: elastic force over reference neighbors of the same material
+    // Reference neighbors of the same material: the elastic force
+    // (solid.rs:343-374) and, when the neighbor also sits in the current
+    // 3x3x3 cells, hourglass control (solid.rs:430-443; kernel(dX) is
+    // non-zero exactly for these pairs).
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMat)) continue;
         const uint32_t j = e & ~kSameMat;
         const float4 g = a.rl.gw[k];
-        const float V2 = m1 / a.pd[a.slot_of[j]].w;
+        const uint32_t sj = a.slot_of[j];
+        const float4 xj = a.pd[sj];
+        const float d2 = xj.w;
+        const float V2 = m1 / d2;
         const float s = -V1 * V2;
         const float4 Aj0 = a.A[3 * j], Aj1 = a.A[3 * j + 1], Aj2 = a.A[3 * j + 2];
         const float4 c0 = make_float4(s * (Ai0.x + Aj0.x), s * (Ai0.y + Aj0.y), s * (Ai0.z + Aj0.z), 0.f);
@@ -324,14 +377,37 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
         fx += (c0.x * g.x + c1.x * g.y) + c2.x * g.z;
         if (P.dim >= 2) fy += (c0.y * g.x + c1.y * g.y) + c2.y * g.z;
         if (P.dim >= 3) fz += (c0.z * g.x + c1.z * g.y) + c2.z * g.z;
+        if (in_stencil(a.coord[sj], ci)) {
+            const float3 dx = sub3(xj, xi);
+            const float3 dX = sub3(a.ref[j], Xi);
+            const float diff = P.h2 - dot3(dX, dX);
+            const float l = sqrtf(dot3(dx, dx));
+            const float4 Fj0 = a.F[3 * j], Fj1 = a.F[3 * j + 1], Fj2 = a.F[3 * j + 2];
+            const float ex = ((0.5f * (Fi0.x + Fj0.x)) * dX.x + (0.5f * (Fi1.x + Fj1.x)) * dX.y) +
+                             (0.5f * (Fi2.x + Fj2.x)) * dX.z - dx.x;
+            const float ey = ((0.5f * (Fi0.y + Fj0.y)) * dX.x + (0.5f * (Fi1.y + Fj1.y)) * dX.y) +
+                             (0.5f * (Fi2.y + Fj2.y)) * dX.z - dx.y;
+            const float ez = ((0.5f * (Fi0.z + Fj0.z)) * dX.x + (0.5f * (Fi1.z + Fj1.z)) * dX.y) +
+                             (0.5f * (Fi2.z + Fj2.z)) * dX.z - dx.z;
+            const float kern = P.kconst * diff * diff * diff;
+            const float sh = (((100000000.0f * m1 * m1 / (d1 * d2)) *
+                               (0.5f * ((ex * dx.x + ey * dx.y) + ez * dx.z) / (l + P.hg_h))) *
+                              (1.0f / (l * l + P.eps_hh))) *
+                             kern;
+            const float den = l + P.eps_h;
+            fx -= (sh * dx.x) / den;
+            fy -= (sh * dx.y) / den;
+            fz -= (sh * dx.z) / den;
+        }
     }
-    // solid.rs:378-453: hourglass control and self-contact over current
-    // neighbors of the same material (boundary and other-material pairs add
-    // nothing in that loop)
-    const float4 Xi = a.ref[i];
-    const float4 Fi0 = a.F[3 * i], Fi1 = a.F[3 * i + 1], Fi2 = a.F[3 * i + 2];
-    const Grid& g = P.grid;
-    if (finite3(xi)) {
+    // Self-contact (solid.rs:428,445-450): same-material neighbors in the
+    // current cells whose reference distance exceeds r_cut.  Skipped when
+    // every solid is inside the box and r_cut - max|dx in stencil| exceeds
+    // 2 max|u_k - u_0|, which bounds |dX| below r_cut for all such pairs.
+    const float U = __uint_as_float(a.contact_bound[0]);
+    const bool maybe = !mm.plastic && (a.contact_slack <= 0.0f || a.contact_bound[1] != 0u || !(2.0f * U < a.contact_slack));
+    if (maybe && finite3(xi)) {
+        const Grid& g = P.grid;
         const CellCoord cc = cell_coord(xi, g);
         const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
         for (int dz = -1; dz <= 1; ++dz) {
@@ -342,44 +418,20 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
                 if (y < 0 || y >= (int)g.sub[1]) continue;
                 const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
                 for (uint32_t k = a.start[row + x0]; k < a.start[row + x1 + 1]; ++k) {
-                    const float4 vj = a.vs[k];
-                    if (__float_as_uint(vj.w) != mat) continue;
+                    if (__float_as_uint(a.vs[k].w) != mat) continue;
                     const uint32_t sj = a.sid_sorted[k];
                     if (sj == kInvalid) continue;
                     const float4 xj = a.xs[k];
                     const float3 dx = sub3(xj, xi);
                     const float3 dX = sub3(a.ref[sj], Xi);
                     const float dXX = dot3(dX, dX), dxx = dot3(dx, dx);
-                    const bool in_contact = dXX > P.rcut2 && dxx < P.rcut2;
-                    const float diff = P.h2 - dXX;
-                    if (!(diff > 0.0f) && !(in_contact && !mm.plastic)) continue;
+                    if (!(dXX > P.rcut2 && dxx < P.rcut2)) continue;
                     const float l = sqrtf(dxx);
-                    if (diff > 0.0f) {
-                        const float4 Fj0 = a.F[3 * sj], Fj1 = a.F[3 * sj + 1], Fj2 = a.F[3 * sj + 2];
-                        const float ex = ((0.5f * (Fi0.x + Fj0.x)) * dX.x + (0.5f * (Fi1.x + Fj1.x)) * dX.y) +
-                                         (0.5f * (Fi2.x + Fj2.x)) * dX.z - dx.x;
-                        const float ey = ((0.5f * (Fi0.y + Fj0.y)) * dX.x + (0.5f * (Fi1.y + Fj1.y)) * dX.y) +
-                                         (0.5f * (Fi2.y + Fj2.y)) * dX.z - dx.y;
-                        const float ez = ((0.5f * (Fi0.z + Fj0.z)) * dX.x + (0.5f * (Fi1.z + Fj1.z)) * dX.y) +
-                                         (0.5f * (Fi2.z + Fj2.z)) * dX.z - dx.z;
-                        const float kern = P.kconst * diff * diff * diff;
-                        const float d2 = xj.w;
-                        const float s = (((100000000.0f * m1 * m1 / (d1 * d2)) *
-                                          (0.5f * ((ex * dx.x + ey * dx.y) + ez * dx.z) / (l + P.hg_h))) *
-                                         (1.0f / (l * l + P.eps_hh))) *
-                                        kern;
-                        const float den = l + P.eps_h;
-                        fx -= (s * dx.x) / den;
-                        fy -= (s * dx.y) / den;
-                        fz -= (s * dx.z) / den;
-                    }
-                    if (in_contact && !mm.plastic) {
-                        const float dr = fmaxf(P.rcut - l, 0.0f);
-                        const float cs = -5000.0f * sqrtf(dr * P.r_geom);
-                        fx += (cs * dx.x) / l;
-                        fy += (cs * dx.y) / l;
-                        fz += (cs * dx.z) / l;
-                    }
+                    const float dr = fmaxf(P.rcut - l, 0.0f);
+                    const float cs = -5000.0f * sqrtf(dr * P.r_geom);
+                    fx += (cs * dx.x) / l;
+                    fy += (cs * dx.y) / l;
+                    fz += (cs * dx.z) / l;
                 }
             }
         }
@@ -406,6 +458,7 @@ int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const
 
 int launch_solid(const SolidArgs& a, const Params& P, const StageCoefs& c, cudaStream_t st) {
     if (a.ns == 0) return 0;
+    cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
     k_solid_stress<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P, c);
     k_solid_forces<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P);
     return 2;
