@@ -94,16 +94,19 @@ def test_self_contact_matches_oracle():
     """Two blocks of one material whose reference positions are far apart
     but whose current positions touch: the self-contact term is active."""
     s = 0.01
-    a = scenes.lattice((0.2, 0.2, 0.2), (4, 4, 4), s)
-    b = scenes.lattice((0.2 + 20 * 2 * s, 0.2, 0.2), (4, 4, 4), s)
+    # lattices sit half a spacing off the cell faces: the contact and
+    # hourglass terms depend on which cells a particle is in, so a particle on
+    # a face would make the result hinge on the last bit of its coordinate
+    a = scenes.lattice((0.205, 0.205, 0.205), (4, 4, 4), s)
+    b = scenes.lattice((0.205 + 20 * 2 * s, 0.205, 0.205), (4, 4, 4), s)
     mats = np.array([scenes.elastic_solid(1000.0, -2e5, -1e5, mass=1000.0 * s ** 3)])
     p = scenes.particles(np.concatenate([a, b]), 0, 1000.0)
     sc = scenes.Scene(particles=p, boundary=np.zeros(0, PARTICLE_DTYPE), materials=mats,
                       bounds_min=(0.0, 0.0, 0.0, 0.0), bounds_dim=(1.0, 1.0, 1.0, 0.0), h=2 * s,
-                      integrator="midpoint", dt=1e-5, gravity=0.0, name="self_contact")
+                      integrator="midpoint", dt=1e-4, gravity=0.0, name="self_contact")
     state = p.copy()
-    state["pos"][64:, 0] -= 20 * 2 * s - 4 * s - 1.5 * 2 * s  # block b now 1.5 h to the right of block a
-    sim, g, r, r64 = run_both(sc, state, 10)
+    state["pos"][64:, 0] -= 20 * 2 * s - 4 * s - 0.5 * 2 * s  # block b now h/2 to the right of block a
+    sim, g, r, r64 = run_both(sc, state, 20)
     moved = np.abs(r["vel"][:, 0]).max()
-    assert moved > 0, "contact must push the blocks"
+    assert moved > 1e-4, "contact must push the blocks"
     compare("self_contact", g, r, r64, 2e-5)
