@@ -173,6 +173,8 @@ def load_library():
         "arp_sim_stats": [c_sim, ctypes.POINTER(ArpStats)],
         "arp_sim_launch_count": [c_sim, ctypes.POINTER(ctypes.c_uint64)],
     }
+    sig["arp_grid_build_noalloc"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ArpAABB), ctypes.c_float,
+                                     ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args

@@ -14,6 +14,8 @@
 #pragma once
 
 #include <cstdint>
+#include <string>
+
 #include <cuda_runtime.h>
 
 #include "../../include/arphys.h"
@@ -97,6 +99,9 @@ struct StageBuffers {
     const float4* prev2_pd;
     const float4* prev2_vm;
 };
+
+// Record `msg` as the calling thread's last error and return `code`.
+arp_status set_error(arp_status code, const std::string& msg);
 
 // ---- neighbor grid (neighbor.cu) -------------------------------------------
 struct GridBuffers {

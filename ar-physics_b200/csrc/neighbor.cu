@@ -14,7 +14,11 @@
 //      records the largest occupancy and cells over the reference's 128.
 // Memory traffic per particle: 16 B position read, 4+4 B key/rank write and
 // read, 4 B perm write, 4+4 B perm read/write in the run sort.
+#include <algorithm>
+#include <cmath>
 #include <cstdio>
+#include <mutex>
+#include <string>
 
 #include "grid.cuh"
 
@@ -82,8 +86,9 @@ __device__ __forceinline__ void block_excl_scan(uint32_t v, uint32_t& excl) {
     excl = warp_tot[warp] + inc - v;
 }
 
-__global__ void k_scan_tiles(uint32_t* __restrict__ count, uint32_t len, uint32_t* __restrict__ out,
-                             uint32_t* __restrict__ block_sums) {
+// `count` and `out` may be the same array (the allocation-free build scans in
+// place), so they are not declared __restrict__.
+__global__ void k_scan_tiles(uint32_t* count, uint32_t len, uint32_t* out, uint32_t* __restrict__ block_sums) {
     __shared__ uint32_t last_total;
     const uint32_t base = blockIdx.x * kScanTile + threadIdx.x * kScanItems;
     uint32_t v[kScanItems];
@@ -260,6 +265,57 @@ __global__ void k_count_neighbors(const float4* __restrict__ xs, const uint32_t*
 
 inline uint32_t blocks_for(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / (uint32_t)t; }
 
+// ---- allocation-free grid build ---------------------------------------------
+// Scratch of arp_grid_build_noalloc: arrival ranks of up to kNoAllocMaxParticles
+// particles, then the scan's tile totals.  The histogram and its scan live in
+// the caller's cell_start array, and cell keys are recomputed from the
+// positions instead of stored.  4 MiB + 4 KiB per GPU that loads the library.
+constexpr uint32_t kNoAllocMaxParticles = 1u << 20;
+constexpr uint32_t kNoAllocMaxCells = (1u << 22) - 2;  // cell_start then holds at most 2^22 entries
+constexpr uint32_t kNoAllocMaxTiles = (kNoAllocMaxCells + 2 + kScanTile - 1) / kScanTile;
+__device__ __align__(256) uint32_t g_noalloc_scratch[kNoAllocMaxParticles + kNoAllocMaxTiles];
+
+__global__ void k_rank_noalloc(const float4* __restrict__ pos, uint32_t n, Grid grid, uint32_t* __restrict__ count,
+                               uint32_t* __restrict__ rank) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    const uint32_t k = finite3(p) ? cell_id(cell_coord(p, grid), grid) : grid.ncells;
+    rank[i] = atomicAdd(&count[k], 1u);
+}
+
+__global__ void k_scatter_noalloc(const float4* __restrict__ pos, uint32_t n, Grid grid,
+                                  const uint32_t* __restrict__ start, const uint32_t* __restrict__ rank,
+                                  uint32_t* __restrict__ perm) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4 p = pos[i];
+    const uint32_t k = finite3(p) ? cell_id(cell_coord(p, grid), grid) : grid.ncells;
+    perm[start[k] + rank[i]] = i;
+}
+
+// Device address of g_noalloc_scratch, looked up once per device with that
+// device current (host code may not use the symbol itself as an address).
+constexpr int kMaxDevices = 64;
+std::mutex g_noalloc_mu;
+uint32_t* g_noalloc_ptr[kMaxDevices] = {};
+
+cudaError_t noalloc_scratch(uint32_t** out) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    if (dev < 0 || dev >= kMaxDevices) return cudaErrorInvalidDevice;
+    std::lock_guard<std::mutex> lock(g_noalloc_mu);
+    if (!g_noalloc_ptr[dev]) {
+        void* p = nullptr;
+        e = cudaGetSymbolAddress(&p, g_noalloc_scratch);
+        if (e != cudaSuccess) return e;
+        g_noalloc_ptr[dev] = static_cast<uint32_t*>(p);
+    }
+    *out = g_noalloc_ptr[dev];
+    return cudaSuccess;
+}
+
 }  // namespace
 
 int build_grid(const float4* pos, uint32_t n, const Grid& grid, GridBuffers& gb, DevStats* stats,
@@ -324,3 +380,52 @@ int count_neighbors(const float4* xs, const uint32_t* start, uint32_t n, const f
 }
 
 }  // namespace arp
+
+// ---- C ABI: allocation-free grid build ----------------------------------------
+extern "C" arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, const arp_aabb* bounds,
+                                             float kernel_radius, uint32_t* cell_start,
+                                             uint32_t cell_start_capacity, uint32_t* perm, void* stream) {
+    using namespace arp;
+    if (!bounds) return set_error(ARP_ERR_INVALID_ARG, "bounds is null");
+    if (!(kernel_radius > 0.0f)) return set_error(ARP_ERR_INVALID_ARG, "kernel_radius must be positive");
+    if (bounds->dim[3] > 0.0f) return set_error(ARP_ERR_UNSUPPORTED, "4-dimensional boxes are not supported");
+    if (n > kNoAllocMaxParticles)
+        return set_error(ARP_ERR_CAPACITY, "arp_grid_build_noalloc: n exceeds the 1048576-particle maximum");
+    if (n > 0 && (!pos_den || !perm)) return set_error(ARP_ERR_INVALID_ARG, "null position or perm pointer");
+    if (!cell_start) return set_error(ARP_ERR_INVALID_ARG, "cell_start is null");
+    if (reinterpret_cast<uintptr_t>(pos_den) % 16 != 0)
+        return set_error(ARP_ERR_INVALID_ARG, "pos_den must be 16-byte aligned (float4 records)");
+    Grid g{};
+    uint64_t nc = 1;
+    for (int a = 0; a < 3; ++a) {
+        if (!std::isfinite(bounds->min[a]) || !std::isfinite(bounds->dim[a]) || bounds->dim[a] < 0.0f)
+            return set_error(ARP_ERR_INVALID_ARG, "bounds must be finite with non-negative extent");
+        g.min[a] = bounds->min[a];
+        g.dim[a] = bounds->dim[a];
+        g.sub[a] = (uint32_t)std::max(1.0f, bounds->dim[a] / kernel_radius);  // neighbor_list.rs:201-206
+        nc *= g.sub[a];
+    }
+    if (nc > kNoAllocMaxCells)
+        return set_error(ARP_ERR_CAPACITY, "arp_grid_build_noalloc: the grid exceeds the 4194302-cell maximum");
+    g.ncells = (uint32_t)nc;
+    if ((uint64_t)cell_start_capacity < nc + 2)
+        return set_error(ARP_ERR_CAPACITY, "cell_start must hold n_cells + 2 entries (" + std::to_string(nc + 2) +
+                                               ")");
+    uint32_t* scratch = nullptr;
+    cudaError_t e = noalloc_scratch(&scratch);
+    if (e != cudaSuccess) return set_error(ARP_ERR_CUDA, std::string("cudaGetSymbolAddress: ") + cudaGetErrorString(e));
+    uint32_t* rank = scratch;
+    uint32_t* tile_sums = scratch + kNoAllocMaxParticles;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const uint32_t len = g.ncells + 2;
+    e = cudaMemsetAsync(cell_start, 0, (size_t)len * sizeof(uint32_t), st);
+    if (e != cudaSuccess) return set_error(ARP_ERR_CUDA, std::string("cudaMemsetAsync: ") + cudaGetErrorString(e));
+    const float4* pos = static_cast<const float4*>(pos_den);
+    if (n > 0) k_rank_noalloc<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, g, cell_start, rank);
+    exclusive_scan(cell_start, len, cell_start, tile_sums, st);  // in place: counts become starts
+    if (n > 0) k_scatter_noalloc<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, g, cell_start, rank, perm);
+    k_sort_runs<<<blocks_for(g.ncells + 1, kThreads), kThreads, 0, st>>>(cell_start, g.ncells, perm, nullptr, nullptr);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_error(ARP_ERR_CUDA, std::string("grid build launch: ") + cudaGetErrorString(e));
+    return ARP_OK;
+}

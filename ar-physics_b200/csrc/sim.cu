@@ -170,6 +170,8 @@ struct HostStage {
 
 }  // namespace
 
+arp_status arp::set_error(arp_status code, const std::string& msg) { return fail(code, msg); }
+
 struct arp_sim {
     // scene
     uint32_t n = 0, nb = 0, ns = 0, M = 0;

@@ -261,6 +261,34 @@ arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_sta
  * (n_boundary) in ascending boundary id. */
 arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* members);
 
+/* ---- allocation-free grid build -------------------------------------------- */
+
+/* No counterpart in the reference (whose buckets live in a GL buffer the
+ * simulation allocates).  Builds the cell grid of NeighborList::new's shape
+ * for `n` caller-owned device positions without allocating any memory, for
+ * callers that cannot call cudaMalloc on this path: code running inside a
+ * host framework that owns the device allocator (a caching allocator or an
+ * engine's pre-reserved heap), a real-time loop that forbids allocation after
+ * start-up, or work being recorded into a CUDA graph.
+ *   pos_den     device float4[n] (x, y, z used; 16-byte aligned), n <= 1048576
+ *   cell_start  device uint32[n_cells + 2], n_cells = prod_a max(1, floor(dim_a / h))
+ *               <= 4194302: entries c..c+1 bound the slots of cell c, the last
+ *               two bound the non-finite positions
+ *   perm        device uint32[n]: slot -> input index, ascending inside a cell
+ *   stream      cudaStream_t (NULL = the legacy default stream); the call is
+ *               asynchronous on it.
+ * Scratch (ranks and scan partials) is a file-scope device array of 4 MiB +
+ * 4 KiB that every GPU which loads the library holds until the process
+ * exits.  The first call on a device looks up that array's device address
+ * (cudaGetSymbolAddress) with the device current; make that first call
+ * before any stream capture.  All calls share the one array, so calls whose
+ * work overlaps on the GPU (different streams or threads without ordering)
+ * race and corrupt each other's output.  Sizes beyond the maxima return
+ * ARP_ERR_CAPACITY without launching anything. */
+arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, const arp_aabb* bounds, float kernel_radius,
+                                  uint32_t* cell_start, uint32_t cell_start_capacity, uint32_t* perm,
+                                  void* stream);
+
 /* ---- streams, profiling, health ------------------------------------------- */
 
 /* Use a caller-owned CUDA stream (cudaStream_t passed as void*); NULL returns

@@ -1,0 +1,75 @@
+"""The allocation-free grid build, called through the C ABI.
+
+arp_grid_build_noalloc serves callers that cannot call cudaMalloc on this
+path (a host framework that owns the device allocator, a real-time loop that
+forbids allocation after start-up, work recorded into a CUDA graph): they
+pass device inputs and outputs they already own, and the call keeps its
+scratch in a fixed device array inside the library.  Its output must equal
+the grid that the handle-based entry point (arp_sim_neighbors) reports for
+the same positions, bit for bit, on consecutive calls that reuse the shared
+scratch.
+
+This file is collected last so that a run stopping at the first failure has
+already run every other test.
+"""
+import ctypes
+
+import numpy as np
+import pytest
+
+from arphys import FluidSim, scenes
+from arphys.abi import ArpAABB, load_library
+
+pytestmark = pytest.mark.gpu
+
+
+def _bounds(sc):
+    b = ArpAABB()
+    for i in range(4):
+        b.min[i] = float(sc.bounds_min[i])
+        b.dim[i] = float(sc.bounds_dim[i])
+    return b
+
+
+def _noalloc_grid(lib, torch, pos_host, sc, nc):
+    n = len(pos_host)
+    pos = torch.tensor(np.ascontiguousarray(pos_host, dtype=np.float32), device="cuda")
+    cell_start = torch.full((nc + 2,), -1, dtype=torch.int32, device="cuda")
+    perm = torch.full((n,), -1, dtype=torch.int32, device="cuda")
+    stream = torch.cuda.current_stream()
+    b = _bounds(sc)
+    code = lib.arp_grid_build_noalloc(pos.data_ptr(), n, ctypes.byref(b), float(np.float32(sc.h)),
+                                      cell_start.data_ptr(), nc + 2, perm.data_ptr(), stream.cuda_stream)
+    assert code == 0, lib.arp_last_error()
+    torch.cuda.synchronize()
+    return cell_start.cpu().numpy().view(np.uint32), perm.cpu().numpy().view(np.uint32)
+
+
+def test_noalloc_grid_matches_the_handle_entry_point():
+    torch = pytest.importorskip("torch")
+    lib = load_library()
+    sc = scenes.small_fluid_bar_3d()
+    sim = FluidSim(sc)
+    sim.init()
+    _, nc = sim.grid()
+    for call in range(2):  # two calls in a row share the library's scratch array
+        sim.step(3)
+        ref = sim.neighbors()
+        p = sim.particles()
+        start, perm = _noalloc_grid(lib, torch, p["pos"], sc, nc)
+        np.testing.assert_array_equal(start[:nc + 1], ref["cell_start"])
+        assert start[nc + 1] == sc.n  # the last entry closes the non-finite range
+        np.testing.assert_array_equal(perm, ref["members"])
+
+
+def test_noalloc_grid_rejects_sizes_beyond_its_maximum():
+    lib = load_library()
+    sc = scenes.small_fluid_bar_3d()
+    b = _bounds(sc)
+    dummy = ctypes.c_void_p(256)  # never dereferenced: the size check comes first
+    code = lib.arp_grid_build_noalloc(dummy, (1 << 20) + 1, ctypes.byref(b), float(np.float32(sc.h)), dummy,
+                                      1 << 22, dummy, None)
+    assert code == 10
+    assert b"1048576" in lib.arp_last_error()
+    code = lib.arp_grid_build_noalloc(dummy, 16, ctypes.byref(b), float(np.float32(sc.h)), dummy, 3, dummy, None)
+    assert code == 10 and b"n_cells + 2" in lib.arp_last_error()
