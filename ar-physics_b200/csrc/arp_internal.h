@@ -137,6 +137,17 @@ int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* 
                  float4* vm_out, const uint32_t* a_in, uint32_t* a_out, const uint32_t* b_in, uint32_t* b_out,
                  const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st);
 
+// Particle records (caller order) to structure of arrays in caller order, and
+// back from cell order into caller order (the state exchange of the C ABI).
+int records_to_soa(const arp_particle* in, uint32_t n, const uint32_t* sid_of, float4* pd, float4* vm, uint32_t* orig,
+                   uint32_t* sid, cudaStream_t st);
+int soa_to_records(const float4* pd, const float4* vm, const uint32_t* orig, const uint32_t* sid, uint32_t n,
+                   float pos_w, arp_particle* out, cudaStream_t st);
+// Sets flag bit 0 when a record's material differs from mat_of, bit 1 when a
+// w component differs from pos_w / zero.
+int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, float pos_w, uint32_t* flag,
+                  cudaStream_t st);
+
 // slot_of[sid[k]] = k for solid slots.
 int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st);
 // Neighbor counts within h of each sorted particle (mobile + boundary),

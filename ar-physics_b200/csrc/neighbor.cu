@@ -222,6 +222,45 @@ __global__ void k_gather_state(const uint32_t* __restrict__ perm, uint32_t n, co
     }
 }
 
+// Particle records (48 B, caller order) -> structure of arrays in caller order.
+__global__ void k_records_to_soa(const arp_particle* __restrict__ in, uint32_t n, const uint32_t* __restrict__ sid_of,
+                                 float4* __restrict__ pd, float4* __restrict__ vm, uint32_t* __restrict__ orig,
+                                 uint32_t* __restrict__ sid) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float4* r = reinterpret_cast<const float4*>(in + i);
+    const float4 h = r[0], p = r[1], v = r[2];  // (den, mat, solid_id, pad), pos, vel
+    pd[i] = make_float4(p.x, p.y, p.z, h.x);
+    vm[i] = make_float4(v.x, v.y, v.z, h.y);  // material id bits
+    orig[i] = i;
+    sid[i] = sid_of[i];
+}
+
+// Bit 0: a record's material differs from the handle's; bit 1: a w component
+// differs from the handle's common w / zero.
+__global__ void k_check_records(const arp_particle* __restrict__ in, uint32_t n, const uint32_t* __restrict__ mat_of,
+                                float pos_w, uint32_t* __restrict__ flag) {
+    uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const arp_particle& r = in[i];
+    uint32_t bad = (r.mat != mat_of[i]) ? 1u : 0u;
+    if (r.pos[3] != pos_w || r.vel[3] != 0.0f) bad |= 2u;
+    if (bad) atomicOr(flag, bad);
+}
+
+// Cell-ordered structure of arrays -> particle records in caller order.
+__global__ void k_soa_to_records(const float4* __restrict__ pd, const float4* __restrict__ vm,
+                                 const uint32_t* __restrict__ orig, const uint32_t* __restrict__ sid, uint32_t n,
+                                 float pos_w, arp_particle* __restrict__ out) {
+    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 p = pd[k], v = vm[k];
+    float4* r = reinterpret_cast<float4*>(out + orig[k]);
+    r[0] = make_float4(p.w, v.w, __uint_as_float(sid[k]), 0.0f);
+    r[1] = make_float4(p.x, p.y, p.z, pos_w);
+    r[2] = make_float4(v.x, v.y, v.z, 0.0f);
+}
+
 __global__ void k_index_solids(const uint32_t* __restrict__ sid, uint32_t n, uint32_t* __restrict__ slot_of) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
@@ -363,6 +402,27 @@ int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* 
     if (n == 0) return 0;
     k_gather_state<<<blocks_for(n, kThreads), kThreads, 0, st>>>(perm, n, pd_in, pd_out, vm_in, vm_out, a_in, a_out,
                                                                  b_in, b_out, c_in, c_out, ps_out, mats);
+    return 1;
+}
+
+int records_to_soa(const arp_particle* in, uint32_t n, const uint32_t* sid_of, float4* pd, float4* vm, uint32_t* orig,
+                   uint32_t* sid, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_records_to_soa<<<blocks_for(n, kThreads), kThreads, 0, st>>>(in, n, sid_of, pd, vm, orig, sid);
+    return 1;
+}
+
+int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, float pos_w, uint32_t* flag,
+                  cudaStream_t st) {
+    if (n == 0) return 0;
+    k_check_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(in, n, mat_of, pos_w, flag);
+    return 1;
+}
+
+int soa_to_records(const float4* pd, const float4* vm, const uint32_t* orig, const uint32_t* sid, uint32_t n,
+                   float pos_w, arp_particle* out, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_soa_to_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pd, vm, orig, sid, n, pos_w, out);
     return 1;
 }
 

@@ -138,36 +138,6 @@ struct StateBuf {
     DevBuf<float4> pd, vm;
 };
 
-// Page-locked host staging for state uploads and downloads.
-struct HostStage {
-    float4* pd = nullptr;
-    float4* vm = nullptr;
-    uint32_t* orig = nullptr;
-    uint32_t* sid = nullptr;
-    size_t cap = 0;
-    cudaError_t ensure(size_t n) {
-        if (cap >= n && pd) return cudaSuccess;
-        release();
-        n = n ? n : 1;
-        cudaError_t e;
-        if ((e = cudaMallocHost(&pd, n * sizeof(float4))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(&vm, n * sizeof(float4))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(&orig, n * sizeof(uint32_t))) != cudaSuccess) return e;
-        if ((e = cudaMallocHost(&sid, n * sizeof(uint32_t))) != cudaSuccess) return e;
-        cap = n;
-        return cudaSuccess;
-    }
-    void release() {
-        if (pd) cudaFreeHost(pd);
-        if (vm) cudaFreeHost(vm);
-        if (orig) cudaFreeHost(orig);
-        if (sid) cudaFreeHost(sid);
-        pd = vm = nullptr;
-        orig = sid = nullptr;
-        cap = 0;
-    }
-};
-
 }  // namespace
 
 arp_status arp::set_error(arp_status code, const std::string& msg) { return fail(code, msg); }
@@ -197,7 +167,6 @@ struct arp_sim {
 
     cudaStream_t own_stream = nullptr, stream = nullptr;
     uint64_t launches = 0;
-    HostStage stage;
 
     // device: materials
     DevBuf<DevMat> d_mats;
@@ -206,6 +175,10 @@ struct arp_sim {
     StateBuf Y, T, S[2], X, acc, kst[4];
     DevBuf<uint32_t> orig, orig_r, sid, sid_r, sid_sorted, slot_of;
     DevBuf<float> ps, bps;  // p / rho^2 of sorted particles / boundary particles
+    DevBuf<arp_particle> records;      // device copy of caller-order Particle records (state exchange)
+    DevBuf<uint32_t> sid_of_caller_d;  // caller id -> solid id
+    DevBuf<uint32_t> mat_of_caller_d;  // caller id -> material id
+    DevBuf<uint32_t> check_flag;
     // boundary (cell-sorted)
     DevBuf<float4> b_pd, b_vm;
     DevBuf<uint32_t> b_orig, b_start, sid_of_bidx;
@@ -239,7 +212,6 @@ struct arp_sim {
             for (auto e : m.e) ev_free.push_back(e);
         for (auto e : ev_free) cudaEventDestroy(e);
         if (own_stream) cudaStreamDestroy(own_stream);
-        stage.release();
     }
 
     bool solid_branch() const { return ns > 1; }  // shaders/mod.rs:51: solids.len() > 1
@@ -744,6 +716,18 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->sid_sorted.alloc(n));
     CUDA_TRY(S->slot_of.alloc(ns));
     CUDA_TRY(S->ps.alloc(n));
+    CUDA_TRY(S->sid_of_caller_d.alloc(n));
+    CUDA_TRY(S->mat_of_caller_d.alloc(n));
+    CUDA_TRY(S->check_flag.alloc(1));
+    {
+        std::vector<uint32_t> mo(S->n);
+        for (uint32_t i = 0; i < S->n; ++i) mo[i] = S->host_particles[i].mat;
+        if (S->n)
+            CUDA_TRY(cudaMemcpy(S->mat_of_caller_d.p, mo.data(), S->n * sizeof(uint32_t), cudaMemcpyHostToDevice));
+    }
+    if (S->n)
+        CUDA_TRY(cudaMemcpy(S->sid_of_caller_d.p, S->sid_of_caller.data(), S->n * sizeof(uint32_t),
+                            cudaMemcpyHostToDevice));
     CUDA_TRY(S->bps.alloc(nb));
     CUDA_TRY(S->b_pd.alloc(nb));
     CUDA_TRY(S->b_vm.alloc(nb));
@@ -791,20 +775,6 @@ arp_status allocate(arp_sim* S) {
     }
     CUDA_TRY(S->d_inter.alloc(di.size()));
     CUDA_TRY(cudaMemcpy(S->d_inter.p, di.data(), di.size() * sizeof(DevInter), cudaMemcpyHostToDevice));
-    return ARP_OK;
-}
-
-// Download the state into the pinned staging buffers (cell order).
-arp_status download(arp_sim* S) {
-    const uint32_t n = S->n;
-    CUDA_TRY(S->stage.ensure(n));
-    if (!n) return ARP_OK;
-    cudaStream_t st = S->stream;
-    CUDA_TRY(cudaMemcpyAsync(S->stage.pd, S->Y.pd.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(S->stage.vm, S->Y.vm.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(S->stage.orig, S->orig.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaMemcpyAsync(S->stage.sid, S->sid.p, n * sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
-    CUDA_TRY(cudaStreamSynchronize(st));
     return ARP_OK;
 }
 
@@ -913,21 +883,13 @@ arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap) 
         for (uint32_t i = 0; i < sim->n; ++i) out[i].solid_id = sim->sid_of_caller[i];
         return ARP_OK;
     }
-    ARP_TRY(download(sim));
-    const float4* pd = sim->stage.pd;
-    const float4* vm = sim->stage.vm;
-    const uint32_t* orig = sim->stage.orig;
-    const uint32_t* sid = sim->stage.sid;
-    for (uint32_t k = 0; k < sim->n; ++k) {
-        arp_particle& p = out[orig[k]];
-        p.den = pd[k].w;
-        std::memcpy(&p.mat, &vm[k].w, 4);
-        p.solid_id = sid[k];
-        p._pad0 = 0;
-        p.pos[0] = pd[k].x; p.pos[1] = pd[k].y; p.pos[2] = pd[k].z; p.pos[3] = sim->pos_w;
-        p.vel[0] = vm[k].x; p.vel[1] = vm[k].y; p.vel[2] = vm[k].z; p.vel[3] = 0.0f;
-    }
-    return ARP_OK;
+    const uint32_t n = sim->n;
+    if (!sim->records.p) CUDA_TRY(sim->records.alloc(n));
+    sim->launches += soa_to_records(sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, n, sim->pos_w, sim->records.p,
+                                    sim->stream);
+    if (n) CUDA_TRY(cudaMemcpyAsync(out, sim->records.p, n * sizeof(arp_particle), cudaMemcpyDeviceToHost, sim->stream));
+    CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    return check_launch("get_particles");
 }
 
 arp_status arp_sim_get_solids(arp_sim* sim, arp_solid_particle* out, uint32_t cap) {
@@ -982,30 +944,21 @@ arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t 
     ARP_TRY(need_init(sim));
     if (!in && n) return fail(ARP_ERR_INVALID_ARG, "null argument");
     if (n != sim->n) return fail(ARP_ERR_INVALID_ARG, "particle count differs from the handle's");
-    CUDA_TRY(sim->stage.ensure(n));
-    float4* pd = sim->stage.pd;
-    float4* vm = sim->stage.vm;
-    uint32_t* orig = sim->stage.orig;
-    uint32_t* sid = sim->stage.sid;
-    for (uint32_t i = 0; i < n; ++i) {
-        const arp_particle& p = in[i];
-        if (p.mat != sim->host_particles[i].mat) return fail(ARP_ERR_INVALID_ARG, "material of a particle changed");
-        if (p.pos[3] != sim->pos_w || p.vel[3] != 0.0f)
-            return fail(ARP_ERR_UNSUPPORTED, "w components must keep their values");
-        pd[i] = make_float4(p.pos[0], p.pos[1], p.pos[2], p.den);
-        float mf;
-        std::memcpy(&mf, &p.mat, 4);
-        vm[i] = make_float4(p.vel[0], p.vel[1], p.vel[2], mf);
-        orig[i] = i;
-        sid[i] = sim->sid_of_caller[i];
-    }
     cudaStream_t st = sim->stream;
     if (n) {
-        CUDA_TRY(cudaMemcpyAsync(sim->Y.pd.p, pd, n * sizeof(float4), cudaMemcpyHostToDevice, st));
-        CUDA_TRY(cudaMemcpyAsync(sim->Y.vm.p, vm, n * sizeof(float4), cudaMemcpyHostToDevice, st));
-        CUDA_TRY(cudaMemcpyAsync(sim->orig.p, orig, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
-        CUDA_TRY(cudaMemcpyAsync(sim->sid.p, sid, n * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
+        if (!sim->records.p) CUDA_TRY(sim->records.alloc(n));
+        CUDA_TRY(cudaMemcpyAsync(sim->records.p, in, n * sizeof(arp_particle), cudaMemcpyHostToDevice, st));
+        uint32_t flag = 0;
+        CUDA_TRY(cudaMemsetAsync(sim->check_flag.p, 0, sizeof(uint32_t), st));
+        sim->launches += check_records(sim->records.p, n, sim->mat_of_caller_d.p, sim->pos_w, sim->check_flag.p, st);
+        CUDA_TRY(cudaMemcpyAsync(&flag, sim->check_flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
+        if (flag & 1u) return fail(ARP_ERR_INVALID_ARG, "material of a particle changed");
+        if (flag & 2u) return fail(ARP_ERR_UNSUPPORTED, "w components must keep their values");
+        sim->launches += records_to_soa(sim->records.p, n, sim->sid_of_caller_d.p, sim->Y.pd.p, sim->Y.vm.p,
+                                        sim->orig.p, sim->sid.p, st);
+        CUDA_TRY(cudaStreamSynchronize(st));
+        ARP_TRY(check_launch("set_particles"));
     }
     return ARP_OK;
 }

@@ -149,3 +149,22 @@ def test_profile_and_launch_counters():
     assert sim.launch_count() - before == prof["launches"]
     st = sim.stats()
     assert st["nonfinite_positions"] == 0 and st["max_cell_occupancy"] > 0
+
+
+def test_state_round_trip_and_validation():
+    sc = small_3d()
+    sim = make(sc)
+    sim.step(2)
+    p = sim.particles()
+    sim.set_particles(p)
+    q = sim.particles()
+    assert p.tobytes() == q.tobytes()
+    bad = p.copy()
+    bad["mat"][5] = (bad["mat"][5] + 1) % len(sc.materials)
+    with pytest.raises(Exception) as e:
+        sim.set_particles(bad)
+    assert "material" in str(e.value)
+    bad = p.copy()
+    bad["pos"][3, 3] = 1.0
+    with pytest.raises(Exception):
+        sim.set_particles(bad)
