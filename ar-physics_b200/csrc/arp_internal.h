@@ -222,6 +222,7 @@ struct SolidArgs {
     const uint32_t* sid_sorted;
     const DevMat* mats;
     uint32_t ns;
+    int all_order2;           // every solid material has strain_order 2
 };
 int launch_solid(const SolidArgs& a, const Params& P, const StageCoefs& c, cudaStream_t st);
 

@@ -158,6 +158,7 @@ struct arp_sim {
     float time = 0;
     bool initialized = false;
     bool any_stiff_immobile = false;
+    bool all_order2 = true;  // every stiff material uses strain order 2
     Params P{};
 
     std::vector<arp_particle> host_particles;  // caller order (initial state)
@@ -540,6 +541,7 @@ arp_status do_step(arp_sim* S) {
             a.sid_sorted = sid_sorted;
             a.mats = S->d_mats.p;
             a.ns = ns;
+            a.all_order2 = S->all_order2 ? 1 : 0;
             sl = launch_solid(a, S->P, c, st);
             S->launches += sl;
             cur_ep = a.ep_next;
@@ -663,8 +665,10 @@ arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
             S->inter[size_t(i) * M + j] = x;
             S->inter[size_t(j) * M + i] = x;
         }
-    for (const auto& m : S->mats)
+    for (const auto& m : S->mats) {
         if (m.immobile && is_stiff(m)) S->any_stiff_immobile = true;
+        if (is_stiff(m) && m.strain_order != 2) S->all_order2 = false;
+    }
     S->bounds = sc->bounds;
     S->dim = 0;
     for (int a = 0; a < 4; ++a)

@@ -151,9 +151,11 @@ __device__ inline M4 mat_sqrt_db(const M4& Xm) {  // Denman-Beavers, solid.rs:11
     }
     return Y;
 }
+template <bool ORDER2>
 __device__ inline M4 seth_hill(const M4& F, int two_m, uint32_t dim) {  // solid.rs:147-168
     M4 C = m4_mul(m4_transpose(F), F);
     pad_unit(C, dim);
+    if (ORDER2) return m4_scale(1.0f / 2.0f, m4_sub(m4_mul(m4_ident(), C), m4_ident()));
     if (two_m == 0) return m4_scale(0.5f, mat_log5(C));
     const int a = two_m < 0 ? -two_m : two_m;
     const int m = a >> 1;
@@ -163,9 +165,11 @@ __device__ inline M4 seth_hill(const M4& F, int two_m, uint32_t dim) {  // solid
     if (two_m < 0) Cm = m4_inverse(Cm);
     return m4_scale(1.0f / (float)two_m, m4_sub(Cm, m4_ident()));
 }
+template <bool ORDER2>
 __device__ inline M4 seth_hill_rate(const M4& F, const M4& Fd, int two_m, uint32_t dim) {  // solid.rs:170-204
     M4 dC = m4_mul(m4_transpose(Fd), F);
     dC = m4_add(dC, m4_transpose(dC));
+    if (ORDER2) return m4_scale(1.0f / 2.0f, m4_mul(m4_ident(), dC));
     M4 C = m4_mul(m4_transpose(F), F);
     pad_unit(C, dim);
     if (two_m == 0) return m4_mul(m4_scale(0.5f, dC), m4_inverse(C));
@@ -197,6 +201,9 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
     return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
 }
 
+// ORDER2: every solid material uses strain order 2 (Green-Lagrange), so the
+// log-series, square-root and inverse paths are compiled out.
+template <bool ORDER2>
 __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P, StageCoefs c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ns) return;
@@ -208,6 +215,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P
     // strain.rs:139-160: F = sum V dx (x) (L gradW), Fdot likewise with dv
     float F[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     float Fd[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
+#pragma unroll 4
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMat;
         const float4 g = a.rl.gw[k];
@@ -277,8 +285,8 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P
         }
     }
     // solid.rs:334-341
-    const M4 strain = m4_add(seth_hill(Fm, mm.strain_order, P.dim), EP);
-    const M4 rate = seth_hill_rate(Fm, Fdm, mm.strain_order, P.dim);
+    const M4 strain = m4_add(seth_hill<ORDER2>(Fm, mm.strain_order, P.dim), EP);
+    const M4 rate = seth_hill_rate<ORDER2>(Fm, Fdm, mm.strain_order, P.dim);
     const M4 pk2 = m4_add(hooke(strain, mm.lam, mm.mu, P.dim), hooke(rate, mm.lam_d, mm.mu_d, P.dim));
     const M4 sigma = m4_mul(Fm, m4_transpose(pk2));
     const M4 A = m4_mul(sigma, Lm);
@@ -359,6 +367,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
     // (solid.rs:343-374) and, when the neighbor also sits in the current
     // 3x3x3 cells, hourglass control (solid.rs:430-443; kernel(dX) is
     // non-zero exactly for these pairs).
+#pragma unroll 2
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMat)) continue;
@@ -459,7 +468,10 @@ int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const
 int launch_solid(const SolidArgs& a, const Params& P, const StageCoefs& c, cudaStream_t st) {
     if (a.ns == 0) return 0;
     cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
-    k_solid_stress<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P, c);
+    if (a.all_order2)
+        k_solid_stress<true><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P, c);
+    else
+        k_solid_stress<false><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P, c);
     k_solid_forces<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P);
     return 2;
 }
