@@ -238,7 +238,6 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
                     }
                 }
                 const uint32_t jb = a.start[c0], je = a.start[c1];
-#pragma unroll 4
                 for (uint32_t j = jb; j < je; ++j) {
                     if (j != k && hit(a.xs[j])) {  // the particle itself contributes exactly zero
                         if (cnt < kListCap) my[cnt++ * kFluidThreads] = j;
@@ -248,7 +247,6 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
             }
         }
         // pass 2: pair math over the collected hits
-#pragma unroll 2
         for (uint32_t e = 0; e < cnt; ++e) {
             const uint32_t j = my[e * kFluidThreads];
             if (j & kBoundaryBit) boundary_pair(j & ~kBoundaryBit);

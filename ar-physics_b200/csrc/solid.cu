@@ -215,7 +215,6 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P
     // strain.rs:139-160: F = sum V dx (x) (L gradW), Fdot likewise with dv
     float F[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     float Fd[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-#pragma unroll 4
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMat;
         const float4 g = a.rl.gw[k];
@@ -367,7 +366,6 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
     // (solid.rs:343-374) and, when the neighbor also sits in the current
     // 3x3x3 cells, hourglass control (solid.rs:430-443; kernel(dX) is
     // non-zero exactly for these pairs).
-#pragma unroll 2
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMat)) continue;
