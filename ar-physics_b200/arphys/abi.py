@@ -173,6 +173,9 @@ def load_library():
         "arp_sim_stats": [c_sim, ctypes.POINTER(ArpStats)],
         "arp_sim_launch_count": [c_sim, ctypes.POINTER(ctypes.c_uint64)],
     }
+    sig["arp_sim_create_batch"] = [ctypes.POINTER(ArpScene), ctypes.c_uint32, ctypes.POINTER(c_sim)]
+    sig["arp_sim_num_scenes"] = [c_sim, u32p]
+    sig["arp_sim_scene_range"] = [c_sim, ctypes.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p]
     sig["arp_grid_build_noalloc"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ArpAABB), ctypes.c_float,
                                      ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
     for name, args in sig.items():

@@ -29,6 +29,32 @@ class FluidSim:
         return cls(scene)
 
     @classmethod
+    def batch(cls, scenes):
+        """Several independent scenes stepped together (arp_sim_create_batch)."""
+        from .abi import ArpScene
+        L = load_library()
+        structs, keep = [], []
+        for sc in scenes:
+            st, k = scene_struct(sc)
+            structs.append(st)
+            keep.append(k)
+        arr = (ArpScene * len(structs))(*structs)
+        h = ctypes.c_void_p()
+        check(L.arp_sim_create_batch(arr, len(structs), ctypes.byref(h)))
+        return cls(_handle=h)
+
+    def num_scenes(self):
+        t = ctypes.c_uint32()
+        check(self._L.arp_sim_num_scenes(self._h, ctypes.byref(t)))
+        return t.value
+
+    def scene_range(self, k):
+        """(first_particle, n_particles, first_boundary, n_boundary, first_cell, n_cells) of scene k."""
+        v = [ctypes.c_uint32() for _ in range(6)]
+        check(self._L.arp_sim_scene_range(self._h, int(k), *[ctypes.byref(x) for x in v]))
+        return tuple(x.value for x in v)
+
+    @classmethod
     def from_toml(cls, path):
         L = load_library()
         h = ctypes.c_void_p()
@@ -107,10 +133,13 @@ class FluidSim:
         return out
 
     def interactions(self):
+        """The n_materials^2 interaction block of a single scene (all blocks,
+        flat, for a batch)."""
         m = self.num_materials()
-        out = np.zeros(m * m, dtype=INTERACTION_DTYPE)
+        cap = max(m * m, 1) if self.num_scenes() == 1 else 32 * 32 * self.num_scenes()
+        out = np.zeros(cap, dtype=INTERACTION_DTYPE)
         check(self._L.arp_sim_get_interactions(self._h, ptr(out), len(out)))
-        return out.reshape(m, m)
+        return out.reshape(m, m) if self.num_scenes() == 1 else out
 
     def set_particles(self, p):
         p = np.ascontiguousarray(p, dtype=PARTICLE_DTYPE)

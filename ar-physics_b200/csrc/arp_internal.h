@@ -24,9 +24,9 @@ namespace arp {
 
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kBucketSlots = 128;  // neighbor_list.rs:45
-constexpr int kMaxMaterials = 32;
+constexpr int kMaxMaterials = 32;  // per scene
 
-// Uniform grid of NeighborList::new (neighbor_list.rs:199-217).
+// Uniform grid of NeighborList::new (neighbor_list.rs:199-217), one scene.
 struct Grid {
     float min[3];
     float dim[3];
@@ -34,7 +34,8 @@ struct Grid {
     uint32_t ncells;
 };
 
-// Per-material constants the kernels read (a subset of `Material`).
+// Per-material constants the kernels read (a subset of `Material`), in one
+// table over all scenes of a batch.
 struct DevMat {
     float mass, start_den, sound_speed, target_den;
     float visc, bulk_visc, lam, mu;
@@ -42,6 +43,8 @@ struct DevMat {
     float work_hardening_exp, kinematic_hardening, relaxation_time, vol0;  // vol0 = mass / start_den
     uint32_t state_eq, stiff, plastic;
     int32_t strain_order;
+    uint32_t scene;   // scene the material belongs to
+    uint32_t local;   // index inside that scene's material list
 };
 
 struct DevInter {
@@ -49,16 +52,37 @@ struct DevInter {
     float strength, radius, dampening, friction;
 };
 
-// Scalars shared by the force kernels.  Products are rounded exactly as the
-// shaders group them (e.g. EPSILON*h*h = (0.1*h)*h).
-struct Params {
+// Scalars of one scene.  Products are rounded exactly as the shaders group
+// them (e.g. EPSILON*h*h = (0.1*h)*h).  A single simulation is a batch of one
+// scene; the cells of scene k are global cells cell_base .. cell_base+ncells.
+struct SceneP {
     Grid grid;
-    uint32_t dim, nmat;
+    uint32_t cell_base;
+    uint32_t dim;                     // the reference's count of non-zero box axes
+    uint32_t mat_base, nmat;          // global material range of the scene
+    uint32_t inter_base;              // first entry of its nmat x nmat interaction block
     float h, h2, kconst, g;
-    float eps_hh;   // (0.1f * h) * h
-    float eps_h;    // 0.1f * h
-    float hg_h;     // (10 * 0.1f) * h
-    float rcut, rcut2, r_geom;  // 8h, (8h)^2, h*h/(8h)
+    float eps_hh;                     // (0.1f * h) * h
+    float eps_h;                      // 0.1f * h
+    float hg_h;                       // (10 * 0.1f) * h
+    float rcut, rcut2, r_geom;        // 8h, (8h)^2, h*h/(8h)
+    float contact_slack;              // r_cut - largest in-stencil |dx|, 0 when unbounded
+};
+
+// The fields of a material the fluid pair loop reads (32 B).
+struct FluidMat {
+    float mass, c, d0, visc, bulk;
+    uint32_t eos, stiff, pad;
+};
+
+// Kernel-wide view of the batch tables.
+struct Tables {
+    const SceneP* scenes;
+    const DevMat* mats;
+    const FluidMat* fmats;
+    const DevInter* inter;
+    uint32_t ncells;                  // total cells of all scenes (the non-finite bucket follows)
+    uint32_t max_nmat;                // largest per-scene material count
 };
 
 // Health counters written by device code.
@@ -118,8 +142,10 @@ struct GridBuffers {
 // Build cell_start / perm for `n` positions.  Counting sort: keys and
 // histogram, exclusive scan, scatter, then ascending slot order within each
 // cell.  Returns the number of kernel launches issued.
-int build_grid(const float4* pos, uint32_t n, const Grid& grid, GridBuffers& gb, DevStats* stats,
-               const uint32_t* boundary_start, cudaStream_t st);
+// The scene of item i is mats[material].scene, the material read from
+// vm[i].w (bits) when vm is given, else from mat_u32[i].
+int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uint32_t n, const Tables& T,
+               GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st);
 
 // Exclusive scan of `len` counts into out (len entries); clears `count`.
 int exclusive_scan(uint32_t* count, uint32_t len, uint32_t* out, uint32_t* block_sums, cudaStream_t st);
@@ -139,21 +165,23 @@ int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* 
 
 // Particle records (caller order) to structure of arrays in caller order, and
 // back from cell order into caller order (the state exchange of the C ABI).
-int records_to_soa(const arp_particle* in, uint32_t n, const uint32_t* sid_of, float4* pd, float4* vm, uint32_t* orig,
-                   uint32_t* sid, cudaStream_t st);
+// Records carry each scene's own material index; the device state carries the
+// batch-wide one (mat_of[i] for caller id i; mats[].local maps back).
+int records_to_soa(const arp_particle* in, uint32_t n, const uint32_t* sid_of, const uint32_t* mat_of, float4* pd,
+                   float4* vm, uint32_t* orig, uint32_t* sid, cudaStream_t st);
 int soa_to_records(const float4* pd, const float4* vm, const uint32_t* orig, const uint32_t* sid, uint32_t n,
-                   float pos_w, arp_particle* out, cudaStream_t st);
-// Sets flag bit 0 when a record's material differs from mat_of, bit 1 when a
-// w component differs from pos_w / zero.
-int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, float pos_w, uint32_t* flag,
-                  cudaStream_t st);
+                   float pos_w, const DevMat* mats, arp_particle* out, cudaStream_t st);
+// Sets flag bit 0 when a record's material differs from the handle's, bit 1
+// when a w component differs from pos_w / zero.
+int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, const DevMat* mats, float pos_w,
+                  uint32_t* flag, cudaStream_t st);
 
 // slot_of[sid[k]] = k for solid slots.
 int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st);
 // Neighbor counts within h of each sorted particle (mobile + boundary),
 // computed with separately rounded float products for bit-exact output.
-int count_neighbors(const float4* xs, const uint32_t* start, uint32_t n, const float4* bxs,
-                    const uint32_t* bstart, const Params& P, uint32_t* out_sorted, cudaStream_t st);
+int count_neighbors(const float4* xs, const float4* vs, const uint32_t* start, uint32_t n, const float4* bxs,
+                    const uint32_t* bstart, const Tables& T, uint32_t* out_sorted, cudaStream_t st);
 
 // ---- fluid forces + stage update (fluid.cu) ---------------------------------
 struct FluidArgs {
@@ -165,19 +193,17 @@ struct FluidArgs {
     const uint32_t* bstart;  // boundary cell start
     const uint32_t* perm;    // sorted -> storage slot (nullptr = identity)
     const uint32_t* sid;     // storage-order solid id
-    const uint32_t* sid_of_boundary_index;  // solid id of mobile particle with caller id == boundary caller id
+    const uint32_t* sid_of_boundary_index;  // per boundary caller id: solid id of the scene's mobile particle
+                                            // with the same in-scene index, or invalid
     const uint32_t* borig;   // boundary caller ids, sorted
     const float* ps;         // p / rho^2 of each sorted particle
     const float* bps;        // p / rho^2 of each sorted boundary particle
     const float4* ksol;      // per-solid solid-term acceleration (nullptr when the solid branch is off)
-    const DevMat* mats;
-    const DevInter* inter;
     uint32_t n;
-    uint32_t n_mobile_total;  // particle count for the Q2 range check
     int solid_branch;
     int any_stiff_immobile;
 };
-int launch_fluid(const FluidArgs& a, const Params& P, const StageCoefs& c, const StageBuffers& b,
+int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
                  cudaStream_t st);
 
 // ---- solids (solid.cu) ------------------------------------------------------
@@ -190,10 +216,10 @@ struct SolidRefList {
 // Reference-neighbor lists: counts per solid (pass 1), then after an
 // exclusive scan of the counts into rl.off, the entries and L (pass 2).
 // `gb` holds a grid built over the reference positions.
-int ref_lists_count(const float4* ref, uint32_t ns, const GridBuffers& gb, const Params& P, uint32_t* count,
-                    cudaStream_t st);
+int ref_lists_count(const float4* ref, const uint32_t* mat_of_solid, uint32_t ns, const GridBuffers& gb,
+                    const Tables& T, uint32_t* count, cudaStream_t st);
 int ref_lists_fill(const float4* ref, const uint32_t* mat_of_solid, uint32_t ns, const GridBuffers& gb,
-                   const Params& P, const DevMat* mats, SolidRefList& rl, float4* L, cudaStream_t st);
+                   const Tables& T, SolidRefList& rl, float4* L, cudaStream_t st);
 
 struct SolidArgs {
     const float4* pd;         // stage state, storage order
@@ -215,15 +241,13 @@ struct SolidArgs {
     float4* ksol;             // [ns] solid-term acceleration
     const uint2* coord;       // storage-order packed cell coordinates of the stage grid
     uint32_t* contact_bound;  // [2] max |u_i - u_0| bits, outside-box flag (cleared per stage)
-    float contact_slack;      // r_cut - (largest in-stencil |dx|), 0 when no bound applies
     const float4* xs;         // sorted stage positions (current-neighbor loop)
     const float4* vs;
     const uint32_t* start;
     const uint32_t* sid_sorted;
-    const DevMat* mats;
     uint32_t ns;
     int all_order2;           // every solid material has strain_order 2
 };
-int launch_solid(const SolidArgs& a, const Params& P, const StageCoefs& c, cudaStream_t st);
+int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st);
 
 }  // namespace arp

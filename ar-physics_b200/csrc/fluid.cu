@@ -26,11 +26,6 @@ namespace arp {
 
 namespace {
 
-struct FluidMat {
-    float mass, c, d0, visc, bulk;
-    uint32_t eos, stiff, pad;
-};
-
 __device__ __forceinline__ float pow7(float x) {
     const float x2 = x * x;
     const float x3 = x2 * x;
@@ -58,8 +53,14 @@ __device__ __forceinline__ float contact_potential(uint32_t eq, float r, float s
 struct Self {
     float3 x, v;
     float d1, m1, pterm1, f1, bf1;
-    uint32_t mat;
+    uint32_t mat;     // global material id
+    uint32_t li;      // index inside its scene's material list
     bool elastic;
+    // material and interaction tables of the particle's scene: shared-memory
+    // copies for the block's first scene, global tables otherwise
+    const FluidMat* mt;
+    const DevInter* it;
+    uint32_t mbase, nm;
 };
 
 struct Acc {
@@ -69,10 +70,14 @@ struct Acc {
 
 // One neighbor pair inside the kernel radius (the caller has tested it).
 // `ptj` is p_j / rho_j^2 of the neighbor, precomputed per particle.
+// The scene scalars the pair terms read, held in registers.
+struct PairK {
+    float h2, kconst, eps_hh;
+};
+
 template <int DIM, bool BOUNDARY>
 __device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, float ptj, uint32_t mat2, bool elastic2,
-                                     const FluidMat* __restrict__ sm, const DevInter* __restrict__ si,
-                                     uint32_t nmat, const Params& P, Acc& acc) {
+                                     const PairK& P, Acc& acc) {
     const float rx = xj.x - s.x.x, ry = xj.y - s.x.y, rz = DIM == 3 ? xj.z - s.x.z : 0.0f;
     const float r2 = DIM == 3 ? (rx * rx + ry * ry) + rz * rz : rx * rx + ry * ry;
     const float diff = fmaxf(P.h2 - r2, 0.0f);
@@ -80,14 +85,15 @@ __device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, float 
     const float gx = gws * rx, gy = gws * ry, gz = gws * rz;
     const float vx = vj.x - s.v.x, vy = vj.y - s.v.y, vz = DIM == 3 ? vj.z - s.v.z : 0.0f;
     const float d2 = xj.w;
-    const FluidMat m2 = sm[mat2];
+    const uint32_t lj = mat2 - s.mbase;
+    const FluidMat m2 = s.mt[lj];
     const float vgw = DIM == 3 ? (vx * gx + vy * gy) + vz * gz : vx * gx + vy * gy;
     if (!BOUNDARY) acc.den += m2.mass * vgw;
     const float pf = s.m1 * m2.mass * (s.pterm1 + ptj);
     acc.f.x += pf * gx;
     acc.f.y += pf * gy;
     acc.f.z += pf * gz;
-    const DevInter it = si[s.mat * nmat + mat2];
+    const DevInter it = s.it[s.li * s.nm + lj];
     if (it.potential != ARP_CONTACT_ZERO) {
         const float cp = contact_potential(it.potential, sqrtf(r2), it.radius, it.strength);
         if (cp != 0.0f) {
@@ -159,16 +165,17 @@ constexpr int kListCap = 48;                  // hits held per thread before the
 constexpr uint32_t kBoundaryBit = 0x80000000u;
 
 template <int DIM>
-__global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, StageCoefs c, StageBuffers b) {
+__global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);  // [kListCap][blockDim]
     FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * kFluidThreads);
-    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * P.nmat);
-    for (uint32_t i = threadIdx.x; i < P.nmat; i += blockDim.x) {
-        const DevMat m = a.mats[i];
-        sm[i] = FluidMat{m.mass, m.sound_speed, m.target_den, m.visc, m.bulk_visc, m.state_eq, m.stiff, 0u};
-    }
-    for (uint32_t i = threadIdx.x; i < P.nmat * P.nmat; i += blockDim.x) si[i] = a.inter[i];
+    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
+    // materials and interactions of the scene of the block's first particle
+    const uint32_t k_first = min(blockIdx.x * blockDim.x, a.n - 1u);
+    const uint32_t scene0 = T.mats[__float_as_uint(a.vs[k_first].w)].scene;
+    const SceneP& sp0 = T.scenes[scene0];
+    for (uint32_t i = threadIdx.x; i < sp0.nmat; i += blockDim.x) sm[i] = T.fmats[sp0.mat_base + i];
+    for (uint32_t i = threadIdx.x; i < sp0.nmat * sp0.nmat; i += blockDim.x) si[i] = T.inter[sp0.inter_base + i];
     __syncthreads();
 
     const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
@@ -181,8 +188,17 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
     s.x = make_float3(xi.x, xi.y, xi.z);
     s.v = make_float3(vi.x, vi.y, vi.z);
     s.mat = __float_as_uint(vi.w);
+    const uint32_t scene = T.mats[s.mat].scene;
+    const SceneP& P = T.scenes[scene];
+    const PairK K{P.h2, P.kconst, P.eps_hh};
+    const float g_acc = P.g;
+    s.mbase = P.mat_base;
+    s.nm = P.nmat;
+    s.li = s.mat - P.mat_base;
+    s.mt = scene == scene0 ? sm : T.fmats + P.mat_base;
+    s.it = scene == scene0 ? si : T.inter + P.inter_base;
     s.d1 = xi.w;
-    const FluidMat m1 = sm[s.mat];
+    const FluidMat m1 = s.mt[s.li];
     s.m1 = m1.mass;
     s.f1 = m1.visc;
     s.bf1 = m1.bulk;
@@ -199,18 +215,17 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
         const float4 vj = a.bvs[jb];
         const uint32_t mat2 = __float_as_uint(vj.w);
         bool elastic2 = false;
-        if (a.any_stiff_immobile && sm[mat2].stiff) {
+        if (a.any_stiff_immobile && s.mt[mat2 - s.mbase].stiff) {
             // fluid.rs:227: the boundary index reads the mobile array's solid id
-            const uint32_t bi = a.borig[jb];
-            elastic2 = bi < a.n_mobile_total && a.sid_of_boundary_index[bi] != kInvalid;
+            elastic2 = a.sid_of_boundary_index[a.borig[jb]] != kInvalid;
         }
-        pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, sm, si, P.nmat, P, acc);
+        pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, K, acc);
     };
     auto mobile_pair = [&](uint32_t j) {
         const float4 xj = a.xs[j];
         const float4 vj = a.vs[j];
         const uint32_t mat2 = __float_as_uint(vj.w);
-        pair<DIM, false>(s, xj, vj, a.ps[j], mat2, sm[mat2].stiff != 0u, sm, si, P.nmat, P, acc);
+        pair<DIM, false>(s, xj, vj, a.ps[j], mat2, s.mt[mat2 - s.mbase].stiff != 0u, K, acc);
     };
     // pass 1: candidates of the 3x3(x3) cells whose squared distance is
     // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0)) go to
@@ -218,17 +233,18 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
     auto hit = [&](float4 q) {
         const float rx = q.x - xi.x, ry = q.y - xi.y;
         const float r2 = DIM == 3 ? (rx * rx + ry * ry) + (q.z - xi.z) * (q.z - xi.z) : rx * rx + ry * ry;
-        return P.h2 - r2 > 0.0f;
+        return K.h2 - r2 > 0.0f;
     };
     if (finite3(xi)) {
-        const Grid& g = P.grid;
+        const Grid g = P.grid;
+        const uint32_t cell_base = P.cell_base;
         const CellCoord cc = cell_coord(xi, g);
         const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
         const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
         const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
         for (int z = zlo; z <= zhi; ++z) {
             for (int y = ylo; y <= yhi; ++y) {
-                const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t row = cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
                 const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
                 const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
                 for (uint32_t j = bb; j < be; ++j) {
@@ -256,7 +272,7 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
 
     // derivative record (fluid.rs:329-333), plus the solid term when active
     float4 kpd = make_float4(vi.x, vi.y, vi.z, acc.den);
-    float4 kvm = make_float4(__fdiv_rn(acc.f.x, s.d1), __fadd_rn(__fdiv_rn(acc.f.y, s.d1), -P.g),
+    float4 kvm = make_float4(__fdiv_rn(acc.f.x, s.d1), __fadd_rn(__fdiv_rn(acc.f.y, s.d1), -g_acc),
                              __fdiv_rn(acc.f.z, s.d1), 0.0f);
     if (a.solid_branch && sid != kInvalid) {
         const float4 ks = a.ksol[sid];
@@ -319,16 +335,17 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Params P, 
 
 }  // namespace
 
-int launch_fluid(const FluidArgs& a, const Params& P, const StageCoefs& c, const StageBuffers& b, cudaStream_t st) {
+int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
+                 cudaStream_t st) {
     if (a.n == 0) return 0;
     const int threads = kFluidThreads;
     const uint32_t blocks = (a.n + threads - 1) / threads;
-    const size_t smem = sizeof(uint32_t) * kListCap * kFluidThreads + sizeof(FluidMat) * P.nmat +
-                        sizeof(DevInter) * P.nmat * P.nmat;
-    if (P.dim == 3)
-        k_fluid<3><<<blocks, threads, smem, st>>>(a, P, c, b);
+    const size_t smem = sizeof(uint32_t) * kListCap * kFluidThreads + sizeof(FluidMat) * T.max_nmat +
+                        sizeof(DevInter) * T.max_nmat * T.max_nmat;
+    if (kdim == 3)
+        k_fluid<3><<<blocks, threads, smem, st>>>(a, T, c, b);
     else
-        k_fluid<2><<<blocks, threads, smem, st>>>(a, P, c, b);
+        k_fluid<2><<<blocks, threads, smem, st>>>(a, T, c, b);
     return 1;
 }
 

@@ -31,7 +31,13 @@ constexpr int kScanThreads = 1024;
 constexpr int kScanItems = 4;  // per thread
 constexpr int kScanTile = kScanThreads * kScanItems;
 
-__global__ void k_cell_keys(const float4* __restrict__ pos, uint32_t n, Grid grid, uint32_t* __restrict__ key,
+__device__ __forceinline__ uint32_t scene_of(const float4* vm, const uint32_t* mat_u32, uint32_t i, const Tables& T) {
+    const uint32_t m = vm ? __float_as_uint(vm[i].w) : (mat_u32 ? mat_u32[i] : 0u);
+    return T.mats[m].scene;
+}
+
+__global__ void k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vm,
+                            const uint32_t* __restrict__ mat_u32, uint32_t n, Tables T, uint32_t* __restrict__ key,
                             uint32_t* __restrict__ rank, uint32_t* __restrict__ count, uint2* __restrict__ coord,
                             DevStats* stats) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
@@ -39,12 +45,14 @@ __global__ void k_cell_keys(const float4* __restrict__ pos, uint32_t n, Grid gri
     float4 p = pos[i];
     uint32_t k;
     if (!finite3(p)) {
-        k = grid.ncells;
+        k = T.ncells;
         if (coord) coord[i] = make_uint2(0xFFFFFFFFu, 0xFFFFFFFFu);
         if (stats) atomicAdd(&stats->nonfinite_positions, 1u);
     } else {
+        const SceneP& sp = T.scenes[scene_of(vm, mat_u32, i, T)];
+        const Grid& grid = sp.grid;
         const CellCoord cc = cell_coord(p, grid);
-        k = cell_id(cc, grid);
+        k = sp.cell_base + cell_id(cc, grid);
         if (coord) coord[i] = make_uint2((uint32_t)cc.x | ((uint32_t)cc.y << 16), (uint32_t)cc.z);
         if (stats) {
             // a coordinate on the upper face would hash one past the last cell
@@ -224,14 +232,14 @@ __global__ void k_gather_state(const uint32_t* __restrict__ perm, uint32_t n, co
 
 // Particle records (48 B, caller order) -> structure of arrays in caller order.
 __global__ void k_records_to_soa(const arp_particle* __restrict__ in, uint32_t n, const uint32_t* __restrict__ sid_of,
-                                 float4* __restrict__ pd, float4* __restrict__ vm, uint32_t* __restrict__ orig,
-                                 uint32_t* __restrict__ sid) {
+                                 const uint32_t* __restrict__ mat_of, float4* __restrict__ pd, float4* __restrict__ vm,
+                                 uint32_t* __restrict__ orig, uint32_t* __restrict__ sid) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const float4* r = reinterpret_cast<const float4*>(in + i);
     const float4 h = r[0], p = r[1], v = r[2];  // (den, mat, solid_id, pad), pos, vel
     pd[i] = make_float4(p.x, p.y, p.z, h.x);
-    vm[i] = make_float4(v.x, v.y, v.z, h.y);  // material id bits
+    vm[i] = make_float4(v.x, v.y, v.z, __uint_as_float(mat_of[i]));  // batch-wide material id
     orig[i] = i;
     sid[i] = sid_of[i];
 }
@@ -239,11 +247,11 @@ __global__ void k_records_to_soa(const arp_particle* __restrict__ in, uint32_t n
 // Bit 0: a record's material differs from the handle's; bit 1: a w component
 // differs from the handle's common w / zero.
 __global__ void k_check_records(const arp_particle* __restrict__ in, uint32_t n, const uint32_t* __restrict__ mat_of,
-                                float pos_w, uint32_t* __restrict__ flag) {
+                                const DevMat* __restrict__ mats, float pos_w, uint32_t* __restrict__ flag) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= n) return;
     const arp_particle& r = in[i];
-    uint32_t bad = (r.mat != mat_of[i]) ? 1u : 0u;
+    uint32_t bad = (r.mat != mats[mat_of[i]].local) ? 1u : 0u;
     if (r.pos[3] != pos_w || r.vel[3] != 0.0f) bad |= 2u;
     if (bad) atomicOr(flag, bad);
 }
@@ -251,12 +259,13 @@ __global__ void k_check_records(const arp_particle* __restrict__ in, uint32_t n,
 // Cell-ordered structure of arrays -> particle records in caller order.
 __global__ void k_soa_to_records(const float4* __restrict__ pd, const float4* __restrict__ vm,
                                  const uint32_t* __restrict__ orig, const uint32_t* __restrict__ sid, uint32_t n,
-                                 float pos_w, arp_particle* __restrict__ out) {
+                                 float pos_w, const DevMat* __restrict__ mats, arp_particle* __restrict__ out) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 p = pd[k], v = vm[k];
     float4* r = reinterpret_cast<float4*>(out + orig[k]);
-    r[0] = make_float4(p.w, v.w, __uint_as_float(sid[k]), 0.0f);
+    const uint32_t local = mats[__float_as_uint(v.w)].local;  // the scene's own material index
+    r[0] = make_float4(p.w, __uint_as_float(local), __uint_as_float(sid[k]), 0.0f);
     r[1] = make_float4(p.x, p.y, p.z, pos_w);
     r[2] = make_float4(v.x, v.y, v.z, 0.0f);
 }
@@ -274,14 +283,15 @@ __device__ __forceinline__ bool within_h_exact(float4 q, float4 p, float h2) {
     return __fsub_rn(h2, d) > 0.0f;
 }
 
-__global__ void k_count_neighbors(const float4* __restrict__ xs, const uint32_t* __restrict__ start, uint32_t n,
-                                  const float4* __restrict__ bxs, const uint32_t* __restrict__ bstart, Params P,
-                                  uint32_t* __restrict__ out) {
+__global__ void k_count_neighbors(const float4* __restrict__ xs, const float4* __restrict__ vs,
+                                  const uint32_t* __restrict__ start, uint32_t n, const float4* __restrict__ bxs,
+                                  const uint32_t* __restrict__ bstart, Tables T, uint32_t* __restrict__ out) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const float4 p = xs[k];
     uint32_t cnt = 0;
     if (finite3(p)) {
+        const SceneP& P = T.scenes[scene_of(vs, nullptr, k, T)];
         const Grid& g = P.grid;
         const CellCoord c = cell_coord(p, g);
         const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, (int)g.sub[0] - 1);
@@ -291,7 +301,7 @@ __global__ void k_count_neighbors(const float4* __restrict__ xs, const uint32_t*
             for (int dy = -1; dy <= 1; ++dy) {
                 const int y = c.y + dy;
                 if (y < 0 || y >= (int)g.sub[1]) continue;
-                const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
                 const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
                 if (bstart)
                     for (uint32_t j = bstart[c0]; j < bstart[c1]; ++j) cnt += within_h_exact(bxs[j], p, P.h2);
@@ -357,22 +367,22 @@ cudaError_t noalloc_scratch(uint32_t** out) {
 
 }  // namespace
 
-int build_grid(const float4* pos, uint32_t n, const Grid& grid, GridBuffers& gb, DevStats* stats,
-               const uint32_t* boundary_start, cudaStream_t st) {
+int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uint32_t n, const Tables& T,
+               GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st) {
     int launches = 0;
     if (n > 0) {
-        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, grid, gb.key, gb.rank, gb.count, gb.coord,
-                                                                  stats);
+        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, vm, mat_u32, n, T, gb.key, gb.rank, gb.count,
+                                                                  gb.coord, stats);
         ++launches;
     }
     // cells, the non-finite bucket, and the total
-    launches += exclusive_scan(gb.count, grid.ncells + 2, gb.start, gb.block_sums, st);
+    launches += exclusive_scan(gb.count, T.ncells + 2, gb.start, gb.block_sums, st);
     if (n > 0) {
         k_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>(gb.key, gb.rank, n, gb.start, gb.perm);
         ++launches;
     }
-    k_sort_runs<<<blocks_for(grid.ncells + 1, kThreads), kThreads, 0, st>>>(gb.start, grid.ncells, gb.perm,
-                                                                            boundary_start, stats);
+    k_sort_runs<<<blocks_for(T.ncells + 1, kThreads), kThreads, 0, st>>>(gb.start, T.ncells, gb.perm,
+                                                                         boundary_start, stats);
     ++launches;
     return launches;
 }
@@ -405,24 +415,24 @@ int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* 
     return 1;
 }
 
-int records_to_soa(const arp_particle* in, uint32_t n, const uint32_t* sid_of, float4* pd, float4* vm, uint32_t* orig,
-                   uint32_t* sid, cudaStream_t st) {
+int records_to_soa(const arp_particle* in, uint32_t n, const uint32_t* sid_of, const uint32_t* mat_of, float4* pd,
+                   float4* vm, uint32_t* orig, uint32_t* sid, cudaStream_t st) {
     if (n == 0) return 0;
-    k_records_to_soa<<<blocks_for(n, kThreads), kThreads, 0, st>>>(in, n, sid_of, pd, vm, orig, sid);
+    k_records_to_soa<<<blocks_for(n, kThreads), kThreads, 0, st>>>(in, n, sid_of, mat_of, pd, vm, orig, sid);
     return 1;
 }
 
-int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, float pos_w, uint32_t* flag,
-                  cudaStream_t st) {
+int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, const DevMat* mats, float pos_w,
+                  uint32_t* flag, cudaStream_t st) {
     if (n == 0) return 0;
-    k_check_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(in, n, mat_of, pos_w, flag);
+    k_check_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(in, n, mat_of, mats, pos_w, flag);
     return 1;
 }
 
 int soa_to_records(const float4* pd, const float4* vm, const uint32_t* orig, const uint32_t* sid, uint32_t n,
-                   float pos_w, arp_particle* out, cudaStream_t st) {
+                   float pos_w, const DevMat* mats, arp_particle* out, cudaStream_t st) {
     if (n == 0) return 0;
-    k_soa_to_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pd, vm, orig, sid, n, pos_w, out);
+    k_soa_to_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pd, vm, orig, sid, n, pos_w, mats, out);
     return 1;
 }
 
@@ -432,10 +442,10 @@ int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_
     return 1;
 }
 
-int count_neighbors(const float4* xs, const uint32_t* start, uint32_t n, const float4* bxs, const uint32_t* bstart,
-                    const Params& P, uint32_t* out_sorted, cudaStream_t st) {
+int count_neighbors(const float4* xs, const float4* vs, const uint32_t* start, uint32_t n, const float4* bxs,
+                    const uint32_t* bstart, const Tables& T, uint32_t* out_sorted, cudaStream_t st) {
     if (n == 0) return 0;
-    k_count_neighbors<<<blocks_for(n, kThreads), kThreads, 0, st>>>(xs, start, n, bxs, bstart, P, out_sorted);
+    k_count_neighbors<<<blocks_for(n, kThreads), kThreads, 0, st>>>(xs, vs, start, n, bxs, bstart, T, out_sorted);
     return 1;
 }
 

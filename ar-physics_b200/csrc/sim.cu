@@ -144,14 +144,26 @@ arp_status arp::set_error(arp_status code, const std::string& msg) { return fail
 
 struct arp_sim {
     // scene
+    // One entry per scene of the batch (a single simulation has one).
+    struct SceneHost {
+        uint32_t p_base, n;       // caller-order particle range
+        uint32_t b_base, nb;      // boundary range
+        uint32_t mat_base, nmat;  // global material range
+        uint32_t inter_base;      // interaction block (nmat x nmat)
+        bool flat_z;              // every particle shares one z and moves in the plane
+        arp_aabb bounds;
+        float h, gravity, alpha;
+        SceneP sp;
+    };
+    std::vector<SceneHost> scenes;
     uint32_t n = 0, nb = 0, ns = 0, M = 0;
-    uint32_t dim = 0;      // the reference's count of non-zero box axes
-    int kdim = 3;          // 2 when every particle shares one z and z has no extent
+    uint32_t dim = 0;      // the reference's count of non-zero box axes (scene 0)
+    int kdim = 3;          // 2 when every scene is flat in z
     float pos_w = 0.0f;    // common w coordinate of all positions
-    std::vector<arp_material> mats;
-    std::vector<arp_interaction> inter;
-    arp_aabb bounds{};
-    float h = 0, timestep = 0, dt_sub = 0, gravity = 0, alpha = 0;
+    bool have_w = false;
+    std::vector<arp_material> mats;       // all scenes, scene order
+    std::vector<arp_interaction> inter;   // per-scene blocks, scene order
+    float h = 0, timestep = 0, dt_sub = 0;
     uint32_t subticks = 1;
     int integrator = 0;
     Tableau tab{};
@@ -159,7 +171,10 @@ struct arp_sim {
     bool initialized = false;
     bool any_stiff_immobile = false;
     bool all_order2 = true;  // every stiff material uses strain order 2
-    Params P{};
+    uint32_t ncells = 0;     // cells of all scenes
+    uint32_t max_nmat = 0;
+    Tables tables{};
+    std::vector<uint32_t> scene_of_material;
 
     std::vector<arp_particle> host_particles;  // caller order (initial state)
     std::vector<arp_particle> host_boundary;
@@ -169,8 +184,10 @@ struct arp_sim {
     cudaStream_t own_stream = nullptr, stream = nullptr;
     uint64_t launches = 0;
 
-    // device: materials
+    // device: scene and material tables
+    DevBuf<SceneP> d_scenes;
     DevBuf<DevMat> d_mats;
+    DevBuf<FluidMat> d_fmats;
     DevBuf<DevInter> d_inter;
     // mobile state: Y (y0), T (reorder target / y_new), S[2] (stage states)
     StateBuf Y, T, S[2], X, acc, kst[4];
@@ -188,7 +205,6 @@ struct arp_sim {
     DevBuf<uint32_t> g_key, g_rank, g_count, g_start, g_perm, g_bsums;
     DevBuf<uint2> g_coord, coord_s;  // grid coordinates per slot; storage-order copy for stage 0
     DevBuf<uint32_t> contact_bound;
-    float contact_slack = 0.0f;
     uint32_t grid_cap = 0;
     // solids
     DevBuf<float4> ref, L, F, A, ksol;
@@ -227,7 +243,7 @@ arp_status alloc_state(StateBuf& s, size_t n) {
 }
 
 arp_status ensure_grid(arp_sim* S, uint32_t cap) {
-    const uint32_t nc = S->P.grid.ncells;
+    const uint32_t nc = S->ncells;
     if (S->grid_cap >= cap && S->g_start.p) return ARP_OK;
     cap = std::max(cap, 1u);
     CUDA_TRY(S->g_key.alloc(cap));
@@ -283,35 +299,37 @@ void harvest_marks(arp_sim* S) {
     S->marks.clear();
 }
 
-void upload_params(arp_sim* S) {
-    Params& P = S->P;
+// Scalars and grid of one scene (neighbor_list.rs:201-206, kernel.rs:335-338,
+// the shader constants of fluid.rs / solid.rs).
+arp_status scene_params(arp_sim::SceneHost& H, uint32_t dim) {
+    SceneP& P = H.sp;
     for (int a = 0; a < 3; ++a) {
-        P.grid.min[a] = S->bounds.min[a];
-        P.grid.dim[a] = S->bounds.dim[a];
+        P.grid.min[a] = H.bounds.min[a];
+        P.grid.dim[a] = H.bounds.dim[a];
     }
     uint64_t nc = 1;
     for (int a = 0; a < 4; ++a) {
-        const float q = std::max(1.0f, S->bounds.dim[a] / S->h);  // neighbor_list.rs:201-206
-        const uint32_t s = (uint32_t)q;
-        if (a < 3) P.grid.sub[a] = s;
-        nc *= s;
+        const float q = std::max(1.0f, H.bounds.dim[a] / H.h);
+        const uint32_t sub = (uint32_t)q;
+        if (a < 3) P.grid.sub[a] = sub;
+        nc *= sub;
     }
+    if (nc > (1ull << 30)) return fail(ARP_ERR_UNSUPPORTED, "a scene's grid has more than 2^30 cells");
     P.grid.ncells = (uint32_t)nc;
-    P.dim = S->dim;
-    P.nmat = S->M;
-    P.h = S->h;
-    P.h2 = S->h * S->h;
-    P.kconst = norm_const_f32(S->dim, S->h);
-    P.g = S->gravity;
+    P.dim = dim;
+    P.h = H.h;
+    P.h2 = H.h * H.h;
+    P.kconst = norm_const_f32(dim, H.h);
+    P.g = H.gravity;
     const float eps = 0.1f;
-    volatile float t = eps * S->h;
+    volatile float t = eps * H.h;
     P.eps_h = t;
-    P.eps_hh = t * S->h;
+    P.eps_hh = t * H.h;
     volatile float ten_eps = 10.0f * eps;
-    P.hg_h = ten_eps * S->h;
-    P.rcut = 8.0f * S->h;
+    P.hg_h = ten_eps * H.h;
+    P.rcut = 8.0f * H.h;
     P.rcut2 = P.rcut * P.rcut;
-    volatile float hh = S->h * S->h;
+    volatile float hh = H.h * H.h;
     P.r_geom = hh / P.rcut;
     // Largest |dx| between particles inside the box whose cells are within one
     // cell per axis: 2 * |cell diagonal|.  An axis of zero extent contributes
@@ -319,22 +337,26 @@ void upload_params(arp_sim* S) {
     double cs2 = 0.0;
     bool bounded = true;
     for (int a = 0; a < 3; ++a) {
-        if (S->bounds.dim[a] > 0.0f) {
-            const double cs = (double)S->bounds.dim[a] / (double)P.grid.sub[a];
+        if (H.bounds.dim[a] > 0.0f) {
+            const double cs = (double)H.bounds.dim[a] / (double)P.grid.sub[a];
             cs2 += cs * cs;
-        } else if (!(a == 2 && S->kdim == 2)) {
+        } else if (!(a == 2 && H.flat_z)) {
             bounded = false;
         }
     }
     const double slack = 0.999 * (double)P.rcut - 2.0 * std::sqrt(cs2);
-    S->contact_slack = bounded && slack > 0.0 ? (float)slack : 0.0f;
+    P.contact_slack = bounded && slack > 0.0 ? (float)slack : 0.0f;
+    P.mat_base = H.mat_base;
+    P.nmat = H.nmat;
+    P.inter_base = H.inter_base;
+    return ARP_OK;
 }
 
 // Solid data, boundary grid, reference neighbor lists (FluidSim::init).
 arp_status do_init(arp_sim* S) {
     cudaStream_t st = S->stream;
     const uint32_t n = S->n, nb = S->nb, ns = S->ns;
-    const uint32_t nc = S->P.grid.ncells;
+    const uint32_t nc = S->ncells;
     ARP_TRY(ensure_grid(S, std::max({n, nb, ns, 1u})));
 
     // mobile state in caller order
@@ -380,7 +402,7 @@ arp_status do_init(arp_sim* S) {
             CUDA_TRY(cudaMemcpyAsync(tmp_vm.p, bvm.data(), nb * sizeof(float4), cudaMemcpyHostToDevice, st));
             CUDA_TRY(cudaMemcpyAsync(tmp_o.p, bo.data(), nb * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         }
-        S->launches += build_grid(tmp_pd.p, nb, S->P.grid, S->gb, nullptr, nullptr, st);
+        S->launches += build_grid(tmp_pd.p, tmp_vm.p, nullptr, nb, S->tables, S->gb, nullptr, nullptr, st);
         S->launches += gather_state(S->gb.perm, nb, tmp_pd.p, S->b_pd.p, tmp_vm.p, S->b_vm.p, tmp_o.p,
                                     S->b_orig.p, nullptr, nullptr, nullptr, nullptr, S->bps.p, S->d_mats.p, st);
         CUDA_TRY(cudaMemcpyAsync(S->b_start.p, S->gb.start, (size_t(nc) + 2) * sizeof(uint32_t),
@@ -389,8 +411,10 @@ arp_status do_init(arp_sim* S) {
         ARP_TRY(check_launch("boundary grid"));
     }
     if (S->any_stiff_immobile) {
+        // the scene's boundary index b read as an index into the scene's mobile particles
         std::vector<uint32_t> sb(std::max(nb, 1u), kInvalid);
-        for (uint32_t b = 0; b < nb; ++b) sb[b] = b < n ? S->sid_of_caller[b] : kInvalid;
+        for (const auto& H : S->scenes)
+            for (uint32_t b = 0; b < H.nb; ++b) sb[H.b_base + b] = b < H.n ? S->sid_of_caller[H.p_base + b] : kInvalid;
         CUDA_TRY(cudaMemcpy(S->sid_of_bidx.p, sb.data(), sb.size() * sizeof(uint32_t), cudaMemcpyHostToDevice));
     }
 
@@ -407,11 +431,11 @@ arp_status do_init(arp_sim* S) {
         CUDA_TRY(cudaMemcpyAsync(S->mat_of_solid.p, mos.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemsetAsync(S->ep.p, 0, size_t(ns) * 4 * sizeof(float4), st));
         // grid over reference positions (neighbor_list.rs:266-275, mode 1)
-        S->launches += build_grid(S->ref.p, ns, S->P.grid, S->gb, nullptr, nullptr, st);
+        S->launches += build_grid(S->ref.p, nullptr, S->mat_of_solid.p, ns, S->tables, S->gb, nullptr, nullptr, st);
         DevBuf<uint32_t> cnt;
         CUDA_TRY(cnt.alloc(size_t(ns) + 1));
         CUDA_TRY(cudaMemsetAsync(cnt.p, 0, (size_t(ns) + 1) * sizeof(uint32_t), st));
-        S->launches += ref_lists_count(S->ref.p, ns, S->gb, S->P, cnt.p, st);
+        S->launches += ref_lists_count(S->ref.p, S->mat_of_solid.p, ns, S->gb, S->tables, cnt.p, st);
         CUDA_TRY(S->rl_off.alloc(size_t(ns) + 1));
         S->launches += exclusive_scan(cnt.p, ns + 1, S->rl_off.p, S->gb.block_sums, st);
         uint32_t nnz = 0;
@@ -421,7 +445,7 @@ arp_status do_init(arp_sim* S) {
         CUDA_TRY(S->rl_gw.alloc(std::max(nnz, 1u)));
         S->rl_nnz = nnz;
         SolidRefList rl{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, nnz};
-        S->launches += ref_lists_fill(S->ref.p, S->mat_of_solid.p, ns, S->gb, S->P, S->d_mats.p, rl, S->L.p, st);
+        S->launches += ref_lists_fill(S->ref.p, S->mat_of_solid.p, ns, S->gb, S->tables, rl, S->L.p, st);
         CUDA_TRY(cudaStreamSynchronize(st));
         ARP_TRY(check_launch("reference neighbor lists"));
     }
@@ -448,7 +472,7 @@ arp_status do_step(arp_sim* S) {
     // 1. sort y0 into cell order
     arp_sim::Mark mk{};
     mark(S, mk, 0);
-    S->launches += build_grid(S->Y.pd.p, n, S->P.grid, S->gb, S->d_stats.p, bstart, st);
+    S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
     S->launches += gather_state(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
                                 S->orig_r.p, S->sid.p, S->sid_r.p, ns > 1 ? S->gb.coord : nullptr,
                                 ns > 1 ? S->coord_s.p : nullptr, S->ps.p, S->d_mats.p, st);
@@ -498,7 +522,7 @@ arp_status do_step(arp_sim* S) {
         if (s > 0) {
             if (S->profiling && s > 0) mark(S, mk, 0);
             l0 = S->launches;
-            S->launches += build_grid(cur_pd, n, S->P.grid, S->gb, S->d_stats.p, bstart, st);
+            S->launches += build_grid(cur_pd, cur_vm, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
             S->launches += gather_state(S->gb.perm, n, cur_pd, S->X.pd.p, cur_vm, S->X.vm.p, sb ? S->sid.p : nullptr,
                                         sb ? S->sid_sorted.p : nullptr, nullptr, nullptr, nullptr, nullptr, S->ps.p,
                                         S->d_mats.p, st);
@@ -534,15 +558,13 @@ arp_status do_step(arp_sim* S) {
             a.ksol = S->ksol.p;
             a.coord = s == 0 ? S->coord_s.p : S->gb.coord;  // storage-order coordinates of this stage's grid
             a.contact_bound = S->contact_bound.p;
-            a.contact_slack = S->contact_slack;
             a.xs = xs;
             a.vs = vs;
             a.start = S->gb.start;
             a.sid_sorted = sid_sorted;
-            a.mats = S->d_mats.p;
             a.ns = ns;
             a.all_order2 = S->all_order2 ? 1 : 0;
-            sl = launch_solid(a, S->P, c, st);
+            sl = launch_solid(a, S->tables, c, st);
             S->launches += sl;
             cur_ep = a.ep_next;
         }
@@ -562,15 +584,12 @@ arp_status do_step(arp_sim* S) {
         f.ps = S->ps.p;
         f.bps = S->bps.p;
         f.ksol = sb ? S->ksol.p : nullptr;
-        f.mats = S->d_mats.p;
-        f.inter = S->d_inter.p;
         f.n = n;
-        f.n_mobile_total = n;
         f.solid_branch = sb ? 1 : 0;
         f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
         B.next_pd = next_pd;
         B.next_vm = next_vm;
-        S->launches += launch_fluid(f, S->P, c, B, st);
+        S->launches += launch_fluid(f, S->tables, S->kdim, c, B, st);
         mark(S, mk, 3);
         if (S->profiling) {
             S->marks.push_back(mk);
@@ -590,11 +609,14 @@ arp_status do_step(arp_sim* S) {
     return check_launch("step");
 }
 
-arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
+// Validate one scene and append it to the batch: particles, boundary and
+// materials are concatenated in scene order, material ids remapped into the
+// batch's table, the interaction matrix resolved into the scene's block.
+arp_status append_scene(const arp_scene* sc, arp_sim* S) {
     if (!sc) return fail(ARP_ERR_INVALID_ARG, "scene is null");
     if (sc->n_materials == 0 || !sc->materials) return fail(ARP_ERR_INVALID_ARG, "scene has no materials");
     if (sc->n_materials > (uint32_t)kMaxMaterials)
-        return fail(ARP_ERR_UNSUPPORTED, "more than 32 materials");
+        return fail(ARP_ERR_UNSUPPORTED, "more than 32 materials in one scene");
     if (sc->n_particles && !sc->particles) return fail(ARP_ERR_INVALID_ARG, "particles is null");
     if (sc->n_boundary && !sc->boundary) return fail(ARP_ERR_INVALID_ARG, "boundary is null");
     if (!(sc->kernel_radius > 0.0f) || !std::isfinite(sc->kernel_radius))
@@ -602,31 +624,59 @@ arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
     if (!std::isfinite(sc->timestep)) return fail(ARP_ERR_INVALID_ARG, "timestep must be finite");
     if (sc->integrator == ARP_INT_VERLET)
         return fail(ARP_ERR_UNSUPPORTED, "the velocity-Verlet integrator is not implemented; use an RK tableau");
-    if (!make_tableau(sc->integrator, S->tab)) return fail(ARP_ERR_INVALID_ARG, "unknown integrator id");
+    Tableau tab;
+    if (!make_tableau(sc->integrator, tab)) return fail(ARP_ERR_INVALID_ARG, "unknown integrator id");
     if (sc->bounds.dim[3] > 0.0f) return fail(ARP_ERR_UNSUPPORTED, "4-dimensional boxes are not supported");
     for (int a = 0; a < 4; ++a)
         if (!std::isfinite(sc->bounds.min[a]) || !std::isfinite(sc->bounds.dim[a]) || sc->bounds.dim[a] < 0.0f)
             return fail(ARP_ERR_INVALID_ARG, "bounds must be finite with non-negative extent");
-    S->M = sc->n_materials;
-    S->mats.assign(sc->materials, sc->materials + S->M);
-    S->n = sc->n_particles;
-    S->nb = sc->n_boundary;
-    S->host_particles.assign(sc->particles, sc->particles + S->n);
-    S->host_boundary.assign(sc->boundary, sc->boundary + S->nb);
-    bool have_w = false;
+    const uint32_t subticks = sc->subticks ? sc->subticks : 1;
+    const bool first = S->scenes.empty();
+    if (first) {
+        S->tab = tab;
+        S->integrator = sc->integrator;
+        S->timestep = sc->timestep;
+        S->subticks = subticks;
+        S->dt_sub = sc->timestep / (float)subticks;
+        S->h = sc->kernel_radius;
+    } else if (sc->integrator != S->integrator || sc->timestep != S->timestep || subticks != S->subticks) {
+        return fail(ARP_ERR_UNSUPPORTED, "all scenes of a batch must share integrator, time step and subticks");
+    }
+    uint32_t dim = 0;
+    for (int a = 0; a < 4; ++a)
+        if (sc->bounds.dim[a] > 0.0f) dim++;
+    if (dim == 0) return fail(ARP_ERR_INVALID_ARG, "bounds have no extent");
+    if (first) S->dim = dim;
+
+    arp_sim::SceneHost H{};
+    H.p_base = S->n;
+    H.n = sc->n_particles;
+    H.b_base = S->nb;
+    H.nb = sc->n_boundary;
+    H.mat_base = S->M;
+    H.nmat = sc->n_materials;
+    H.inter_base = (uint32_t)S->inter.size();
+    H.bounds = sc->bounds;
+    H.h = sc->kernel_radius;
+    H.gravity = sc->gravity;
+    H.alpha = sc->artificial_viscocity;
+    const uint32_t scene_idx = (uint32_t)S->scenes.size();
+    const uint32_t M = sc->n_materials;
+    const arp_material* mats = sc->materials;
+
     bool flat_z = sc->bounds.dim[2] == 0.0f;
     float z0 = 0.0f;
     bool have_z = false;
     auto check_p = [&](const arp_particle& p, bool boundary) -> arp_status {
-        if (p.mat >= S->M) return fail(ARP_ERR_INVALID_ARG, "particle material index out of range");
-        const bool imm = S->mats[p.mat].immobile != 0;
+        if (p.mat >= M) return fail(ARP_ERR_INVALID_ARG, "particle material index out of range");
+        const bool imm = mats[p.mat].immobile != 0;
         if (imm != boundary)
             return fail(ARP_ERR_INVALID_ARG, boundary ? "boundary particle uses a mobile material"
                                                       : "mobile particle uses an immobile material");
         if (!std::isfinite(p.pos[3])) return fail(ARP_ERR_INVALID_ARG, "non-finite w coordinate");
-        if (!have_w) {
+        if (!S->have_w) {
             S->pos_w = p.pos[3];
-            have_w = true;
+            S->have_w = true;
         } else if (p.pos[3] != S->pos_w) {
             return fail(ARP_ERR_UNSUPPORTED, "positions must share one w coordinate (4D motion is not supported)");
         }
@@ -640,12 +690,27 @@ arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
         if (p.vel[2] != 0.0f) flat_z = false;
         return ARP_OK;
     };
-    for (uint32_t i = 0; i < S->n; ++i) ARP_TRY(check_p(S->host_particles[i], false));
-    for (uint32_t i = 0; i < S->nb; ++i) ARP_TRY(check_p(S->host_boundary[i], true));
-    S->kdim = flat_z ? 2 : 3;
-    // mod.rs:93-111 interaction matrix
-    const uint32_t M = S->M;
-    S->inter.assign(size_t(M) * M, arp_interaction{0, 0, 0, 0, 0});
+    for (uint32_t i = 0; i < sc->n_particles; ++i) ARP_TRY(check_p(sc->particles[i], false));
+    for (uint32_t i = 0; i < sc->n_boundary; ++i) ARP_TRY(check_p(sc->boundary[i], true));
+    H.flat_z = flat_z;
+    for (uint32_t i = 0; i < sc->n_particles; ++i) {
+        arp_particle p = sc->particles[i];
+        p.mat += H.mat_base;
+        S->host_particles.push_back(p);
+    }
+    for (uint32_t i = 0; i < sc->n_boundary; ++i) {
+        arp_particle p = sc->boundary[i];
+        p.mat += H.mat_base;
+        S->host_boundary.push_back(p);
+    }
+    for (uint32_t i = 0; i < M; ++i) {
+        S->mats.push_back(mats[i]);
+        S->scene_of_material.push_back(scene_idx);
+        if (mats[i].immobile && is_stiff(mats[i])) S->any_stiff_immobile = true;
+        if (is_stiff(mats[i]) && mats[i].strain_order != 2) S->all_order2 = false;
+    }
+    // mod.rs:93-111 interaction matrix of the scene
+    std::vector<arp_interaction> block(size_t(M) * M, arp_interaction{0, 0, 0, 0, 0});
     auto given = [&](uint32_t i, uint32_t j) -> bool {
         if (!sc->interactions) return false;
         if (!sc->interaction_given) return true;
@@ -657,31 +722,34 @@ arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
             if (given(i, j)) x = sc->interactions[size_t(i) * M + j];
             else if (given(j, i)) x = sc->interactions[size_t(j) * M + i];
             else if (i != j) {
-                const arp_material& a = S->mats[i];
-                const arp_material& b = S->mats[j];
+                const arp_material& a = mats[i];
+                const arp_material& b = mats[j];
                 if (a.state_eq != ARP_EOS_ZERO && b.state_eq != ARP_EOS_ZERO) x = arp_interaction{0, 0, 0, 0, 0};
                 else x = arp_interaction{ARP_CONTACT_LINEAR, 10000.0f, sc->kernel_radius * 2.0f, 0.0f, a.visc + b.visc};
             }
-            S->inter[size_t(i) * M + j] = x;
-            S->inter[size_t(j) * M + i] = x;
+            block[size_t(i) * M + j] = x;
+            block[size_t(j) * M + i] = x;
         }
-    for (const auto& m : S->mats) {
-        if (m.immobile && is_stiff(m)) S->any_stiff_immobile = true;
-        if (is_stiff(m) && m.strain_order != 2) S->all_order2 = false;
-    }
-    S->bounds = sc->bounds;
-    S->dim = 0;
-    for (int a = 0; a < 4; ++a)
-        if (sc->bounds.dim[a] > 0.0f) S->dim++;
-    if (S->dim == 0) return fail(ARP_ERR_INVALID_ARG, "bounds have no extent");
-    S->h = sc->kernel_radius;
-    S->timestep = sc->timestep;
-    S->subticks = sc->subticks ? sc->subticks : 1;
-    S->dt_sub = sc->timestep / (float)S->subticks;
-    S->gravity = sc->gravity;
-    S->alpha = sc->artificial_viscocity;
-    S->integrator = sc->integrator;
-    // particles.rs:488-506: solid ids in particle order for stiff materials
+    S->inter.insert(S->inter.end(), block.begin(), block.end());
+    ARP_TRY(scene_params(H, dim));
+    if ((uint64_t)S->ncells + H.sp.grid.ncells + 2 > (1ull << 31))
+        return fail(ARP_ERR_UNSUPPORTED, "the batch's grids have more than 2^31 cells");
+    H.sp.cell_base = S->ncells;
+    S->ncells += H.sp.grid.ncells;
+    S->n += H.n;
+    S->nb += H.nb;
+    S->M += M;
+    S->max_nmat = std::max(S->max_nmat, M);
+    S->scenes.push_back(H);
+    return ARP_OK;
+}
+
+// Solid ids in particle order for stiff materials (particles.rs:488-506), in
+// the concatenated caller order of the batch.
+void finalize_scenes(arp_sim* S) {
+    bool all_flat = true;
+    for (const auto& H : S->scenes) all_flat = all_flat && H.flat_z;
+    S->kdim = all_flat ? 2 : 3;
     S->sid_of_caller.assign(S->n, kInvalid);
     S->part_of_solid.clear();
     for (uint32_t i = 0; i < S->n; ++i)
@@ -690,17 +758,11 @@ arp_status validate_and_copy(const arp_scene* sc, arp_sim* S) {
             S->part_of_solid.push_back(i);
         }
     S->ns = (uint32_t)S->part_of_solid.size();
-    upload_params(S);
-    if ((uint64_t)S->P.grid.ncells * 1 > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "grid has more than 2^31 cells");
-    uint64_t nc = 1;
-    for (int a = 0; a < 4; ++a) nc *= std::max<uint64_t>(1, (uint64_t)std::max(1.0f, S->bounds.dim[a] / S->h));
-    if (nc > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "grid has more than 2^31 cells");
-    return ARP_OK;
 }
 
 arp_status allocate(arp_sim* S) {
     const size_t n = std::max(S->n, 1u), nb = std::max(S->nb, 1u), ns = std::max(S->ns, 1u);
-    const size_t nc = S->P.grid.ncells;
+    const size_t nc = S->ncells;
     ARP_TRY(alloc_state(S->Y, n));
     ARP_TRY(alloc_state(S->T, n));
     ARP_TRY(alloc_state(S->S[0], n));
@@ -768,17 +830,35 @@ arp_status allocate(arp_sim* S) {
         d.vol0 = m.mass / m.start_den;
         d.state_eq = m.state_eq; d.stiff = is_stiff(m) ? 1u : 0u; d.plastic = m.plastic ? 1u : 0u;
         d.strain_order = m.strain_order;
+        d.scene = S->scene_of_material[i];
+        d.local = i - S->scenes[d.scene].mat_base;
         dm[i] = d;
     }
     CUDA_TRY(S->d_mats.alloc(S->M));
     CUDA_TRY(cudaMemcpy(S->d_mats.p, dm.data(), S->M * sizeof(DevMat), cudaMemcpyHostToDevice));
-    std::vector<DevInter> di(size_t(S->M) * S->M);
+    std::vector<FluidMat> fm(S->M);
+    for (uint32_t i = 0; i < S->M; ++i)
+        fm[i] = FluidMat{dm[i].mass, dm[i].sound_speed, dm[i].target_den, dm[i].visc, dm[i].bulk_visc, dm[i].state_eq,
+                         dm[i].stiff, 0u};
+    CUDA_TRY(S->d_fmats.alloc(S->M));
+    CUDA_TRY(cudaMemcpy(S->d_fmats.p, fm.data(), S->M * sizeof(FluidMat), cudaMemcpyHostToDevice));
+    std::vector<SceneP> sp;
+    for (const auto& H : S->scenes) sp.push_back(H.sp);
+    CUDA_TRY(S->d_scenes.alloc(sp.size()));
+    CUDA_TRY(cudaMemcpy(S->d_scenes.p, sp.data(), sp.size() * sizeof(SceneP), cudaMemcpyHostToDevice));
+    std::vector<DevInter> di(S->inter.size());
     for (size_t i = 0; i < di.size(); ++i) {
         const arp_interaction& x = S->inter[i];
         di[i] = DevInter{x.potential, x.strength, x.radius, x.dampening, x.friction};
     }
     CUDA_TRY(S->d_inter.alloc(di.size()));
     CUDA_TRY(cudaMemcpy(S->d_inter.p, di.data(), di.size() * sizeof(DevInter), cudaMemcpyHostToDevice));
+    S->tables.scenes = S->d_scenes.p;
+    S->tables.mats = S->d_mats.p;
+    S->tables.fmats = S->d_fmats.p;
+    S->tables.inter = S->d_inter.p;
+    S->tables.ncells = S->ncells;
+    S->tables.max_nmat = S->max_nmat;
     return ARP_OK;
 }
 
@@ -795,14 +875,17 @@ extern "C" {
 const char* arp_last_error(void) { return g_last_error.c_str(); }
 uint32_t arp_abi_version(void) { return ARP_ABI_VERSION; }
 
-arp_status arp_sim_create(const arp_scene* scene, arp_sim** out) {
+arp_status arp_sim_create_batch(const arp_scene* scenes, uint32_t count, arp_sim** out) {
     g_last_error.clear();
     if (!out) return fail(ARP_ERR_INVALID_ARG, "out is null");
     *out = nullptr;
+    if (!scenes || count == 0) return fail(ARP_ERR_INVALID_ARG, scenes ? "no scenes" : "scene is null");
     arp_sim* S = new (std::nothrow) arp_sim();
     if (!S) return fail(ARP_ERR_OUT_OF_MEMORY, "host allocation failed");
-    arp_status s = validate_and_copy(scene, S);
+    arp_status s = ARP_OK;
+    for (uint32_t k = 0; k < count && s == ARP_OK; ++k) s = append_scene(&scenes[k], S);
     if (s == ARP_OK) {
+        finalize_scenes(S);
         cudaError_t e = cudaStreamCreateWithFlags(&S->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) s = fail(ARP_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
         S->stream = S->own_stream;
@@ -813,6 +896,35 @@ arp_status arp_sim_create(const arp_scene* scene, arp_sim** out) {
         return s;
     }
     *out = S;
+    return ARP_OK;
+}
+
+arp_status arp_sim_create(const arp_scene* scene, arp_sim** out) {
+    if (!scene) {
+        if (out) *out = nullptr;
+        return fail(ARP_ERR_INVALID_ARG, "scene is null");
+    }
+    return arp_sim_create_batch(scene, 1, out);
+}
+
+arp_status arp_sim_num_scenes(const arp_sim* sim, uint32_t* out) {
+    if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = (uint32_t)sim->scenes.size();
+    return ARP_OK;
+}
+
+arp_status arp_sim_scene_range(const arp_sim* sim, uint32_t scene, uint32_t* first_particle, uint32_t* n_particles,
+                               uint32_t* first_boundary, uint32_t* n_boundary, uint32_t* first_cell,
+                               uint32_t* n_cells) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (scene >= sim->scenes.size()) return fail(ARP_ERR_INVALID_ARG, "scene index out of range");
+    const auto& H = sim->scenes[scene];
+    if (first_particle) *first_particle = H.p_base;
+    if (n_particles) *n_particles = H.n;
+    if (first_boundary) *first_boundary = H.b_base;
+    if (n_boundary) *n_boundary = H.nb;
+    if (first_cell) *first_cell = H.sp.cell_base;
+    if (n_cells) *n_cells = H.sp.grid.ncells;
     return ARP_OK;
 }
 
@@ -884,13 +996,16 @@ arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap) 
     if (cap < sim->n) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_particles");
     if (!sim->initialized) {
         std::memcpy(out, sim->host_particles.data(), sim->n * sizeof(arp_particle));
-        for (uint32_t i = 0; i < sim->n; ++i) out[i].solid_id = sim->sid_of_caller[i];
+        for (uint32_t i = 0; i < sim->n; ++i) {
+            out[i].solid_id = sim->sid_of_caller[i];
+            out[i].mat -= sim->scenes[sim->scene_of_material[out[i].mat]].mat_base;
+        }
         return ARP_OK;
     }
     const uint32_t n = sim->n;
     if (!sim->records.p) CUDA_TRY(sim->records.alloc(n));
-    sim->launches += soa_to_records(sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, n, sim->pos_w, sim->records.p,
-                                    sim->stream);
+    sim->launches += soa_to_records(sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, n, sim->pos_w, sim->d_mats.p,
+                                    sim->records.p, sim->stream);
     if (n) CUDA_TRY(cudaMemcpyAsync(out, sim->records.p, n * sizeof(arp_particle), cudaMemcpyDeviceToHost, sim->stream));
     CUDA_TRY(cudaStreamSynchronize(sim->stream));
     return check_launch("get_particles");
@@ -926,7 +1041,10 @@ arp_status arp_sim_get_boundary(arp_sim* sim, arp_particle* out, uint32_t cap) {
     if (!sim || (!out && sim->nb)) return fail(ARP_ERR_INVALID_ARG, "null argument");
     if (cap < sim->nb) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_boundary");
     std::memcpy(out, sim->host_boundary.data(), sim->nb * sizeof(arp_particle));
-    for (uint32_t i = 0; i < sim->nb; ++i) out[i].solid_id = kInvalid;
+    for (uint32_t i = 0; i < sim->nb; ++i) {
+        out[i].solid_id = kInvalid;
+        out[i].mat -= sim->scenes[sim->scene_of_material[out[i].mat]].mat_base;
+    }
     return ARP_OK;
 }
 
@@ -939,7 +1057,8 @@ arp_status arp_sim_get_materials(const arp_sim* sim, arp_material* out, uint32_t
 
 arp_status arp_sim_get_interactions(const arp_sim* sim, arp_interaction* out, uint32_t cap) {
     if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
-    if (cap < sim->M * sim->M) return fail(ARP_ERR_CAPACITY, "output holds fewer than n_materials^2 records");
+    if (cap < sim->inter.size())
+        return fail(ARP_ERR_CAPACITY, "output holds fewer records than the interaction blocks of all scenes");
     std::memcpy(out, sim->inter.data(), sim->inter.size() * sizeof(arp_interaction));
     return ARP_OK;
 }
@@ -954,13 +1073,14 @@ arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t 
         CUDA_TRY(cudaMemcpyAsync(sim->records.p, in, n * sizeof(arp_particle), cudaMemcpyHostToDevice, st));
         uint32_t flag = 0;
         CUDA_TRY(cudaMemsetAsync(sim->check_flag.p, 0, sizeof(uint32_t), st));
-        sim->launches += check_records(sim->records.p, n, sim->mat_of_caller_d.p, sim->pos_w, sim->check_flag.p, st);
+        sim->launches += check_records(sim->records.p, n, sim->mat_of_caller_d.p, sim->d_mats.p, sim->pos_w,
+                                       sim->check_flag.p, st);
         CUDA_TRY(cudaMemcpyAsync(&flag, sim->check_flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaStreamSynchronize(st));
         if (flag & 1u) return fail(ARP_ERR_INVALID_ARG, "material of a particle changed");
         if (flag & 2u) return fail(ARP_ERR_UNSUPPORTED, "w components must keep their values");
-        sim->launches += records_to_soa(sim->records.p, n, sim->sid_of_caller_d.p, sim->Y.pd.p, sim->Y.vm.p,
-                                        sim->orig.p, sim->sid.p, st);
+        sim->launches += records_to_soa(sim->records.p, n, sim->sid_of_caller_d.p, sim->mat_of_caller_d.p,
+                                        sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, st);
         CUDA_TRY(cudaStreamSynchronize(st));
         ARP_TRY(check_launch("set_particles"));
     }
@@ -987,24 +1107,25 @@ arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n
 arp_status arp_sim_grid(const arp_sim* sim, uint32_t subdivisions[4], uint32_t* n_cells) {
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
     if (subdivisions) {
-        for (int a = 0; a < 3; ++a) subdivisions[a] = sim->P.grid.sub[a];
+        for (int a = 0; a < 3; ++a) subdivisions[a] = sim->scenes[0].sp.grid.sub[a];
         subdivisions[3] = 1;
     }
-    if (n_cells) *n_cells = sim->P.grid.ncells;
+    if (n_cells) *n_cells = sim->ncells;
     return ARP_OK;
 }
 
 arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_start, uint32_t* members,
                              uint32_t* nbr_count) {
     ARP_TRY(need_init(sim));
-    const uint32_t n = sim->n, nc = sim->P.grid.ncells;
+    const uint32_t n = sim->n, nc = sim->ncells;
     cudaStream_t st = sim->stream;
-    sim->launches += build_grid(sim->Y.pd.p, n, sim->P.grid, sim->gb, nullptr, nullptr, st);
-    sim->launches += gather_sorted(sim->gb.perm, n, sim->Y.pd.p, sim->X.pd.p, nullptr, nullptr, nullptr, nullptr,
-                                   nullptr, nullptr, st);
+    sim->launches += build_grid(sim->Y.pd.p, sim->Y.vm.p, nullptr, n, sim->tables, sim->gb, nullptr, nullptr, st);
+    sim->launches += gather_sorted(sim->gb.perm, n, sim->Y.pd.p, sim->X.pd.p, sim->Y.vm.p, sim->X.vm.p, nullptr,
+                                   nullptr, nullptr, nullptr, st);
     DevBuf<uint32_t> cnt;
     CUDA_TRY(cnt.alloc(n));
-    sim->launches += count_neighbors(sim->X.pd.p, sim->gb.start, n, sim->b_pd.p, sim->b_start.p, sim->P, cnt.p, st);
+    sim->launches += count_neighbors(sim->X.pd.p, sim->X.vm.p, sim->gb.start, n, sim->b_pd.p, sim->b_start.p, sim->tables,
+                                     cnt.p, st);
     std::vector<uint32_t> key(n), perm(n), start(size_t(nc) + 2), orig(n), c(n);
     if (n) {
         CUDA_TRY(cudaMemcpyAsync(key.data(), sim->gb.key, n * 4, cudaMemcpyDeviceToHost, st));
@@ -1029,7 +1150,7 @@ arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_sta
 
 arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* members) {
     ARP_TRY(need_init(sim));
-    const uint32_t nb = sim->nb, nc = sim->P.grid.ncells;
+    const uint32_t nb = sim->nb, nc = sim->ncells;
     if (cell_start)
         CUDA_TRY(cudaMemcpy(cell_start, sim->b_start.p, (size_t(nc) + 1) * 4, cudaMemcpyDeviceToHost));
     if (members && nb) CUDA_TRY(cudaMemcpy(members, sim->b_orig.p, size_t(nb) * 4, cudaMemcpyDeviceToHost));

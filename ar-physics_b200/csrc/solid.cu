@@ -46,7 +46,7 @@ __device__ __forceinline__ void pad_unit(M4& C, uint32_t dim) {
 template <class F>
 __device__ __forceinline__ void for_ref_neighbors(uint32_t i, const float4* __restrict__ ref,
                                                   const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
-                                                  const Params& P, F&& f) {
+                                                  const SceneP& P, F&& f) {
     const float4 xi = ref[i];
     if (!finite3(xi)) return;
     const Grid& g = P.grid;
@@ -58,7 +58,7 @@ __device__ __forceinline__ void for_ref_neighbors(uint32_t i, const float4* __re
         for (int dy = -1; dy <= 1; ++dy) {
             const int y = c.y + dy;
             if (y < 0 || y >= (int)g.sub[1]) continue;
-            const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+            const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
             for (uint32_t k = start[row + x0]; k < start[row + x1 + 1]; ++k) {
                 const uint32_t j = perm[k];
                 if (j == i) continue;
@@ -70,23 +70,26 @@ __device__ __forceinline__ void for_ref_neighbors(uint32_t i, const float4* __re
     }
 }
 
-__global__ void k_ref_count(const float4* __restrict__ ref, uint32_t ns, const uint32_t* __restrict__ start,
-                            const uint32_t* __restrict__ perm, Params P, uint32_t* __restrict__ count) {
+__global__ void k_ref_count(const float4* __restrict__ ref, const uint32_t* __restrict__ mat_of, uint32_t ns,
+                            const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, Tables T,
+                            uint32_t* __restrict__ count) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     uint32_t n = 0;
+    const SceneP& P = T.scenes[T.mats[mat_of[i]].scene];
     for_ref_neighbors(i, ref, start, perm, P, [&](uint32_t, float3, float) { ++n; });
     count[i] = n;
 }
 
 __global__ void k_ref_fill(const float4* __restrict__ ref, const uint32_t* __restrict__ mat_of, uint32_t ns,
-                           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, Params P,
-                           const DevMat* __restrict__ mats, const uint32_t* __restrict__ off,
-                           uint32_t* __restrict__ nbr, float4* __restrict__ gw) {
+                           const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, Tables T,
+                           const uint32_t* __restrict__ off, uint32_t* __restrict__ nbr, float4* __restrict__ gw) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     uint32_t w = off[i];
     const uint32_t mi = mat_of[i];
+    const DevMat* mats = T.mats;
+    const SceneP& P = T.scenes[mats[mi].scene];
     for_ref_neighbors(i, ref, start, perm, P, [&](uint32_t j, float3 dX, float diff) {
         const float s = -6.0f * P.kconst * diff * diff;
         const uint32_t mj = mat_of[j];
@@ -98,11 +101,12 @@ __global__ void k_ref_fill(const float4* __restrict__ ref, const uint32_t* __res
 
 // L = inverse(sum_j V_j gradW (x) dX), unit diagonal on the unused axes
 // (strain.rs:107-136).  Stored as three float4 columns.
-__global__ void k_ref_L(const float4* __restrict__ ref, uint32_t ns, const uint32_t* __restrict__ off,
-                        const uint32_t* __restrict__ nbr, const float4* __restrict__ gw, Params P,
-                        float4* __restrict__ L) {
+__global__ void k_ref_L(const float4* __restrict__ ref, const uint32_t* __restrict__ mat_of, uint32_t ns,
+                        const uint32_t* __restrict__ off, const uint32_t* __restrict__ nbr,
+                        const float4* __restrict__ gw, Tables T, float4* __restrict__ L) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
+    const SceneP& P = T.scenes[T.mats[mat_of[i]].scene];
     M4 C = m4_zero();
     const float4 xi = ref[i];
     for (uint32_t k = off[i]; k < off[i + 1]; ++k) {
@@ -204,13 +208,14 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
 // ORDER2: every solid material uses strain order 2 (Green-Lagrange), so the
 // log-series, square-root and inverse paths are compiled out.
 template <bool ORDER2>
-__global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Params P, StageCoefs c) {
+__global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T, StageCoefs c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ns) return;
     const uint32_t slot = a.slot_of[i];
     const float4 xi = a.pd[slot];
     const float4 vi = a.vm[slot];
-    const DevMat mm = a.mats[__float_as_uint(vi.w)];
+    const DevMat mm = T.mats[__float_as_uint(vi.w)];
+    const SceneP& P = T.scenes[mm.scene];
     const float4 L0 = a.L[3 * i], L1 = a.L[3 * i + 1], L2 = a.L[3 * i + 2];
     // strain.rs:139-160: F = sum V dx (x) (L gradW), Fdot likewise with dv
     float F[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
@@ -348,13 +353,14 @@ __device__ __forceinline__ bool in_stencil(uint2 a, uint2 b) {
            dz <= 1;
 }
 
-__global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P) {
+__global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ns) return;
     const uint32_t slot = a.slot_of[i];
     const float4 xi = a.pd[slot];
     const uint32_t mat = __float_as_uint(a.vm[slot].w);
-    const DevMat mm = a.mats[mat];
+    const DevMat mm = T.mats[mat];
+    const SceneP& P = T.scenes[mm.scene];
     const float m1 = mm.mass, d1 = xi.w;
     const float V1 = m1 / d1;
     const float4 Ai0 = a.A[3 * i], Ai1 = a.A[3 * i + 1], Ai2 = a.A[3 * i + 2];
@@ -412,7 +418,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
     // every solid is inside the box and r_cut - max|dx in stencil| exceeds
     // 2 max|u_k - u_0|, which bounds |dX| below r_cut for all such pairs.
     const float U = __uint_as_float(a.contact_bound[0]);
-    const bool maybe = !mm.plastic && (a.contact_slack <= 0.0f || a.contact_bound[1] != 0u || !(2.0f * U < a.contact_slack));
+    const bool maybe = !mm.plastic && (P.contact_slack <= 0.0f || a.contact_bound[1] != 0u || !(2.0f * U < P.contact_slack));
     if (maybe && finite3(xi)) {
         const Grid& g = P.grid;
         const CellCoord cc = cell_coord(xi, g);
@@ -423,7 +429,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
             for (int dy = -1; dy <= 1; ++dy) {
                 const int y = cc.y + dy;
                 if (y < 0 || y >= (int)g.sub[1]) continue;
-                const uint32_t row = (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
                 for (uint32_t k = a.start[row + x0]; k < a.start[row + x1 + 1]; ++k) {
                     if (__float_as_uint(a.vs[k].w) != mat) continue;
                     const uint32_t sj = a.sid_sorted[k];
@@ -449,28 +455,28 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Params P
 
 }  // namespace
 
-int ref_lists_count(const float4* ref, uint32_t ns, const GridBuffers& gb, const Params& P, uint32_t* count,
-                          cudaStream_t st) {
-    k_ref_count<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, ns, gb.start, gb.perm, P, count);
+int ref_lists_count(const float4* ref, const uint32_t* mat_of, uint32_t ns, const GridBuffers& gb, const Tables& T,
+                    uint32_t* count, cudaStream_t st) {
+    k_ref_count<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, gb.start, gb.perm, T, count);
     return 1;
 }
 
-int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const GridBuffers& gb,
-                         const Params& P, const DevMat* mats, SolidRefList& rl, float4* L, cudaStream_t st) {
-    k_ref_fill<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, gb.start, gb.perm, P, mats, rl.off,
-                                                              rl.nbr, rl.gw);
-    k_ref_L<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, ns, rl.off, rl.nbr, rl.gw, P, L);
+int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const GridBuffers& gb, const Tables& T,
+                   SolidRefList& rl, float4* L, cudaStream_t st) {
+    k_ref_fill<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, gb.start, gb.perm, T, rl.off, rl.nbr,
+                                                              rl.gw);
+    k_ref_L<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, rl.off, rl.nbr, rl.gw, T, L);
     return 2;
 }
 
-int launch_solid(const SolidArgs& a, const Params& P, const StageCoefs& c, cudaStream_t st) {
+int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st) {
     if (a.ns == 0) return 0;
     cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
     if (a.all_order2)
-        k_solid_stress<true><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P, c);
+        k_solid_stress<true><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, T, c);
     else
-        k_solid_stress<false><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P, c);
-    k_solid_forces<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, P);
+        k_solid_stress<false><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, T, c);
+    k_solid_forces<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, T);
     return 2;
 }
 

@@ -196,6 +196,19 @@ typedef struct arp_device_view {
 
 /* FluidSim::new, src/soft_body/mod.rs:58-166. */
 arp_status arp_sim_create(const arp_scene* scene, arp_sim** out);
+/* Several independent scenes stepped together (the batched form; the
+ * reference has no batching).  Scenes keep their own box, kernel radius,
+ * gravity, materials and interactions; they must share the integrator, time
+ * step and subticks.  Particles of scene k occupy the caller-order range
+ * reported by arp_sim_scene_range, and records carry each scene's own
+ * material indices.  arp_sim_create(s) is arp_sim_create_batch(s, 1). */
+arp_status arp_sim_create_batch(const arp_scene* scenes, uint32_t count, arp_sim** out);
+arp_status arp_sim_num_scenes(const arp_sim* sim, uint32_t* out);
+/* Caller-order particle range, boundary range and global cell range of one
+ * scene (any output may be NULL). */
+arp_status arp_sim_scene_range(const arp_sim* sim, uint32_t scene, uint32_t* first_particle,
+                               uint32_t* n_particles, uint32_t* first_boundary, uint32_t* n_boundary,
+                               uint32_t* first_cell, uint32_t* n_cells);
 /* FluidSim::new after examples/test_mods/config.rs:298-474 parses a scene
  * file and src/soft_body/material_region/mod.rs:56-155 seeds its regions. */
 arp_status arp_sim_create_from_toml(const char* path, arp_sim** out);
@@ -229,7 +242,8 @@ arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap);
 arp_status arp_sim_get_solids(arp_sim* sim, arp_solid_particle* out, uint32_t cap);
 arp_status arp_sim_get_boundary(arp_sim* sim, arp_particle* out, uint32_t cap);
 arp_status arp_sim_get_materials(const arp_sim* sim, arp_material* out, uint32_t cap);
-/* The resolved n_materials^2 interaction table (src/soft_body/mod.rs:93-111). */
+/* The resolved interaction tables (src/soft_body/mod.rs:93-111): one
+ * n_materials^2 block per scene, in scene order. */
 arp_status arp_sim_get_interactions(const arp_sim* sim, arp_interaction* out, uint32_t cap);
 /* Replace the mobile state (den, pos, vel) of all particles, caller order;
  * mat and solid_id of the input must match the handle's. */
@@ -247,7 +261,8 @@ arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n
 
 /* ---- neighbor grid (src/soft_body/neighbor_list.rs) ------------------------ */
 
-/* Grid shape: subdivisions as NeighborList::new computes them (:199-217). */
+/* Grid shape: subdivisions as NeighborList::new computes them (:199-217) for
+ * scene 0, and the cell count of all scenes. */
 arp_status arp_sim_grid(const arp_sim* sim, uint32_t subdivisions[4], uint32_t* n_cells);
 /* Build the grid for the current positions and copy it out in the reference's
  * terms: `cell_of[i]` = bucket of mobile particle i (caller order), or
