@@ -175,6 +175,11 @@ def load_library():
     }
     sig["arp_sim_create_batch"] = [ctypes.POINTER(ArpScene), ctypes.c_uint32, ctypes.POINTER(c_sim)]
     sig["arp_sim_num_scenes"] = [c_sim, u32p]
+    sig["arp_sim_set_graph"] = [c_sim, ctypes.c_int]
+    sig["arp_sim_autotune"] = [c_sim, ctypes.POINTER(ctypes.c_int)]
+    sig["arp_sim_set_fluid_variant"] = [c_sim, ctypes.c_int]
+    sig["arp_sim_fluid_variant"] = [c_sim, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
+                                     ctypes.POINTER(ctypes.c_int)]
     sig["arp_sim_scene_range"] = [c_sim, ctypes.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p]
     sig["arp_grid_build_noalloc"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ArpAABB), ctypes.c_float,
                                      ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]

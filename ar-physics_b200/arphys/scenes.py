@@ -212,3 +212,52 @@ def stretched_bar(n=(20, 4, 4), spacing=0.01, stretch=1.01, lam=-1e5, mu=-1e5, d
     x0 = ref[:, 0].mean()
     stretched[:, 0] = x0 + (ref[:, 0] - x0) * stretch
     return sc, stretched
+
+
+def batched_scenes(count=256, seed=3, spacing=0.01, n_min=2048, n_max=65536, integrator="midpoint", dt=1e-4,
+                   c0=20.0, rho0=1000.0, alpha=0.1, steps=200):
+    """Independent 3D scenes for the batched form: particle counts
+    log-uniform in [n_min, n_max]; each scene a seeded mix of 1-3 Tait fluid
+    blocks and 0-2 elastic blocks (E log-uniform in [1e4, 1e6], nu = 0.3,
+    strain order 2 standing in for the Neo-Hookean model, which the reference
+    does not have) above a one-layer floor, with its own h drawn uniformly in
+    [1.5, 2.5] x spacing.  The counts include the floor."""
+    rng = np.random.default_rng(seed)
+    out = []
+    s = spacing
+    for k in range(count):
+        n_target = int(round(np.exp(rng.uniform(np.log(n_min), np.log(n_max)))))
+        h = float(rng.uniform(1.5, 2.5) * s)
+        n_fluid = int(rng.integers(1, 4))
+        n_solid = int(rng.integers(0, 3))
+        side = int(np.ceil(1.6 * n_target ** (1.0 / 3.0)))
+        box = side * s
+        floor_n = side * side
+        n_body = max(n_target - floor_n, 64)
+        shares = rng.dirichlet(np.ones(n_fluid + n_solid)) * n_body
+        mats = [immobile(0.0, mass=1.0 * s ** 3), liquid(rho0, c0, h, alpha, mass=rho0 * s ** 3)]
+        mobile = []
+        x_cursor = 0.5 * s
+        for b, share in enumerate(shares):
+            m = max(2, int(round(share ** (1.0 / 3.0))))
+            mx = min(m, side - 1)
+            my = min(max(2, int(round(share / (mx * mx)))), side - 2)
+            if x_cursor + mx * s > box:
+                x_cursor = 0.5 * s
+            z0 = 0.5 * s + rng.uniform(0, max(box - mx * s, 0) * 0.5)
+            pos = lattice((x_cursor, 0.5 * s, z0), (mx, my, mx), s)
+            pos = jitter(pos, 1e-4, rng)
+            x_cursor += (mx + 2) * s
+            if b < n_fluid:
+                mobile.append(particles(pos, 1, rho0))
+            else:
+                E = float(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
+                lam, mu = lame_from_young(E, 0.3)
+                mats.append(elastic_solid(rho0, lam, mu, mass=rho0 * s ** 3))
+                mobile.append(particles(pos, len(mats) - 1, rho0))
+        floor = lattice((0.5 * s, -0.5 * s, 0.5 * s), (side, 1, side), s)
+        out.append(Scene(particles=np.concatenate(mobile), boundary=particles(floor, 0, 1.0), materials=np.array(mats),
+                         bounds_min=(0.0, 0.0, 0.0, 0.0), bounds_dim=(box, box, box, 0.0), h=h, integrator=integrator,
+                         dt=dt, gravity=9.81, alpha=alpha, name=f"batched_{k}",
+                         meta={"steps": steps, "n_target": n_target}))
+    return out

@@ -178,6 +178,23 @@ class FluidSim:
         check(self._L.arp_sim_boundary_cells(self._h, ptr(start), ptr(members)))
         return start, members[:self.nb]
 
+    def set_graph(self, on=True):
+        """Replay pairs of steps from a captured CUDA graph."""
+        check(self._L.arp_sim_set_graph(self._h, int(bool(on))))
+
+    def autotune(self):
+        v = ctypes.c_int()
+        check(self._L.arp_sim_autotune(self._h, ctypes.byref(v)))
+        return v.value
+
+    def set_fluid_variant(self, v):
+        check(self._L.arp_sim_set_fluid_variant(self._h, int(v)))
+
+    def fluid_variant(self):
+        v, cap, pers = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._L.arp_sim_fluid_variant(self._h, ctypes.byref(v), ctypes.byref(cap), ctypes.byref(pers)))
+        return dict(variant=v.value, list_capacity=cap.value, persistent=bool(pers.value))
+
     def set_stream(self, stream_handle):
         check(self._L.arp_sim_set_stream(self._h, ctypes.c_void_p(stream_handle)))
 

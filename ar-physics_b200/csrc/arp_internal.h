@@ -67,6 +67,7 @@ struct SceneP {
     float hg_h;                       // (10 * 0.1f) * h
     float rcut, rcut2, r_geom;        // 8h, (8h)^2, h*h/(8h)
     float contact_slack;              // r_cut - largest in-stencil |dx|, 0 when unbounded
+    uint32_t solid_branch;            // the scene has more than one solid (shaders/mod.rs:51)
 };
 
 // The fields of a material the fluid pair loop reads (32 B).
@@ -203,8 +204,18 @@ struct FluidArgs {
     int solid_branch;
     int any_stiff_immobile;
 };
+// Launch shapes of the fluid kernel the autotuner chooses between: hit-list
+// capacity per thread, and one tile per block or persistent blocks taking
+// tiles from an atomic work counter.
+struct FluidVariant {
+    int cap;
+    int persistent;
+};
+constexpr int kNumFluidVariants = 6;
+extern const FluidVariant kFluidVariants[kNumFluidVariants];
+// `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
-                 cudaStream_t st);
+                 int variant, uint32_t* tile_counter, cudaStream_t st);
 
 // ---- solids (solid.cu) ------------------------------------------------------
 struct SolidRefList {

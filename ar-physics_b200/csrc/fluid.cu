@@ -20,6 +20,8 @@
 // particles) is combined into the next stage state y0 + sum c_j k_j and the
 // b-weighted accumulator with separately rounded products and sums, the same
 // order the oracle uses.
+#include <algorithm>
+
 #include "grid.cuh"
 
 namespace arp {
@@ -161,25 +163,49 @@ __device__ __forceinline__ float4 axpy(float c, float4 k, float4 t) {
 }
 
 constexpr int kFluidThreads = 128;
-constexpr int kListCap = 48;                  // hits held per thread before they are consumed
 constexpr uint32_t kBoundaryBit = 0x80000000u;
 
-template <int DIM>
-__global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
-    extern __shared__ __align__(16) unsigned char smem_raw[];
-    uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);  // [kListCap][blockDim]
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * kFluidThreads);
-    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
-    // materials and interactions of the scene of the block's first particle
-    const uint32_t k_first = min(blockIdx.x * blockDim.x, a.n - 1u);
-    const uint32_t scene0 = T.mats[__float_as_uint(a.vs[k_first].w)].scene;
-    const SceneP& sp0 = T.scenes[scene0];
-    for (uint32_t i = threadIdx.x; i < sp0.nmat; i += blockDim.x) sm[i] = T.fmats[sp0.mat_base + i];
-    for (uint32_t i = threadIdx.x; i < sp0.nmat * sp0.nmat; i += blockDim.x) si[i] = T.inter[sp0.inter_base + i];
-    __syncthreads();
+// Copy one scene's fluid materials and interaction block into shared memory.
+__device__ __forceinline__ void load_scene_tables(const Tables& T, uint32_t scene, FluidMat* sm, DevInter* si) {
+    const SceneP& sp = T.scenes[scene];
+    for (uint32_t i = threadIdx.x; i < sp.nmat; i += blockDim.x) sm[i] = T.fmats[sp.mat_base + i];
+    for (uint32_t i = threadIdx.x; i < sp.nmat * sp.nmat; i += blockDim.x) si[i] = T.inter[sp.inter_base + i];
+}
 
-    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= a.n) return;
+// Pass 2: pair terms of the listed hits, in list order; empties the list.
+template <int DIM>
+__device__ __forceinline__ void consume_hits(const uint32_t* my, uint32_t& cnt, const Self& s, const FluidArgs& a,
+                                             const PairK& K, Acc& acc) {
+    for (uint32_t e = 0; e < cnt; ++e) {
+        const uint32_t j = my[e * kFluidThreads];
+        if (j & kBoundaryBit) {
+            const uint32_t jb = j & ~kBoundaryBit;
+            const float4 xj = a.bxs[jb];
+            const float4 vj = a.bvs[jb];
+            const uint32_t mat2 = __float_as_uint(vj.w);
+            bool elastic2 = false;
+            if (a.any_stiff_immobile && s.mt[mat2 - s.mbase].stiff) {
+                // fluid.rs:227: the boundary index reads the mobile array's solid id
+                elastic2 = a.sid_of_boundary_index[a.borig[jb]] != kInvalid;
+            }
+            pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, K, acc);
+        } else {
+            const float4 xj = a.xs[j];
+            const float4 vj = a.vs[j];
+            const uint32_t mat2 = __float_as_uint(vj.w);
+            pair<DIM, false>(s, xj, vj, a.ps[j], mat2, s.mt[mat2 - s.mbase].stiff != 0u, K, acc);
+        }
+    }
+    cnt = 0;
+}
+
+// Fluid forces and the stage update of sorted particle k.  `lst` is the
+// thread's column of the hit list ([CAP][kFluidThreads]); `sm`/`si` hold the
+// tables of scene `scene0`.
+template <int DIM, int CAP>
+__device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, const Tables& T, const StageCoefs& c,
+                                               const StageBuffers& b, uint32_t* lst, const FluidMat* sm,
+                                               const DevInter* si, uint32_t scene0) {
     const float4 xi = a.xs[k];
     const float4 vi = a.vs[k];
     const uint32_t slot = a.perm ? a.perm[k] : k;
@@ -208,28 +234,13 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, 
     Acc acc;
     acc.den = 0.0f;
     acc.f = make_float3(0.0f, 0.0f, 0.0f);
-    uint32_t* my = lst + threadIdx.x;
+    uint32_t* my = lst;
     uint32_t cnt = 0;
-    auto boundary_pair = [&](uint32_t jb) {
-        const float4 xj = a.bxs[jb];
-        const float4 vj = a.bvs[jb];
-        const uint32_t mat2 = __float_as_uint(vj.w);
-        bool elastic2 = false;
-        if (a.any_stiff_immobile && s.mt[mat2 - s.mbase].stiff) {
-            // fluid.rs:227: the boundary index reads the mobile array's solid id
-            elastic2 = a.sid_of_boundary_index[a.borig[jb]] != kInvalid;
-        }
-        pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, K, acc);
-    };
-    auto mobile_pair = [&](uint32_t j) {
-        const float4 xj = a.xs[j];
-        const float4 vj = a.vs[j];
-        const uint32_t mat2 = __float_as_uint(vj.w);
-        pair<DIM, false>(s, xj, vj, a.ps[j], mat2, s.mt[mat2 - s.mbase].stiff != 0u, K, acc);
-    };
     // pass 1: candidates of the 3x3(x3) cells whose squared distance is
-    // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0)) go to
-    // the thread's list; hits past its capacity are evaluated on the spot
+    // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0)) are
+    // appended to the thread's list; a full list is consumed before scanning
+    // on, so pairs are always evaluated in candidate order whatever the
+    // list capacity
     auto hit = [&](float4 q) {
         const float rx = q.x - xi.x, ry = q.y - xi.y;
         const float r2 = DIM == 3 ? (rx * rx + ry * ry) + (q.z - xi.z) * (q.z - xi.z) : rx * rx + ry * ry;
@@ -242,39 +253,53 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, 
         const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
         const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
         const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
-        for (int z = zlo; z <= zhi; ++z) {
-            for (int y = ylo; y <= yhi; ++y) {
-                const uint32_t row = cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
-                const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
-                for (uint32_t j = bb; j < be; ++j) {
-                    if (hit(a.bxs[j])) {
-                        if (cnt < kListCap) my[cnt++ * kFluidThreads] = j | kBoundaryBit;
-                        else boundary_pair(j);
+        // resumable walk over (row, section, index): each row of the
+        // neighborhood contributes its boundary range, then its mobile range
+        int y = ylo, z = zlo;
+        bool mobile = false;
+        uint32_t j = 0, je = 0;
+        bool done = false;
+        auto open_range = [&]() {
+            const uint32_t row = cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+            const uint32_t* st = mobile ? a.start : a.bstart;
+            j = st[row + (uint32_t)x0];
+            je = st[row + (uint32_t)x1 + 1u];
+        };
+        open_range();
+        do {
+            while (cnt < CAP) {
+                if (j < je) {
+                    if (mobile) {
+                        if (j != k && hit(a.xs[j])) my[cnt++ * kFluidThreads] = j;  // self contributes zero
+                    } else if (hit(a.bxs[j])) {
+                        my[cnt++ * kFluidThreads] = j | kBoundaryBit;
                     }
-                }
-                const uint32_t jb = a.start[c0], je = a.start[c1];
-                for (uint32_t j = jb; j < je; ++j) {
-                    if (j != k && hit(a.xs[j])) {  // the particle itself contributes exactly zero
-                        if (cnt < kListCap) my[cnt++ * kFluidThreads] = j;
-                        else mobile_pair(j);
+                    ++j;
+                } else {
+                    if (!mobile) {
+                        mobile = true;
+                    } else {
+                        mobile = false;
+                        if (++y > yhi) {
+                            y = ylo;
+                            if (++z > zhi) {
+                                done = true;
+                                break;
+                            }
+                        }
                     }
+                    open_range();
                 }
             }
-        }
-        // pass 2: pair math over the collected hits
-        for (uint32_t e = 0; e < cnt; ++e) {
-            const uint32_t j = my[e * kFluidThreads];
-            if (j & kBoundaryBit) boundary_pair(j & ~kBoundaryBit);
-            else mobile_pair(j);
-        }
+            consume_hits<DIM>(my, cnt, s, a, K, acc);  // pass 2
+        } while (!done);
     }
 
     // derivative record (fluid.rs:329-333), plus the solid term when active
     float4 kpd = make_float4(vi.x, vi.y, vi.z, acc.den);
     float4 kvm = make_float4(__fdiv_rn(acc.f.x, s.d1), __fadd_rn(__fdiv_rn(acc.f.y, s.d1), -g_acc),
                              __fdiv_rn(acc.f.z, s.d1), 0.0f);
-    if (a.solid_branch && sid != kInvalid) {
+    if (a.solid_branch && sid != kInvalid && P.solid_branch) {
         const float4 ks = a.ksol[sid];
         kpd.x = __fadd_rn(kpd.x, vi.x);
         kpd.y = __fadd_rn(kpd.y, vi.y);
@@ -333,20 +358,95 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, 
     }
 }
 
+// One 128-particle tile per block.
+template <int DIM, int CAP>
+__global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * kFluidThreads);
+    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
+    const uint32_t k0 = blockIdx.x * kFluidThreads;
+    const uint32_t scene0 = T.mats[__float_as_uint(a.vs[min(k0, a.n - 1u)].w)].scene;
+    load_scene_tables(T, scene0, sm, si);
+    __syncthreads();
+    const uint32_t k = k0 + threadIdx.x;
+    if (k < a.n) fluid_particle<DIM, CAP>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+}
+
+// Persistent form: each block keeps taking the next 128-particle tile of the
+// cell-sorted, scene-concatenated order from an atomic work counter, so
+// scenes of very different sizes share the SMs without a tail of idle
+// blocks.  Blocks never wait on each other.
+template <int DIM, int CAP>
+__global__ void __launch_bounds__(kFluidThreads) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c,
+                                                                    StageBuffers b, uint32_t* tile_counter) {
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * kFluidThreads);
+    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
+    __shared__ uint32_t tile_s;
+    uint32_t loaded = kInvalid;
+    const uint32_t ntiles = (a.n + kFluidThreads - 1) / kFluidThreads;
+    for (;;) {
+        if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
+        __syncthreads();
+        const uint32_t tile = tile_s;
+        if (tile >= ntiles) break;
+        const uint32_t k0 = tile * kFluidThreads;
+        const uint32_t scene0 = T.mats[__float_as_uint(a.vs[k0].w)].scene;
+        if (scene0 != loaded) {
+            load_scene_tables(T, scene0, sm, si);
+            loaded = scene0;
+        }
+        __syncthreads();
+        const uint32_t k = k0 + threadIdx.x;
+        if (k < a.n) fluid_particle<DIM, CAP>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+        __syncthreads();
+    }
+}
+
+template <int DIM, int CAP>
+void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, bool persistent,
+                    uint32_t* tile_counter, cudaStream_t st) {
+    const size_t smem = sizeof(uint32_t) * CAP * kFluidThreads + sizeof(FluidMat) * T.max_nmat +
+                        sizeof(DevInter) * T.max_nmat * T.max_nmat;
+    if (!persistent) {
+        const uint32_t blocks = (a.n + kFluidThreads - 1) / kFluidThreads;
+        k_fluid<DIM, CAP><<<blocks, kFluidThreads, smem, st>>>(a, T, c, b);
+        return;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, CAP>, kFluidThreads, smem);
+    per_sm = per_sm > 0 ? per_sm : 1;
+    int sms = 148;
+    int dev = 0;
+    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+    const uint32_t ntiles = (a.n + kFluidThreads - 1) / kFluidThreads;
+    const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
+    cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
+    k_fluid_persistent<DIM, CAP><<<blocks, kFluidThreads, smem, st>>>(a, T, c, b, tile_counter);
+}
+
 }  // namespace
 
+const FluidVariant kFluidVariants[kNumFluidVariants] = {
+    {48, 0}, {32, 0}, {64, 0}, {48, 1}, {32, 1}, {64, 1},
+};
+
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
-                 cudaStream_t st) {
+                 int variant, uint32_t* tile_counter, cudaStream_t st) {
     if (a.n == 0) return 0;
-    const int threads = kFluidThreads;
-    const uint32_t blocks = (a.n + threads - 1) / threads;
-    const size_t smem = sizeof(uint32_t) * kListCap * kFluidThreads + sizeof(FluidMat) * T.max_nmat +
-                        sizeof(DevInter) * T.max_nmat * T.max_nmat;
-    if (kdim == 3)
-        k_fluid<3><<<blocks, threads, smem, st>>>(a, T, c, b);
-    else
-        k_fluid<2><<<blocks, threads, smem, st>>>(a, T, c, b);
-    return 1;
+    const FluidVariant v = kFluidVariants[variant < 0 || variant >= kNumFluidVariants ? 0 : variant];
+    const bool pers = v.persistent != 0;
+#define ARP_FLUID_CASE(D, C) \
+    if (kdim == D && v.cap == C) {                            \
+        launch_variant<D, C>(a, T, c, b, pers, tile_counter, st); \
+        return 1;                                                 \
+    }
+    ARP_FLUID_CASE(3, 48) ARP_FLUID_CASE(3, 32) ARP_FLUID_CASE(3, 64)
+    ARP_FLUID_CASE(2, 48) ARP_FLUID_CASE(2, 32) ARP_FLUID_CASE(2, 64)
+#undef ARP_FLUID_CASE
+    return 0;
 }
 
 }  // namespace arp

@@ -12,7 +12,10 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
+#include <mutex>
 #include <new>
+#include <tuple>
 #include <string>
 #include <vector>
 
@@ -205,6 +208,8 @@ struct arp_sim {
     DevBuf<uint32_t> g_key, g_rank, g_count, g_start, g_perm, g_bsums;
     DevBuf<uint2> g_coord, coord_s;  // grid coordinates per slot; storage-order copy for stage 0
     DevBuf<uint32_t> contact_bound;
+    DevBuf<uint32_t> tile_counter;  // work queue of the persistent fluid kernel
+    int fluid_variant = 0;
     uint32_t grid_cap = 0;
     // solids
     DevBuf<float4> ref, L, F, A, ksol;
@@ -213,6 +218,21 @@ struct arp_sim {
     DevBuf<float4> rl_gw;
     uint32_t rl_nnz = 0;
     DevBuf<DevStats> d_stats;
+
+    // CUDA graph of two integrator steps (every buffer swap of a step is
+    // undone by the next, so the captured pointers stay valid)
+    bool use_graph = false;
+    cudaGraph_t graph = nullptr;
+    cudaGraphExec_t graph_exec = nullptr;
+    cudaStream_t graph_stream = nullptr;
+    uint64_t graph_launches = 0;  // kernels per replay
+    void drop_graph() {
+        if (graph_exec) cudaGraphExecDestroy(graph_exec);
+        if (graph) cudaGraphDestroy(graph);
+        graph_exec = nullptr;
+        graph = nullptr;
+        graph_stream = nullptr;
+    }
 
     // profiling
     bool profiling = false;
@@ -225,6 +245,7 @@ struct arp_sim {
     uint64_t prof_steps = 0, prof_launches = 0, prof_l[3] = {0, 0, 0};
 
     ~arp_sim() {
+        drop_graph();
         for (auto& m : marks)
             for (auto e : m.e) ev_free.push_back(e);
         for (auto e : ev_free) cudaEventDestroy(e);
@@ -454,6 +475,8 @@ arp_status do_init(arp_sim* S) {
     return ARP_OK;
 }
 
+arp_status run_autotune(arp_sim* S, bool force);
+
 void mark(arp_sim* S, arp_sim::Mark& m, int k) {
     if (!S->profiling) return;
     m.e[k] = take_event(S);
@@ -589,7 +612,7 @@ arp_status do_step(arp_sim* S) {
         f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
         B.next_pd = next_pd;
         B.next_vm = next_vm;
-        S->launches += launch_fluid(f, S->tables, S->kdim, c, B, st);
+        S->launches += launch_fluid(f, S->tables, S->kdim, c, B, S->fluid_variant, S->tile_counter.p, st);
         mark(S, mk, 3);
         if (S->profiling) {
             S->marks.push_back(mk);
@@ -758,6 +781,11 @@ void finalize_scenes(arp_sim* S) {
             S->part_of_solid.push_back(i);
         }
     S->ns = (uint32_t)S->part_of_solid.size();
+    for (auto& H : S->scenes) {
+        uint32_t cnt = 0;
+        for (uint32_t i = H.p_base; i < H.p_base + H.n; ++i) cnt += S->sid_of_caller[i] != kInvalid;
+        H.sp.solid_branch = cnt > 1 ? 1u : 0u;
+    }
 }
 
 arp_status allocate(arp_sim* S) {
@@ -808,6 +836,7 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->ksol.alloc(ns));
     CUDA_TRY(S->coord_s.alloc(S->ns > 1 ? n : 1));
     CUDA_TRY(S->contact_bound.alloc(2));
+    CUDA_TRY(S->tile_counter.alloc(1));
     CUDA_TRY(S->ep.alloc(4 * ns));
     CUDA_TRY(S->ep_t.alloc(4 * ns));
     CUDA_TRY(S->ep_s[0].alloc(4 * ns));
@@ -859,6 +888,102 @@ arp_status allocate(arp_sim* S) {
     S->tables.inter = S->d_inter.p;
     S->tables.ncells = S->ncells;
     S->tables.max_nmat = S->max_nmat;
+    return ARP_OK;
+}
+
+// ---- autotuner -----------------------------------------------------------------
+// Chooses the fluid kernel's launch shape (hit-list capacity, one tile per
+// block or persistent tile queue) by timing every variant on the live stage-0
+// state.  All variants evaluate the same pairs in the same order, so the
+// choice changes speed, never results.  Choices are cached per (kernel
+// dimension, log2 particle count, quarter-octave of h / particle spacing).
+std::mutex g_tune_mu;
+std::map<std::tuple<int, int, int>, int> g_tune_cache;
+
+std::tuple<int, int, int> tune_key(const arp_sim* S) {
+    double acc = 0.0;
+    for (uint32_t i = 0; i < S->n; ++i) {
+        const uint32_t m = S->host_particles[i].mat;
+        const auto& H = S->scenes[S->scene_of_material[m]];
+        const double vol = (double)S->mats[m].mass / (double)S->mats[m].start_den;
+        const double spacing = vol > 0 ? std::pow(vol, 1.0 / std::max(1u, H.sp.dim)) : H.h;
+        acc += std::log2((double)H.h / spacing);
+    }
+    const double ratio = S->n ? acc / S->n : 0.0;
+    const int nbits = S->n ? (int)std::ceil(std::log2((double)S->n)) : 0;
+    return std::make_tuple(S->kdim, nbits, (int)std::lround(4.0 * ratio));
+}
+
+arp_status run_autotune(arp_sim* S, bool force) {
+    const auto key = tune_key(S);
+    if (!force) {
+        std::lock_guard<std::mutex> lock(g_tune_mu);
+        auto it = g_tune_cache.find(key);
+        if (it != g_tune_cache.end()) {
+            S->fluid_variant = it->second;
+            return ARP_OK;
+        }
+    }
+    const uint32_t n = S->n;
+    if (n == 0) return ARP_OK;
+    cudaStream_t st = S->stream;
+    // stage-0 inputs: y0 sorted into cell order (the state itself is unchanged)
+    S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, nullptr, S->b_start.p, st);
+    S->launches += gather_state(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p, S->orig_r.p,
+                                S->sid.p, S->sid_r.p, nullptr, nullptr, S->ps.p, S->d_mats.p, st);
+    std::swap(S->Y, S->T);
+    std::swap(S->orig, S->orig_r);
+    std::swap(S->sid, S->sid_r);
+    const Tableau& tab = S->tab;
+    const bool last = tab.stages == 1;
+    StageCoefs c{};
+    c.last = last ? 1 : 0;
+    if (!last) c.c_self = (float)(tab.a[1][0] * (double)S->dt_sub);
+    c.c_acc = (float)(tab.b[0] * (double)S->dt_sub);
+    c.acc_first = 1;
+    StageBuffers B{};
+    B.y0_pd = S->Y.pd.p;
+    B.y0_vm = S->Y.vm.p;
+    B.acc_pd = S->acc.pd.p;
+    B.acc_vm = S->acc.vm.p;
+    B.next_pd = last ? S->T.pd.p : S->S[0].pd.p;  // scratch at this point
+    B.next_vm = last ? S->T.vm.p : S->S[0].vm.p;
+    FluidArgs f{};
+    f.xs = S->Y.pd.p;
+    f.vs = S->Y.vm.p;
+    f.start = S->gb.start;
+    f.bxs = S->b_pd.p;
+    f.bvs = S->b_vm.p;
+    f.bstart = S->b_start.p;
+    f.sid = S->sid.p;
+    f.sid_of_boundary_index = S->sid_of_bidx.p;
+    f.borig = S->b_orig.p;
+    f.ps = S->ps.p;
+    f.bps = S->bps.p;
+    f.n = n;
+    f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
+    cudaEvent_t e0 = take_event(S), e1 = take_event(S);
+    float best = 1e30f;
+    int best_v = 0;
+    for (int v = 0; v < kNumFluidVariants; ++v) {
+        S->launches += launch_fluid(f, S->tables, S->kdim, c, B, v, S->tile_counter.p, st);  // warm-up
+        CUDA_TRY(cudaEventRecord(e0, st));
+        for (int r = 0; r < 3; ++r) S->launches += launch_fluid(f, S->tables, S->kdim, c, B, v, S->tile_counter.p, st);
+        CUDA_TRY(cudaEventRecord(e1, st));
+        CUDA_TRY(cudaEventSynchronize(e1));
+        float ms = 0;
+        CUDA_TRY(cudaEventElapsedTime(&ms, e0, e1));
+        if (ms < best) {
+            best = ms;
+            best_v = v;
+        }
+    }
+    S->ev_free.push_back(e0);
+    S->ev_free.push_back(e1);
+    ARP_TRY(check_launch("autotune"));
+    S->fluid_variant = best_v;
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune_cache[key] = best_v;
     return ARP_OK;
 }
 
@@ -949,12 +1074,86 @@ arp_status arp_sim_destroy(arp_sim* sim) {
 
 arp_status arp_sim_init(arp_sim* sim) {
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
-    return do_init(sim);
+    ARP_TRY(do_init(sim));
+    return run_autotune(sim, false);
+}
+
+arp_status arp_sim_autotune(arp_sim* sim, int* variant) {
+    ARP_TRY(need_init(sim));
+    sim->drop_graph();
+    ARP_TRY(run_autotune(sim, true));
+    if (variant) *variant = sim->fluid_variant;
+    return ARP_OK;
+}
+
+arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (variant < 0 || variant >= kNumFluidVariants) return fail(ARP_ERR_INVALID_ARG, "variant out of range");
+    sim->drop_graph();
+    sim->fluid_variant = variant;
+    return ARP_OK;
+}
+
+arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* list_capacity, int* persistent) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (variant) *variant = sim->fluid_variant;
+    if (list_capacity) *list_capacity = kFluidVariants[sim->fluid_variant].cap;
+    if (persistent) *persistent = kFluidVariants[sim->fluid_variant].persistent;
+    return ARP_OK;
+}
+
+// Capture two steps into a graph on the handle's stream.  Host-side effects
+// of the captured steps (time, launch count) are applied per replay instead.
+arp_status capture_graph(arp_sim* S) {
+    S->drop_graph();
+    const float t0 = S->time;
+    const uint64_t l0 = S->launches;
+    const bool prof = S->profiling;
+    S->profiling = false;
+    CUDA_TRY(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
+    arp_status st = do_step(S);
+    if (st == ARP_OK) st = do_step(S);
+    cudaGraph_t g = nullptr;
+    cudaError_t e = cudaStreamEndCapture(S->stream, &g);
+    S->profiling = prof;
+    S->time = t0;
+    S->graph_launches = S->launches - l0;
+    S->launches = l0;
+    if (st != ARP_OK) {
+        if (g) cudaGraphDestroy(g);
+        return st;
+    }
+    if (e != cudaSuccess) return fail(ARP_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    S->graph = g;
+    e = cudaGraphInstantiate(&S->graph_exec, g, 0);
+    if (e != cudaSuccess) {
+        S->drop_graph();
+        return fail(ARP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
+    }
+    S->graph_stream = S->stream;
+    return ARP_OK;
 }
 
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
     ARP_TRY(need_init(sim));
-    for (uint32_t i = 0; i < nsteps; ++i) ARP_TRY(do_step(sim));
+    uint32_t i = 0;
+    if (sim->use_graph && !sim->profiling && nsteps >= 2) {
+        if (!sim->graph_exec || sim->graph_stream != sim->stream) ARP_TRY(capture_graph(sim));
+        for (; i + 2 <= nsteps; i += 2) {
+            CUDA_TRY(cudaGraphLaunch(sim->graph_exec, sim->stream));
+            sim->time += sim->dt_sub;
+            sim->time += sim->dt_sub;
+            sim->launches += sim->graph_launches;
+        }
+    }
+    for (; i < nsteps; ++i) ARP_TRY(do_step(sim));
+    return ARP_OK;
+}
+
+arp_status arp_sim_set_graph(arp_sim* sim, int enable) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (!enable) sim->drop_graph();
+    sim->use_graph = enable != 0;
     return ARP_OK;
 }
 
@@ -1161,6 +1360,7 @@ arp_status arp_sim_set_stream(arp_sim* sim, void* stream) {
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
     CUDA_TRY(cudaStreamSynchronize(sim->stream));
     sim->stream = stream ? (cudaStream_t)stream : sim->own_stream;
+    if (sim->graph_stream != sim->stream) sim->drop_graph();
     return ARP_OK;
 }
 

@@ -216,6 +216,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
     const float4 vi = a.vm[slot];
     const DevMat mm = T.mats[__float_as_uint(vi.w)];
     const SceneP& P = T.scenes[mm.scene];
+    if (!P.solid_branch) return;  // a scene with a single solid skips the solid term
     const float4 L0 = a.L[3 * i], L1 = a.L[3 * i + 1], L2 = a.L[3 * i + 2];
     // strain.rs:139-160: F = sum V dx (x) (L gradW), Fdot likewise with dv
     float F[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
@@ -361,6 +362,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
     const uint32_t mat = __float_as_uint(a.vm[slot].w);
     const DevMat mm = T.mats[mat];
     const SceneP& P = T.scenes[mm.scene];
+    if (!P.solid_branch) return;
     const float m1 = mm.mass, d1 = xi.w;
     const float V1 = m1 / d1;
     const float4 Ai0 = a.A[3 * i], Ai1 = a.A[3 * i + 1], Ai2 = a.A[3 * i + 2];
