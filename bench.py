@@ -147,6 +147,56 @@ def cpu_baseline(sc, max_seconds=20.0, max_steps=5):
                       f"(C++ oracle, float, OpenMP x{cores})", "seconds": dt}
 
 
+def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
+    """256 independent scenes (2,048-65,536 particles each, own h, fluid
+    blocks and elastic blocks): stepped as one batch (one set of launches per
+    stage, replayed from a CUDA graph) and as a loop over 256 separate
+    simulations, both on one GPU."""
+    from arphys import FluidSim, scenes
+    scs = scenes.batched_scenes()
+    parts = int(sum(sc.n + sc.nb for sc in scs))
+    batch = FluidSim.batch(scs)
+    batch.init()
+    batch.set_stream(stream.cuda_stream)
+    batch.set_graph(True)
+    batch.step(4)
+    torch.cuda.synchronize()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    batch.step(steps_batch)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_batch = e0.elapsed_time(e1) / 1000.0
+    variant = batch.fluid_variant()
+    batch.close()
+    sims = []
+    for sc in scs:
+        sim = FluidSim(sc)
+        sim.init()
+        sim.set_stream(stream.cuda_stream)
+        sims.append(sim)
+    for sim in sims:
+        sim.step(1)
+    torch.cuda.synchronize()
+    e0.record(stream)
+    for _ in range(rounds_loop):
+        for sim in sims:
+            sim.step(1)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_loop = e0.elapsed_time(e1) / 1000.0
+    for sim in sims:
+        sim.close()
+    batched = len(scs) * steps_batch / t_batch
+    loop = len(scs) * rounds_loop / t_loop
+    return {"scenes": len(scs), "particles": parts, "integrator": "rk2",
+            "scene_steps_per_s": batched, "particle_steps_per_s": parts * steps_batch / t_batch,
+            "ms_per_step": t_batch * 1000.0 / steps_batch,
+            "per_scene_loop_scene_steps_per_s": loop, "speedup_vs_per_scene_loop": batched / loop,
+            "fluid_launch_shape": variant,
+            "note": "working set > L2 (no flush); batch replayed from a CUDA graph; loop = one simulation per scene"}
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference's path cannot run here (Rust + OpenGL
     compute shaders, no GL stack), so the CPU restatement of its shaders is
@@ -275,6 +325,9 @@ def run_ours(args, rank, world, local_rank):
         "config": dict(config_of(sc, args.config), parallelism=f"replicas x{world}"),
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
     }
+    line["fluid_launch_shape"] = sim.fluid_variant()
+    if rank == 0 and not args.no_batched:
+        line["batched"] = run_batched(torch, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(sc)
     if rank == 0:
@@ -290,6 +343,7 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--config", default="c2", choices=["c1", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--no-batched", action="store_true")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
