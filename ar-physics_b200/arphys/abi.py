@@ -69,7 +69,7 @@ class ArpProfile(ctypes.Structure):
         ("steps", ctypes.c_uint64), ("launches", ctypes.c_uint64),
         ("neighbor_ms", ctypes.c_double), ("solid_ms", ctypes.c_double), ("fluid_ms", ctypes.c_double),
         ("integrate_ms", ctypes.c_double), ("fluid_launches", ctypes.c_uint64),
-        ("neighbor_launches", ctypes.c_uint64), ("solid_launches", ctypes.c_uint64),
+        ("neighbor_launches", ctypes.c_uint64), ("solid_launches", ctypes.c_uint64), ("stages", ctypes.c_uint64),
     ]
 
 

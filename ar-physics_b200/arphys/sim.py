@@ -191,9 +191,9 @@ class FluidSim:
         check(self._L.arp_sim_set_fluid_variant(self._h, int(v)))
 
     def fluid_variant(self):
-        v, cap, pers = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
-        check(self._L.arp_sim_fluid_variant(self._h, ctypes.byref(v), ctypes.byref(cap), ctypes.byref(pers)))
-        return dict(variant=v.value, list_capacity=cap.value, persistent=bool(pers.value))
+        v, blk, pers = ctypes.c_int(), ctypes.c_int(), ctypes.c_int()
+        check(self._L.arp_sim_fluid_variant(self._h, ctypes.byref(v), ctypes.byref(blk), ctypes.byref(pers)))
+        return dict(variant=v.value, block=blk.value, persistent=bool(pers.value))
 
     def set_stream(self, stream_handle):
         check(self._L.arp_sim_set_stream(self._h, ctypes.c_void_p(stream_handle)))

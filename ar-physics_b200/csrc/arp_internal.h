@@ -43,8 +43,9 @@ struct DevMat {
     float work_hardening_exp, kinematic_hardening, relaxation_time, vol0;  // vol0 = mass / start_den
     uint32_t state_eq, stiff, plastic;
     int32_t strain_order;
-    uint32_t scene;   // scene the material belongs to
-    uint32_t local;   // index inside that scene's material list
+    uint32_t scene;       // scene the material belongs to
+    uint32_t local;       // index inside that scene's material list
+    uint32_t solid_base;  // first batch-wide solid id of that scene
 };
 
 struct DevInter {
@@ -200,18 +201,21 @@ struct FluidArgs {
     const float* ps;         // p / rho^2 of each sorted particle
     const float* bps;        // p / rho^2 of each sorted boundary particle
     const float4* ksol;      // per-solid solid-term acceleration (nullptr when the solid branch is off)
+    uint32_t* overflow;        // [n] particles whose hit list filled up
+    uint32_t* overflow_count;  // their number (cleared before each launch)
     uint32_t n;
     int solid_branch;
     int any_stiff_immobile;
 };
-// Launch shapes of the fluid kernel the autotuner chooses between: hit-list
-// capacity per thread, and one tile per block or persistent blocks taking
-// tiles from an atomic work counter.
+// Launch shapes of the fluid kernel the autotuner chooses between: threads
+// per block, and one tile per block or persistent blocks taking tiles from
+// an atomic work counter.  Every shape evaluates the same pairs in the same
+// order, so results do not depend on the choice.
 struct FluidVariant {
-    int cap;
+    int block;
     int persistent;
 };
-constexpr int kNumFluidVariants = 6;
+constexpr int kNumFluidVariants = 4;
 extern const FluidVariant kFluidVariants[kNumFluidVariants];
 // `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,

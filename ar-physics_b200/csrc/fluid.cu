@@ -56,13 +56,12 @@ struct Self {
     float3 x, v;
     float d1, m1, pterm1, f1, bf1;
     uint32_t mat;     // global material id
-    uint32_t li;      // index inside its scene's material list
     bool elastic;
-    // material and interaction tables of the particle's scene: shared-memory
-    // copies for the block's first scene, global tables otherwise
+    // material table and interaction row of the particle's scene, indexed by
+    // the neighbor's global material id (shared-memory copies for the block's
+    // first scene, the global tables otherwise)
     const FluidMat* mt;
     const DevInter* it;
-    uint32_t mbase, nm;
 };
 
 struct Acc {
@@ -87,15 +86,14 @@ __device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, float 
     const float gx = gws * rx, gy = gws * ry, gz = gws * rz;
     const float vx = vj.x - s.v.x, vy = vj.y - s.v.y, vz = DIM == 3 ? vj.z - s.v.z : 0.0f;
     const float d2 = xj.w;
-    const uint32_t lj = mat2 - s.mbase;
-    const FluidMat m2 = s.mt[lj];
+    const FluidMat m2 = s.mt[mat2];
     const float vgw = DIM == 3 ? (vx * gx + vy * gy) + vz * gz : vx * gx + vy * gy;
     if (!BOUNDARY) acc.den += m2.mass * vgw;
     const float pf = s.m1 * m2.mass * (s.pterm1 + ptj);
     acc.f.x += pf * gx;
     acc.f.y += pf * gy;
     acc.f.z += pf * gz;
-    const DevInter it = s.it[s.li * s.nm + lj];
+    const DevInter it = s.it[mat2];
     if (it.potential != ARP_CONTACT_ZERO) {
         const float cp = contact_potential(it.potential, sqrtf(r2), it.radius, it.strength);
         if (cp != 0.0f) {
@@ -162,7 +160,7 @@ __device__ __forceinline__ float4 axpy(float c, float4 k, float4 t) {
                        __fadd_rn(t.z, __fmul_rn(c, k.z)), __fadd_rn(t.w, __fmul_rn(c, k.w)));
 }
 
-constexpr int kFluidThreads = 128;
+constexpr int kListCap = 48;                  // hits held per thread before they are consumed
 constexpr uint32_t kBoundaryBit = 0x80000000u;
 
 // Copy one scene's fluid materials and interaction block into shared memory.
@@ -172,37 +170,37 @@ __device__ __forceinline__ void load_scene_tables(const Tables& T, uint32_t scen
     for (uint32_t i = threadIdx.x; i < sp.nmat * sp.nmat; i += blockDim.x) si[i] = T.inter[sp.inter_base + i];
 }
 
-// Pass 2: pair terms of the listed hits, in list order; empties the list.
+// Pair terms of one hit: a boundary particle (index | kBoundaryBit) or a
+// mobile one.
 template <int DIM>
-__device__ __forceinline__ void consume_hits(const uint32_t* my, uint32_t& cnt, const Self& s, const FluidArgs& a,
-                                             const PairK& K, Acc& acc) {
-    for (uint32_t e = 0; e < cnt; ++e) {
-        const uint32_t j = my[e * kFluidThreads];
-        if (j & kBoundaryBit) {
-            const uint32_t jb = j & ~kBoundaryBit;
-            const float4 xj = a.bxs[jb];
-            const float4 vj = a.bvs[jb];
-            const uint32_t mat2 = __float_as_uint(vj.w);
-            bool elastic2 = false;
-            if (a.any_stiff_immobile && s.mt[mat2 - s.mbase].stiff) {
-                // fluid.rs:227: the boundary index reads the mobile array's solid id
-                elastic2 = a.sid_of_boundary_index[a.borig[jb]] != kInvalid;
-            }
-            pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, K, acc);
-        } else {
-            const float4 xj = a.xs[j];
-            const float4 vj = a.vs[j];
-            const uint32_t mat2 = __float_as_uint(vj.w);
-            pair<DIM, false>(s, xj, vj, a.ps[j], mat2, s.mt[mat2 - s.mbase].stiff != 0u, K, acc);
+__device__ __forceinline__ void eval_hit(uint32_t j, const Self& s, const FluidArgs& a, const PairK& K, Acc& acc) {
+    if (j & kBoundaryBit) {
+        const uint32_t jb = j & ~kBoundaryBit;
+        const float4 xj = a.bxs[jb];
+        const float4 vj = a.bvs[jb];
+        const uint32_t mat2 = __float_as_uint(vj.w);
+        bool elastic2 = false;
+        if (a.any_stiff_immobile && s.mt[mat2].stiff) {
+            // fluid.rs:227: the boundary index reads the mobile array's solid id
+            elastic2 = a.sid_of_boundary_index[a.borig[jb]] != kInvalid;
         }
+        pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, K, acc);
+    } else {
+        const float4 xj = a.xs[j];
+        const float4 vj = a.vs[j];
+        const uint32_t mat2 = __float_as_uint(vj.w);
+        pair<DIM, false>(s, xj, vj, a.ps[j], mat2, s.mt[mat2].stiff != 0u, K, acc);
     }
-    cnt = 0;
 }
 
 // Fluid forces and the stage update of sorted particle k.  `lst` is the
-// thread's column of the hit list ([CAP][kFluidThreads]); `sm`/`si` hold the
+// thread's column of the hit list ([kListCap][BLOCK]); `sm`/`si` hold the
 // tables of scene `scene0`.
-template <int DIM, int CAP>
+// DIRECT: evaluate every hit during the scan (the overflow kernel) instead
+// of through the list; a list that fills up hands the particle to that kernel
+// through the overflow queue and writes nothing.  Either way the pairs are
+// summed in candidate order.
+template <int DIM, int BLOCK, bool DIRECT>
 __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, const Tables& T, const StageCoefs& c,
                                                const StageBuffers& b, uint32_t* lst, const FluidMat* sm,
                                                const DevInter* si, uint32_t scene0) {
@@ -218,13 +216,12 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     const SceneP& P = T.scenes[scene];
     const PairK K{P.h2, P.kconst, P.eps_hh};
     const float g_acc = P.g;
-    s.mbase = P.mat_base;
-    s.nm = P.nmat;
-    s.li = s.mat - P.mat_base;
-    s.mt = scene == scene0 ? sm : T.fmats + P.mat_base;
-    s.it = scene == scene0 ? si : T.inter + P.inter_base;
+    const uint32_t li = s.mat - P.mat_base;
+    // pre-offset so that [global id] lands on the scene's entry
+    s.mt = (scene == scene0 ? sm : T.fmats + P.mat_base) - P.mat_base;
+    s.it = (scene == scene0 ? si : T.inter + P.inter_base) + li * P.nmat - P.mat_base;
     s.d1 = xi.w;
-    const FluidMat m1 = s.mt[s.li];
+    const FluidMat m1 = s.mt[s.mat];
     s.m1 = m1.mass;
     s.f1 = m1.visc;
     s.bf1 = m1.bulk;
@@ -236,15 +233,22 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     acc.f = make_float3(0.0f, 0.0f, 0.0f);
     uint32_t* my = lst;
     uint32_t cnt = 0;
+    bool full = false;
     // pass 1: candidates of the 3x3(x3) cells whose squared distance is
-    // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0)) are
-    // appended to the thread's list; a full list is consumed before scanning
-    // on, so pairs are always evaluated in candidate order whatever the
-    // list capacity
+    // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0))
     auto hit = [&](float4 q) {
         const float rx = q.x - xi.x, ry = q.y - xi.y;
         const float r2 = DIM == 3 ? (rx * rx + ry * ry) + (q.z - xi.z) * (q.z - xi.z) : rx * rx + ry * ry;
         return K.h2 - r2 > 0.0f;
+    };
+    auto take = [&](uint32_t j) {
+        if (DIRECT) {
+            eval_hit<DIM>(j, s, a, K, acc);
+        } else if (cnt < kListCap) {
+            my[cnt++ * BLOCK] = j;
+        } else {
+            full = true;
+        }
     };
     if (finite3(xi)) {
         const Grid g = P.grid;
@@ -253,46 +257,26 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
         const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
         const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
         const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
-        // resumable walk over (row, section, index): each row of the
-        // neighborhood contributes its boundary range, then its mobile range
-        int y = ylo, z = zlo;
-        bool mobile = false;
-        uint32_t j = 0, je = 0;
-        bool done = false;
-        auto open_range = [&]() {
-            const uint32_t row = cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-            const uint32_t* st = mobile ? a.start : a.bstart;
-            j = st[row + (uint32_t)x0];
-            je = st[row + (uint32_t)x1 + 1u];
-        };
-        open_range();
-        do {
-            while (cnt < CAP) {
-                if (j < je) {
-                    if (mobile) {
-                        if (j != k && hit(a.xs[j])) my[cnt++ * kFluidThreads] = j;  // self contributes zero
-                    } else if (hit(a.bxs[j])) {
-                        my[cnt++ * kFluidThreads] = j | kBoundaryBit;
-                    }
-                    ++j;
-                } else {
-                    if (!mobile) {
-                        mobile = true;
-                    } else {
-                        mobile = false;
-                        if (++y > yhi) {
-                            y = ylo;
-                            if (++z > zhi) {
-                                done = true;
-                                break;
-                            }
-                        }
-                    }
-                    open_range();
-                }
+        for (int z = zlo; z <= zhi && !full; ++z) {
+            for (int y = ylo; y <= yhi && !full; ++y) {
+                const uint32_t row = cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
+                const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
+                for (uint32_t j = bb; j < be; ++j)
+                    if (hit(a.bxs[j])) take(j | kBoundaryBit);
+                const uint32_t jb = a.start[c0], je = a.start[c1];
+                for (uint32_t j = jb; j < je; ++j)
+                    if (j != k && hit(a.xs[j])) take(j);  // the particle itself contributes exactly zero
             }
-            consume_hits<DIM>(my, cnt, s, a, K, acc);  // pass 2
-        } while (!done);
+        }
+        if (!DIRECT) {
+            if (full) {
+                a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
+                return;
+            }
+            // pass 2: pair math over the collected hits
+            for (uint32_t e = 0; e < cnt; ++e) eval_hit<DIM>(my[e * BLOCK], s, a, K, acc);
+        }
     }
 
     // derivative record (fluid.rs:329-333), plus the solid term when active
@@ -358,41 +342,41 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     }
 }
 
-// One 128-particle tile per block.
-template <int DIM, int CAP>
-__global__ void __launch_bounds__(kFluidThreads) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+// One tile of BLOCK sorted particles per block.
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * kFluidThreads);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * BLOCK);
     DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
-    const uint32_t k0 = blockIdx.x * kFluidThreads;
+    const uint32_t k0 = blockIdx.x * BLOCK;
     const uint32_t scene0 = T.mats[__float_as_uint(a.vs[min(k0, a.n - 1u)].w)].scene;
     load_scene_tables(T, scene0, sm, si);
     __syncthreads();
     const uint32_t k = k0 + threadIdx.x;
-    if (k < a.n) fluid_particle<DIM, CAP>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+    if (k < a.n) fluid_particle<DIM, BLOCK, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
 }
 
-// Persistent form: each block keeps taking the next 128-particle tile of the
-// cell-sorted, scene-concatenated order from an atomic work counter, so
-// scenes of very different sizes share the SMs without a tail of idle
-// blocks.  Blocks never wait on each other.
-template <int DIM, int CAP>
-__global__ void __launch_bounds__(kFluidThreads) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c,
-                                                                    StageBuffers b, uint32_t* tile_counter) {
+// Persistent form: each block keeps taking the next tile of the cell-sorted,
+// scene-concatenated order from an atomic work counter, so scenes of very
+// different sizes share the SMs without a tail of idle blocks.  Blocks never
+// wait on each other.
+template <int DIM, int BLOCK>
+__global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
+                                                            uint32_t* tile_counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * kFluidThreads);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * BLOCK);
     DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
     __shared__ uint32_t tile_s;
     uint32_t loaded = kInvalid;
-    const uint32_t ntiles = (a.n + kFluidThreads - 1) / kFluidThreads;
+    const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
     for (;;) {
         if (threadIdx.x == 0) tile_s = atomicAdd(tile_counter, 1u);
         __syncthreads();
         const uint32_t tile = tile_s;
         if (tile >= ntiles) break;
-        const uint32_t k0 = tile * kFluidThreads;
+        const uint32_t k0 = tile * BLOCK;
         const uint32_t scene0 = T.mats[__float_as_uint(a.vs[k0].w)].scene;
         if (scene0 != loaded) {
             load_scene_tables(T, scene0, sm, si);
@@ -400,37 +384,52 @@ __global__ void __launch_bounds__(kFluidThreads) k_fluid_persistent(FluidArgs a,
         }
         __syncthreads();
         const uint32_t k = k0 + threadIdx.x;
-        if (k < a.n) fluid_particle<DIM, CAP>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+        if (k < a.n) fluid_particle<DIM, BLOCK, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
         __syncthreads();
     }
 }
 
-template <int DIM, int CAP>
+// Particles whose hit list filled up, one thread each, evaluating their
+// pairs during the scan.
+template <int DIM>
+__global__ void __launch_bounds__(128) k_fluid_overflow(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    const uint32_t cnt = *a.overflow_count;
+    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
+        fluid_particle<DIM, 128, true>(a.overflow[i], a, T, c, b, nullptr, nullptr, nullptr, kInvalid);
+}
+
+template <int DIM, int BLOCK>
 void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, bool persistent,
                     uint32_t* tile_counter, cudaStream_t st) {
-    const size_t smem = sizeof(uint32_t) * CAP * kFluidThreads + sizeof(FluidMat) * T.max_nmat +
+    const size_t smem = sizeof(uint32_t) * kListCap * BLOCK + sizeof(FluidMat) * T.max_nmat +
                         sizeof(DevInter) * T.max_nmat * T.max_nmat;
-    if (!persistent) {
-        const uint32_t blocks = (a.n + kFluidThreads - 1) / kFluidThreads;
-        k_fluid<DIM, CAP><<<blocks, kFluidThreads, smem, st>>>(a, T, c, b);
-        return;
+    if (smem > 48 * 1024) {
+        cudaFuncSetAttribute(k_fluid<DIM, BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_fluid_persistent<DIM, BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, CAP>, kFluidThreads, smem);
-    per_sm = per_sm > 0 ? per_sm : 1;
+    const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
     int sms = 148;
     int dev = 0;
     if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
-    const uint32_t ntiles = (a.n + kFluidThreads - 1) / kFluidThreads;
+    cudaMemsetAsync(a.overflow_count, 0, sizeof(uint32_t), st);
+    if (!persistent) {
+        k_fluid<DIM, BLOCK><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
+        k_fluid_overflow<DIM><<<sms, 128, 0, st>>>(a, T, c, b);
+        return;
+    }
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, BLOCK>, BLOCK, smem);
+    per_sm = per_sm > 0 ? per_sm : 1;
     const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
     cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
-    k_fluid_persistent<DIM, CAP><<<blocks, kFluidThreads, smem, st>>>(a, T, c, b, tile_counter);
+    k_fluid_persistent<DIM, BLOCK><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
+    k_fluid_overflow<DIM><<<sms, 128, 0, st>>>(a, T, c, b);
 }
 
 }  // namespace
 
 const FluidVariant kFluidVariants[kNumFluidVariants] = {
-    {48, 0}, {32, 0}, {64, 0}, {48, 1}, {32, 1}, {64, 1},
+    {128, 0}, {256, 0}, {128, 1}, {256, 1},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -438,15 +437,14 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
     if (a.n == 0) return 0;
     const FluidVariant v = kFluidVariants[variant < 0 || variant >= kNumFluidVariants ? 0 : variant];
     const bool pers = v.persistent != 0;
-#define ARP_FLUID_CASE(D, C) \
-    if (kdim == D && v.cap == C) {                            \
-        launch_variant<D, C>(a, T, c, b, pers, tile_counter, st); \
-        return 1;                                                 \
+    if (kdim == 3) {
+        if (v.block == 256) launch_variant<3, 256>(a, T, c, b, pers, tile_counter, st);
+        else launch_variant<3, 128>(a, T, c, b, pers, tile_counter, st);
+    } else {
+        if (v.block == 256) launch_variant<2, 256>(a, T, c, b, pers, tile_counter, st);
+        else launch_variant<2, 128>(a, T, c, b, pers, tile_counter, st);
     }
-    ARP_FLUID_CASE(3, 48) ARP_FLUID_CASE(3, 32) ARP_FLUID_CASE(3, 64)
-    ARP_FLUID_CASE(2, 48) ARP_FLUID_CASE(2, 32) ARP_FLUID_CASE(2, 64)
-#undef ARP_FLUID_CASE
-    return 0;
+    return 2;  // the tile kernel and the overflow kernel
 }
 
 }  // namespace arp

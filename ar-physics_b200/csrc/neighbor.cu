@@ -264,8 +264,10 @@ __global__ void k_soa_to_records(const float4* __restrict__ pd, const float4* __
     if (k >= n) return;
     const float4 p = pd[k], v = vm[k];
     float4* r = reinterpret_cast<float4*>(out + orig[k]);
-    const uint32_t local = mats[__float_as_uint(v.w)].local;  // the scene's own material index
-    r[0] = make_float4(p.w, __uint_as_float(local), __uint_as_float(sid[k]), 0.0f);
+    const DevMat& m = mats[__float_as_uint(v.w)];
+    const uint32_t sk = sid[k];
+    // the scene's own material index and solid id
+    r[0] = make_float4(p.w, __uint_as_float(m.local), __uint_as_float(sk == kInvalid ? sk : sk - m.solid_base), 0.0f);
     r[1] = make_float4(p.x, p.y, p.z, pos_w);
     r[2] = make_float4(v.x, v.y, v.z, 0.0f);
 }

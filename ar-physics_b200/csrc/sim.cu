@@ -153,6 +153,7 @@ struct arp_sim {
         uint32_t b_base, nb;      // boundary range
         uint32_t mat_base, nmat;  // global material range
         uint32_t inter_base;      // interaction block (nmat x nmat)
+        uint32_t s_base;          // first batch-wide solid id
         bool flat_z;              // every particle shares one z and moves in the plane
         arp_aabb bounds;
         float h, gravity, alpha;
@@ -209,6 +210,7 @@ struct arp_sim {
     DevBuf<uint2> g_coord, coord_s;  // grid coordinates per slot; storage-order copy for stage 0
     DevBuf<uint32_t> contact_bound;
     DevBuf<uint32_t> tile_counter;  // work queue of the persistent fluid kernel
+    DevBuf<uint32_t> overflow, overflow_count;  // particles with more hits than the fluid list holds
     int fluid_variant = 0;
     uint32_t grid_cap = 0;
     // solids
@@ -242,7 +244,7 @@ struct arp_sim {
     };
     std::vector<Mark> marks;
     double acc_ms[3] = {0, 0, 0};  // neighbor, solid, fluid
-    uint64_t prof_steps = 0, prof_launches = 0, prof_l[3] = {0, 0, 0};
+    uint64_t prof_steps = 0, prof_stages = 0, prof_launches = 0, prof_l[3] = {0, 0, 0};
 
     ~arp_sim() {
         drop_graph();
@@ -609,16 +611,20 @@ arp_status do_step(arp_sim* S) {
         f.ksol = sb ? S->ksol.p : nullptr;
         f.n = n;
         f.solid_branch = sb ? 1 : 0;
+        f.overflow = S->overflow.p;
+        f.overflow_count = S->overflow_count.p;
         f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
         B.next_pd = next_pd;
         B.next_vm = next_vm;
-        S->launches += launch_fluid(f, S->tables, S->kdim, c, B, S->fluid_variant, S->tile_counter.p, st);
+        const int fl = launch_fluid(f, S->tables, S->kdim, c, B, S->fluid_variant, S->tile_counter.p, st);
+        S->launches += fl;
         mark(S, mk, 3);
         if (S->profiling) {
             S->marks.push_back(mk);
             S->prof_l[0] += nl;
             S->prof_l[1] += sl;
-            S->prof_l[2] += 1;
+            S->prof_l[2] += (uint64_t)fl;
+            S->prof_stages++;
             nl = 0;
             mk = arp_sim::Mark{};
             if (S->marks.size() > 256) harvest_marks(S);
@@ -781,10 +787,13 @@ void finalize_scenes(arp_sim* S) {
             S->part_of_solid.push_back(i);
         }
     S->ns = (uint32_t)S->part_of_solid.size();
+    uint32_t base = 0;
     for (auto& H : S->scenes) {
         uint32_t cnt = 0;
         for (uint32_t i = H.p_base; i < H.p_base + H.n; ++i) cnt += S->sid_of_caller[i] != kInvalid;
         H.sp.solid_branch = cnt > 1 ? 1u : 0u;
+        H.s_base = base;
+        base += cnt;
     }
 }
 
@@ -837,6 +846,8 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->coord_s.alloc(S->ns > 1 ? n : 1));
     CUDA_TRY(S->contact_bound.alloc(2));
     CUDA_TRY(S->tile_counter.alloc(1));
+    CUDA_TRY(S->overflow.alloc(n));
+    CUDA_TRY(S->overflow_count.alloc(1));
     CUDA_TRY(S->ep.alloc(4 * ns));
     CUDA_TRY(S->ep_t.alloc(4 * ns));
     CUDA_TRY(S->ep_s[0].alloc(4 * ns));
@@ -861,6 +872,7 @@ arp_status allocate(arp_sim* S) {
         d.strain_order = m.strain_order;
         d.scene = S->scene_of_material[i];
         d.local = i - S->scenes[d.scene].mat_base;
+        d.solid_base = S->scenes[d.scene].s_base;
         dm[i] = d;
     }
     CUDA_TRY(S->d_mats.alloc(S->M));
@@ -962,6 +974,8 @@ arp_status run_autotune(arp_sim* S, bool force) {
     f.bps = S->bps.p;
     f.n = n;
     f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
+    f.overflow = S->overflow.p;
+    f.overflow_count = S->overflow_count.p;
     cudaEvent_t e0 = take_event(S), e1 = take_event(S);
     float best = 1e30f;
     int best_v = 0;
@@ -1094,10 +1108,10 @@ arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant) {
     return ARP_OK;
 }
 
-arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* list_capacity, int* persistent) {
+arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent) {
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
     if (variant) *variant = sim->fluid_variant;
-    if (list_capacity) *list_capacity = kFluidVariants[sim->fluid_variant].cap;
+    if (block) *block = kFluidVariants[sim->fluid_variant].block;
     if (persistent) *persistent = kFluidVariants[sim->fluid_variant].persistent;
     return ARP_OK;
 }
@@ -1196,8 +1210,10 @@ arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap) 
     if (!sim->initialized) {
         std::memcpy(out, sim->host_particles.data(), sim->n * sizeof(arp_particle));
         for (uint32_t i = 0; i < sim->n; ++i) {
-            out[i].solid_id = sim->sid_of_caller[i];
-            out[i].mat -= sim->scenes[sim->scene_of_material[out[i].mat]].mat_base;
+            const auto& H = sim->scenes[sim->scene_of_material[out[i].mat]];
+            const uint32_t sg = sim->sid_of_caller[i];
+            out[i].solid_id = sg == kInvalid ? sg : sg - H.s_base;
+            out[i].mat -= H.mat_base;
         }
         return ARP_OK;
     }
@@ -1222,8 +1238,9 @@ arp_status arp_sim_get_solids(arp_sim* sim, arp_solid_particle* out, uint32_t ca
     for (uint32_t s = 0; s < ns; ++s) {
         arp_solid_particle& r = out[s];
         std::memset(&r, 0, sizeof(r));
-        r.part_id = sim->part_of_solid[s];
-        const arp_particle& p = sim->host_particles[r.part_id];
+        const uint32_t caller = sim->part_of_solid[s];
+        const arp_particle& p = sim->host_particles[caller];
+        r.part_id = caller - sim->scenes[sim->scene_of_material[p.mat]].p_base;  // index inside its scene
         for (int a = 0; a < 3; ++a) r.ref_pos[a] = p.pos[a];
         r.ref_pos[3] = sim->pos_w;
         for (int c = 0; c < 4; ++c) {
@@ -1381,6 +1398,7 @@ arp_status arp_sim_profile_read(arp_sim* sim, arp_profile* out) {
     if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
     harvest_marks(sim);
     out->steps = sim->prof_steps;
+    out->stages = sim->prof_stages;
     out->launches = sim->prof_l[0] + sim->prof_l[1] + sim->prof_l[2];
     out->neighbor_ms = sim->acc_ms[0];
     out->solid_ms = sim->acc_ms[1];
@@ -1392,6 +1410,7 @@ arp_status arp_sim_profile_read(arp_sim* sim, arp_profile* out) {
     for (double& x : sim->acc_ms) x = 0;
     for (auto& x : sim->prof_l) x = 0;
     sim->prof_steps = 0;
+    sim->prof_stages = 0;
     return ARP_OK;
 }
 

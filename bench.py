@@ -307,8 +307,8 @@ def run_ours(args, rank, world, local_rank):
            "path": "arp_sim_set_particles (host Particle records) + arp_sim_step(1) + arp_sim_get_particles"}
 
     peak, peak_kind = load_peaks()
-    fl = prof["fluid_launches"]
-    fluid_ms = prof["fluid_ms"] / fl if fl else float("nan")
+    fl = prof["stages"]
+    fluid_ms = prof["fluid_ms"] / fl if fl else float("nan")  # per stage: tile kernel + overflow kernel
     alg_bytes = 96.0 * sc.n  # per stage: read y_s 32 B + read y0 32 B + write y_{s+1} 32 B per particle
     achieved = alg_bytes / (fluid_ms / 1000.0) / 1e9
     traffic = load_traffic().get(f"fluid_{args.config}")

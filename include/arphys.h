@@ -170,6 +170,7 @@ typedef struct arp_profile {
     uint64_t fluid_launches;
     uint64_t neighbor_launches;
     uint64_t solid_launches;
+    uint64_t stages;             /* Runge-Kutta stages evaluated */
 } arp_profile;
 
 /* Health counters collected on the device during steps. */
@@ -225,14 +226,14 @@ arp_status arp_sim_update(arp_sim* sim);
 /* `nsteps` integrator steps of timestep/subticks (update() without the
  * subtick grouping). */
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps);
-/* Time every launch shape of the fluid kernel (hit-list capacity 32/48/64,
+/* Time every launch shape of the fluid kernel (128 or 256 threads per block,
  * one tile per block or persistent blocks on a tile queue) on the current
  * state and keep the fastest; arp_sim_init does this once per (dimension,
  * particle count, h/spacing) bucket and reuses the choice afterwards.  The
  * shapes evaluate identical arithmetic, so results do not depend on it. */
 arp_status arp_sim_autotune(arp_sim* sim, int* variant);
-arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* list_capacity, int* persistent);
-/* Pin the fluid kernel's launch shape (0 .. 5). */
+arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent);
+/* Pin the fluid kernel's launch shape (0 .. 3). */
 arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant);
 /* Replay pairs of steps from a CUDA graph captured on the handle's stream
  * (captured on first use and again after the stream changes; profiling

@@ -89,7 +89,7 @@ def test_graph_replay_matches_plain_steps():
 def test_fluid_launch_shapes_give_identical_results():
     sc = scenes.small_fluid_bar_3d(seed=21)
     ref = None
-    for v in range(6):
+    for v in range(4):
         sim = FluidSim(sc)
         sim.init()
         sim.set_fluid_variant(v)
@@ -105,7 +105,7 @@ def test_autotuner_reports_a_variant():
     sim.init()
     v = sim.autotune()
     info = sim.fluid_variant()
-    assert info["variant"] == v and info["list_capacity"] in (32, 48, 64)
+    assert info["variant"] == v and info["block"] in (128, 256)
 
 
 def test_batched_workload_sample_matches_the_oracle():

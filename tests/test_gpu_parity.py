@@ -144,7 +144,8 @@ def test_profile_and_launch_counters():
     sim.step(3)
     prof = sim.profile_read()
     assert prof["steps"] == 3
-    assert prof["fluid_launches"] == 12  # RK4: one fused fluid kernel per stage
+    assert prof["stages"] == 12  # RK4
+    assert prof["fluid_launches"] == 24  # per stage: the fused fluid kernel and its overflow kernel
     assert prof["fluid_ms"] > 0 and prof["neighbor_ms"] > 0
     assert sim.launch_count() - before == prof["launches"]
     st = sim.stats()
