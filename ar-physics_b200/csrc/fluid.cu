@@ -160,7 +160,6 @@ __device__ __forceinline__ float4 axpy(float c, float4 k, float4 t) {
                        __fadd_rn(t.z, __fmul_rn(c, k.z)), __fadd_rn(t.w, __fmul_rn(c, k.w)));
 }
 
-constexpr int kListCap = 48;                  // hits held per thread before they are consumed
 constexpr uint32_t kBoundaryBit = 0x80000000u;
 
 // Copy one scene's fluid materials and interaction block into shared memory.
@@ -194,13 +193,13 @@ __device__ __forceinline__ void eval_hit(uint32_t j, const Self& s, const FluidA
 }
 
 // Fluid forces and the stage update of sorted particle k.  `lst` is the
-// thread's column of the hit list ([kListCap][BLOCK]); `sm`/`si` hold the
+// thread's column of the hit list ([CAP][BLOCK]); `sm`/`si` hold the
 // tables of scene `scene0`.
 // DIRECT: evaluate every hit during the scan (the overflow kernel) instead
 // of through the list; a list that fills up hands the particle to that kernel
 // through the overflow queue and writes nothing.  Either way the pairs are
 // summed in candidate order.
-template <int DIM, int BLOCK, bool DIRECT>
+template <int DIM, int BLOCK, int CAP, bool DIRECT>
 __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, const Tables& T, const StageCoefs& c,
                                                const StageBuffers& b, uint32_t* lst, const FluidMat* sm,
                                                const DevInter* si, uint32_t scene0) {
@@ -244,7 +243,7 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     auto take = [&](uint32_t j) {
         if (DIRECT) {
             eval_hit<DIM>(j, s, a, K, acc);
-        } else if (cnt < kListCap) {
+        } else if (cnt < CAP) {
             my[cnt++ * BLOCK] = j;
         } else {
             full = true;
@@ -343,30 +342,30 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
 }
 
 // One tile of BLOCK sorted particles per block.
-template <int DIM, int BLOCK>
+template <int DIM, int BLOCK, int CAP>
 __global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * BLOCK);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * BLOCK);
     DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
     const uint32_t k0 = blockIdx.x * BLOCK;
     const uint32_t scene0 = T.mats[__float_as_uint(a.vs[min(k0, a.n - 1u)].w)].scene;
     load_scene_tables(T, scene0, sm, si);
     __syncthreads();
     const uint32_t k = k0 + threadIdx.x;
-    if (k < a.n) fluid_particle<DIM, BLOCK, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+    if (k < a.n) fluid_particle<DIM, BLOCK, CAP, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
 }
 
 // Persistent form: each block keeps taking the next tile of the cell-sorted,
 // scene-concatenated order from an atomic work counter, so scenes of very
 // different sizes share the SMs without a tail of idle blocks.  Blocks never
 // wait on each other.
-template <int DIM, int BLOCK>
+template <int DIM, int BLOCK, int CAP>
 __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
                                                             uint32_t* tile_counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * kListCap * BLOCK);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * BLOCK);
     DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
     __shared__ uint32_t tile_s;
     uint32_t loaded = kInvalid;
@@ -384,7 +383,7 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables 
         }
         __syncthreads();
         const uint32_t k = k0 + threadIdx.x;
-        if (k < a.n) fluid_particle<DIM, BLOCK, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+        if (k < a.n) fluid_particle<DIM, BLOCK, CAP, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
         __syncthreads();
     }
 }
@@ -393,43 +392,45 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables 
 // pairs during the scan.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_fluid_overflow(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
-    const uint32_t cnt = *a.overflow_count;
-    for (uint32_t i = blockIdx.x * blockDim.x + threadIdx.x; i < cnt; i += gridDim.x * blockDim.x)
-        fluid_particle<DIM, 128, true>(a.overflow[i], a, T, c, b, nullptr, nullptr, nullptr, kInvalid);
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < *a.overflow_count)
+        fluid_particle<DIM, 128, 1, true>(a.overflow[i], a, T, c, b, nullptr, nullptr, nullptr, kInvalid);
 }
 
-template <int DIM, int BLOCK>
+template <int DIM, int BLOCK, int CAP>
 void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, bool persistent,
                     uint32_t* tile_counter, cudaStream_t st) {
-    const size_t smem = sizeof(uint32_t) * kListCap * BLOCK + sizeof(FluidMat) * T.max_nmat +
+    const size_t smem = sizeof(uint32_t) * CAP * BLOCK + sizeof(FluidMat) * T.max_nmat +
                         sizeof(DevInter) * T.max_nmat * T.max_nmat;
     if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_fluid<DIM, BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_fluid_persistent<DIM, BLOCK>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_fluid<DIM, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_fluid_persistent<DIM, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     }
     const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
-    int sms = 148;
-    int dev = 0;
-    if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
     cudaMemsetAsync(a.overflow_count, 0, sizeof(uint32_t), st);
     if (!persistent) {
-        k_fluid<DIM, BLOCK><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
-        k_fluid_overflow<DIM><<<sms, 128, 0, st>>>(a, T, c, b);
-        return;
+        k_fluid<DIM, BLOCK, CAP><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
+    } else {
+        int per_sm = 0;
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, BLOCK, CAP>, BLOCK, smem);
+        per_sm = per_sm > 0 ? per_sm : 1;
+        int sms = 148;
+        int dev = 0;
+        if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+        const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
+        cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
+        k_fluid_persistent<DIM, BLOCK, CAP><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
     }
-    int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, BLOCK>, BLOCK, smem);
-    per_sm = per_sm > 0 ? per_sm : 1;
-    const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
-    cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
-    k_fluid_persistent<DIM, BLOCK><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
-    k_fluid_overflow<DIM><<<sms, 128, 0, st>>>(a, T, c, b);
+    // one thread per possible overflowed particle; threads past the count exit
+    k_fluid_overflow<DIM><<<(a.n + 127) / 128, 128, 0, st>>>(a, T, c, b);
 }
 
 }  // namespace
 
 const FluidVariant kFluidVariants[kNumFluidVariants] = {
-    {128, 0}, {256, 0}, {128, 1}, {256, 1},
+    {128, 48, 0}, {256, 48, 0}, {128, 48, 1}, {256, 48, 1},
+    {128, 96, 0}, {256, 96, 0}, {128, 96, 1}, {256, 96, 1},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -437,14 +438,15 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
     if (a.n == 0) return 0;
     const FluidVariant v = kFluidVariants[variant < 0 || variant >= kNumFluidVariants ? 0 : variant];
     const bool pers = v.persistent != 0;
-    if (kdim == 3) {
-        if (v.block == 256) launch_variant<3, 256>(a, T, c, b, pers, tile_counter, st);
-        else launch_variant<3, 128>(a, T, c, b, pers, tile_counter, st);
-    } else {
-        if (v.block == 256) launch_variant<2, 256>(a, T, c, b, pers, tile_counter, st);
-        else launch_variant<2, 128>(a, T, c, b, pers, tile_counter, st);
+#define ARP_FLUID(D, B, C)                                                  \
+    if (kdim == D && v.block == B && v.cap == C) {                          \
+        launch_variant<D, B, C>(a, T, c, b, pers, tile_counter, st);        \
+        return 2; /* the tile kernel and the overflow kernel */             \
     }
-    return 2;  // the tile kernel and the overflow kernel
+    ARP_FLUID(3, 128, 48) ARP_FLUID(3, 256, 48) ARP_FLUID(3, 128, 96) ARP_FLUID(3, 256, 96)
+    ARP_FLUID(2, 128, 48) ARP_FLUID(2, 256, 48) ARP_FLUID(2, 128, 96) ARP_FLUID(2, 256, 96)
+#undef ARP_FLUID
+    return 0;
 }
 
 }  // namespace arp

@@ -1109,6 +1109,7 @@ arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant) {
 }
 
 arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent) {
+    // (the hit-list capacity of the shape is kFluidVariants[variant].cap)
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
     if (variant) *variant = sim->fluid_variant;
     if (block) *block = kFluidVariants[sim->fluid_variant].block;

@@ -89,7 +89,7 @@ def test_graph_replay_matches_plain_steps():
 def test_fluid_launch_shapes_give_identical_results():
     sc = scenes.small_fluid_bar_3d(seed=21)
     ref = None
-    for v in range(4):
+    for v in range(8):
         sim = FluidSim(sc)
         sim.init()
         sim.set_fluid_variant(v)
