@@ -110,6 +110,22 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
+def max_over_ranks(value, device):
+    """The largest `value` over all ranks (the job's time is its slowest
+    rank's); a no-op without a process group."""
+    import torch
+    if not (torch.distributed.is_available() and torch.distributed.is_initialized()):
+        return float(value)
+    t = torch.tensor([float(value)], device=device, dtype=torch.float64)
+    torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
+    return float(t.item())
+
+
+def aggregate_rate(units_per_rank, world, seconds):
+    """Whole-job throughput: the units all ranks processed over the max time."""
+    return units_per_rank * world / seconds
+
+
 def make_scene(name):
     from arphys import scenes
     if name == "c1":
@@ -238,6 +254,8 @@ def run_ours(args, rank, world, local_rank):
     sc = make_scene(args.config)
     sim = FluidSim(sc)
     sim.init()
+    if args.fluid_variant is not None:
+        sim.set_fluid_variant(args.fluid_variant)
     # a dedicated stream: the library launches on it and the events below are
     # recorded on it (torch's default stream is the legacy NULL stream, which
     # the library's own non-blocking stream does not order against)
@@ -273,13 +291,9 @@ def run_ours(args, rank, world, local_rank):
     launches = sim.launch_count() - l0
     prof = sim.profile_read()
     sim.profile_enable(False)
-    total_ms = sum(a.elapsed_time(b) for a, b in evs)
-    if dist:
-        t = torch.tensor([total_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        total_ms = float(t.item())
+    total_ms = max_over_ranks(sum(a.elapsed_time(b) for a, b in evs), "cuda")
     parts = sc.n + sc.nb
-    value = parts * args.steps * world / (total_ms / 1000.0)
+    value = aggregate_rate(parts * args.steps, world, total_ms / 1000.0)
 
     # end to end through the C ABI: host records in, one step, host records out,
     # the records living in page-locked host memory
@@ -295,11 +309,7 @@ def run_ours(args, rank, world, local_rank):
         sim.step(1)
         sim.particles(out=host)
         e2e_ms.append((time.perf_counter() - t0) * 1000)
-    e2e_step_ms = statistics.median(e2e_ms)
-    if dist:
-        t = torch.tensor([e2e_step_ms], device="cuda", dtype=torch.float64)
-        torch.distributed.all_reduce(t, op=torch.distributed.ReduceOp.MAX)
-        e2e_step_ms = float(t.item())
+    e2e_step_ms = max_over_ranks(statistics.median(e2e_ms), "cuda")
     rec = PARTICLE_DTYPE.itemsize  # the reference's 48-byte Particle record
     e2e = {"value": parts * world / (e2e_step_ms / 1000.0), "unit": UNIT,
            "h2d_bytes_per_step": sc.n * rec, "d2h_bytes_per_step": sc.n * rec,
@@ -344,6 +354,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c1", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--fluid-variant", type=int, default=None, help="pin the fluid launch shape (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
