@@ -183,6 +183,10 @@ def load_library():
     sig["arp_sim_scene_range"] = [c_sim, ctypes.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p]
     sig["arp_grid_build_noalloc"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ArpAABB), ctypes.c_float,
                                      ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p]
+    sig["arp_scene_file_load"] = [ctypes.c_char_p, ctypes.POINTER(ctypes.c_void_p)]
+    sig["arp_scene_file_scene"] = [ctypes.c_void_p, ctypes.POINTER(ArpScene)]
+    sig["arp_scene_file_name"] = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p)]
+    sig["arp_scene_file_free"] = [ctypes.c_void_p]
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args

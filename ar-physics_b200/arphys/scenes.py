@@ -21,6 +21,7 @@ import math
 
 import numpy as np
 
+from .abi import INTEGRATORS as INTEGRATOR_IDS
 from .abi import (PARTICLE_DTYPE, MATERIAL_DTYPE, INTERACTION_DTYPE, INVALID, EOS_ZERO, EOS_TAIT,
                   EOS_IDEAL_GAS)
 
@@ -261,3 +262,42 @@ def batched_scenes(count=256, seed=3, spacing=0.01, n_min=2048, n_max=65536, int
                          dt=dt, gravity=9.81, alpha=alpha, name=f"batched_{k}",
                          meta={"steps": steps, "n_target": n_target}))
     return out
+
+
+def load_toml(path):
+    """A scene file in the reference's TOML schema (examples/test_mods/config.rs)
+    parsed and seeded by the library (arp_scene_file_load), copied into a
+    `Scene`.  Errors raise `ArpError`: ARP_ERR_IO, ARP_ERR_PARSE, or
+    ARP_ERR_UNSUPPORTED for STL regions."""
+    import ctypes
+    from .abi import ArpScene, check, load_library
+    L = load_library()
+    f = ctypes.c_void_p()
+    check(L.arp_scene_file_load(str(path).encode(), ctypes.byref(f)))
+    try:
+        sc = ArpScene()
+        check(L.arp_scene_file_scene(f, ctypes.byref(sc)))
+        name = ctypes.c_char_p()
+        check(L.arp_scene_file_name(f, ctypes.byref(name)))
+
+        def copy(addr, count, dtype):
+            out = np.zeros(count, dtype=dtype)
+            if count:
+                ctypes.memmove(out.ctypes.data, addr, count * dtype.itemsize)
+            return out
+
+        m = sc.n_materials
+        inv = {v: k for k, v in reversed(list(INTEGRATOR_IDS.items()))}
+        return Scene(
+            particles=copy(sc.particles, sc.n_particles, PARTICLE_DTYPE),
+            boundary=copy(sc.boundary, sc.n_boundary, PARTICLE_DTYPE),
+            materials=copy(sc.materials, m, MATERIAL_DTYPE),
+            bounds_min=tuple(float(sc.bounds.min[i]) for i in range(4)),
+            bounds_dim=tuple(float(sc.bounds.dim[i]) for i in range(4)),
+            h=float(sc.kernel_radius), integrator=inv[sc.integrator], dt=float(sc.timestep),
+            subticks=int(sc.subticks), gravity=float(sc.gravity), alpha=float(sc.artificial_viscocity),
+            interactions=copy(sc.interactions, m * m, INTERACTION_DTYPE).reshape(m, m),
+            interaction_given=copy(sc.interaction_given, m * m, np.dtype(np.uint8)).reshape(m, m),
+            name=name.value.decode(), meta={"source": str(path)})
+    finally:
+        L.arp_scene_file_free(f)

@@ -1,13 +1,851 @@
-// scene_loader.cpp -- TOML scene loader (placeholder until the parser lands).
+// scene_loader.cpp -- scene files in the reference's TOML schema.
+//
+// Restates examples/test_mods/config.rs:62-474 (the schema and its defaults),
+// src/soft_body/material_region/region.rs:21-272 (AABB, AABE, Transformed,
+// Difference, Union, Intersection) and material_region/mod.rs:230-329
+// (hex/HCP lattice seeding and the mass rule) on top of a small TOML reader.
+// Tables iterate in sorted key order as toml 0.5's BTreeMap does, which fixes
+// the material order: boundaries by name, then objects by name.  Arithmetic
+// follows the Rust code's f32/f64 choices; this file is compiled without
+// floating-point contraction so lattice coordinates accumulate exactly as
+// there.  STL regions ("model") are not supported; "on_click" objects are
+// interactive additions and are not part of the initial scene.
 #include "scene_loader.h"
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstdlib>
+#include <cstring>
+#include <fstream>
+#include <map>
+#include <memory>
+#include <sstream>
+#include <stdexcept>
+#include <string>
+#include <vector>
 
 namespace arp {
 
+// ---- TOML subset -----------------------------------------------------------
+
+struct TVal {
+    enum Kind { Str, Int, Float, Bool, Arr, Tab } kind = Tab;
+    std::string s;
+    double num = 0;
+    bool b = false;
+    std::vector<TVal> arr;
+    std::map<std::string, TVal> tab;
+    bool is_num() const { return kind == Int || kind == Float; }
+};
+
+struct ParseError : std::runtime_error {
+    using std::runtime_error::runtime_error;
+};
+// Valid input that this loader does not implement (ARP_ERR_UNSUPPORTED).
+struct Unsupported : ParseError {
+    using ParseError::ParseError;
+};
+
+class TomlReader {
+public:
+    explicit TomlReader(const std::string& text) : t_(text) {}
+
+    TVal parse() {
+        TVal root;
+        TVal* cur = &root;
+        for (;;) {
+            skip_ws_nl();
+            if (p_ >= t_.size()) break;
+            if (t_[p_] == '[') {
+                ++p_;
+                if (p_ < t_.size() && t_[p_] == '[') throw Unsupported(where() + "arrays of tables are not supported");
+                std::vector<std::string> path = key_path(']');
+                expect(']');
+                cur = &root;
+                for (const auto& k : path) cur = &table_child(*cur, k);
+            } else {
+                std::vector<std::string> path = key_path('=');
+                expect('=');
+                TVal v = value();
+                TVal* t = cur;
+                for (size_t i = 0; i + 1 < path.size(); ++i) t = &table_child(*t, path[i]);
+                if (t->tab.count(path.back())) fail("duplicate key " + path.back());
+                t->tab[path.back()] = std::move(v);
+            }
+            skip_ws();
+            if (p_ < t_.size() && t_[p_] == '#') skip_comment();
+            if (p_ < t_.size() && t_[p_] != '\n' && t_[p_] != '\r') fail("expected end of line");
+        }
+        return root;
+    }
+
+private:
+    const std::string& t_;
+    size_t p_ = 0;
+
+    std::string where() const {
+        size_t line = 1;
+        for (size_t i = 0; i < p_ && i < t_.size(); ++i) line += t_[i] == '\n';
+        return "line " + std::to_string(line) + ": ";
+    }
+    [[noreturn]] void fail(const std::string& m) { throw ParseError(where() + m); }
+    void skip_ws() {
+        while (p_ < t_.size() && (t_[p_] == ' ' || t_[p_] == '\t')) ++p_;
+    }
+    void skip_comment() {
+        while (p_ < t_.size() && t_[p_] != '\n') ++p_;
+    }
+    void skip_ws_nl() {
+        for (;;) {
+            while (p_ < t_.size() && std::isspace((unsigned char)t_[p_])) ++p_;
+            if (p_ < t_.size() && t_[p_] == '#') {
+                skip_comment();
+                continue;
+            }
+            break;
+        }
+    }
+    void expect(char c) {
+        skip_ws();
+        if (p_ >= t_.size() || t_[p_] != c) fail(std::string("expected '") + c + "'");
+        ++p_;
+    }
+    TVal& table_child(TVal& t, const std::string& k) {
+        if (t.kind != TVal::Tab) fail("key " + k + " is not a table");
+        TVal& c = t.tab[k];
+        return c;
+    }
+    std::string bare_or_quoted_key() {
+        skip_ws();
+        if (p_ < t_.size() && t_[p_] == '"') return basic_string();
+        size_t b = p_;
+        while (p_ < t_.size() && (std::isalnum((unsigned char)t_[p_]) || t_[p_] == '_' || t_[p_] == '-')) ++p_;
+        if (b == p_) fail("expected a key");
+        return t_.substr(b, p_ - b);
+    }
+    std::vector<std::string> key_path(char end) {
+        std::vector<std::string> path;
+        for (;;) {
+            path.push_back(bare_or_quoted_key());
+            skip_ws();
+            if (p_ < t_.size() && t_[p_] == '.') {
+                ++p_;
+                continue;
+            }
+            if (p_ < t_.size() && t_[p_] == end) return path;
+            fail("unexpected character in key");
+        }
+    }
+    std::string basic_string() {
+        ++p_;  // opening quote
+        std::string out;
+        while (p_ < t_.size() && t_[p_] != '"') {
+            char c = t_[p_++];
+            if (c == '\\' && p_ < t_.size()) {
+                char e = t_[p_++];
+                switch (e) {
+                    case 'n': out += '\n'; break;
+                    case 't': out += '\t'; break;
+                    case '"': out += '"'; break;
+                    case '\\': out += '\\'; break;
+                    default: out += e;
+                }
+            } else {
+                if (c == '\n') fail("newline in string");
+                out += c;
+            }
+        }
+        if (p_ >= t_.size()) fail("unterminated string");
+        ++p_;
+        return out;
+    }
+    TVal value() {
+        skip_ws();
+        if (p_ >= t_.size()) fail("expected a value");
+        TVal v;
+        char c = t_[p_];
+        if (c == '"') {
+            v.kind = TVal::Str;
+            v.s = basic_string();
+        } else if (c == '\'') {
+            ++p_;
+            size_t b = p_;
+            while (p_ < t_.size() && t_[p_] != '\'') ++p_;
+            if (p_ >= t_.size()) fail("unterminated string");
+            v.kind = TVal::Str;
+            v.s = t_.substr(b, p_ - b);
+            ++p_;
+        } else if (c == '[') {
+            ++p_;
+            v.kind = TVal::Arr;
+            for (;;) {
+                skip_ws_nl();
+                if (p_ < t_.size() && t_[p_] == ']') {
+                    ++p_;
+                    break;
+                }
+                v.arr.push_back(value());
+                skip_ws_nl();
+                if (p_ < t_.size() && t_[p_] == ',') {
+                    ++p_;
+                    continue;
+                }
+                skip_ws_nl();
+                if (p_ < t_.size() && t_[p_] == ']') {
+                    ++p_;
+                    break;
+                }
+                fail("expected ',' or ']' in array");
+            }
+        } else if (c == '{') {
+            ++p_;
+            v.kind = TVal::Tab;
+            skip_ws();
+            if (p_ < t_.size() && t_[p_] == '}') {
+                ++p_;
+                return v;
+            }
+            for (;;) {
+                std::vector<std::string> path = key_path('=');
+                expect('=');
+                TVal x = value();
+                TVal* t = &v;
+                for (size_t i = 0; i + 1 < path.size(); ++i) t = &table_child(*t, path[i]);
+                t->tab[path.back()] = std::move(x);
+                skip_ws();
+                if (p_ < t_.size() && t_[p_] == ',') {
+                    ++p_;
+                    continue;
+                }
+                if (p_ < t_.size() && t_[p_] == '}') {
+                    ++p_;
+                    break;
+                }
+                fail("expected ',' or '}' in inline table");
+            }
+        } else if (t_.compare(p_, 4, "true") == 0) {
+            v.kind = TVal::Bool;
+            v.b = true;
+            p_ += 4;
+        } else if (t_.compare(p_, 5, "false") == 0) {
+            v.kind = TVal::Bool;
+            v.b = false;
+            p_ += 5;
+        } else {
+            size_t b = p_;
+            while (p_ < t_.size() && (std::isalnum((unsigned char)t_[p_]) || std::strchr("+-._", t_[p_]))) ++p_;
+            std::string tok;
+            for (size_t i = b; i < p_; ++i)
+                if (t_[i] != '_') tok += t_[i];
+            if (tok.empty()) fail("expected a value");
+            const bool is_float = tok.find_first_of(".eE") != std::string::npos || tok == "inf" ||
+                                  tok == "+inf" || tok == "-inf" || tok == "nan";
+            char* end = nullptr;
+            if (is_float) {
+                v.kind = TVal::Float;
+                v.num = std::strtod(tok.c_str(), &end);
+            } else {
+                v.kind = TVal::Int;
+                v.num = (double)std::strtoll(tok.c_str(), &end, 10);
+            }
+            if (!end || *end != '\0') fail("bad number " + tok);
+        }
+        return v;
+    }
+};
+
+// ---- values with the schema's defaults (config.rs:62-118) ------------------
+
+using Table = std::map<std::string, TVal>;
+
+const TVal* get(const Table& t, const char* k) {
+    auto it = t.find(k);
+    return it == t.end() ? nullptr : &it->second;
+}
+double num_or(const Table& t, const char* k, double def) {
+    const TVal* v = get(t, k);
+    if (!v) return def;
+    if (!v->is_num()) throw ParseError(std::string("key ") + k + " must be a number");
+    return v->num;
+}
+std::string str_or(const Table& t, const char* k, const std::string& def) {
+    const TVal* v = get(t, k);
+    if (!v) return def;
+    if (v->kind != TVal::Str) throw ParseError(std::string("key ") + k + " must be a string");
+    return v->s;
+}
+// to_vec4 (config.rs:62-66): missing components are zero
+void to_vec4(const TVal& a, float out[4]) {
+    for (int i = 0; i < 4; ++i) out[i] = 0.0f;
+    if (a.kind != TVal::Arr) throw ParseError("expected an array of numbers");
+    for (size_t i = 0; i < 4 && i < a.arr.size(); ++i) {
+        if (!a.arr[i].is_num()) throw ParseError("expected an array of numbers");
+        out[i] = (float)a.arr[i].num;
+    }
+}
+void vec4_or(const Table& t, const char* k, const float def[4], float out[4]) {
+    const TVal* v = get(t, k);
+    if (!v) {
+        for (int i = 0; i < 4; ++i) out[i] = def[i];
+        return;
+    }
+    to_vec4(*v, out);
+}
+// get_packing (config.rs:107-109)
+float packing_of(const Table& t, float h) {
+    return (float)num_or(t, "packing", num_or(t, "spacing", 0.5 * (double)h) / (double)h);
+}
+
+// ---- regions (region.rs) -----------------------------------------------------
+
+struct Box4 {
+    float min[4], dim[4];
+};
+
+struct Region {
+    virtual ~Region() = default;
+    virtual Box4 bound() const = 0;
+    virtual bool contains(const float p[4]) const = 0;
+};
+using RegionP = std::shared_ptr<Region>;
+
+struct RAABB : Region {
+    Box4 b;
+    Box4 bound() const override { return b; }
+    bool contains(const float p[4]) const override {  // region.rs:68-75
+        for (int i = 0; i < 4; ++i)
+            if (p[i] < b.min[i] || p[i] - b.min[i] > b.dim[i]) return false;
+        return true;
+    }
+};
+
+struct RAABE : Region {
+    float center[4], radii[4];
+    Box4 bound() const override {  // region.rs:80-86
+        Box4 r;
+        for (int i = 0; i < 4; ++i) {
+            r.min[i] = center[i] - radii[i];
+            r.dim[i] = 2.0f * radii[i];
+        }
+        return r;
+    }
+    bool contains(const float p[4]) const override {  // region.rs:88-107, in f64
+        double lhs = 0.0;
+        for (int i = 0; i < 4; ++i) {
+            const double d = (double)(p[i] - center[i]);
+            const double r = (double)radii[i];
+            if (r > 0.0) {
+                double coeff = 1.0;
+                for (int j = 0; j < 4; ++j)
+                    if (radii[j] > 0.0f && j != i) coeff = coeff * (double)radii[j];
+                lhs = lhs + d * d * coeff * coeff;
+            }
+        }
+        double rhs = 1.0;
+        for (int i = 0; i < 4; ++i)
+            if (radii[i] > 0.0f) rhs = rhs * (double)radii[i];
+        return lhs <= rhs * rhs;
+    }
+};
+
+struct RTransformed : Region {  // region.rs:125-217
+    RegionP base;
+    float a[4][4];  // column-major: a[col][row]
+    float t[4];
+    Box4 bound() const override {
+        const Box4 bb = base->bound();
+        float mn[4], mx[4];
+        for (int i = 0; i < 4; ++i) {
+            mn[i] = t[i];
+            mx[i] = t[i];
+        }
+        for (int i = 0; i < 4; ++i) {
+            float a_min = 0.0f;
+            for (int j = 0; j < 4; ++j) a_min += a[j][i] * bb.min[j];
+            mn[i] += a_min;
+            mx[i] += a_min;
+            for (int j = 0; j < 4; ++j) mn[i] += std::fmin(a[j][i] * bb.dim[j], 0.0f);
+            for (int j = 0; j < 4; ++j) mx[i] += std::fmax(a[j][i] * bb.dim[j], 0.0f);
+        }
+        Box4 r;  // AABB::from_min_max
+        for (int i = 0; i < 4; ++i) {
+            r.min[i] = mn[i];
+            r.dim[i] = mx[i] - mn[i];
+        }
+        return r;
+    }
+    bool contains(const float p[4]) const override {
+        float v[4], m[4][4];
+        for (int i = 0; i < 4; ++i) v[i] = p[i] - t[i];
+        std::memcpy(m, a, sizeof(m));
+        auto row_mul = [&](int row, int col, float f) {
+            for (int k = col; k < 4; ++k) m[k][row] *= f;
+            v[row] *= f;
+        };
+        auto row_sum = [&](int row, int col, float f, int dest) {
+            for (int k = col; k < 4; ++k) m[k][dest] += f * m[k][row];
+            v[dest] += f * v[row];
+        };
+        auto swap_rows = [&](int r1, int r2, int col) {
+            for (int k = col; k < 4; ++k) std::swap(m[k][r1], m[k][r2]);
+            std::swap(v[r1], v[r2]);
+        };
+        int i = 0, j = 0;  // Gauss-Jordan elimination as region.rs:175-203
+        while (i < 4 && j < 4) {
+            if (m[j][i] != 0.0f) {
+                const float pivot = m[j][i];
+                if (pivot != 1.0f) row_mul(i, j, 1.0f / pivot);
+                for (int k = 0; k < 4; ++k) {
+                    if (k != i && m[j][k] != 0.0f) row_sum(i, j, -m[j][k], k);
+                }
+                ++i;
+                ++j;
+            } else {
+                bool cont = false;
+                for (int k = i + 1; k < 4; ++k) {
+                    if (m[j][k] != 0.0f) {
+                        swap_rows(i, k, j);
+                        cont = true;
+                    }
+                }
+                if (!cont) ++j;
+            }
+        }
+        return base->contains(v);
+    }
+};
+
+struct RDifference : Region {
+    RegionP l, r;
+    Box4 bound() const override { return l->bound(); }
+    bool contains(const float p[4]) const override { return l->contains(p) && !r->contains(p); }
+};
+
+struct RUnion : Region {
+    RegionP l, r;
+    Box4 bound() const override {  // region.rs:232-242
+        const Box4 a = l->bound(), b = r->bound();
+        Box4 o;
+        for (int i = 0; i < 4; ++i) {
+            const float m1 = a.min[i] + a.dim[i], m2 = b.min[i] + b.dim[i];
+            o.min[i] = std::fmin(a.min[i], b.min[i]);
+            o.dim[i] = std::fmax(m1, m2) - o.min[i];
+        }
+        return o;
+    }
+    bool contains(const float p[4]) const override { return l->contains(p) || r->contains(p); }
+};
+
+struct RIntersection : Region {
+    RegionP l, r;
+    Box4 bound() const override {  // region.rs:250-266
+        const Box4 a = l->bound(), b = r->bound();
+        Box4 o;
+        for (int i = 0; i < 4; ++i) {
+            const float m1 = a.min[i] + a.dim[i], m2 = b.min[i] + b.dim[i];
+            o.min[i] = std::fmax(a.min[i], b.min[i]);
+            o.dim[i] = std::fmin(m1, m2) - o.min[i];
+        }
+        return o;
+    }
+    bool contains(const float p[4]) const override { return l->contains(p) && r->contains(p); }
+};
+
+RegionP aabb_border(const Box4& b, float depth) {  // region.rs:37-46
+    auto outer = std::make_shared<RAABB>();
+    outer->b = b;
+    auto inner = std::make_shared<RAABB>();
+    for (int i = 0; i < 4; ++i) {
+        const float c = b.min[i] + 0.5f * b.dim[i];
+        inner->b.min[i] = std::fmin(b.min[i] + depth, c);
+        inner->b.dim[i] = std::fmax(b.dim[i] - 2.0f * depth, 0.0f);
+    }
+    auto d = std::make_shared<RDifference>();
+    d->l = outer;
+    d->r = inner;
+    return d;
+}
+
+RegionP aabe_border(const RAABE& e, float depth) {  // region.rs:54-63
+    auto outer = std::make_shared<RAABE>(e);
+    auto inner = std::make_shared<RAABE>(e);
+    for (int i = 0; i < 4; ++i) inner->radii[i] = std::fmax(e.radii[i] - depth, 0.0f);
+    auto d = std::make_shared<RDifference>();
+    d->l = outer;
+    d->r = inner;
+    return d;
+}
+
+RegionP parse_region_from_mat(const Table& t);
+
+RegionP parse_base(const Table& t) {  // config.rs:180-239
+    if (get(t, "model")) throw Unsupported("STL regions (\"model\") are not supported");
+    const TVal* border_v = get(t, "border");
+    if (border_v && !border_v->is_num()) throw ParseError("border must be a number");
+    float dim[4] = {0, 0, 0, 0}, mn[4] = {0, 0, 0, 0};
+    bool boxed;
+    if (const TVal* d = get(t, "dim"); d && d->kind == TVal::Arr) {
+        boxed = true;
+        to_vec4(*d, dim);
+    } else if (const TVal* r = get(t, "radii"); r && r->kind == TVal::Arr) {
+        boxed = false;
+        to_vec4(*r, dim);
+        for (int i = 0; i < 4; ++i) dim[i] *= 2.0f;
+    } else if (const TVal* dd = get(t, "diameters"); dd && dd->kind == TVal::Arr) {
+        boxed = false;
+        to_vec4(*dd, dim);
+    } else {
+        return parse_region_from_mat(t);
+    }
+    if (const TVal* m = get(t, "min"); m && m->kind == TVal::Arr) {
+        to_vec4(*m, mn);
+    } else if (const TVal* c = get(t, "center"); c && c->kind == TVal::Arr) {
+        to_vec4(*c, mn);
+        for (int i = 0; i < 4; ++i) mn[i] -= 0.5f * dim[i];
+    }
+    if (boxed) {
+        Box4 b;
+        for (int i = 0; i < 4; ++i) {
+            b.min[i] = mn[i];
+            b.dim[i] = dim[i];
+        }
+        if (border_v) return aabb_border(b, (float)border_v->num);
+        auto r = std::make_shared<RAABB>();
+        r->b = b;
+        return r;
+    }
+    RAABE e;
+    for (int i = 0; i < 4; ++i) {
+        dim[i] *= 0.5f;
+        mn[i] += dim[i];
+        e.center[i] = mn[i];
+        e.radii[i] = dim[i];
+    }
+    if (border_v) return aabe_border(e, (float)border_v->num);
+    return std::make_shared<RAABE>(e);
+}
+
+RegionP parse_region(const Table& t) {  // config.rs:130-178
+    RegionP base = parse_base(t);
+    if (!get(t, "translation") && !get(t, "scale") && !get(t, "rotation")) return base;
+    const float zero[4] = {0, 0, 0, 0}, zaxis[4] = {0, 0, 1, 0};
+    float trans[4], rot[4], scale[4] = {1, 1, 1, 1};
+    vec4_or(t, "translation", zero, trans);
+    const TVal* rv = get(t, "rotation");
+    if (rv && rv->kind == TVal::Float) {
+        rot[0] = 0;
+        rot[1] = 0;
+        rot[2] = 1;
+        rot[3] = (float)rv->num;
+    } else {
+        vec4_or(t, "rotation", zaxis, rot);
+    }
+    const TVal* sv = get(t, "scale");
+    if (sv && sv->kind == TVal::Float) {
+        for (int i = 0; i < 4; ++i) scale[i] = (float)sv->num;
+    } else if (sv && sv->kind == TVal::Arr) {
+        for (size_t i = 0; i < sv->arr.size() && i < 4; ++i) {
+            if (!sv->arr[i].is_num()) throw ParseError("scale must hold numbers");
+            scale[i] = (float)sv->arr[i].num;
+        }
+    }
+    const float pi = 3.14159265358979323846f;
+    const float ang = rot[3] * (pi / 180.0f);  // f32::to_radians
+    const float c = std::cos(ang), s = std::sin(ang);
+    const float u_l = std::sqrt(rot[0] * rot[0] + rot[1] * rot[1] + rot[2] * rot[2]);
+    const float u[3] = {rot[0] / u_l, rot[1] / u_l, rot[2] / u_l};
+    float m[4][4] = {
+        {c + u[0] * u[0] * (1.0f - c), u[0] * u[1] * (1.0f - c) + u[2] * s, u[0] * u[2] * (1.0f - c) - u[1] * s, 0.0f},
+        {u[1] * u[2] * (1.0f - c) - u[1] * s, c + u[1] * u[1] * (1.0f - c), u[1] * u[2] * (1.0f - c) + u[0] * s, 0.0f},
+        {u[0] * u[2] * (1.0f - c) + u[1] * s, u[1] * u[2] * (1.0f - c) - u[0] * s, c + u[2] * u[2] * (1.0f - c), 0.0f},
+        {0.0f, 0.0f, 0.0f, 1.0f}};
+    for (int i = 0; i < 4; ++i)
+        for (int j = 0; j < 4; ++j) m[i][j] *= scale[i];
+    auto r = std::make_shared<RTransformed>();
+    r->base = base;
+    std::memcpy(r->a, m, sizeof(m));
+    std::memcpy(r->t, trans, sizeof(trans));
+    return r;
+}
+
+template <class Node>
+RegionP fold(const TVal& arr) {  // config.rs:124-128
+    if (arr.kind != TVal::Arr || arr.arr.empty()) throw ParseError("region list must be a non-empty array");
+    RegionP acc;
+    for (const TVal& e : arr.arr) {
+        if (e.kind != TVal::Tab) throw ParseError("region list entries must be tables");
+        RegionP r = parse_region(e.tab);
+        if (!acc) {
+            acc = r;
+        } else {
+            auto n = std::make_shared<Node>();
+            n->l = acc;
+            n->r = r;
+            acc = n;
+        }
+    }
+    return acc;
+}
+
+RegionP parse_region_from_mat(const Table& t) {  // config.rs:242-252
+    if (const TVal* a = get(t, "union"); a && a->kind == TVal::Arr) return fold<RUnion>(*a);
+    if (const TVal* a = get(t, "difference"); a && a->kind == TVal::Arr) return fold<RDifference>(*a);
+    if (const TVal* a = get(t, "intersection"); a && a->kind == TVal::Arr) return fold<RIntersection>(*a);
+    if (const TVal* r = get(t, "region"); r && r->kind == TVal::Tab) return parse_region(r->tab);
+    throw ParseError("material has no region table and no union, difference or intersection array");
+}
+
+// ---- seeding (material_region/mod.rs:230-329) --------------------------------
+
+struct Velocity {
+    float vel[4] = {0, 0, 0, 0};
+    float w[6] = {0, 0, 0, 0, 0, 0};
+    float center[4] = {0, 0, 0, 0};
+    void at(const float p[4], float out[4]) const {  // config.rs:412-423
+        const float r[4] = {p[0] - center[0], p[1] - center[1], p[2] - center[2], p[3] - center[3]};
+        out[0] = w[1] * r[2] - w[2] * r[1] - w[3] * r[3] + vel[0];
+        out[1] = w[2] * r[0] - w[0] * r[2] + w[4] * r[3] + vel[1];
+        out[2] = w[0] * r[1] - w[1] * r[0] - w[5] * r[3] + vel[2];
+        out[3] = w[3] * r[0] - w[4] * r[1] + w[5] * r[3] + vel[3];
+    }
+};
+
+// Candidates of the staggered lattice with pitch packing*h inside the
+// region's bound; returns the particles inside the region and sets the mass.
+void gen_particles(const Region& region, float packing, float kernel_h, arp_material& mat, uint32_t mat_id,
+                   const Velocity* velf, std::vector<arp_particle>& out) {
+    const float h = packing * kernel_h;
+    if (!(h > 0.0f) || !std::isfinite(h)) throw ParseError("particle spacing (packing * kernel_radius) must be positive");
+    const Box4 bound = region.bound();
+    uint64_t num_in_box = 0;
+    float pos[4] = {bound.min[0], bound.min[1], bound.min[2], bound.min[3]};
+    const float start_density = mat.start_den;
+    const float sq2 = std::sqrt(2.0f), sq3 = std::sqrt(3.0f), sq8 = std::sqrt(8.0f);
+    float offset2 = 0.0f;
+    const uint64_t kLimit = 1ull << 31;
+    for (;;) {
+        float offset = 0.0f;
+        pos[1] = bound.min[1] + offset2;
+        for (;;) {
+            pos[0] = bound.min[0] + (offset + offset2);
+            for (;;) {
+                if (++num_in_box > kLimit) throw ParseError("a region seeds more than 2^31 lattice sites");
+                if (region.contains(pos)) {
+                    arp_particle p{};
+                    for (int i = 0; i < 4; ++i) p.pos[i] = pos[i];
+                    if (velf) velf->at(pos, p.vel);
+                    p.den = start_density;
+                    p.mat = mat_id;
+                    p.solid_id = 0xFFFFFFFFu;
+                    out.push_back(p);
+                }
+                pos[0] += h;
+                if (pos[0] - bound.min[0] > bound.dim[0] || bound.dim[0] == 0.0f) break;
+            }
+            pos[1] += h / sq2;
+            offset = offset == 0.0f ? h / 2.0f : 0.0f;
+            if (pos[1] - bound.min[1] > bound.dim[1] || bound.dim[1] == 0.0f) break;
+        }
+        pos[2] += h / sq3;
+        offset2 = offset2 == 0.0f ? h / sq8 : 0.0f;
+        if (pos[2] - bound.min[2] > bound.dim[2] || bound.dim[2] == 0.0f) break;
+    }
+    double content = 1.0;  // the f64 product of the nonzero extents, then times the density
+    for (int i = 0; i < 4; ++i)
+        if (bound.dim[i] > 0.0f) content = content * (double)bound.dim[i];
+    const double box_mass = (double)start_density * content;
+    mat.mass = (float)(box_mass / (double)num_in_box);
+}
+
+// ---- the schema (config.rs:296-474) ----------------------------------------------
+
+struct Obj {
+    std::string name;
+    const Table* table;
+    bool boundary;
+};
+
+arp_interaction parse_interaction(const Table& t, double h) {  // config.rs:255-277
+    arp_interaction it{};
+    it.strength = (float)num_or(t, "contact_strength", 10000.0);
+    it.radius = (float)num_or(t, "contact_radius", num_or(t, "contact_factor", 2.0) * h);
+    it.friction = (float)num_or(t, "friction", 0.0);
+    it.dampening = (float)num_or(t, "dampening", 0.0);
+    const std::string pot = str_or(t, "potential", "");
+    if (pot == "Zero" || pot == "zero") it.potential = ARP_CONTACT_ZERO;
+    else if (pot == "Constant" || pot == "constant") it.potential = ARP_CONTACT_CONSTANT;
+    else if (pot == "Linear" || pot == "linear") it.potential = ARP_CONTACT_LINEAR;
+    else if (pot == "Tait" || pot == "tait") it.potential = ARP_CONTACT_TAIT;
+    else if (pot == "Hertz" || pot == "hertz") it.potential = ARP_CONTACT_HERTZ;
+    else if (pot == "LennardJones" || pot == "Lennard-Jones" || pot == "Lennard Jones" || pot == "lennard jones" ||
+             pot == "lennard-jones")
+        it.potential = ARP_CONTACT_LENNARD_JONES;
+    else it.potential = ARP_CONTACT_LINEAR;
+    return it;
+}
+
+int integrator_id(const std::string& s) {  // examples/test.rs:165-180
+    std::string l = s;
+    std::transform(l.begin(), l.end(), l.begin(), [](unsigned char c) { return (char)std::tolower(c); });
+    if (l == "verlet") return ARP_INT_VERLET;
+    if (l == "euler" || l == "rk1") return ARP_INT_EULER;
+    if (l == "midpoint" || l == "rk2") return ARP_INT_MIDPOINT;
+    if (l == "heun2" || l == "heun") return ARP_INT_HEUN2;
+    if (l == "ralston") return ARP_INT_RALSTON;
+    if (l == "rk3") return ARP_INT_RK3;
+    if (l == "heun3") return ARP_INT_HEUN3;
+    if (l == "rk4") return ARP_INT_RK4;
+    if (l == "rk_3_8") return ARP_INT_RK_3_8;
+    throw ParseError("invalid integrator " + s);
+}
+
+void build_scene(const TVal& root, LoadedScene& out) {
+    const Table& top = root.tab;
+    out.name = str_or(top, "name", "Fluid Test");
+    out.subticks = (uint32_t)num_or(top, "subticks", 1);
+    out.h = (float)num_or(top, "kernel_radius", 1.0 / 64.0);
+    out.dt = (float)num_or(top, "time_step", 0.01);
+    out.alpha = (float)num_or(top, "artificial_viscocity", 50.0);
+    out.gravity = (float)num_or(top, "gravity", 1.0);
+    const float dmin[4] = {-1, -1, 0, 0}, ddim[4] = {2, 2, 0, 0};
+    vec4_or(top, "min", dmin, out.bounds.min);
+    vec4_or(top, "dim", ddim, out.bounds.dim);
+    out.integrator = integrator_id(str_or(top, "integrator", "verlet"));
+    const float h = out.h;
+    const float alpha = out.alpha;
+
+    std::vector<Obj> objs;
+    std::map<std::pair<std::string, std::string>, arp_interaction> inter_map;
+    auto collect_interactions = [&](const std::string& name, const Table& t) {  // config.rs:279-294
+        for (const auto& kv : t) {
+            if (kv.second.kind != TVal::Tab) continue;
+            if (kv.first == "region" || kv.first == "union" || kv.first == "intersection" || kv.first == "difference")
+                continue;
+            inter_map[{name, kv.first}] = parse_interaction(kv.second.tab, (double)h);
+        }
+    };
+    if (const TVal* b = get(top, "boundaries"); b && b->kind == TVal::Tab)
+        for (const auto& kv : b->tab) {
+            if (kv.second.kind != TVal::Tab) throw ParseError("boundary " + kv.first + " must be a table");
+            objs.push_back({kv.first, &kv.second.tab, true});
+        }
+    std::vector<Obj> mobile;
+    if (const TVal* o = get(top, "objects"); o && o->kind == TVal::Tab)
+        for (const auto& kv : o->tab) {
+            if (kv.second.kind != TVal::Tab) throw ParseError("object " + kv.first + " must be a table");
+            if (get(kv.second.tab, "on_click")) continue;  // interactive additions (config.rs:426-446)
+            objs.push_back({kv.first, &kv.second.tab, false});
+        }
+
+    for (uint32_t idx = 0; idx < objs.size(); ++idx) {
+        const Obj& ob = objs[idx];
+        const Table& t = *ob.table;
+        arp_material m{};
+        Velocity vel;
+        const bool moving = !ob.boundary;
+        if (ob.boundary) {  // config.rs:330-348, Material::new_immobile
+            m.visc = (float)num_or(t, "friction", 0.0);
+            m.start_den = 1.0f;
+            m.target_den = 1.0f;
+            m.immobile = 1;
+        } else {  // config.rs:352-424
+            m.start_den = (float)num_or(t, "start_density", num_or(t, "density", 1.0));
+            m.target_den = (float)num_or(t, "target_density", num_or(t, "density", 1.0));
+            m.sound_speed = (float)num_or(t, "speed_of_sound", 0.0);
+            m.visc = (float)num_or(t, "viscocity", num_or(t, "friction", 0.0));
+            m.bulk_visc = (float)num_or(t, "bulk_viscocity", (double)(alpha * h * m.sound_speed));
+            const TVal* st = get(t, "state");
+            if (!st) st = get(t, "state_equation");
+            if (!st) {
+                if (get(t, "speed_of_sound"))
+                    m.state_eq = (get(t, "start_density") || get(t, "target_density")) ? ARP_EOS_IDEAL_GAS
+                                                                                       : ARP_EOS_TAIT;
+                else m.state_eq = ARP_EOS_ZERO;
+            } else {
+                if (st->kind != TVal::Str) throw ParseError("state must be a string");
+                const std::string& v = st->s;
+                if (v == "Tait" || v == "tait" || v == "Liquid" || v == "liquid") m.state_eq = ARP_EOS_TAIT;
+                else if (v == "Ideal_Gas" || v == "ideal_gas" || v == "gas" || v == "Gas") m.state_eq = ARP_EOS_IDEAL_GAS;
+                else if (v == "Constant" || v == "constant") m.state_eq = ARP_EOS_CONSTANT;
+                else throw ParseError("Invalid state equation: " + v);
+            }
+            m.strain_order = (int32_t)num_or(t, "strain_order", 2);
+            m.normal_stiffness = (float)num_or(t, "normal_stiffness", 0.0);
+            m.shear_stiffness = (float)num_or(t, "shear_stiffness", 0.0);
+            m.normal_damp = (float)num_or(t, "normal_dampening", 0.0);
+            m.shear_damp = (float)num_or(t, "shear_dampening", 0.0);
+            if (get(t, "yield_strength") || get(t, "relaxation_time")) {
+                m.plastic = 1;
+                m.yield_strength = (float)num_or(t, "yield_strength", 0.0);
+                m.work_hardening = (float)num_or(t, "work_hardening", 0.0);
+                m.work_hardening_exp = (float)num_or(t, "work_hardening_exp", 2.0);
+                m.kinematic_hardening = (float)num_or(t, "kinematic_hardening", 0.0);
+                m.thermal_softening = (float)num_or(t, "thermal_softening", 0.0);
+                m.relaxation_time = (float)num_or(t, "relaxation_time", 1.0);
+            }
+            const float zero[4] = {0, 0, 0, 0};
+            vec4_or(t, "velocity", zero, vel.vel);
+            if (const TVal* av = get(t, "angular_velocity")) {
+                if (av->kind != TVal::Arr) throw ParseError("angular_velocity must be an array");
+                for (size_t i = 0; i < av->arr.size() && i < 6; ++i) {
+                    if (!av->arr[i].is_num()) throw ParseError("angular_velocity must hold numbers");
+                    vel.w[i] = (float)av->arr[i].num;
+                }
+            }
+        }
+        RegionP region = parse_region_from_mat(t);
+        if (moving) {
+            const Box4 b = region->bound();  // AABB::center
+            for (int i = 0; i < 4; ++i) vel.center[i] = b.min[i] + 0.5f * b.dim[i];
+        }
+        std::vector<arp_particle> ps;
+        gen_particles(*region, packing_of(t, h), h, m, idx, moving ? &vel : nullptr, ps);
+        out.materials.push_back(m);
+        auto& dst = m.immobile ? out.boundary : out.particles;
+        dst.insert(dst.end(), ps.begin(), ps.end());
+        collect_interactions(ob.name, t);
+    }
+    // config.rs:453-466 then FluidSim::new's resolution (done by arp_sim_create)
+    const size_t M = objs.size();
+    out.interactions.assign(M * M, arp_interaction{});
+    out.given.assign(M * M, 0);
+    for (size_t i = 0; i < M; ++i)
+        for (size_t j = 0; j < M; ++j) {
+            auto it = inter_map.find({objs[i].name, objs[j].name});
+            if (it == inter_map.end()) it = inter_map.find({objs[j].name, objs[i].name});
+            if (it != inter_map.end()) {
+                out.interactions[i * M + j] = it->second;
+                out.given[i * M + j] = 1;
+            }
+        }
+}
+
 arp_status load_scene_toml(const char* path, LoadedScene& out, std::string& err) {
-    (void)path;
-    (void)out;
-    err = "TOML scene loading is not implemented in this build";
-    return ARP_ERR_UNSUPPORTED;
+    std::ifstream f(path, std::ios::binary);
+    if (!f) {
+        err = std::string("cannot open ") + path;
+        return ARP_ERR_IO;
+    }
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string text = ss.str();
+    try {
+        TomlReader r(text);
+        TVal root = r.parse();
+        out = LoadedScene{};
+        build_scene(root, out);
+    } catch (const Unsupported& e) {
+        err = std::string(path) + ": " + e.what();
+        return ARP_ERR_UNSUPPORTED;
+    } catch (const ParseError& e) {
+        err = std::string(path) + ": " + e.what();
+        return ARP_ERR_PARSE;
+    } catch (const std::exception& e) {
+        err = std::string(path) + ": " + e.what();
+        return ARP_ERR_PARSE;
+    }
+    return ARP_OK;
 }
 
 }  // namespace arp

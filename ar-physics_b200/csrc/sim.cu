@@ -13,6 +13,7 @@
 #include <cstdio>
 #include <cstring>
 #include <map>
+#include <memory>
 #include <mutex>
 #include <new>
 #include <tuple>
@@ -1077,6 +1078,39 @@ arp_status arp_sim_create_from_toml(const char* path, arp_sim** out) {
     if (s != ARP_OK) return fail(s, err);
     arp_scene sc = ls.as_scene();
     return arp_sim_create(&sc, out);
+}
+
+struct arp_scene_file {
+    arp::LoadedScene scene;
+};
+
+arp_status arp_scene_file_load(const char* path, arp_scene_file** out) {
+    g_last_error.clear();
+    if (!path || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = nullptr;
+    auto f = std::make_unique<arp_scene_file>();
+    std::string err;
+    arp_status s = arp::load_scene_toml(path, f->scene, err);
+    if (s != ARP_OK) return fail(s, err);
+    *out = f.release();
+    return ARP_OK;
+}
+
+arp_status arp_scene_file_scene(const arp_scene_file* file, arp_scene* out) {
+    if (!file || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *out = file->scene.as_scene();
+    return ARP_OK;
+}
+
+arp_status arp_scene_file_name(const arp_scene_file* file, const char** name) {
+    if (!file || !name) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *name = file->scene.name.c_str();
+    return ARP_OK;
+}
+
+arp_status arp_scene_file_free(arp_scene_file* file) {
+    delete file;
+    return ARP_OK;
 }
 
 arp_status arp_sim_destroy(arp_sim* sim) {

@@ -213,6 +213,26 @@ arp_status arp_sim_scene_range(const arp_sim* sim, uint32_t scene, uint32_t* fir
 /* FluidSim::new after examples/test_mods/config.rs:298-474 parses a scene
  * file and src/soft_body/material_region/mod.rs:56-155 seeds its regions. */
 arp_status arp_sim_create_from_toml(const char* path, arp_sim** out);
+
+/* ---- scene files (host only; no CUDA call) ----------------------------------- */
+
+/* A scene file in the schema of examples/test_mods/config.rs, parsed and
+ * seeded on the host.  Replaces `Config::parse` (config.rs:298-474) followed by
+ * the seeding loop of `FluidSim::new` (src/soft_body/mod.rs:70-86, which calls
+ * `MaterialRegion::gen_particles`, material_region/mod.rs:56-156): materials in
+ * object order (boundaries, then objects, each by name), boundary and mobile
+ * particles in that order, the n_materials^2 interaction table with a `given`
+ * flag per entry.  STL regions ("model") give ARP_ERR_UNSUPPORTED; objects
+ * with "on_click" are interactive additions and are skipped; an integrator
+ * name outside the reference's list gives ARP_ERR_PARSE, as does any schema
+ * error the reference would panic on. */
+typedef struct arp_scene_file arp_scene_file;
+arp_status arp_scene_file_load(const char* path, arp_scene_file** out);
+/* Points `out` at the file's records; valid until arp_scene_file_free. */
+arp_status arp_scene_file_scene(const arp_scene_file* file, arp_scene* out);
+/* The scene's "name" (default "Fluid Test"), NUL-terminated, owned by `file`. */
+arp_status arp_scene_file_name(const arp_scene_file* file, const char** name);
+arp_status arp_scene_file_free(arp_scene_file* file);
 /* FluidSim::init, src/soft_body/mod.rs:213-233. */
 arp_status arp_sim_init(arp_sim* sim);
 /* Drop of FluidSim. */

@@ -1,0 +1,213 @@
+"""Scene files: the library's TOML loader (arp_scene_file_load) against the
+oracle restatement (oracle/scene_oracle.py) and hand-computed cases.
+
+The loader replaces Config::parse (examples/test_mods/config.rs:298-474) and
+the seeding in FluidSim::new (src/soft_body/mod.rs:70-86 calling
+MaterialRegion::gen_particles, material_region/mod.rs:56-156).  Seeding is
+integer and float32 work done on the host, so every record must agree bit for
+bit.  These tests call no CUDA function.
+"""
+import ctypes
+import glob
+import os
+
+import numpy as np
+import pytest
+
+from arphys import FluidSim, scenes
+from arphys.abi import ArpError
+from oracle import scene_oracle
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+SCENES = sorted(glob.glob(os.path.join(HERE, "golden", "scenes", "*.toml")))
+# The reference's own example scenes, read as data when its tree is mounted
+# next to this one; the tests that use them skip otherwise.
+REFERENCE_EXAMPLES = sorted(glob.glob("/root/reference/examples/*.toml"))
+
+f32 = np.float32
+
+
+def _write(tmp_path, text, name="scene.toml"):
+    p = tmp_path / name
+    p.write_text(text)
+    return str(p)
+
+
+def assert_same_scene(lib_scene, orc):
+    for key, recs in (("particles", lib_scene.particles), ("boundary", lib_scene.boundary)):
+        o = orc[key]
+        assert len(recs) == len(o["pos"]), key
+        np.testing.assert_array_equal(recs["pos"], o["pos"], err_msg=key)
+        np.testing.assert_array_equal(recs["vel"], o["vel"], err_msg=key)
+        np.testing.assert_array_equal(recs["den"], o["den"], err_msg=key)
+        np.testing.assert_array_equal(recs["mat"], o["mat"], err_msg=key)
+    assert len(lib_scene.materials) == len(orc["materials"])
+    for got, want in zip(lib_scene.materials, orc["materials"]):
+        for field in scene_oracle.MATERIAL_FIELDS:
+            assert got[field] == want[field], (field, got[field], want[field])
+    m = len(orc["materials"])
+    for i in range(m):
+        for j in range(m):
+            want = orc["interactions"][i][j]
+            assert bool(lib_scene.interaction_given[i, j]) == (want is not None), (i, j)
+            if want is not None:
+                got = lib_scene.interactions[i, j]
+                for field in ("potential", "strength", "radius", "friction", "dampening"):
+                    assert got[field] == want[field], (i, j, field)
+    assert f32(lib_scene.h) == orc["h"]
+    assert f32(lib_scene.dt) == orc["dt"]
+    assert f32(lib_scene.gravity) == orc["gravity"]
+    assert f32(lib_scene.alpha) == orc["alpha"]
+    assert lib_scene.subticks == orc["subticks"]
+    assert lib_scene.name == orc["name"]
+    np.testing.assert_array_equal(np.array(lib_scene.bounds_min, f32), orc["bounds_min"])
+    np.testing.assert_array_equal(np.array(lib_scene.bounds_dim, f32), orc["bounds_dim"])
+
+
+@pytest.mark.parametrize("path", SCENES, ids=[os.path.basename(p) for p in SCENES])
+def test_committed_scene_matches_the_oracle(path):
+    assert_same_scene(scenes.load_toml(path), scene_oracle.load(path))
+
+
+@pytest.mark.skipif(not REFERENCE_EXAMPLES, reason="the reference's example scenes are not mounted")
+@pytest.mark.parametrize("path", REFERENCE_EXAMPLES, ids=[os.path.basename(p) for p in REFERENCE_EXAMPLES])
+def test_reference_example_scene_matches_the_oracle(path):
+    try:
+        orc = scene_oracle.load(path)
+    except scene_oracle.SceneError as err:
+        assert "STL" in str(err)
+        with pytest.raises(ArpError) as e:
+            scenes.load_toml(path)
+        assert e.value.code == 6
+        return
+    assert_same_scene(scenes.load_toml(path), orc)
+
+
+def test_lattice_known_answer(tmp_path):
+    """A 0.2 x 0.1 box at pitch 0.1 (packing 1, h 0.1): rows alternate the
+    x offset h/2 and advance y by h/sqrt(2); a row stops after the step that
+    leaves the box; the mass divides the box's mass by every lattice site."""
+    path = _write(tmp_path, """
+kernel_radius = 0.1
+integrator = "euler"
+min = [0.0, 0.0]
+dim = [1.0, 1.0]
+[objects.a]
+  packing = 1.0
+  density = 1000.0
+  region = {min = [0.0, 0.0], dim = [0.2, 0.1]}
+""")
+    sc = scenes.load_toml(path)
+    h = f32(0.1)
+    dy = f32(h / np.sqrt(f32(2.0)))
+    want = [(0.0, 0.0), (h, 0.0), (f32(h + h), 0.0), (f32(h / f32(2)), dy),
+            (f32(f32(h / f32(2)) + h), dy)]
+    np.testing.assert_array_equal(sc.particles["pos"][:, :2], np.array(want, f32))
+    assert np.all(sc.particles["pos"][:, 2:] == 0)
+    assert sc.materials["mass"][0] == f32(1000.0 * (float(f32(0.2)) * float(f32(0.1))) / 5)
+    assert np.all(sc.particles["den"] == 1000.0)
+    assert sc.integrator == "euler"
+
+
+def test_rotation_keeps_the_reference_matrix(tmp_path):
+    """config.rs:158-163 builds the rotation with u[1]*u[2]*(1-c) - u[1]*s in
+    column 1, row 0, where Rodrigues' formula has u[0]*u[1]*(1-c) - u[2]*s.
+    About the z axis the "rotation" by theta is therefore the shear
+    (x, y) -> (c x, s x + c y), and the loader keeps it: the seeded particles
+    are the lattice sites whose preimage under that map lies in the box."""
+    path = _write(tmp_path, """
+kernel_radius = 0.02
+integrator = "rk4"
+[objects.bar]
+  region = {min = [0.0, 0.0], dim = [0.3, 0.1], rotation = 30.0}
+""")
+    p = scenes.load_toml(path).particles["pos"].astype(np.float64)
+    assert len(p) > 50
+    c, s = np.cos(np.radians(30.0)), np.sin(np.radians(30.0))
+    x = p[:, 0] / c
+    y = (p[:, 1] - s * x) / c
+    eps = 1e-5
+    assert x.min() >= -eps and x.max() <= 0.3 + eps
+    assert y.min() >= -eps and y.max() <= 0.1 + eps
+    # a true rotation by 30 degrees would not hold these sites
+    xr, yr = c * p[:, 0] + s * p[:, 1], -s * p[:, 0] + c * p[:, 1]
+    assert (yr < -eps).any() or (yr > 0.1 + eps).any() or (xr > 0.3 + eps).any()
+
+
+def test_object_order_state_inference_and_interaction_lookup(tmp_path):
+    path = _write(tmp_path, """
+kernel_radius = 0.05
+artificial_viscocity = 2.0
+integrator = "rk2"
+[objects.zeta]
+  speed_of_sound = 10.0
+  density = 3.0
+  region = {min = [0.0, 0.0], dim = [0.1, 0.1]}
+[objects.alpha]
+  speed_of_sound = 10.0
+  start_density = 1.0
+  region = {min = [0.2, 0.2], dim = [0.1, 0.1]}
+  zeta = {contact_strength = 5.0}
+[objects.mid]
+  region = {min = [0.4, 0.4], dim = [0.1, 0.1]}
+[boundaries.floor]
+  friction = 0.25
+  region = {min = [-0.5, -0.5], dim = [1.0, 0.1]}
+  mid = {potential = "zero", contact_factor = 3.0}
+""")
+    sc = scenes.load_toml(path)
+    m = sc.materials
+    # boundaries first, then objects, each in key order: floor, alpha, mid, zeta
+    assert list(m["immobile"]) == [1, 0, 0, 0]
+    assert m["visc"][0] == f32(0.25) and m["start_den"][0] == 1 and m["target_den"][0] == 1
+    assert list(m["state_eq"]) == [0, 2, 0, 3]  # ideal gas needs a start/target density key
+    assert m["bulk_visc"][3] == f32(f32(2.0) * f32(0.05)) * f32(10.0)
+    assert m["target_den"][3] == 3.0 and m["start_den"][3] == 3.0
+    g, it = sc.interaction_given, sc.interactions
+    assert g[1, 3] and g[3, 1] and it[3, 1]["strength"] == 5.0  # found under (alpha, zeta)
+    assert it[1, 3]["radius"] == f32(2.0 * float(f32(0.05))) and it[1, 3]["potential"] == 2
+    assert g[0, 2] and g[2, 0] and it[2, 0]["potential"] == 0
+    assert it[0, 2]["radius"] == f32(3.0 * float(f32(0.05)))
+    assert not g[0, 1] and not g[1, 1]
+    assert set(np.unique(sc.boundary["mat"])) == {0}
+    assert set(np.unique(sc.particles["mat"])) == {1, 2, 3}
+
+
+def test_defaults_scene_loads_and_verlet_is_rejected_at_create():
+    path = os.path.join(HERE, "golden", "scenes", "defaults.toml")
+    sc = scenes.load_toml(path)
+    assert sc.name == "Fluid Test" and sc.integrator == "verlet"
+    assert f32(sc.h) == f32(1.0 / 64.0) and f32(sc.dt) == f32(0.01)
+    assert sc.bounds_min[:2] == (-1.0, -1.0) and sc.bounds_dim[:2] == (2.0, 2.0)
+    with pytest.raises(ArpError) as e:
+        FluidSim.from_toml(path)
+    assert e.value.code == 6
+
+
+@pytest.mark.parametrize("text,code,needle", [
+    ("kernel_radius = = 1\n", 8, "line 1"),
+    ("integrator = \"leapfrog\"\n[objects.a]\n  region = {min = [0.0, 0.0], dim = [0.1, 0.1]}\n", 8, "integrator"),
+    ("[objects.a]\n  state = \"plasma\"\n  region = {min = [0.0, 0.0], dim = [0.1, 0.1]}\n", 8, "plasma"),
+    ("[objects.a]\n  density = 1.0\n", 8, "region"),
+    ("[objects.a]\n  region = {model = \"part.stl\"}\n", 6, "STL"),
+    ("[[objects]]\nname = \"a\"\n", 6, "arrays of tables"),
+    ("[objects.a]\n  packing = 0.0\n  region = {min = [0.0, 0.0], dim = [0.1, 0.1]}\n", 8, "spacing"),
+])
+def test_scene_file_errors(tmp_path, text, code, needle):
+    path = _write(tmp_path, text)
+    with pytest.raises(ArpError) as e:
+        scenes.load_toml(path)
+    assert e.value.code == code and needle in str(e.value)
+
+
+def test_missing_scene_file_is_an_io_error(tmp_path):
+    with pytest.raises(ArpError) as e:
+        scenes.load_toml(str(tmp_path / "absent.toml"))
+    assert e.value.code == 9
+
+
+def test_scene_file_handle_calls_reject_null(lib):
+    assert lib.arp_scene_file_load(None, None) == 1
+    assert lib.arp_scene_file_scene(None, None) == 1
+    assert lib.arp_scene_file_name(None, None) == 1
+    assert lib.arp_scene_file_free(None) == 0
