@@ -187,6 +187,9 @@ def load_library():
     sig["arp_scene_file_scene"] = [ctypes.c_void_p, ctypes.POINTER(ArpScene)]
     sig["arp_scene_file_name"] = [ctypes.c_void_p, ctypes.POINTER(ctypes.c_char_p)]
     sig["arp_scene_file_free"] = [ctypes.c_void_p]
+    sig["arp_scene_file_on_click_count"] = [ctypes.c_void_p, u32p]
+    sig["arp_scene_file_on_click"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), u32p,
+                                      ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args

@@ -288,6 +288,16 @@ def load_toml(path):
 
         m = sc.n_materials
         inv = {v: k for k, v in reversed(list(INTEGRATOR_IDS.items()))}
+        count = ctypes.c_uint32()
+        check(L.arp_scene_file_on_click_count(f, ctypes.byref(count)))
+        on_click = []
+        for i in range(count.value):
+            pp, n, rel = ctypes.c_void_p(), ctypes.c_uint32(), ctypes.c_int()
+            mat = np.zeros(1, dtype=MATERIAL_DTYPE)
+            check(L.arp_scene_file_on_click(f, i, ctypes.byref(pp), ctypes.byref(n), mat.ctypes.data,
+                                            ctypes.byref(rel)))
+            on_click.append(dict(particles=copy(pp.value, n.value, PARTICLE_DTYPE), material=mat[0],
+                                 relative=bool(rel.value)))
         return Scene(
             particles=copy(sc.particles, sc.n_particles, PARTICLE_DTYPE),
             boundary=copy(sc.boundary, sc.n_boundary, PARTICLE_DTYPE),
@@ -298,6 +308,6 @@ def load_toml(path):
             subticks=int(sc.subticks), gravity=float(sc.gravity), alpha=float(sc.artificial_viscocity),
             interactions=copy(sc.interactions, m * m, INTERACTION_DTYPE).reshape(m, m),
             interaction_given=copy(sc.interaction_given, m * m, np.dtype(np.uint8)).reshape(m, m),
-            name=name.value.decode(), meta={"source": str(path)})
+            name=name.value.decode(), meta={"source": str(path), "on_click": on_click})
     finally:
         L.arp_scene_file_free(f)

@@ -730,18 +730,19 @@ void build_scene(const TVal& root, LoadedScene& out) {
             if (kv.second.kind != TVal::Tab) throw ParseError("boundary " + kv.first + " must be a table");
             objs.push_back({kv.first, &kv.second.tab, true});
         }
-    std::vector<Obj> mobile;
+    std::vector<Obj> clicks;
     if (const TVal* o = get(top, "objects"); o && o->kind == TVal::Tab)
         for (const auto& kv : o->tab) {
             if (kv.second.kind != TVal::Tab) throw ParseError("object " + kv.first + " must be a table");
-            if (get(kv.second.tab, "on_click")) continue;  // interactive additions (config.rs:426-446)
-            objs.push_back({kv.first, &kv.second.tab, false});
+            // objects with "on_click" are interactive additions (config.rs:426-446)
+            (get(kv.second.tab, "on_click") ? clicks : objs).push_back({kv.first, &kv.second.tab, false});
         }
 
-    for (uint32_t idx = 0; idx < objs.size(); ++idx) {
-        const Obj& ob = objs[idx];
+    // one material and its seeded particles, as config.rs:328-424 and
+    // MaterialRegion::gen_particles build them
+    auto seed = [&](const Obj& ob, uint32_t idx, arp_material& m, std::vector<arp_particle>& ps) {
         const Table& t = *ob.table;
-        arp_material m{};
+        m = arp_material{};
         Velocity vel;
         const bool moving = !ob.boundary;
         if (ob.boundary) {  // config.rs:330-348, Material::new_immobile
@@ -799,12 +800,25 @@ void build_scene(const TVal& root, LoadedScene& out) {
             const Box4 b = region->bound();  // AABB::center
             for (int i = 0; i < 4; ++i) vel.center[i] = b.min[i] + 0.5f * b.dim[i];
         }
-        std::vector<arp_particle> ps;
         gen_particles(*region, packing_of(t, h), h, m, idx, moving ? &vel : nullptr, ps);
+    };
+    for (uint32_t idx = 0; idx < objs.size(); ++idx) {
+        arp_material m{};
+        std::vector<arp_particle> ps;
+        seed(objs[idx], idx, m, ps);
         out.materials.push_back(m);
         auto& dst = m.immobile ? out.boundary : out.particles;
         dst.insert(dst.end(), ps.begin(), ps.end());
-        collect_interactions(ob.name, t);
+        collect_interactions(objs[idx].name, *objs[idx].table);
+    }
+    // FluidSim::add_particles seeds with material id 0 (mod.rs:182)
+    for (const Obj& ob : clicks) {
+        LoadedScene::Addition add;
+        add.name = ob.name;
+        const TVal* oc = get(*ob.table, "on_click");
+        add.relative = oc->kind == TVal::Str && oc->s == "Relative";
+        seed(ob, 0, add.material, add.particles);
+        out.on_click.push_back(std::move(add));
     }
     // config.rs:453-466 then FluidSim::new's resolution (done by arp_sim_create)
     const size_t M = objs.size();

@@ -19,6 +19,15 @@ struct LoadedScene {
     uint32_t subticks = 1;
     int integrator = ARP_INT_VERLET;
     std::string name;
+    // objects marked "on_click": seeded, not part of the initial scene; a host
+    // passes them to add_particles (with an offset when `relative`)
+    struct Addition {
+        std::string name;
+        std::vector<arp_particle> particles;
+        arp_material material{};
+        bool relative = false;
+    };
+    std::vector<Addition> on_click;
 
     arp_scene as_scene() const {
         arp_scene s{};

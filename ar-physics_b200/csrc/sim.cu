@@ -155,6 +155,9 @@ struct arp_sim {
         uint32_t mat_base, nmat;  // global material range
         uint32_t inter_base;      // interaction block (nmat x nmat)
         uint32_t s_base;          // first batch-wide solid id
+        uint32_t dummy_solid;     // 1 when created without solids: the reference then keeps a
+                                  // placeholder solid entry 0 (particles.rs:502), so solids added
+                                  // later are numbered from 1 and count one more
         bool flat_z;              // every particle shares one z and moves in the plane
         arp_aabb bounds;
         float h, gravity, alpha;
@@ -185,6 +188,9 @@ struct arp_sim {
     std::vector<arp_particle> host_boundary;
     std::vector<uint32_t> sid_of_caller;       // caller id -> solid id
     std::vector<uint32_t> part_of_solid;       // solid id -> caller id
+    std::vector<float4> host_ref;              // solid id -> reference position (set by init)
+    std::vector<float4> host_ep;               // solid id -> plastic strain columns, kept across add_particles
+    bool any_solid_branch = false;             // some scene has more than one solid entry
 
     cudaStream_t own_stream = nullptr, stream = nullptr;
     uint64_t launches = 0;
@@ -255,7 +261,7 @@ struct arp_sim {
         if (own_stream) cudaStreamDestroy(own_stream);
     }
 
-    bool solid_branch() const { return ns > 1; }  // shaders/mod.rs:51: solids.len() > 1
+    bool solid_branch() const { return any_solid_branch; }  // shaders/mod.rs:51: solids.len() > 1
 };
 
 namespace {
@@ -444,16 +450,25 @@ arp_status do_init(arp_sim* S) {
 
     // solids: reference positions, plastic strain = 0, neighbor lists, L
     if (ns > 0) {
-        std::vector<float4> refh(ns);
+        // reference positions: the positions at creation, or carried over by
+        // add_particles (new solids then start from their position when added)
+        const size_t kept = S->host_ref.size() <= ns ? S->host_ref.size() : 0;
         std::vector<uint32_t> mos(ns);
+        S->host_ref.resize(ns);
         for (uint32_t s = 0; s < ns; ++s) {
             const arp_particle& p = S->host_particles[S->part_of_solid[s]];
-            refh[s] = make_float4(p.pos[0], p.pos[1], p.pos[2], 0.0f);
+            if (s >= kept) S->host_ref[s] = make_float4(p.pos[0], p.pos[1], p.pos[2], 0.0f);
             mos[s] = p.mat;
         }
-        CUDA_TRY(cudaMemcpyAsync(S->ref.p, refh.data(), ns * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(S->ref.p, S->host_ref.data(), ns * sizeof(float4), cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemcpyAsync(S->mat_of_solid.p, mos.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemsetAsync(S->ep.p, 0, size_t(ns) * 4 * sizeof(float4), st));
+        if (!S->host_ep.empty()) {
+            const size_t ne = std::min(S->host_ep.size(), size_t(ns) * 4);
+            CUDA_TRY(cudaMemcpyAsync(S->ep.p, S->host_ep.data(), ne * sizeof(float4), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+            S->host_ep.clear();
+        }
         // grid over reference positions (neighbor_list.rs:266-275, mode 1)
         S->launches += build_grid(S->ref.p, nullptr, S->mat_of_solid.p, ns, S->tables, S->gb, nullptr, nullptr, st);
         DevBuf<uint32_t> cnt;
@@ -500,8 +515,8 @@ arp_status do_step(arp_sim* S) {
     mark(S, mk, 0);
     S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
     S->launches += gather_state(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
-                                S->orig_r.p, S->sid.p, S->sid_r.p, ns > 1 ? S->gb.coord : nullptr,
-                                ns > 1 ? S->coord_s.p : nullptr, S->ps.p, S->d_mats.p, st);
+                                S->orig_r.p, S->sid.p, S->sid_r.p, sb ? S->gb.coord : nullptr,
+                                sb ? S->coord_s.p : nullptr, S->ps.p, S->d_mats.p, st);
     std::swap(S->Y, S->T);
     std::swap(S->orig, S->orig_r);
     std::swap(S->sid, S->sid_r);
@@ -775,8 +790,9 @@ arp_status append_scene(const arp_scene* sc, arp_sim* S) {
 }
 
 // Solid ids in particle order for stiff materials (particles.rs:488-506), in
-// the concatenated caller order of the batch.
-void finalize_scenes(arp_sim* S) {
+// the concatenated caller order of the batch.  `creating` marks the first call
+// for a handle, which decides each scene's placeholder solid entry.
+void finalize_scenes(arp_sim* S, bool creating) {
     bool all_flat = true;
     for (const auto& H : S->scenes) all_flat = all_flat && H.flat_z;
     S->kdim = all_flat ? 2 : 3;
@@ -789,10 +805,13 @@ void finalize_scenes(arp_sim* S) {
         }
     S->ns = (uint32_t)S->part_of_solid.size();
     uint32_t base = 0;
+    S->any_solid_branch = false;
     for (auto& H : S->scenes) {
         uint32_t cnt = 0;
         for (uint32_t i = H.p_base; i < H.p_base + H.n; ++i) cnt += S->sid_of_caller[i] != kInvalid;
-        H.sp.solid_branch = cnt > 1 ? 1u : 0u;
+        if (creating) H.dummy_solid = cnt == 0 ? 1u : 0u;
+        H.sp.solid_branch = cnt + H.dummy_solid > 1 ? 1u : 0u;
+        S->any_solid_branch = S->any_solid_branch || H.sp.solid_branch;
         H.s_base = base;
         base += cnt;
     }
@@ -844,7 +863,7 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->F.alloc(3 * ns));
     CUDA_TRY(S->A.alloc(3 * ns));
     CUDA_TRY(S->ksol.alloc(ns));
-    CUDA_TRY(S->coord_s.alloc(S->ns > 1 ? n : 1));
+    CUDA_TRY(S->coord_s.alloc(S->solid_branch() ? n : 1));
     CUDA_TRY(S->contact_bound.alloc(2));
     CUDA_TRY(S->tile_counter.alloc(1));
     CUDA_TRY(S->overflow.alloc(n));
@@ -873,7 +892,7 @@ arp_status allocate(arp_sim* S) {
         d.strain_order = m.strain_order;
         d.scene = S->scene_of_material[i];
         d.local = i - S->scenes[d.scene].mat_base;
-        d.solid_base = S->scenes[d.scene].s_base;
+        d.solid_base = S->scenes[d.scene].s_base - S->scenes[d.scene].dummy_solid;  // reported id = global - base
         dm[i] = d;
     }
     CUDA_TRY(S->d_mats.alloc(S->M));
@@ -1025,7 +1044,7 @@ arp_status arp_sim_create_batch(const arp_scene* scenes, uint32_t count, arp_sim
     arp_status s = ARP_OK;
     for (uint32_t k = 0; k < count && s == ARP_OK; ++k) s = append_scene(&scenes[k], S);
     if (s == ARP_OK) {
-        finalize_scenes(S);
+        finalize_scenes(S, true);
         cudaError_t e = cudaStreamCreateWithFlags(&S->own_stream, cudaStreamNonBlocking);
         if (e != cudaSuccess) s = fail(ARP_ERR_CUDA, std::string("cudaStreamCreate: ") + cudaGetErrorString(e));
         S->stream = S->own_stream;
@@ -1105,6 +1124,24 @@ arp_status arp_scene_file_scene(const arp_scene_file* file, arp_scene* out) {
 arp_status arp_scene_file_name(const arp_scene_file* file, const char** name) {
     if (!file || !name) return fail(ARP_ERR_INVALID_ARG, "null argument");
     *name = file->scene.name.c_str();
+    return ARP_OK;
+}
+
+arp_status arp_scene_file_on_click_count(const arp_scene_file* file, uint32_t* count) {
+    if (!file || !count) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *count = (uint32_t)file->scene.on_click.size();
+    return ARP_OK;
+}
+
+arp_status arp_scene_file_on_click(const arp_scene_file* file, uint32_t index, const arp_particle** particles,
+                                   uint32_t* n, arp_material* material, int* relative) {
+    if (!file) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (index >= file->scene.on_click.size()) return fail(ARP_ERR_INVALID_ARG, "on_click index out of range");
+    const auto& a = file->scene.on_click[index];
+    if (particles) *particles = a.particles.data();
+    if (n) *n = (uint32_t)a.particles.size();
+    if (material) *material = a.material;
+    if (relative) *relative = a.relative ? 1 : 0;
     return ARP_OK;
 }
 
@@ -1247,7 +1284,7 @@ arp_status arp_sim_get_particles(arp_sim* sim, arp_particle* out, uint32_t cap) 
         for (uint32_t i = 0; i < sim->n; ++i) {
             const auto& H = sim->scenes[sim->scene_of_material[out[i].mat]];
             const uint32_t sg = sim->sid_of_caller[i];
-            out[i].solid_id = sg == kInvalid ? sg : sg - H.s_base;
+            out[i].solid_id = sg == kInvalid ? sg : sg - (H.s_base - H.dummy_solid);
             out[i].mat -= H.mat_base;
         }
         return ARP_OK;
@@ -1276,7 +1313,13 @@ arp_status arp_sim_get_solids(arp_sim* sim, arp_solid_particle* out, uint32_t ca
         const uint32_t caller = sim->part_of_solid[s];
         const arp_particle& p = sim->host_particles[caller];
         r.part_id = caller - sim->scenes[sim->scene_of_material[p.mat]].p_base;  // index inside its scene
-        for (int a = 0; a < 3; ++a) r.ref_pos[a] = p.pos[a];
+        if (s < sim->host_ref.size()) {
+            r.ref_pos[0] = sim->host_ref[s].x;
+            r.ref_pos[1] = sim->host_ref[s].y;
+            r.ref_pos[2] = sim->host_ref[s].z;
+        } else {
+            for (int a = 0; a < 3; ++a) r.ref_pos[a] = p.pos[a];
+        }
         r.ref_pos[3] = sim->pos_w;
         for (int c = 0; c < 4; ++c) {
             r.stress[4 * c + 0] = ep[4 * s + c].x;
@@ -1348,11 +1391,121 @@ arp_status arp_sim_device_state(arp_sim* sim, arp_device_view* out) {
     return ARP_OK;
 }
 
+// The derived PartialEq of Material (material.rs:9-27): every field equal.
+static bool same_material(const arp_material& a, const arp_material& b) {
+    return a.immobile == b.immobile && a.mass == b.mass && a.start_den == b.start_den && a.state_eq == b.state_eq &&
+           a.sound_speed == b.sound_speed && a.target_den == b.target_den && a.visc == b.visc &&
+           a.bulk_visc == b.bulk_visc && a.strain_order == b.strain_order &&
+           a.normal_stiffness == b.normal_stiffness && a.shear_stiffness == b.shear_stiffness &&
+           a.normal_damp == b.normal_damp && a.shear_damp == b.shear_damp && a.plastic == b.plastic &&
+           a.yield_strength == b.yield_strength && a.work_hardening == b.work_hardening &&
+           a.work_hardening_exp == b.work_hardening_exp && a.kinematic_hardening == b.kinematic_hardening &&
+           a.thermal_softening == b.thermal_softening && a.relaxation_time == b.relaxation_time;
+}
+
+// interaction.rs:42-50
+static arp_interaction default_between(const arp_material& a, const arp_material& b, float h) {
+    if (a.state_eq != ARP_EOS_ZERO && b.state_eq != ARP_EOS_ZERO) return arp_interaction{0, 0, 0, 0, 0};
+    return arp_interaction{ARP_CONTACT_LINEAR, 10000.0f, h * 2.0f, 0.0f, a.visc + b.visc};
+}
+
 arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n, const arp_material* material,
                                  const float* offset, int* material_added) {
-    (void)p; (void)n; (void)material; (void)offset; (void)material_added;
     ARP_TRY(need_init(sim));
-    return fail(ARP_ERR_UNSUPPORTED, "add_particles is not implemented in this build");
+    if (material_added) *material_added = 0;
+    if (!material || (n && !p)) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (n == 0) return ARP_OK;  // particles.rs:548: nothing added, no material
+    if (sim->scenes.size() != 1) return fail(ARP_ERR_UNSUPPORTED, "add_particles on a batch of scenes");
+    if (material->immobile)
+        return fail(ARP_ERR_UNSUPPORTED, "added particles join the mobile set; an immobile material is not supported");
+    if ((uint64_t)sim->n + n > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "more than 2^31 particles");
+    arp_sim::SceneHost& H = sim->scenes[0];
+    // particles.rs:550-566: a solid material is always new, any other reuses
+    // the first equal material
+    const bool stiff = is_stiff(*material);
+    uint32_t id = sim->M;
+    if (!stiff)
+        for (uint32_t i = 0; i < sim->M; ++i)
+            if (same_material(sim->mats[i], *material)) {
+                id = i;
+                break;
+            }
+    const bool add_mat = id == sim->M;
+    if (add_mat && sim->M + 1 > (uint32_t)kMaxMaterials)
+        return fail(ARP_ERR_UNSUPPORTED, "more than 32 materials in one scene");
+    // mod.rs:184-191: the offset is added in f32 to every component
+    std::vector<arp_particle> added(p, p + n);
+    for (auto& x : added) {
+        if (offset)
+            for (int a = 0; a < 4; ++a) x.pos[a] += offset[a];
+        x.mat = id;
+        x.solid_id = kInvalid;
+        for (int a = 0; a < 4; ++a)
+            if (!std::isfinite(x.pos[a]) || !std::isfinite(x.vel[a]))
+                return fail(ARP_ERR_INVALID_ARG, "non-finite position or velocity");
+        if (sim->have_w && x.pos[3] != sim->pos_w)
+            return fail(ARP_ERR_UNSUPPORTED, "positions must share one w coordinate (4D motion is not supported)");
+        if (x.vel[3] != 0.0f) return fail(ARP_ERR_UNSUPPORTED, "velocities must have zero w component");
+    }
+    // the current state in caller order, with each solid's reference position
+    // and plastic strain
+    std::vector<arp_particle> cur(sim->n);
+    if (sim->n) ARP_TRY(arp_sim_get_particles(sim, cur.data(), sim->n));
+    const uint32_t ns_old = sim->ns;
+    std::vector<float4> ep_old(4 * size_t(ns_old));
+    if (ns_old) {
+        CUDA_TRY(cudaMemcpyAsync(ep_old.data(), sim->ep.p, ep_old.size() * sizeof(float4), cudaMemcpyDeviceToHost,
+                                 sim->stream));
+        CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    }
+    sim->drop_graph();
+
+    // new material and its interaction row and column (particles.rs:571-604)
+    if (add_mat) {
+        const uint32_t old = sim->M;
+        sim->mats.push_back(*material);
+        sim->scene_of_material.push_back(0);
+        if (stiff && material->strain_order != 2) sim->all_order2 = false;
+        std::vector<arp_interaction> ni;
+        ni.reserve(size_t(old + 1) * (old + 1));
+        for (uint32_t i = 0; i < old; ++i) {
+            for (uint32_t j = 0; j < old; ++j) ni.push_back(sim->inter[size_t(i) * old + j]);
+            ni.push_back(default_between(sim->mats[i], sim->mats[old], sim->h));
+        }
+        for (uint32_t i = 0; i < old; ++i) ni.push_back(default_between(sim->mats[old], sim->mats[i], sim->h));
+        ni.push_back(stiff ? arp_interaction{0, 0, 0, 0, 0} : default_between(sim->mats[old], sim->mats[old], sim->h));
+        sim->inter = ni;
+        sim->M = old + 1;
+        H.nmat = sim->M;
+        sim->max_nmat = std::max(sim->max_nmat, sim->M);
+    }
+    // the state becomes the initial state of a handle with the particles appended
+    sim->host_particles = cur;
+    for (auto& x : sim->host_particles) x.solid_id = kInvalid;
+    sim->host_particles.insert(sim->host_particles.end(), added.begin(), added.end());
+    if (!sim->have_w) {
+        sim->pos_w = added[0].pos[3];
+        sim->have_w = true;
+    }
+    bool flat = H.bounds.dim[2] == 0.0f;
+    const float z0 = sim->host_particles[0].pos[2];
+    for (const auto& x : sim->host_particles) flat = flat && x.pos[2] == z0 && x.vel[2] == 0.0f;
+    for (const auto& x : sim->host_boundary) flat = flat && x.pos[2] == z0;
+    H.flat_z = flat;
+    H.n += n;
+    sim->n += n;
+    ARP_TRY(scene_params(H, H.sp.dim));  // material count and flatness enter the scene parameters
+    finalize_scenes(sim, false);
+    // solid ids of existing particles are unchanged (they precede the new ones)
+    sim->host_ep = std::move(ep_old);
+    sim->host_ep.resize(4 * size_t(sim->ns), make_float4(0.f, 0.f, 0.f, 0.f));
+    sim->records.release();
+    sim->initialized = false;
+    ARP_TRY(allocate(sim));
+    ARP_TRY(do_init(sim));
+    ARP_TRY(run_autotune(sim, false));
+    if (material_added) *material_added = add_mat ? 1 : 0;
+    return ARP_OK;
 }
 
 arp_status arp_sim_grid(const arp_sim* sim, uint32_t subdivisions[4], uint32_t* n_cells) {

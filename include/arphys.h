@@ -233,6 +233,14 @@ arp_status arp_scene_file_scene(const arp_scene_file* file, arp_scene* out);
 /* The scene's "name" (default "Fluid Test"), NUL-terminated, owned by `file`. */
 arp_status arp_scene_file_name(const arp_scene_file* file, const char** name);
 arp_status arp_scene_file_free(arp_scene_file* file);
+/* The file's objects marked "on_click" (config.rs:426-446), by name: seeded
+ * with the file's kernel radius and material id 0, as FluidSim::add_particles
+ * seeds them (src/soft_body/mod.rs:180-182).  A host passes one to
+ * arp_sim_add_particles, with the pointer position as `offset` when
+ * `*relative` is 1 (examples/test_mods/renderer.rs:388-409). */
+arp_status arp_scene_file_on_click_count(const arp_scene_file* file, uint32_t* count);
+arp_status arp_scene_file_on_click(const arp_scene_file* file, uint32_t index, const arp_particle** particles,
+                                   uint32_t* n, arp_material* material, int* relative);
 /* FluidSim::init, src/soft_body/mod.rs:213-233. */
 arp_status arp_sim_init(arp_sim* sim);
 /* Drop of FluidSim. */
@@ -287,9 +295,18 @@ arp_status arp_sim_device_state(arp_sim* sim, arp_device_view* out);
 
 /* FluidSim::add_particles, src/soft_body/mod.rs:180-206 with
  * Particles::add_particles, src/soft_body/particle_state/particles.rs:547-631.
- * `p` holds particles already seeded for `material`; `offset` (4 floats, may
- * be NULL) is added to their positions.  `*material_added` receives 1 when a
- * new material entry was appended. */
+ * `p` holds particles already seeded for `material` (their `mat` and
+ * `solid_id` fields are ignored); `offset` (4 floats, may be NULL) is added to
+ * their positions in f32.  They take the first material equal to `material`
+ * in every field, or a new one (always new for a material with stiffness),
+ * and are appended after the existing particles; the simulated time and the
+ * reference positions and plastic strain of existing solids are kept, new
+ * solids take their current positions as reference.  A new material gets
+ * MatInteraction::default_between with every other material (and itself,
+ * unless it is a solid).  `*material_added` receives 1 when a material entry
+ * was appended.  n == 0 adds nothing.  Requires arp_sim_init; a batch of
+ * scenes or an immobile material gives ARP_ERR_UNSUPPORTED.  Any captured
+ * CUDA graph is dropped. */
 arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n,
                                  const arp_material* material, const float* offset,
                                  int* material_added);

@@ -182,6 +182,7 @@ public:
     uint32_t sub[4];
     uint32_t ncells = 0;
     std::vector<Mat<T>> mats;
+    std::vector<arp_material> raw_mats;  // the f32 records, for sums the reference takes in f32
     std::vector<Inter<T>> inter;
     uint32_t M = 0;
     std::vector<Particle<T>> boundary;
@@ -205,6 +206,7 @@ public:
         M = sc->n_materials;
         for (uint32_t i = 0; i < M; ++i) {
             const arp_material& m = sc->materials[i];
+            raw_mats.push_back(m);
             Mat<T> q;
             q.immobile = m.immobile != 0;
             q.mass = m.mass; q.start_den = m.start_den; q.state_eq = m.state_eq;
@@ -297,6 +299,93 @@ public:
         pos_index.assign(st.p.size(), INVALID);
         ref_index.assign(st.p.size(), INVALID);
         return "";
+    }
+
+    // interaction.rs:42-50 MatInteraction::default_between
+    Inter<T> default_between(const arp_material& a, const arp_material& b) const {
+        if (a.state_eq != 0 && b.state_eq != 0) return Inter<T>{0, 0, 0, 0, 0};
+        return Inter<T>{2u, T(10000.0f), T(hf * 2.0f), T(0), T(a.visc + b.visc)};
+    }
+    static bool same_material(const arp_material& a, const arp_material& b) {  // derived PartialEq
+        return a.immobile == b.immobile && a.mass == b.mass && a.start_den == b.start_den &&
+               a.state_eq == b.state_eq && a.sound_speed == b.sound_speed && a.target_den == b.target_den &&
+               a.visc == b.visc && a.bulk_visc == b.bulk_visc && a.strain_order == b.strain_order &&
+               a.normal_stiffness == b.normal_stiffness && a.shear_stiffness == b.shear_stiffness &&
+               a.normal_damp == b.normal_damp && a.shear_damp == b.shear_damp && a.plastic == b.plastic &&
+               a.yield_strength == b.yield_strength && a.work_hardening == b.work_hardening &&
+               a.work_hardening_exp == b.work_hardening_exp && a.kinematic_hardening == b.kinematic_hardening &&
+               a.thermal_softening == b.thermal_softening && a.relaxation_time == b.relaxation_time;
+    }
+
+    // mod.rs:180-206 FluidSim::add_particles and particles.rs:547-631
+    // Particles::add_particles: the particles (already seeded) are shifted by
+    // `offset` in f32, take the first equal material (a solid material is
+    // always new), and are appended to the current state; new solids get ids
+    // after the existing solid entries (the dummy entry included) and their
+    // reference position is their position now.  Returns whether a material
+    // was appended.  The reference-configuration buckets are refilled at the
+    // next step because the particle count grew (neighbor_list.rs:226-235).
+    bool add_particles(const arp_particle* in, uint32_t n, const arp_material& m, const float* offset) {
+        if (n == 0) return false;
+        const bool stiff = m.normal_stiffness != 0.0f || m.shear_stiffness != 0.0f;
+        uint32_t id = M;
+        if (!stiff)
+            for (uint32_t i = 0; i < M; ++i)
+                if (same_material(raw_mats[i], m)) {
+                    id = i;
+                    break;
+                }
+        const bool added = id == M;
+        if (added) {
+            Mat<T> q;
+            q.immobile = m.immobile != 0;
+            q.mass = m.mass; q.start_den = m.start_den; q.state_eq = m.state_eq;
+            q.sound_speed = m.sound_speed; q.target_den = m.target_den; q.visc = m.visc;
+            q.bulk_visc = m.bulk_visc; q.strain_order = m.strain_order;
+            q.normal_stiffness = m.normal_stiffness; q.shear_stiffness = m.shear_stiffness;
+            q.normal_damp = m.normal_damp; q.shear_damp = m.shear_damp; q.plastic = m.plastic != 0;
+            q.yield_strength = m.yield_strength; q.work_hardening = m.work_hardening;
+            q.work_hardening_exp = m.work_hardening_exp;
+            q.kinematic_hardening = m.kinematic_hardening;
+            q.thermal_softening = m.thermal_softening; q.relaxation_time = m.relaxation_time;
+            mats.push_back(q);
+            raw_mats.push_back(m);
+            const uint32_t old = M;
+            std::vector<Inter<T>> ni;
+            for (uint32_t i = 0; i < old; ++i) {
+                for (uint32_t j = 0; j < old; ++j) ni.push_back(inter[size_t(i) * old + j]);
+                ni.push_back(default_between(raw_mats[i], raw_mats[old]));
+            }
+            for (uint32_t i = 0; i < old; ++i) ni.push_back(default_between(raw_mats[old], raw_mats[i]));
+            ni.push_back(stiff ? Inter<T>{0, 0, 0, 0, 0} : default_between(raw_mats[old], raw_mats[old]));
+            inter = ni;
+            M = old + 1;
+        }
+        const uint32_t p_offset = uint32_t(st.p.size());
+        for (uint32_t k = 0; k < n; ++k) {
+            Particle<T> p;
+            p.den = in[k].den;
+            p.mat = id;
+            p.solid_id = INVALID;
+            for (int c = 0; c < 4; ++c) {
+                float x = in[k].pos[c];
+                if (offset) x += offset[c];
+                p.pos[c] = x;
+                p.vel[c] = in[k].vel[c];
+            }
+            if (stiff) {
+                p.solid_id = uint32_t(st.s.size());
+                Solid<T> s;
+                s.part_id = p_offset + k;
+                s.ref_pos = p.pos;
+                st.s.push_back(s);
+            }
+            st.p.push_back(p);
+        }
+        pos_index.assign(st.p.size(), INVALID);
+        ref_index.assign(st.p.size(), INVALID);
+        ref_filled = false;
+        return added;
     }
 
     uint32_t n_solids() const {
@@ -928,6 +1017,36 @@ int orc_get_state(void* h, double* den, double* pos, double* vel, uint32_t* mat,
             for (int c = 0; c < 4; ++c)
                 for (int r = 0; r < 4; ++r)
                     if (plastic) plastic[16 * s + 4 * c + r] = double(S.st.s[s].stress[c][r]);
+        }
+    });
+    return 0;
+}
+
+int orc_add_particles(void* h, const arp_particle* p, uint32_t n, const arp_material* m, const float* offset,
+                      int* material_added) {
+    if (!m || (n && !p)) return 1;
+    bool added = false;
+    dispatch(h, [&](auto& S) { added = S.add_particles(p, n, *m, offset); });
+    if (material_added) *material_added = added ? 1 : 0;
+    return 0;
+}
+
+int orc_materials(void* h, uint32_t* count, arp_material* out, uint32_t cap) {
+    dispatch(h, [&](auto& S) {
+        if (count) *count = S.M;
+        for (uint32_t i = 0; i < S.M && i < cap && out; ++i) out[i] = S.raw_mats[i];
+    });
+    return 0;
+}
+
+int orc_interactions(void* h, double* out) {  // M x M x (potential, strength, radius, dampening, friction)
+    dispatch(h, [&](auto& S) {
+        for (size_t i = 0; i < S.inter.size(); ++i) {
+            out[5 * i + 0] = double(S.inter[i].potential);
+            out[5 * i + 1] = double(S.inter[i].strength);
+            out[5 * i + 2] = double(S.inter[i].radius);
+            out[5 * i + 3] = double(S.inter[i].dampening);
+            out[5 * i + 4] = double(S.inter[i].friction);
         }
     });
     return 0;

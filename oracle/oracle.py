@@ -42,6 +42,9 @@ def lib():
         L.orc_derivative.argtypes = [vp] * 5
         L.orc_strains.argtypes = [vp, vp]
         L.orc_buckets.argtypes = [vp] * 6
+        L.orc_add_particles.argtypes = [vp, vp, ctypes.c_uint32, vp, vp, ctypes.POINTER(ctypes.c_int)]
+        L.orc_materials.argtypes = [vp, u32p, vp, ctypes.c_uint32]
+        L.orc_interactions.argtypes = [vp, vp]
         _L = L
     return _L
 
@@ -84,6 +87,38 @@ class Oracle:
     @property
     def time(self):
         return lib().orc_time(self.h)
+
+    def _refresh_counts(self):
+        n, nb, ns, nc, dim = (ctypes.c_uint32() for _ in range(5))
+        lib().orc_counts(self.h, ctypes.byref(n), ctypes.byref(nb), ctypes.byref(ns), ctypes.byref(nc),
+                         _p(self.sub), ctypes.byref(dim))
+        self.n, self.nb, self.ns = n.value, nb.value, ns.value
+
+    def add_particles(self, particles, material, offset=None):
+        """FluidSim::add_particles (src/soft_body/mod.rs:180-206); returns True
+        when a material entry was appended."""
+        from arphys.abi import PARTICLE_DTYPE, MATERIAL_DTYPE
+        p = np.ascontiguousarray(particles, dtype=PARTICLE_DTYPE)
+        m = np.ascontiguousarray(np.asarray(material, dtype=MATERIAL_DTYPE).reshape(1))
+        off = None if offset is None else np.ascontiguousarray(offset, dtype=np.float32)
+        added = ctypes.c_int(0)
+        lib().orc_add_particles(self.h, _p(p), len(p), _p(m), _p(off), ctypes.byref(added))
+        self._refresh_counts()
+        return bool(added.value)
+
+    def materials(self):
+        from arphys.abi import MATERIAL_DTYPE
+        cnt = ctypes.c_uint32()
+        lib().orc_materials(self.h, ctypes.byref(cnt), None, 0)
+        out = np.zeros(cnt.value, dtype=MATERIAL_DTYPE)
+        lib().orc_materials(self.h, ctypes.byref(cnt), _p(out), cnt.value)
+        return out
+
+    def interactions(self):
+        m = len(self.materials())
+        out = np.zeros((m, m, 5))
+        lib().orc_interactions(self.h, _p(out))
+        return out
 
     def state(self):
         den = np.zeros(self.n)

@@ -391,7 +391,7 @@ def load(path):
     objs += [(k, v, False) for k, v in sorted(top.get("objects", {}).items()) if "on_click" not in v]
     inter_map = {}
     mats, parts = [], {True: [], False: []}
-    for idx, (oname, t, boundary) in enumerate(objs):
+    def seed(t, boundary):
         m = dict.fromkeys(MATERIAL_FIELDS, 0)
         vel_fn = None
         if boundary:
@@ -438,6 +438,10 @@ def load(path):
         packing = f32(num_or(t, "packing", num_or(t, "spacing", 0.5 * float(h)) / float(h)))
         pos, vel, mass = gen_particles(region, packing, h, m["start_den"], vel_fn)
         m["mass"] = mass
+        return m, pos, vel
+
+    for idx, (oname, t, boundary) in enumerate(objs):
+        m, pos, vel = seed(t, boundary)
         mats.append(m)
         parts[boundary].append(dict(pos=pos, vel=vel, den=np.full(len(pos), m["start_den"], f32),
                                     mat=np.full(len(pos), idx, np.uint32)))
@@ -455,4 +459,11 @@ def load(path):
                           mat=np.concatenate([d["mat"] for d in lst]) if lst else np.zeros(0, np.uint32))
     scene["materials"] = mats
     scene["interactions"] = inter
+    scene["on_click"] = []
+    for oname, t in sorted(top.get("objects", {}).items()):
+        if "on_click" in t:
+            m, pos, vel = seed(t, False)
+            scene["on_click"].append(dict(name=oname, material=m, pos=pos, vel=vel,
+                                          den=np.full(len(pos), m["start_den"], f32),
+                                          relative=t["on_click"] == "Relative"))
     return scene

@@ -62,6 +62,16 @@ def assert_same_scene(lib_scene, orc):
     assert lib_scene.name == orc["name"]
     np.testing.assert_array_equal(np.array(lib_scene.bounds_min, f32), orc["bounds_min"])
     np.testing.assert_array_equal(np.array(lib_scene.bounds_dim, f32), orc["bounds_dim"])
+    clicks = lib_scene.meta["on_click"]
+    assert len(clicks) == len(orc["on_click"])
+    for got, want in zip(clicks, orc["on_click"]):
+        assert got["relative"] == want["relative"]
+        np.testing.assert_array_equal(got["particles"]["pos"], want["pos"])
+        np.testing.assert_array_equal(got["particles"]["vel"], want["vel"])
+        np.testing.assert_array_equal(got["particles"]["den"], want["den"])
+        assert np.all(got["particles"]["mat"] == 0)
+        for field in scene_oracle.MATERIAL_FIELDS:
+            assert got["material"][field] == want["material"][field], field
 
 
 @pytest.mark.parametrize("path", SCENES, ids=[os.path.basename(p) for p in SCENES])
@@ -210,4 +220,19 @@ def test_scene_file_handle_calls_reject_null(lib):
     assert lib.arp_scene_file_load(None, None) == 1
     assert lib.arp_scene_file_scene(None, None) == 1
     assert lib.arp_scene_file_name(None, None) == 1
+    assert lib.arp_scene_file_on_click_count(None, None) == 1
+    assert lib.arp_scene_file_on_click(None, 0, None, None, None, None) == 1
     assert lib.arp_scene_file_free(None) == 0
+
+
+def test_on_click_objects_are_seeded_but_not_in_the_scene():
+    """config.rs:426-446 keeps "on_click" objects out of the scene and its
+    interaction table; they are seeded as FluidSim::add_particles would seed
+    them (material id 0, velocity field about their own bound)."""
+    sc = scenes.load_toml(os.path.join(HERE, "golden", "scenes", "csg_2d.toml"))
+    clicks = sc.meta["on_click"]
+    assert len(clicks) == 1 and clicks[0]["relative"]
+    assert len(sc.materials) == 6  # 2 boundaries + 4 objects; "spawn" is not among them
+    c = clicks[0]["particles"]
+    assert len(c) > 50 and np.all(c["mat"] == 0) and np.all(c["den"] == 1000.0)
+    assert np.all(np.hypot(c["pos"][:, 0], c["pos"][:, 1]) <= 0.05 + 1e-6)
