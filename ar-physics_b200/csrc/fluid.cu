@@ -264,7 +264,17 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
                 for (uint32_t j = bb; j < be; ++j)
                     if (hit(a.bxs[j])) take(j | kBoundaryBit);
                 const uint32_t jb = a.start[c0], je = a.start[c1];
-                for (uint32_t j = jb; j < je; ++j)
+                uint32_t j = jb;
+                for (; j + 3u < je; j += 4u) {  // four loads in flight
+                    const float4 q0 = a.xs[j], q1 = a.xs[j + 1u], q2 = a.xs[j + 2u], q3 = a.xs[j + 3u];
+                    const bool h0 = j != k && hit(q0), h1 = j + 1u != k && hit(q1);
+                    const bool h2 = j + 2u != k && hit(q2), h3 = j + 3u != k && hit(q3);
+                    if (h0) take(j);
+                    if (h1) take(j + 1u);
+                    if (h2) take(j + 2u);
+                    if (h3) take(j + 3u);
+                }
+                for (; j < je; ++j)
                     if (j != k && hit(a.xs[j])) take(j);  // the particle itself contributes exactly zero
             }
         }
