@@ -263,8 +263,12 @@ struct SolidArgs {
     const float4* vs;
     const uint32_t* start;
     const uint32_t* sid_sorted;
+    float4* sx;               // [ns] stage position + density in solid-id order (gathered per stage)
+    float4* sv;               // [ns] stage velocity + material bits in solid-id order
+    uint2* sc;                // [ns] packed cell coordinates in solid-id order
     uint32_t ns;
     int all_order2;           // every solid material has strain_order 2
+    int any_plastic;          // some solid material is plastic; otherwise the plastic strain stays zero
 };
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st);
 

@@ -131,15 +131,16 @@ __device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, float 
                 const float rgw = DIM == 3 ? (rx * gx + ry * gy) + rz * gz : rx * gx + ry * gy;
                 const float q = s.m1 * m2.mass * fsum * rgw;
                 const float dd = s.d1 * d2 * denom;
-                acc.f.x -= (q * vx) / dd;
-                acc.f.y -= (q * vy) / dd;
-                acc.f.z -= (q * vz) / dd;
+                // GLSL division carries 2.5 ulp; the 2-ulp hardware quotient is used here
+                acc.f.x -= __fdividef(q * vx, dd);
+                acc.f.y -= __fdividef(q * vy, dd);
+                acc.f.z -= __fdividef(q * vz, dd);
             }
         }
         const float f_ = s.mat == mat2 ? s.bf1 + m2.bulk : it.dampening;
         if (f_ != 0.0f) {
             const float vr = DIM == 3 ? (vx * rx + vy * ry) + vz * rz : vx * rx + vy * ry;
-            const float q = s.m1 * m2.mass * ((f_ * vr) / ((s.d1 + d2) * denom));
+            const float q = s.m1 * m2.mass * __fdividef(f_ * vr, (s.d1 + d2) * denom);
             acc.f.x -= q * gx;
             acc.f.y -= q * gy;
             acc.f.z -= q * gz;

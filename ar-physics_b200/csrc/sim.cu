@@ -179,6 +179,7 @@ struct arp_sim {
     bool initialized = false;
     bool any_stiff_immobile = false;
     bool all_order2 = true;  // every stiff material uses strain order 2
+    bool any_plastic = false;  // some stiff material is plastic
     uint32_t ncells = 0;     // cells of all scenes
     uint32_t max_nmat = 0;
     Tables tables{};
@@ -223,6 +224,8 @@ struct arp_sim {
     // solids
     DevBuf<float4> ref, L, F, A, ksol;
     DevBuf<float4> ep, ep_t, ep_s[2], ep_acc, ep_kst[4];
+    DevBuf<float4> sx, sv;  // stage state in solid-id order
+    DevBuf<uint2> sc;
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
     DevBuf<float4> rl_gw;
     uint32_t rl_nnz = 0;
@@ -605,6 +608,10 @@ arp_status do_step(arp_sim* S) {
             a.sid_sorted = sid_sorted;
             a.ns = ns;
             a.all_order2 = S->all_order2 ? 1 : 0;
+            a.any_plastic = S->any_plastic ? 1 : 0;
+            a.sx = S->sx.p;
+            a.sv = S->sv.p;
+            a.sc = S->sc.p;
             sl = launch_solid(a, S->tables, c, st);
             S->launches += sl;
             cur_ep = a.ep_next;
@@ -649,7 +656,7 @@ arp_status do_step(arp_sim* S) {
         cur_vm = next_vm;
     }
     std::swap(S->Y, S->T);
-    if (sb) std::swap(S->ep, S->ep_t);
+    if (sb && S->any_plastic) std::swap(S->ep, S->ep_t);  // without plastic materials ep stays zero
     if (S->profiling) S->prof_steps++;
     return check_launch("step");
 }
@@ -753,6 +760,7 @@ arp_status append_scene(const arp_scene* sc, arp_sim* S) {
         S->scene_of_material.push_back(scene_idx);
         if (mats[i].immobile && is_stiff(mats[i])) S->any_stiff_immobile = true;
         if (is_stiff(mats[i]) && mats[i].strain_order != 2) S->all_order2 = false;
+        if (is_stiff(mats[i]) && mats[i].plastic) S->any_plastic = true;
     }
     // mod.rs:93-111 interaction matrix of the scene
     std::vector<arp_interaction> block(size_t(M) * M, arp_interaction{0, 0, 0, 0, 0});
@@ -870,6 +878,9 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->overflow_count.alloc(1));
     CUDA_TRY(S->ep.alloc(4 * ns));
     CUDA_TRY(S->ep_t.alloc(4 * ns));
+    CUDA_TRY(S->sx.alloc(ns));
+    CUDA_TRY(S->sv.alloc(ns));
+    CUDA_TRY(S->sc.alloc(ns));
     CUDA_TRY(S->ep_s[0].alloc(4 * ns));
     CUDA_TRY(S->ep_s[1].alloc(4 * ns));
     CUDA_TRY(S->ep_acc.alloc(4 * ns));
@@ -1466,6 +1477,7 @@ arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n
         sim->mats.push_back(*material);
         sim->scene_of_material.push_back(0);
         if (stiff && material->strain_order != 2) sim->all_order2 = false;
+        if (stiff && material->plastic) sim->any_plastic = true;
         std::vector<arp_interaction> ni;
         ni.reserve(size_t(old + 1) * (old + 1));
         for (uint32_t i = 0; i < old; ++i) {

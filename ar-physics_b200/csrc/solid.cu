@@ -205,15 +205,30 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
     return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
 }
 
+// The stage state of every solid in solid-id order (position, velocity, cell
+// coordinates), so that the per-neighbor reads of the two solid kernels are
+// direct and local: reference neighbors have nearby solid ids.
+__global__ void k_solid_gather(const float4* __restrict__ pd, const float4* __restrict__ vm,
+                               const uint2* __restrict__ coord, const uint32_t* __restrict__ slot_of, uint32_t ns,
+                               float4* __restrict__ sx, float4* __restrict__ sv, uint2* __restrict__ sc) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= ns) return;
+    const uint32_t slot = slot_of[i];
+    sx[i] = pd[slot];
+    sv[i] = vm[slot];
+    sc[i] = coord[slot];
+}
+
 // ORDER2: every solid material uses strain order 2 (Green-Lagrange), so the
 // log-series, square-root and inverse paths are compiled out.
-template <bool ORDER2>
+// PLASTIC: some solid material is plastic; otherwise the plastic strain is
+// zero throughout and its buffers are neither read nor written.
+template <bool ORDER2, bool PLASTIC>
 __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T, StageCoefs c) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ns) return;
-    const uint32_t slot = a.slot_of[i];
-    const float4 xi = a.pd[slot];
-    const float4 vi = a.vm[slot];
+    const float4 xi = a.sx[i];
+    const float4 vi = a.sv[i];
     const DevMat mm = T.mats[__float_as_uint(vi.w)];
     const SceneP& P = T.scenes[mm.scene];
     if (!P.solid_branch) return;  // a scene with a single solid skips the solid term
@@ -224,9 +239,8 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMat;
         const float4 g = a.rl.gw[k];
-        const uint32_t sj = a.slot_of[j];
-        const float3 dx = sub3(a.pd[sj], xi);
-        const float3 dv = sub3(a.vm[sj], vi);
+        const float3 dx = sub3(a.sx[j], xi);
+        const float3 dv = sub3(a.sv[j], vi);
         const float gr[3] = {(L0.x * g.x + L1.x * g.y) + L2.x * g.z, (L0.y * g.x + L1.y * g.y) + L2.y * g.z,
                              (L0.z * g.x + L1.z * g.y) + L2.z * g.z};
         const float x[3] = {dx.x, dx.y, dx.z}, v[3] = {dv.x, dv.y, dv.z};
@@ -255,19 +269,23 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
         Lm.m[cc][3] = Lc[cc].w;
     }
     Lm.m[3][3] = 1.0f;
+    if (PLASTIC) {
 #pragma unroll
-    for (int cc = 0; cc < 4; ++cc) {
-        const float4 e = a.ep[4 * i + cc];
-        EP.m[cc][0] = e.x;
-        EP.m[cc][1] = e.y;
-        EP.m[cc][2] = e.z;
-        EP.m[cc][3] = e.w;
+        for (int cc = 0; cc < 4; ++cc) {
+            const float4 e = a.ep[4 * i + cc];
+            EP.m[cc][0] = e.x;
+            EP.m[cc][1] = e.y;
+            EP.m[cc][2] = e.z;
+            EP.m[cc][3] = e.w;
+        }
+    } else {
+        EP = m4_zero();
     }
     // Bound used to skip the self-contact scan: max |u_i - u_0| over solids
     // (u = x - X) and whether any solid left the box.
     {
         const float4 X0 = a.ref[0];
-        const float4 x0 = a.pd[a.slot_of[0]];
+        const float4 x0 = a.sx[0];
         const float4 Xi = a.ref[i];
         const float ux = (xi.x - Xi.x) - (x0.x - X0.x), uy = (xi.y - Xi.y) - (x0.y - X0.y),
                     uz = (xi.z - Xi.z) - (x0.z - X0.z);
@@ -290,7 +308,8 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
         }
     }
     // solid.rs:334-341
-    const M4 strain = m4_add(seth_hill<ORDER2>(Fm, mm.strain_order, P.dim), EP);
+    const M4 strain = PLASTIC ? m4_add(seth_hill<ORDER2>(Fm, mm.strain_order, P.dim), EP)
+                              : seth_hill<ORDER2>(Fm, mm.strain_order, P.dim);
     const M4 rate = seth_hill_rate<ORDER2>(Fm, Fdm, mm.strain_order, P.dim);
     const M4 pk2 = m4_add(hooke(strain, mm.lam, mm.mu, P.dim), hooke(rate, mm.lam_d, mm.mu_d, P.dim));
     const M4 sigma = m4_mul(Fm, m4_transpose(pk2));
@@ -303,6 +322,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
     // solid.rs:499-517: plastic strain rate (relaxation towards the
     // Johnson-Cook yield surface); the equivalent-strain factor is the
     // shader's integer (dim-1)/dim
+    if (!PLASTIC) return;
     M4 kep = m4_zero();
     if (mm.plastic) {
         const float tr = trace_dim(EP, P.dim);
@@ -357,9 +377,8 @@ __device__ __forceinline__ bool in_stencil(uint2 a, uint2 b) {
 __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.ns) return;
-    const uint32_t slot = a.slot_of[i];
-    const float4 xi = a.pd[slot];
-    const uint32_t mat = __float_as_uint(a.vm[slot].w);
+    const float4 xi = a.sx[i];
+    const uint32_t mat = __float_as_uint(a.sv[i].w);
     const DevMat mm = T.mats[mat];
     const SceneP& P = T.scenes[mm.scene];
     if (!P.solid_branch) return;
@@ -368,7 +387,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
     const float4 Ai0 = a.A[3 * i], Ai1 = a.A[3 * i + 1], Ai2 = a.A[3 * i + 2];
     const float4 Xi = a.ref[i];
     const float4 Fi0 = a.F[3 * i], Fi1 = a.F[3 * i + 1], Fi2 = a.F[3 * i + 2];
-    const uint2 ci = a.coord[slot];
+    const uint2 ci = a.sc[i];
     float fx = 0.f, fy = 0.f, fz = 0.f;
     // Reference neighbors of the same material: the elastic force
     // (solid.rs:343-374) and, when the neighbor also sits in the current
@@ -379,8 +398,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
         if (!(e & kSameMat)) continue;
         const uint32_t j = e & ~kSameMat;
         const float4 g = a.rl.gw[k];
-        const uint32_t sj = a.slot_of[j];
-        const float4 xj = a.pd[sj];
+        const float4 xj = a.sx[j];
         const float d2 = xj.w;
         const float V2 = m1 / d2;
         const float s = -V1 * V2;
@@ -392,7 +410,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
         fx += (c0.x * g.x + c1.x * g.y) + c2.x * g.z;
         if (P.dim >= 2) fy += (c0.y * g.x + c1.y * g.y) + c2.y * g.z;
         if (P.dim >= 3) fz += (c0.z * g.x + c1.z * g.y) + c2.z * g.z;
-        if (in_stencil(a.coord[sj], ci)) {
+        if (in_stencil(a.sc[j], ci)) {
             const float3 dx = sub3(xj, xi);
             const float3 dX = sub3(a.ref[j], Xi);
             const float diff = P.h2 - dot3(dX, dX);
@@ -474,12 +492,14 @@ int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st) {
     if (a.ns == 0) return 0;
     cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
-    if (a.all_order2)
-        k_solid_stress<true><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, T, c);
-    else
-        k_solid_stress<false><<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, T, c);
-    k_solid_forces<<<blocks_for(a.ns, kThreads), kThreads, 0, st>>>(a, T);
-    return 2;
+    k_solid_gather<<<blocks_for(a.ns, 256), 256, 0, st>>>(a.pd, a.vm, a.coord, a.slot_of, a.ns, a.sx, a.sv, a.sc);
+    const uint32_t blocks = blocks_for(a.ns, kThreads);
+    if (a.all_order2 && !a.any_plastic) k_solid_stress<true, false><<<blocks, kThreads, 0, st>>>(a, T, c);
+    else if (a.all_order2) k_solid_stress<true, true><<<blocks, kThreads, 0, st>>>(a, T, c);
+    else if (!a.any_plastic) k_solid_stress<false, false><<<blocks, kThreads, 0, st>>>(a, T, c);
+    else k_solid_stress<false, true><<<blocks, kThreads, 0, st>>>(a, T, c);
+    k_solid_forces<<<blocks, kThreads, 0, st>>>(a, T);
+    return 3;
 }
 
 }  // namespace arp
