@@ -190,6 +190,11 @@ def load_library():
     sig["arp_scene_file_on_click_count"] = [ctypes.c_void_p, u32p]
     sig["arp_scene_file_on_click"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), u32p,
                                       ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
+    sig["arp_sim_set_solid_stiffness"] = [c_sim, ctypes.c_void_p, ctypes.c_uint32]
+    sig["arp_tape_begin"] = [c_sim, ctypes.c_uint32]
+    sig["arp_tape_end"] = [c_sim]
+    sig["arp_tape_steps"] = [c_sim, ctypes.POINTER(ctypes.c_uint64)]
+    sig["arp_tape_backward"] = [c_sim, ctypes.c_void_p, ctypes.c_void_p, ctypes.c_void_p]
     for name, args in sig.items():
         f = getattr(L, name)
         f.argtypes = args

@@ -311,3 +311,49 @@ def load_toml(path):
             name=name.value.decode(), meta={"source": str(path), "on_click": on_click})
     finally:
         L.arp_scene_file_free(f)
+
+
+def cantilever_bar(n=(16, 256, 16), spacing=0.01, seed=4, E_median=1e5, E_sigma=0.3, nu=0.3, clamp_layers=2,
+                   integrator="midpoint", dt=1e-4, v_sigma=0.0, gravity=9.81, target_offset=(0.002, -0.01, 0.002)):
+    """The differentiation workload: an elastic bar of n[0] x n[1] x n[2] lattice
+    sites (spacing 0.01, h = 2 x spacing), standing on its lowest `clamp_layers`
+    layers, which are immobile, under gravity; per-particle Young's modulus
+    lognormal(ln E_median, E_sigma), nu = 0.3, RK2 (midpoint).  The meta holds
+    the per-solid (normal, shear) stiffness (negated Lame pair), the caller ids
+    of the tip (top layer) and a seeded target for the tip centroid."""
+    rng = np.random.default_rng(seed)
+    s = spacing
+    h = 2.0 * s
+    nx, ny, nz = n
+    origin = (0.1 + 0.5 * s, 0.05 + 0.5 * s, 0.1 + 0.5 * s)
+    pos = lattice(origin, (nx, ny, nz), s)
+    layer = np.rint((pos[:, 1] - origin[1]) / s).astype(int)
+    clamp = layer < clamp_layers
+    lam0, mu0 = lame_from_young(E_median, nu)
+    mass = 1000.0 * s ** 3
+    mats = np.array([immobile(0.0, mass=1.0 * s ** 3), elastic_solid(1000.0, lam0, mu0, mass=mass)])
+    vel = np.zeros_like(pos)
+    if v_sigma > 0:
+        vel = rng.normal(0.0, v_sigma, size=pos.shape).astype(np.float32)
+    p = particles(pos[~clamp], 1, 1000.0, vel[~clamp])
+    b = particles(pos[clamp], 0, 1.0)
+    E = np.exp(rng.normal(np.log(E_median), E_sigma, size=len(p))).astype(np.float64)
+    lam, mu = lame_from_young(E, nu)
+    stiff = np.stack([lam, mu], axis=1).astype(np.float32)
+    tip = np.nonzero(layer[~clamp] == ny - 1)[0]
+    target = p["pos"][tip, :3].mean(axis=0) + np.asarray(target_offset, np.float32)
+    box_min = (0.0, 0.0, 0.0, 0.0)
+    box_dim = (2 * origin[0] + nx * s, origin[1] + ny * s + 0.1, 2 * origin[2] + nz * s, 0.0)
+    return Scene(particles=p, boundary=b, materials=mats, bounds_min=box_min, bounds_dim=box_dim, h=h,
+                 integrator=integrator, dt=dt, subticks=1, gravity=gravity, alpha=0.0,
+                 name=f"cantilever_bar_{nx}x{ny}x{nz}",
+                 meta={"stiffness": stiff, "E": E, "nu": nu, "tip": tip, "target": target})
+
+
+def tip_loss(pos, tip, target):
+    """Squared distance of the tip centroid to the target and dL/dx (n x 3)."""
+    c = pos[tip, :3].astype(np.float64).mean(axis=0)
+    d = c - np.asarray(target, np.float64)
+    grad = np.zeros((len(pos), 3))
+    grad[tip] = 2.0 * d / len(tip)
+    return float(d @ d), grad

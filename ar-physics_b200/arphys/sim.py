@@ -219,6 +219,37 @@ class FluidSim:
         check(self._L.arp_sim_launch_count(self._h, ctypes.byref(c)))
         return c.value
 
+    def set_solid_stiffness(self, normal_shear):
+        """Per-solid (normal, shear) stiffness, shape (ns, 2) in solid-id order
+        (None restores the materials' values)."""
+        if normal_shear is None:
+            check(self._L.arp_sim_set_solid_stiffness(self._h, None, 0))
+            return
+        a = np.ascontiguousarray(normal_shear, dtype=np.float32).reshape(-1, 2)
+        check(self._L.arp_sim_set_solid_stiffness(self._h, ptr(a), len(a)))
+
+    def tape_begin(self, checkpoint_every=20):
+        """Record the following steps for reverse-mode differentiation."""
+        check(self._L.arp_tape_begin(self._h, int(checkpoint_every)))
+
+    def tape_end(self):
+        check(self._L.arp_tape_end(self._h))
+
+    def tape_steps(self):
+        t = ctypes.c_uint64()
+        check(self._L.arp_tape_steps(self._h, ctypes.byref(t)))
+        return t.value
+
+    def backward(self, dl_dstate):
+        """dL/d(state at tape begin) and dL/d(per-solid stiffness) from dL/d(current
+        state); states are (n, 8) float arrays (x, y, z, rho, vx, vy, vz, 0) in
+        caller order.  Returns (grad_state0 (n, 8), grad_stiffness (ns, 2))."""
+        d = np.ascontiguousarray(dl_dstate, dtype=np.float32).reshape(self.n, 8)
+        g = np.zeros((self.n, 8), np.float32)
+        gs = np.zeros((max(self.ns, 1), 2), np.float32)
+        check(self._L.arp_tape_backward(self._h, ptr(d), ptr(g), ptr(gs)))
+        return g, gs[:self.ns]
+
     def device_state(self):
         v = ArpDeviceView()
         check(self._L.arp_sim_device_state(self._h, ctypes.byref(v)))

@@ -1,0 +1,715 @@
+// adjoint.cu -- reverse mode of one Runge-Kutta stage of the SPH step.
+//
+// For a stage state Y and the adjoint mu of its derivative record k = f(Y)
+// (one (x, rho) and one (v) float4 per particle), these kernels accumulate
+// lam_Y += J_f(Y)^T mu, hand-derived term by term from the forward kernels:
+//   * k_adj_solid   elastic force (solid.rs:343-374), hourglass control
+//                   (solid.rs:430-443) and the order-2 stress chain
+//                   F, dF/dt -> E, dE/dt -> S (Hooke) -> sigma = F S^T -> A = sigma L
+//                   (strain.rs:139-160, solid.rs:147-204,334-341), plus the
+//                   gradient of the per-solid (normal, shear) stiffness;
+//   * k_adj_strain  F and dF/dt as sums over the reference neighbors;
+//   * k_adj_fluid   every fluid pair term (continuity, pressure with the
+//                   state equation, contact potential, viscosity, artificial
+//                   viscosity; fluid.rs:154-247) and dx/dt = v.
+// Neighbor sets (hits within h, reference lists, the current-cell condition
+// of the hourglass term) are those of the recorded forward stage and are not
+// differentiated.  Each particle gathers the contributions of its own pairs
+// and of its neighbors' pairs (pairwise-symmetric gathers): no atomics, each
+// thread writes only its own particle.  Not differentiated: friction (the
+// tape refuses interactions with a friction coefficient), plastic flow and
+// strain orders other than 2 (refused), self-contact (flagged when a pair is
+// active).
+#include "grid.cuh"
+
+namespace arp {
+
+namespace {
+
+constexpr int kT = 128;
+constexpr uint32_t kSameMatBit = 0x80000000u;
+
+inline uint32_t nblocks(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / (uint32_t)t; }
+
+__device__ __forceinline__ float3 f3(float4 a) { return make_float3(a.x, a.y, a.z); }
+__device__ __forceinline__ float3 add(float3 a, float3 b) { return make_float3(a.x + b.x, a.y + b.y, a.z + b.z); }
+__device__ __forceinline__ float3 sub(float3 a, float3 b) { return make_float3(a.x - b.x, a.y - b.y, a.z - b.z); }
+__device__ __forceinline__ float3 mul(float s, float3 a) { return make_float3(s * a.x, s * a.y, s * a.z); }
+__device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
+__device__ __forceinline__ float3 neg(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
+
+// 3x3 matrices, row-major: m[r][c]
+struct M3 {
+    float m[3][3];
+};
+__device__ __forceinline__ M3 m3_zero() {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = 0.0f;
+    return r;
+}
+// three float4 columns -> matrix
+__device__ __forceinline__ M3 m3_cols(const float4* c) {
+    const float4 c0 = c[0], c1 = c[1], c2 = c[2];
+    M3 r;
+    r.m[0][0] = c0.x; r.m[1][0] = c0.y; r.m[2][0] = c0.z;
+    r.m[0][1] = c1.x; r.m[1][1] = c1.y; r.m[2][1] = c1.z;
+    r.m[0][2] = c2.x; r.m[1][2] = c2.y; r.m[2][2] = c2.z;
+    return r;
+}
+__device__ __forceinline__ void m3_store_cols(const M3& a, float4* c) {
+#pragma unroll
+    for (int j = 0; j < 3; ++j) c[j] = make_float4(a.m[0][j], a.m[1][j], a.m[2][j], 0.0f);
+}
+__device__ __forceinline__ float3 m3_vec(const M3& a, float3 v) {
+    return make_float3(a.m[0][0] * v.x + a.m[0][1] * v.y + a.m[0][2] * v.z,
+                       a.m[1][0] * v.x + a.m[1][1] * v.y + a.m[1][2] * v.z,
+                       a.m[2][0] * v.x + a.m[2][1] * v.y + a.m[2][2] * v.z);
+}
+__device__ __forceinline__ M3 m3_mul(const M3& a, const M3& b) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][0] * b.m[0][j] + a.m[i][1] * b.m[1][j] + a.m[i][2] * b.m[2][j];
+    return r;
+}
+__device__ __forceinline__ M3 m3_t(const M3& a) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[j][i];
+    return r;
+}
+__device__ __forceinline__ void m3_add_outer(M3& a, float s, float3 u, float3 v) {
+    const float uu[3] = {u.x, u.y, u.z}, vv[3] = {v.x, v.y, v.z};
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.m[i][j] += s * uu[i] * vv[j];
+}
+__device__ __forceinline__ void m3_acc(M3& a, const M3& b) {
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) a.m[i][j] += b.m[i][j];
+}
+__device__ __forceinline__ M3 m3_sym(const M3& a) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = 0.5f * (a.m[i][j] + a.m[j][i]);
+    return r;
+}
+
+__device__ __forceinline__ float3 mask_dim(float3 v, uint32_t dim) {
+    return make_float3(v.x, dim >= 2 ? v.y : 0.0f, dim >= 3 ? v.z : 0.0f);
+}
+
+// p / rho^2 of a state equation (fluid.rs:131-138) and its derivative in rho
+__device__ __forceinline__ void eos_pt(uint32_t eq, float rho, float c, float d0, float& pt, float& dpt) {
+    float p = 0.0f, dp = 0.0f;
+    if (eq == ARP_EOS_CONSTANT) {
+        p = c * c;
+    } else if (eq == ARP_EOS_IDEAL_GAS) {
+        p = c * c * (rho - d0);
+        dp = c * c;
+    } else if (eq == ARP_EOS_TAIT) {
+        const float x = rho / d0;
+        const float x2 = x * x, x3 = x2 * x, x6 = x3 * x3;
+        p = (c * c * d0 / 7.0f) * (x6 * x - 1.0f);
+        dp = c * c * x6;
+    }
+    const float ir = 1.0f / rho;
+    pt = p * ir * ir;
+    dpt = dp * ir * ir - 2.0f * p * ir * ir * ir;
+}
+
+// contact potential P(r) in the shader's argument order (strength, r0) and dP/dr
+__device__ __forceinline__ float cpot(uint32_t eq, float r, float S, float R0, float& d) {
+    d = 0.0f;
+    switch (eq) {
+        case ARP_CONTACT_CONSTANT: return r <= R0 ? S : 0.0f;
+        case ARP_CONTACT_LINEAR: d = -S; return S * (R0 - r);
+        case ARP_CONTACT_TAIT: {
+            const float x = R0 / r, x2 = x * x, x3 = x2 * x, x6 = x3 * x3, x7 = x6 * x;
+            d = S / 7.0f * (x7 - 1.0f) - S * x7;
+            return (S * r / 7.0f) * (x7 - 1.0f);
+        }
+        case ARP_CONTACT_LENNARD_JONES: {
+            float f = R0 / r;
+            f *= f * f;
+            f *= f;
+            d = -12.0f * S * f * (f - 1.0f) / r;
+            return S * (f * f - 2.0f * f);
+        }
+        case ARP_CONTACT_HERTZ: {
+            const float x = r / R0, x2 = x * x, x3 = x2 * x, x6 = x3 * x3;
+            d = S * x6;
+            return (S * R0 / 7.0f) * (x6 * x - 1.0f);
+        }
+        default: return 0.0f;
+    }
+}
+
+struct PairSide {
+    float3 x, v;
+    float d, pt;
+    float m, visc, bulk;
+    uint32_t mat;
+    bool elastic;
+};
+struct PairGrad {
+    float3 F;        // forward force contribution to the self particle
+    float3 lr;       // dL/dr, r = x_nbr - x_self
+    float3 lvv;      // dL/d(v_nbr - v_self)
+    float ld_self, ld_nbr, lpt_self, lpt_nbr;
+};
+
+// The fluid pair term of `self` with neighbor `nbr` (fluid.rs:154-214, as the
+// forward kernel evaluates it) and its vector-Jacobian product for weights
+// wd (on d rho/dt) and wF (on the force sum).  Friction is not included.
+template <int DIM, bool BOUNDARY>
+__device__ __forceinline__ void pair_vjp(const PairSide& a, const PairSide& b, const DevInter& it, float h2, float kc,
+                                         float eps_hh, float wd, float3 wF, PairGrad& o) {
+    float3 r = sub(b.x, a.x), vv = sub(b.v, a.v);
+    if (DIM == 2) {
+        r.z = 0.0f;
+        vv.z = 0.0f;
+    }
+    const float r2 = dot(r, r);
+    const float diff = fmaxf(h2 - r2, 0.0f);
+    const float gws = -6.0f * kc * diff * diff;
+    const float3 g = mul(gws, r);
+    float3 F = make_float3(0.f, 0.f, 0.f), lg = F, lr = F, lvv = F;
+    float ld1 = 0.f, ld2 = 0.f;
+    if (!BOUNDARY) {
+        lvv = add(lvv, mul(wd * b.m, g));
+        lg = add(lg, mul(wd * b.m, vv));
+    }
+    const float mm = a.m * b.m;
+    const float pf = mm * (a.pt + b.pt);
+    F = add(F, mul(pf, g));
+    lg = add(lg, mul(pf, wF));
+    const float lpt = mm * dot(wF, g);
+    if (it.potential != ARP_CONTACT_ZERO) {
+        const float R = sqrtf(r2);
+        float dcp;
+        const float cp = cpot(it.potential, R, it.radius, it.strength, dcp);
+        if (cp != 0.0f) {
+            const float cs = b.m * cp / b.d;
+            F = add(F, mul(cs, g));
+            lg = add(lg, mul(cs, wF));
+            const float lcs = dot(wF, g);
+            ld2 -= lcs * cs / b.d;
+            const float lR = lcs * b.m / b.d * dcp;
+            if (R > 0.0f) lr = add(lr, mul(lR / R, r));
+        }
+    }
+    if (!BOUNDARY) {
+        const float denom = r2 + eps_hh;
+        float ldenom = 0.0f;
+        if (!a.elastic) {
+            const float fsum = a.visc + b.visc;
+            if (fsum != 0.0f) {
+                const float rgw = dot(r, g);
+                const float dd = a.d * b.d * denom;
+                const float t = mm * fsum * rgw / dd;
+                F = sub(F, mul(t, vv));
+                lvv = sub(lvv, mul(t, wF));
+                const float lt = -dot(wF, vv);
+                const float lrgw = lt * mm * fsum / dd;
+                ld1 -= lt * t / a.d;
+                ld2 -= lt * t / b.d;
+                ldenom -= lt * t / denom;
+                lr = add(lr, mul(lrgw, g));
+                lg = add(lg, mul(lrgw, r));
+            }
+        }
+        const float f_ = a.mat == b.mat ? a.bulk + b.bulk : it.dampening;
+        if (f_ != 0.0f) {
+            const float vr = dot(vv, r);
+            const float ds = a.d + b.d;
+            const float Q = mm * (f_ * vr / (ds * denom));
+            F = sub(F, mul(Q, g));
+            lg = sub(lg, mul(Q, wF));
+            const float lQ = -dot(wF, g);
+            const float lvr = lQ * mm * f_ / (ds * denom);
+            ld1 -= lQ * Q / ds;
+            ld2 -= lQ * Q / ds;
+            ldenom -= lQ * Q / denom;
+            lvv = add(lvv, mul(lvr, r));
+            lr = add(lr, mul(lvr, vv));
+        }
+        lr = add(lr, mul(2.0f * ldenom, r));
+    }
+    // g = gws(r) r, gws = -6 k (h^2 - r.r)^2
+    lr = add(lr, add(mul(gws, lg), mul(24.0f * kc * diff * dot(lg, r), r)));
+    if (DIM == 2) {
+        lr.z = 0.0f;
+        lvv.z = 0.0f;
+    }
+    o.F = F;
+    o.lr = lr;
+    o.lvv = lvv;
+    o.ld_self = ld1;
+    o.ld_nbr = ld2;
+    o.lpt_self = lpt;
+    o.lpt_nbr = lpt;
+}
+
+template <int DIM>
+__global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float4 xi = a.st.pd[i], vi = a.st.vm[i];
+    const uint32_t mat = __float_as_uint(vi.w);
+    const DevMat& mm = T.mats[mat];
+    const SceneP& P = T.scenes[mm.scene];
+    const FluidMat fm = T.fmats[mat];
+    const uint32_t sid = a.sid[i];
+    PairSide si{f3(xi), f3(vi), xi.w, 0.0f, fm.mass, fm.visc, fm.bulk, mat, sid != kInvalid && fm.stiff != 0u};
+    float dpt_i;
+    eos_pt(fm.eos, xi.w, fm.c, fm.d0, si.pt, dpt_i);
+    const float4 mup = a.mu_pd[i], muv = a.mu_vm[i];
+    const float wd = mup.w;
+    const float3 wF = mul(1.0f / xi.w, f3(muv));
+    const bool solid_term = a.solid_branch && sid != kInvalid && P.solid_branch;
+    float3 lx = make_float3(0.f, 0.f, 0.f);
+    float3 lv = mul(solid_term ? 2.0f : 1.0f, f3(mup));  // dx/dt = v (twice for solids in the solid branch)
+    float lrho = 0.0f;
+    float3 Fs = make_float3(0.f, 0.f, 0.f);
+    const uint32_t li = mat - P.mat_base;
+    const DevInter* row_i = T.inter + P.inter_base + li * P.nmat;
+    if (finite3(xi)) {
+        const Grid g = P.grid;
+        const CellCoord cc = cell_coord(xi, g);
+        const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
+        const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
+        const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
+        for (int z = zlo; z <= zhi; ++z)
+            for (int y = ylo; y <= yhi; ++y) {
+                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
+                for (uint32_t jb = a.bstart[c0]; jb < a.bstart[c1]; ++jb) {
+                    const float4 xb = a.bxs[jb];
+                    const float rx = xb.x - xi.x, ry = xb.y - xi.y, rz = DIM == 3 ? xb.z - xi.z : 0.0f;
+                    if (!(P.h2 - (rx * rx + ry * ry + rz * rz) > 0.0f)) continue;
+                    const float4 vb = a.bvs[jb];
+                    const uint32_t matb = __float_as_uint(vb.w);
+                    const FluidMat fb = T.fmats[matb];
+                    const PairSide sb{f3(xb), f3(vb), xb.w, a.bps[jb], fb.mass, fb.visc, fb.bulk, matb, false};
+                    PairGrad o;
+                    pair_vjp<DIM, true>(si, sb, row_i[matb - P.mat_base], P.h2, P.kconst, P.eps_hh, wd, wF, o);
+                    Fs = add(Fs, o.F);
+                    lx = sub(lx, o.lr);
+                    lv = sub(lv, o.lvv);
+                    lrho += o.ld_self + o.lpt_self * dpt_i;
+                }
+                for (uint32_t k = a.st.start[c0]; k < a.st.start[c1]; ++k) {
+                    const uint32_t j = a.st.perm ? a.st.perm[k] : k;
+                    if (j == i) continue;
+                    const float4 xj = a.st.pd[j];
+                    const float rx = xj.x - xi.x, ry = xj.y - xi.y, rz = DIM == 3 ? xj.z - xi.z : 0.0f;
+                    if (!(P.h2 - (rx * rx + ry * ry + rz * rz) > 0.0f)) continue;
+                    const float4 vj = a.st.vm[j];
+                    const uint32_t matj = __float_as_uint(vj.w);
+                    const FluidMat fj = T.fmats[matj];
+                    const uint32_t sidj = a.sid[j];
+                    PairSide sj{f3(xj), f3(vj), xj.w, 0.0f, fj.mass, fj.visc, fj.bulk, matj,
+                                sidj != kInvalid && fj.stiff != 0u};
+                    float dpt_j;
+                    eos_pt(fj.eos, xj.w, fj.c, fj.d0, sj.pt, dpt_j);
+                    PairGrad o;
+                    pair_vjp<DIM, false>(si, sj, row_i[matj - P.mat_base], P.h2, P.kconst, P.eps_hh, wd, wF, o);
+                    Fs = add(Fs, o.F);
+                    lx = sub(lx, o.lr);
+                    lv = sub(lv, o.lvv);
+                    lrho += o.ld_self + o.lpt_self * dpt_i;
+                    // the neighbor's own pair, in which this particle is the neighbor
+                    const float4 mupj = a.mu_pd[j], muvj = a.mu_vm[j];
+                    const DevInter itj = T.inter[P.inter_base + (matj - P.mat_base) * P.nmat + li];
+                    pair_vjp<DIM, false>(sj, si, itj, P.h2, P.kconst, P.eps_hh, mupj.w, mul(1.0f / xj.w, f3(muvj)), o);
+                    lx = add(lx, o.lr);
+                    lv = add(lv, o.lvv);
+                    lrho += o.ld_nbr + o.lpt_nbr * dpt_i;
+                }
+            }
+    }
+    lrho -= dot(wF, Fs) / xi.w;  // k_v = F / rho
+    if (DIM == 2) {
+        lx.z = 0.0f;
+        lv.z = 0.0f;
+    }
+    float4 lp = a.lam_pd[i], lw = a.lam_vm[i];
+    lp.x += lx.x;
+    lp.y += lx.y;
+    lp.z += lx.z;
+    lp.w += lrho;
+    lw.x += lv.x;
+    lw.y += lv.y;
+    lw.z += lv.z;
+    a.lam_pd[i] = lp;
+    a.lam_vm[i] = lw;
+}
+
+// Hourglass pair term of `self` (solid.rs:430-443 as k_solid_forces evaluates
+// it) and its VJP for weight w: forward force f, dL/d(dx) with dx = x_nbr -
+// x_self, dL/de (e = 0.5 (F_self + F_nbr) dX - dx), dL/d rho_self, rho_nbr.
+struct HgGrad {
+    float3 f, ldx, le;
+    float lda, ldb;
+};
+__device__ __forceinline__ void hg_vjp(float3 dx, float3 dX, const M3& Fa, const M3& Fb, float da, float db, float m,
+                                       float kern, const SceneP& P, float3 w, HgGrad& o) {
+    M3 Fs;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) Fs.m[r][c] = 0.5f * (Fa.m[r][c] + Fb.m[r][c]);
+    const float3 e = sub(m3_vec(Fs, dX), dx);
+    const float l = sqrtf(dot(dx, dx));
+    const float ed = dot(e, dx);
+    const float a1 = 100000000.0f * m * m / (da * db);
+    const float lh = l + P.hg_h;
+    const float b1 = 0.5f * ed / lh;
+    const float c1 = 1.0f / (l * l + P.eps_hh);
+    const float sh = a1 * b1 * c1 * kern;
+    const float den = l + P.eps_h;
+    const float u = sh / den;
+    o.f = mul(-u, dx);
+    const float lu = -dot(w, dx);
+    float3 ldx = mul(-u, w);
+    const float lsh = lu / den;
+    const float lden = -lu * u / den;
+    const float la1 = lsh * b1 * c1 * kern, lb1 = lsh * a1 * c1 * kern, lc1 = lsh * a1 * b1 * kern;
+    o.lda = -la1 * a1 / da;
+    o.ldb = -la1 * a1 / db;
+    const float led = lb1 * 0.5f / lh;
+    float ll = -lb1 * b1 / lh - lc1 * c1 * c1 * 2.0f * l + lden;
+    const float3 le = mul(led, dx);
+    ldx = add(ldx, mul(led, e));
+    ldx = sub(ldx, le);
+    if (l > 0.0f) ldx = add(ldx, mul(ll / l, dx));
+    o.ldx = ldx;
+    o.le = le;
+}
+
+__device__ __forceinline__ bool in_stencil2(uint2 a, uint2 b) {
+    const int dx = (int)(a.x & 0xFFFFu) - (int)(b.x & 0xFFFFu);
+    const int dy = (int)(a.x >> 16) - (int)(b.x >> 16);
+    const int dz = (int)a.y - (int)b.y;
+    return a.y != 0xFFFFFFFFu && b.y != 0xFFFFFFFFu && dx >= -1 && dx <= 1 && dy >= -1 && dy <= 1 && dz >= -1 &&
+           dz <= 1;
+}
+
+__global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.ns) return;
+    const float4 xi = a.st.sx[i], vi = a.st.sv[i];
+    const uint32_t mat = __float_as_uint(vi.w);
+    const DevMat mm = T.mats[mat];
+    const SceneP& P = T.scenes[mm.scene];
+    if (!P.solid_branch) return;
+    const uint32_t slot = a.slot_of[i];
+    const float d1 = xi.w, m1 = mm.mass, V1 = m1 / d1;
+    const float3 w = mul(1.0f / d1, f3(a.mu_vm[slot]));
+    const float3 wdm = mask_dim(w, P.dim);
+    const M3 Ai = m3_cols(a.st.A + 3 * i), Fi = m3_cols(a.st.F + 3 * i);
+    const float3 Xi = f3(a.ref[i]);
+    const uint2 ci = a.st.sc[i];
+    M3 lA = m3_zero(), lFh = m3_zero();
+    float3 lx = make_float3(0.f, 0.f, 0.f), fs = lx;
+    float lrho = 0.0f;
+    const uint32_t k0 = a.rl.off[i], k1 = a.rl.off[i + 1];
+    for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t e = a.rl.nbr[k];
+        if (!(e & kSameMatBit)) continue;
+        const uint32_t j = e & ~kSameMatBit;
+        const float3 g = f3(a.rl.gw[k]);
+        const float4 xj = a.st.sx[j];
+        const float d2 = xj.w;
+        const float c = -V1 * (m1 / d2);
+        const M3 Aj = m3_cols(a.st.A + 3 * j);
+        M3 As;
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int cc = 0; cc < 3; ++cc) As.m[r][cc] = Ai.m[r][cc] + Aj.m[r][cc];
+        const float3 Ag = m3_vec(As, g);
+        fs = add(fs, mul(c, mask_dim(Ag, P.dim)));
+        m3_add_outer(lA, c, wdm, g);
+        lrho += (-c / d1) * dot(wdm, Ag);
+        // the neighbor's elastic term: f_j += c (A_j + A_i) grad_w(X_i - X_j), the gradient being -g
+        const float3 wj = mul(1.0f / d2, f3(a.mu_vm[a.slot_of[j]]));
+        const float3 wjd = mask_dim(wj, P.dim);
+        m3_add_outer(lA, -c, wjd, g);
+        lrho += (c / d1) * dot(wjd, Ag);
+        if (in_stencil2(a.st.sc[j], ci)) {
+            const M3 Fj = m3_cols(a.st.F + 3 * j);
+            const float3 dx = sub(f3(xj), f3(xi));
+            const float3 dX = sub(f3(a.ref[j]), Xi);
+            const float diff = P.h2 - dot(dX, dX);
+            const float kern = P.kconst * diff * diff * diff;
+            HgGrad o;
+            hg_vjp(dx, dX, Fi, Fj, d1, d2, m1, kern, P, w, o);
+            fs = add(fs, o.f);
+            lx = sub(lx, o.ldx);
+            m3_add_outer(lFh, 0.5f, o.le, dX);
+            lrho += o.lda;
+            hg_vjp(neg(dx), neg(dX), Fj, Fi, d2, d1, m1, kern, P, wj, o);
+            lx = add(lx, o.ldx);
+            m3_add_outer(lFh, -0.5f, o.le, dX);
+            lrho += o.ldb;
+        }
+    }
+    // self-contact (solid.rs:445-450) is not differentiated: flag an active pair
+    {
+        const float U = __uint_as_float(a.st.contact_bound[0]);
+        const bool maybe = !mm.plastic && (P.contact_slack <= 0.0f || a.st.contact_bound[1] != 0u ||
+                                          !(2.0f * U < P.contact_slack));
+        if (maybe && finite3(xi)) {
+            const Grid& g = P.grid;
+            const CellCoord cc = cell_coord(xi, g);
+            const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
+            bool active = false;
+            for (int dz = -1; dz <= 1 && !active; ++dz) {
+                const int z = cc.z + dz;
+                if (z < 0 || z >= (int)g.sub[2]) continue;
+                for (int dy = -1; dy <= 1 && !active; ++dy) {
+                    const int y = cc.y + dy;
+                    if (y < 0 || y >= (int)g.sub[1]) continue;
+                    const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                    for (uint32_t k = a.st.start[row + x0]; k < a.st.start[row + x1 + 1] && !active; ++k) {
+                        const uint32_t s2 = a.st.perm ? a.st.perm[k] : k;
+                        if (__float_as_uint(a.st.vm[s2].w) != mat) continue;
+                        const uint32_t sj = a.sid[s2];
+                        if (sj == kInvalid) continue;
+                        const float3 dx = sub(f3(a.st.pd[s2]), f3(xi));
+                        const float3 dX = sub(f3(a.ref[sj]), Xi);
+                        if (dot(dX, dX) > P.rcut2 && dot(dx, dx) < P.rcut2) active = true;
+                    }
+                }
+            }
+            if (active) atomicOr(a.flags, 1u);
+        }
+    }
+    lrho -= dot(w, fs) / d1;  // k_v = f / rho - g
+    // stress chain (order 2): E = (F^T F - I)/2, dE/dt = (dF^T F + F^T dF)/2,
+    // S = Hooke(E; n, s) + Hooke(dE/dt; n_d, s_d), sigma = F S^T, A = sigma L
+    const M3 L = m3_cols(a.L + 3 * i);
+    M3 Fd = m3_zero();
+    for (uint32_t k = k0; k < k1; ++k) {
+        const uint32_t j = a.rl.nbr[k] & ~kSameMatBit;
+        const float4 g4 = a.rl.gw[k];
+        const float3 G = m3_vec(L, f3(g4));
+        const float3 dv = sub(f3(a.st.sv[j]), f3(vi));
+        m3_add_outer(Fd, g4.w, dv, G);
+    }
+    const uint32_t dim = P.dim;
+    M3 E = m3_mul(m3_t(Fi), Fi);
+#pragma unroll
+    for (int q = 0; q < 3; ++q) E.m[q][q] -= 1.0f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) E.m[r][c] *= 0.5f;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if ((uint32_t)q >= dim) E.m[q][q] = 0.0f;  // padded axes: C = 1 there
+    const M3 Ed = m3_sym(m3_mul(m3_t(Fd), Fi));
+    const float2 lm = a.stiff ? a.stiff[i] : make_float2(mm.lam, mm.mu);
+    float trE = 0.f, trEd = 0.f;
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if ((uint32_t)q < dim) {
+            trE += E.m[q][q];
+            trEd += Ed.m[q][q];
+        }
+    M3 S;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c)
+            S.m[r][c] = 2.0f * lm.y * E.m[r][c] + 2.0f * mm.mu_d * Ed.m[r][c] +
+                        (r == c ? lm.x * trE + mm.lam_d * trEd : 0.0f);
+    const M3 lsig = m3_mul(lA, m3_t(L));
+    M3 lF = m3_mul(lsig, S);
+    const M3 lS = m3_mul(m3_t(lsig), Fi);
+    const float trS = lS.m[0][0] + lS.m[1][1] + lS.m[2][2];
+    M3 lE, lEd;
+    float gs = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const bool d = r == c && (uint32_t)r < dim;
+            lE.m[r][c] = 2.0f * lm.y * lS.m[r][c] + (d ? lm.x * trS : 0.0f);
+            lEd.m[r][c] = 2.0f * mm.mu_d * lS.m[r][c] + (d ? mm.lam_d * trS : 0.0f);
+            gs += 2.0f * lS.m[r][c] * E.m[r][c];
+        }
+    const float gn = trE * trS;
+    m3_acc(lF, m3_mul(Fi, m3_sym(lE)));
+    m3_acc(lF, m3_mul(Fd, m3_sym(lEd)));
+    const M3 lFd = m3_mul(Fi, m3_sym(lEd));
+    m3_acc(lF, lFh);
+    m3_store_cols(lF, a.lamF + 3 * i);
+    m3_store_cols(lFd, a.lamFd + 3 * i);
+    float2 gsum = a.g_stiff[i];
+    gsum.x += gn;
+    gsum.y += gs;
+    a.g_stiff[i] = gsum;
+    float4 lp = a.lam_pd[slot];
+    lp.x += lx.x;
+    lp.y += lx.y;
+    lp.z += lx.z;
+    lp.w += lrho;
+    a.lam_pd[slot] = lp;
+}
+
+// F_i = sum_j V_j (x_j - x_i) (x) L_i gradW_ij and dF/dt likewise with v:
+// gather the adjoints of F and dF/dt of the particle and of its reference
+// neighbors into dL/dx and dL/dv.
+__global__ void __launch_bounds__(kT) k_adj_strain(AdjArgs a, Tables T) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.ns) return;
+    const uint32_t mat = __float_as_uint(a.st.sv[i].w);
+    const DevMat& mm = T.mats[mat];
+    const SceneP& P = T.scenes[mm.scene];
+    if (!P.solid_branch) return;
+    const uint32_t slot = a.slot_of[i];
+    const M3 Li = m3_cols(a.L + 3 * i);
+    const M3 lFi = m3_cols(a.lamF + 3 * i), lFdi = m3_cols(a.lamFd + 3 * i);
+    const float Vri = mm.vol0;
+    float3 lx = make_float3(0.f, 0.f, 0.f), lv = lx;
+    for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
+        const uint32_t j = a.rl.nbr[k] & ~kSameMatBit;
+        const float4 g4 = a.rl.gw[k];
+        const float3 g = f3(g4);
+        const float3 G = m3_vec(Li, g);
+        lx = sub(lx, mul(g4.w, m3_vec(lFi, G)));
+        lv = sub(lv, mul(g4.w, m3_vec(lFdi, G)));
+        // in F_j this particle enters with V_i and L_j gradW(X_i - X_j) = -L_j g
+        const M3 Lj = m3_cols(a.L + 3 * j);
+        const float3 Gj = neg(m3_vec(Lj, g));
+        lx = add(lx, mul(Vri, m3_vec(m3_cols(a.lamF + 3 * j), Gj)));
+        lv = add(lv, mul(Vri, m3_vec(m3_cols(a.lamFd + 3 * j), Gj)));
+    }
+    float4 lp = a.lam_pd[slot], lw = a.lam_vm[slot];
+    lp.x += lx.x;
+    lp.y += lx.y;
+    lp.z += lx.z;
+    lw.x += lv.x;
+    lw.y += lv.y;
+    lw.z += lv.z;
+    a.lam_pd[slot] = lp;
+    a.lam_vm[slot] = lw;
+}
+
+struct Later {
+    const float4* pd[4];
+    const float4* vm[4];
+    float c[4];
+    int n;
+};
+
+__device__ __forceinline__ float4 axpy4(float c, float4 x, float4 y) {
+    return make_float4(y.x + c * x.x, y.y + c * x.y, y.z + c * x.z, y.w + c * x.w);
+}
+
+__global__ void k_adj_weights(uint32_t n, float cb, const float4* __restrict__ lp, const float4* __restrict__ lv,
+                              Later L, float4* __restrict__ mp, float4* __restrict__ mv) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    float4 p = axpy4(cb, lp[k], z), v = axpy4(cb, lv[k], z);
+    for (int t = 0; t < L.n; ++t) {
+        p = axpy4(L.c[t], L.pd[t][k], p);
+        v = axpy4(L.c[t], L.vm[t][k], v);
+    }
+    v.w = 0.0f;
+    mp[k] = p;
+    mv[k] = v;
+}
+
+__global__ void k_adj_perm(uint32_t n, const uint32_t* __restrict__ orig, const float4* __restrict__ ip,
+                           const float4* __restrict__ iv, float4* __restrict__ op, float4* __restrict__ ov,
+                           int scatter) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const uint32_t c = orig[k];
+    if (scatter) {
+        op[c] = ip[k];
+        ov[c] = iv[k];
+    } else {
+        op[k] = ip[c];
+        ov[k] = iv[c];
+    }
+}
+
+}  // namespace
+
+int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st) {
+    int launches = 0;
+    if (a.solid_branch && a.ns > 0) {
+        k_adj_solid<<<nblocks(a.ns, kT), kT, 0, st>>>(a, T);
+        k_adj_strain<<<nblocks(a.ns, kT), kT, 0, st>>>(a, T);
+        launches += 2;
+    }
+    if (a.n > 0) {
+        if (kdim == 2) k_adj_fluid<2><<<nblocks(a.n, kT), kT, 0, st>>>(a, T);
+        else k_adj_fluid<3><<<nblocks(a.n, kT), kT, 0, st>>>(a, T);
+        ++launches;
+    }
+    return launches;
+}
+
+int adjoint_stage_weights(uint32_t n, float cb, const float4* lam_pd, const float4* lam_vm, int nlater,
+                          const float* ca, const float4* const* lamY_pd, const float4* const* lamY_vm,
+                          float4* mu_pd, float4* mu_vm, cudaStream_t st) {
+    if (n == 0) return 0;
+    Later L{};
+    L.n = nlater < 4 ? nlater : 4;
+    for (int t = 0; t < L.n; ++t) {
+        L.pd[t] = lamY_pd[t];
+        L.vm[t] = lamY_vm[t];
+        L.c[t] = ca[t];
+    }
+    k_adj_weights<<<nblocks(n, 256), 256, 0, st>>>(n, cb, lam_pd, lam_vm, L, mu_pd, mu_vm);
+    return 1;
+}
+
+int adjoint_step_sum(uint32_t n, const float4* lam_pd, const float4* lam_vm, int stages,
+                     const float4* const* lamY_pd, const float4* const* lamY_vm, float4* out_pd, float4* out_vm,
+                     cudaStream_t st) {
+    if (n == 0) return 0;
+    Later L{};
+    L.n = stages < 4 ? stages : 4;
+    for (int t = 0; t < L.n; ++t) {
+        L.pd[t] = lamY_pd[t];
+        L.vm[t] = lamY_vm[t];
+        L.c[t] = 1.0f;
+    }
+    k_adj_weights<<<nblocks(n, 256), 256, 0, st>>>(n, 1.0f, lam_pd, lam_vm, L, out_pd, out_vm);
+    return 1;
+}
+
+int adjoint_gather(uint32_t n, const uint32_t* orig, const float4* in_pd, const float4* in_vm, float4* out_pd,
+                   float4* out_vm, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_adj_perm<<<nblocks(n, 256), 256, 0, st>>>(n, orig, in_pd, in_vm, out_pd, out_vm, 0);
+    return 1;
+}
+
+int adjoint_scatter(uint32_t n, const uint32_t* orig, const float4* in_pd, const float4* in_vm, float4* out_pd,
+                    float4* out_vm, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_adj_perm<<<nblocks(n, 256), 256, 0, st>>>(n, orig, in_pd, in_vm, out_pd, out_vm, 1);
+    return 1;
+}
+
+}  // namespace arp

@@ -266,10 +266,64 @@ struct SolidArgs {
     float4* sx;               // [ns] stage position + density in solid-id order (gathered per stage)
     float4* sv;               // [ns] stage velocity + material bits in solid-id order
     uint2* sc;                // [ns] packed cell coordinates in solid-id order
+    const float2* stiff;      // [ns] per-solid (normal, shear) stiffness overriding the material's, or null
     uint32_t ns;
     int all_order2;           // every solid material has strain_order 2
     int any_plastic;          // some solid material is plastic; otherwise the plastic strain stays zero
 };
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st);
+
+// ---- adjoint (reverse mode of one integrator step) ------------------------------
+// Quantities of one RK stage saved by a recording forward step.
+struct AdjStage {
+    const float4* pd;          // stage state, storage order (x, y, z, rho)
+    const float4* vm;          // (vx, vy, vz, material bits)
+    const uint32_t* perm;      // sorted index -> slot of the stage grid (null: identity)
+    const uint32_t* start;     // cell starts of the stage grid
+    const float4* F;           // [3*ns] deformation gradient columns
+    const float4* A;           // [3*ns] sigma * L columns
+    const float4* sx;          // [ns] solid-order state
+    const float4* sv;
+    const uint2* sc;           // [ns] packed cell coordinates
+    const uint32_t* contact_bound;  // [2] self-contact gate of the stage
+};
+struct AdjArgs {
+    AdjStage st;
+    const uint32_t* sid;       // slot -> solid id
+    const uint32_t* slot_of;   // solid id -> slot
+    const float4* mu_pd;       // adjoint of the stage derivative k_s, storage order: (x, y, z, rho)
+    const float4* mu_vm;       // (vx, vy, vz, 0)
+    float4* lam_pd;            // adjoint of the stage state Y_s (accumulated)
+    float4* lam_vm;
+    const float4* bxs;         // boundary, cell order
+    const float4* bvs;
+    const uint32_t* bstart;
+    const float* bps;
+    const float4* ref;
+    const float4* L;
+    SolidRefList rl;
+    const float2* stiff;       // per-solid stiffness override or null
+    float4* lamF;              // [3*ns] adjoint of F (columns), scratch
+    float4* lamFd;             // [3*ns] adjoint of dF/dt
+    float2* g_stiff;           // [ns] accumulated dL/d(normal, shear) stiffness
+    uint32_t* flags;           // bit 0: an active self-contact pair (not differentiated)
+    uint32_t n, ns;
+    int solid_branch;
+};
+// One stage VJP: lam_{Y_s} += J_f(Y_s)^T mu_s (+ stiffness gradients).  Returns launches.
+int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st);
+// mu = cb * lam_next + sum_t ca[t] * lamY[t] over the given later stages.
+int adjoint_stage_weights(uint32_t n, float cb, const float4* lam_pd, const float4* lam_vm, int nlater,
+                          const float* ca, const float4* const* lamY_pd, const float4* const* lamY_vm,
+                          float4* mu_pd, float4* mu_vm, cudaStream_t st);
+// lam_out = lam_next + sum_s lamY[s]
+int adjoint_step_sum(uint32_t n, const float4* lam_pd, const float4* lam_vm, int stages,
+                     const float4* const* lamY_pd, const float4* const* lamY_vm, float4* out_pd, float4* out_vm,
+                     cudaStream_t st);
+// Caller order <-> storage order by orig (slot -> caller id).
+int adjoint_gather(uint32_t n, const uint32_t* orig, const float4* in_pd, const float4* in_vm, float4* out_pd,
+                   float4* out_vm, cudaStream_t st);
+int adjoint_scatter(uint32_t n, const uint32_t* orig, const float4* in_pd, const float4* in_vm, float4* out_pd,
+                    float4* out_vm, cudaStream_t st);
 
 }  // namespace arp

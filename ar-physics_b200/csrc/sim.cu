@@ -142,6 +142,29 @@ struct StateBuf {
     DevBuf<float4> pd, vm;
 };
 
+// ---- reverse mode: what a recording forward step keeps, and the tape ----------
+constexpr int kMaxStages = 4;
+struct StepRecord {
+    DevBuf<float4> pd[kMaxStages], vm[kMaxStages];      // stage states, storage order
+    DevBuf<uint32_t> perm[kMaxStages], start[kMaxStages];
+    bool has_perm[kMaxStages] = {false, false, false, false};
+    DevBuf<float4> F[kMaxStages], A[kMaxStages], sx[kMaxStages], sv[kMaxStages];
+    DevBuf<uint2> sc[kMaxStages];
+    DevBuf<uint32_t> cb[kMaxStages];
+    DevBuf<uint32_t> orig, sid, slot_of;                 // of the step (after its reorder)
+};
+struct Checkpoint {
+    DevBuf<float4> pd, vm;
+    DevBuf<uint32_t> orig, sid;
+    float time = 0.0f;
+};
+struct Tape {
+    uint32_t every = 1;
+    uint64_t steps = 0;                 // steps recorded since the tape began
+    std::vector<Checkpoint> ckpts;      // state before step c * every
+    std::vector<StepRecord> recs;       // one segment of recording steps, reused
+};
+
 }  // namespace
 
 arp_status arp::set_error(arp_status code, const std::string& msg) { return fail(code, msg); }
@@ -226,6 +249,12 @@ struct arp_sim {
     DevBuf<float4> ep, ep_t, ep_s[2], ep_acc, ep_kst[4];
     DevBuf<float4> sx, sv;  // stage state in solid-id order
     DevBuf<uint2> sc;
+    DevBuf<float2> stiff;   // per-solid (normal, shear) stiffness, when set
+    bool have_stiff = false;
+    // reverse mode
+    std::unique_ptr<Tape> tape;
+    StepRecord* rec = nullptr;  // set while a recording step runs
+    bool replaying = false;     // steps re-run by the backward pass take no checkpoints
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
     DevBuf<float4> rl_gw;
     uint32_t rl_nnz = 0;
@@ -504,11 +533,50 @@ void mark(arp_sim* S, arp_sim::Mark& m, int k) {
     cudaEventRecord(m.e[k], S->stream);
 }
 
+// Device-to-device copy into a buffer grown to fit.
+template <class T>
+cudaError_t keep(DevBuf<T>& dst, const T* src, size_t count, cudaStream_t st) {
+    if (dst.n < std::max<size_t>(count, 1)) {
+        cudaError_t e = dst.alloc(count);
+        if (e != cudaSuccess) return e;
+    }
+    if (count == 0) return cudaSuccess;
+    return cudaMemcpyAsync(dst.p, src, count * sizeof(T), cudaMemcpyDeviceToDevice, st);
+}
+
+arp_status save_checkpoint(arp_sim* S) {
+    Checkpoint c;
+    CUDA_TRY(keep(c.pd, (const float4*)S->Y.pd.p, S->n, S->stream));
+    CUDA_TRY(keep(c.vm, (const float4*)S->Y.vm.p, S->n, S->stream));
+    CUDA_TRY(keep(c.orig, (const uint32_t*)S->orig.p, S->n, S->stream));
+    CUDA_TRY(keep(c.sid, (const uint32_t*)S->sid.p, S->n, S->stream));
+    c.time = S->time;
+    S->tape->ckpts.push_back(std::move(c));
+    return ARP_OK;
+}
+
+arp_status restore_checkpoint(arp_sim* S, const Checkpoint& c) {
+    const size_t n = S->n;
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(S->Y.pd.p, c.pd.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, S->stream));
+        CUDA_TRY(cudaMemcpyAsync(S->Y.vm.p, c.vm.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, S->stream));
+        CUDA_TRY(cudaMemcpyAsync(S->orig.p, c.orig.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, S->stream));
+        CUDA_TRY(cudaMemcpyAsync(S->sid.p, c.sid.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, S->stream));
+    }
+    S->time = c.time;
+    return ARP_OK;
+}
+
 arp_status do_step(arp_sim* S) {
     cudaStream_t st = S->stream;
     const uint32_t n = S->n, ns = S->ns;
     const Tableau& tab = S->tab;
     const bool sb = S->solid_branch();
+    if (S->tape && !S->replaying) {
+        if (S->tape->steps % S->tape->every == 0) ARP_TRY(save_checkpoint(S));
+        S->tape->steps++;
+    }
+    StepRecord* R = S->rec;
     S->time += S->dt_sub;
     const uint32_t* bstart = S->b_start.p;
     uint64_t l0 = S->launches;
@@ -524,6 +592,11 @@ arp_status do_step(arp_sim* S) {
     std::swap(S->orig, S->orig_r);
     std::swap(S->sid, S->sid_r);
     if (ns) S->launches += index_solids(S->sid.p, n, S->slot_of.p, st);
+    if (R) {
+        CUDA_TRY(keep(R->orig, (const uint32_t*)S->orig.p, n, st));
+        CUDA_TRY(keep(R->sid, (const uint32_t*)S->sid.p, n, st));
+        CUDA_TRY(keep(R->slot_of, (const uint32_t*)S->slot_of.p, ns, st));
+    }
     uint64_t nl = S->launches - l0;
 
     StageBuffers B{};
@@ -579,6 +652,13 @@ arp_status do_step(arp_sim* S) {
         float4* next_pd = last ? S->T.pd.p : S->S[s % 2].pd.p;
         float4* next_vm = last ? S->T.vm.p : S->S[s % 2].vm.p;
         mark(S, mk, 1);
+        if (R) {
+            CUDA_TRY(keep(R->pd[s], cur_pd, n, st));
+            CUDA_TRY(keep(R->vm[s], cur_vm, n, st));
+            CUDA_TRY(keep(R->start[s], (const uint32_t*)S->gb.start, size_t(S->ncells) + 2, st));
+            R->has_perm[s] = s > 0;
+            if (s > 0) CUDA_TRY(keep(R->perm[s], (const uint32_t*)S->gb.perm, n, st));
+        }
 
         uint64_t sl = 0;
         if (sb) {
@@ -612,9 +692,18 @@ arp_status do_step(arp_sim* S) {
             a.sx = S->sx.p;
             a.sv = S->sv.p;
             a.sc = S->sc.p;
+            a.stiff = S->have_stiff ? S->stiff.p : nullptr;
             sl = launch_solid(a, S->tables, c, st);
             S->launches += sl;
             cur_ep = a.ep_next;
+            if (R) {
+                CUDA_TRY(keep(R->F[s], (const float4*)S->F.p, 3 * size_t(ns), st));
+                CUDA_TRY(keep(R->A[s], (const float4*)S->A.p, 3 * size_t(ns), st));
+                CUDA_TRY(keep(R->sx[s], (const float4*)S->sx.p, ns, st));
+                CUDA_TRY(keep(R->sv[s], (const float4*)S->sv.p, ns, st));
+                CUDA_TRY(keep(R->sc[s], (const uint2*)S->sc.p, ns, st));
+                CUDA_TRY(keep(R->cb[s], (const uint32_t*)S->contact_bound.p, 2, st));
+            }
         }
         mark(S, mk, 2);
 
@@ -1234,7 +1323,7 @@ arp_status capture_graph(arp_sim* S) {
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
     ARP_TRY(need_init(sim));
     uint32_t i = 0;
-    if (sim->use_graph && !sim->profiling && nsteps >= 2) {
+    if (sim->use_graph && !sim->profiling && !sim->tape && nsteps >= 2) {
         if (!sim->graph_exec || sim->graph_stream != sim->stream) ARP_TRY(capture_graph(sim));
         for (; i + 2 <= nsteps; i += 2) {
             CUDA_TRY(cudaGraphLaunch(sim->graph_exec, sim->stream));
@@ -1370,6 +1459,7 @@ arp_status arp_sim_get_interactions(const arp_sim* sim, arp_interaction* out, ui
 
 arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t n) {
     ARP_TRY(need_init(sim));
+    if (sim->tape && sim->tape->steps) return fail(ARP_ERR_INVALID_ARG, "a tape is recording steps");
     if (!in && n) return fail(ARP_ERR_INVALID_ARG, "null argument");
     if (n != sim->n) return fail(ARP_ERR_INVALID_ARG, "particle count differs from the handle's");
     cudaStream_t st = sim->stream;
@@ -1429,6 +1519,8 @@ arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n
     if (sim->scenes.size() != 1) return fail(ARP_ERR_UNSUPPORTED, "add_particles on a batch of scenes");
     if (material->immobile)
         return fail(ARP_ERR_UNSUPPORTED, "added particles join the mobile set; an immobile material is not supported");
+    if (sim->tape) return fail(ARP_ERR_UNSUPPORTED, "add_particles while a tape records");
+    if (sim->have_stiff) return fail(ARP_ERR_UNSUPPORTED, "add_particles with per-solid stiffness set");
     if ((uint64_t)sim->n + n > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "more than 2^31 particles");
     arp_sim::SceneHost& H = sim->scenes[0];
     // particles.rs:550-566: a solid material is always new, any other reuses
@@ -1629,6 +1721,210 @@ arp_status arp_sim_stats(arp_sim* sim, arp_stats* out) {
 arp_status arp_sim_launch_count(const arp_sim* sim, uint64_t* out) {
     if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
     *out = sim->launches;
+    return ARP_OK;
+}
+
+arp_status arp_sim_set_solid_stiffness(arp_sim* sim, const float* normal_shear, uint32_t ns) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (!normal_shear) {
+        sim->have_stiff = false;
+        return ARP_OK;
+    }
+    if (ns != sim->ns) return fail(ARP_ERR_INVALID_ARG, "stiffness count differs from the number of solids");
+    sim->drop_graph();
+    if (ns) {
+        CUDA_TRY(sim->stiff.alloc(ns));
+        CUDA_TRY(cudaMemcpyAsync(sim->stiff.p, normal_shear, ns * sizeof(float2), cudaMemcpyHostToDevice,
+                                 sim->stream));
+        CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    }
+    sim->have_stiff = true;
+    return ARP_OK;
+}
+
+arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
+    ARP_TRY(need_init(sim));
+    if (checkpoint_every == 0) return fail(ARP_ERR_INVALID_ARG, "checkpoint interval must be positive");
+    if (sim->any_plastic) return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate plastic flow");
+    if (!sim->all_order2)
+        return fail(ARP_ERR_UNSUPPORTED, "the adjoint differentiates strain order 2 (Green-Lagrange) only");
+    for (const auto& it : sim->inter)
+        if (it.potential != ARP_CONTACT_ZERO && it.friction != 0.0f)
+            return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate contact friction");
+    if (sim->tab.stages > kMaxStages) return fail(ARP_ERR_UNSUPPORTED, "more than 4 stages");
+    sim->drop_graph();
+    sim->tape.reset(new Tape());
+    sim->tape->every = checkpoint_every;
+    return ARP_OK;
+}
+
+arp_status arp_tape_end(arp_sim* sim) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    sim->tape.reset();
+    return ARP_OK;
+}
+
+arp_status arp_tape_steps(const arp_sim* sim, uint64_t* steps) {
+    if (!sim || !steps) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    *steps = sim->tape ? sim->tape->steps : 0;
+    return ARP_OK;
+}
+
+arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_state0, float* grad_stiffness) {
+    ARP_TRY(need_init(sim));
+    if (!sim->tape) return fail(ARP_ERR_INVALID_ARG, "no tape is recording");
+    if (!dl_dstate || !grad_state0) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    Tape& tp = *sim->tape;
+    const uint32_t n = sim->n, ns = sim->ns;
+    const uint64_t total = tp.steps;
+    cudaStream_t st = sim->stream;
+    const int S = sim->tab.stages;
+    // the forward state is put back when the pass ends
+    Checkpoint now;
+    CUDA_TRY(keep(now.pd, (const float4*)sim->Y.pd.p, n, st));
+    CUDA_TRY(keep(now.vm, (const float4*)sim->Y.vm.p, n, st));
+    CUDA_TRY(keep(now.orig, (const uint32_t*)sim->orig.p, n, st));
+    CUDA_TRY(keep(now.sid, (const uint32_t*)sim->sid.p, n, st));
+    now.time = sim->time;
+    // adjoint buffers: caller order (lc), storage order (ls, out), per stage (lY), stage weights (mu)
+    DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, lY_p[kMaxStages], lY_v[kMaxStages];
+    DevBuf<float4> lamF, lamFd;
+    DevBuf<float2> gst;
+    DevBuf<uint32_t> flags;
+    const size_t nn = std::max(n, 1u);
+    for (DevBuf<float4>* b : {&lc_p, &lc_v, &ls_p, &ls_v, &out_p, &out_v, &mu_p, &mu_v}) CUDA_TRY(b->alloc(nn));
+    for (int q = 0; q < S; ++q) {
+        CUDA_TRY(lY_p[q].alloc(nn));
+        CUDA_TRY(lY_v[q].alloc(nn));
+    }
+    CUDA_TRY(lamF.alloc(3 * size_t(std::max(ns, 1u))));
+    CUDA_TRY(lamFd.alloc(3 * size_t(std::max(ns, 1u))));
+    CUDA_TRY(gst.alloc(std::max(ns, 1u)));
+    CUDA_TRY(flags.alloc(1));
+    CUDA_TRY(cudaMemsetAsync(gst.p, 0, std::max(ns, 1u) * sizeof(float2), st));
+    CUDA_TRY(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t), st));
+    {
+        std::vector<float4> hp(nn), hv(nn);
+        for (uint32_t i = 0; i < n; ++i) {
+            const float* d = dl_dstate + 8 * size_t(i);
+            hp[i] = make_float4(d[0], d[1], d[2], d[3]);
+            hv[i] = make_float4(d[4], d[5], d[6], 0.0f);
+        }
+        if (n) {
+            CUDA_TRY(cudaMemcpyAsync(lc_p.p, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaMemcpyAsync(lc_v.p, hv.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
+            CUDA_TRY(cudaStreamSynchronize(st));
+        }
+    }
+    const uint32_t every = tp.every;
+    if (tp.recs.size() < every) tp.recs.resize(every);
+    const uint64_t nseg = (total + every - 1) / every;
+    sim->replaying = true;
+    arp_status status = ARP_OK;
+    for (uint64_t seg = nseg; seg-- > 0 && status == ARP_OK;) {
+        const uint64_t t0 = seg * every, t1 = std::min<uint64_t>(t0 + every, total);
+        status = restore_checkpoint(sim, tp.ckpts[seg]);
+        for (uint64_t t = t0; t < t1 && status == ARP_OK; ++t) {
+            sim->rec = &tp.recs[t - t0];
+            status = do_step(sim);
+            sim->rec = nullptr;
+        }
+        for (uint64_t t = t1; t-- > t0 && status == ARP_OK;) {
+            const StepRecord& R = tp.recs[t - t0];
+            sim->launches += adjoint_gather(n, R.orig.p, lc_p.p, lc_v.p, ls_p.p, ls_v.p, st);
+            for (int q = S - 1; q >= 0; --q) {
+                float ca[kMaxStages];
+                const float4* lp[kMaxStages];
+                const float4* lv[kMaxStages];
+                int nl = 0;
+                for (int u = q + 1; u < S; ++u)
+                    if (sim->tab.a[u][q] != 0.0) {
+                        ca[nl] = (float)(sim->tab.a[u][q] * (double)sim->dt_sub);
+                        lp[nl] = lY_p[u].p;
+                        lv[nl] = lY_v[u].p;
+                        ++nl;
+                    }
+                const float cb = (float)(sim->tab.b[q] * (double)sim->dt_sub);
+                sim->launches += adjoint_stage_weights(n, cb, ls_p.p, ls_v.p, nl, ca, lp, lv, mu_p.p, mu_v.p, st);
+                if (n) {
+                    cudaMemsetAsync(lY_p[q].p, 0, n * sizeof(float4), st);
+                    cudaMemsetAsync(lY_v[q].p, 0, n * sizeof(float4), st);
+                }
+                AdjArgs a{};
+                a.st.pd = R.pd[q].p;
+                a.st.vm = R.vm[q].p;
+                a.st.perm = R.has_perm[q] ? R.perm[q].p : nullptr;
+                a.st.start = R.start[q].p;
+                const bool sb = sim->solid_branch();
+                a.st.F = sb ? R.F[q].p : nullptr;
+                a.st.A = sb ? R.A[q].p : nullptr;
+                a.st.sx = sb ? R.sx[q].p : nullptr;
+                a.st.sv = sb ? R.sv[q].p : nullptr;
+                a.st.sc = sb ? R.sc[q].p : nullptr;
+                a.st.contact_bound = sb ? R.cb[q].p : nullptr;
+                a.sid = R.sid.p;
+                a.slot_of = R.slot_of.p;
+                a.mu_pd = mu_p.p;
+                a.mu_vm = mu_v.p;
+                a.lam_pd = lY_p[q].p;
+                a.lam_vm = lY_v[q].p;
+                a.bxs = sim->b_pd.p;
+                a.bvs = sim->b_vm.p;
+                a.bstart = sim->b_start.p;
+                a.bps = sim->bps.p;
+                a.ref = sim->ref.p;
+                a.L = sim->L.p;
+                a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz};
+                a.stiff = sim->have_stiff ? sim->stiff.p : nullptr;
+                a.lamF = lamF.p;
+                a.lamFd = lamFd.p;
+                a.g_stiff = gst.p;
+                a.flags = flags.p;
+                a.n = n;
+                a.ns = ns;
+                a.solid_branch = sb ? 1 : 0;
+                sim->launches += launch_adjoint_stage(a, sim->tables, sim->kdim, st);
+            }
+            const float4* yp[kMaxStages];
+            const float4* yv[kMaxStages];
+            for (int q = 0; q < S; ++q) {
+                yp[q] = lY_p[q].p;
+                yv[q] = lY_v[q].p;
+            }
+            sim->launches += adjoint_step_sum(n, ls_p.p, ls_v.p, S, yp, yv, out_p.p, out_v.p, st);
+            sim->launches += adjoint_scatter(n, R.orig.p, out_p.p, out_v.p, lc_p.p, lc_v.p, st);
+        }
+        if (status == ARP_OK) {
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) status = fail(ARP_ERR_CUDA, std::string("adjoint: ") + cudaGetErrorString(e));
+        }
+    }
+    sim->replaying = false;
+    sim->rec = nullptr;
+    ARP_TRY(status);
+    ARP_TRY(restore_checkpoint(sim, now));
+    ARP_TRY(check_launch("adjoint"));
+    std::vector<float4> hp(nn), hv(nn);
+    std::vector<float2> hg(std::max(ns, 1u));
+    uint32_t hflags = 0;
+    if (n) {
+        CUDA_TRY(cudaMemcpyAsync(hp.data(), lc_p.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(hv.data(), lc_v.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    }
+    if (ns) CUDA_TRY(cudaMemcpyAsync(hg.data(), gst.p, ns * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaMemcpyAsync(&hflags, flags.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    for (uint32_t i = 0; i < n; ++i) {
+        float* d = grad_state0 + 8 * size_t(i);
+        d[0] = hp[i].x; d[1] = hp[i].y; d[2] = hp[i].z; d[3] = hp[i].w;
+        d[4] = hv[i].x; d[5] = hv[i].y; d[6] = hv[i].z; d[7] = 0.0f;
+    }
+    if (grad_stiffness)
+        for (uint32_t q = 0; q < ns; ++q) {
+            grad_stiffness[2 * q] = hg[q].x;
+            grad_stiffness[2 * q + 1] = hg[q].y;
+        }
+    if (hflags & 1u) return fail(ARP_ERR_UNSUPPORTED, "a self-contact pair was active; it is not differentiated");
     return ARP_OK;
 }
 

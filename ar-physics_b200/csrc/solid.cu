@@ -311,7 +311,8 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
     const M4 strain = PLASTIC ? m4_add(seth_hill<ORDER2>(Fm, mm.strain_order, P.dim), EP)
                               : seth_hill<ORDER2>(Fm, mm.strain_order, P.dim);
     const M4 rate = seth_hill_rate<ORDER2>(Fm, Fdm, mm.strain_order, P.dim);
-    const M4 pk2 = m4_add(hooke(strain, mm.lam, mm.mu, P.dim), hooke(rate, mm.lam_d, mm.mu_d, P.dim));
+    const float2 lm = a.stiff ? a.stiff[i] : make_float2(mm.lam, mm.mu);
+    const M4 pk2 = m4_add(hooke(strain, lm.x, lm.y, P.dim), hooke(rate, mm.lam_d, mm.mu_d, P.dim));
     const M4 sigma = m4_mul(Fm, m4_transpose(pk2));
     const M4 A = m4_mul(sigma, Lm);
 #pragma unroll

@@ -372,6 +372,35 @@ arp_status arp_sim_launch_count(const arp_sim* sim, uint64_t* out);
 const char* arp_last_error(void);
 uint32_t arp_abi_version(void);
 
+/* ---- per-particle stiffness and reverse mode (no counterpart in the reference) -- */
+
+/* Per-solid (normal, shear) stiffness — the Lame pair the reference keeps per
+ * material in `normal_stiffness`/`shear_stiffness` (same sign convention) —
+ * overriding the materials' values in the stress (solid.rs:139-141,339), 2
+ * floats per solid in solid-id order; NULL restores the material values.
+ * `ns` must equal the handle's solid count. */
+arp_status arp_sim_set_solid_stiffness(arp_sim* sim, const float* normal_shear, uint32_t ns);
+
+/* Reverse-mode differentiation of the steps taken after arp_tape_begin.  The
+ * state before every `checkpoint_every`-th step is kept; arp_tape_backward
+ * re-runs each segment from its checkpoint recording the stage states, then
+ * applies the hand-written adjoint of every stage (neighbor sets reused, not
+ * differentiated) in reverse.  CUDA-graph replay is off while a tape records.
+ * Refused (ARP_ERR_UNSUPPORTED) for plastic materials, strain orders other
+ * than 2 and contact friction; a self-contact pair found active during the
+ * backward pass makes it return ARP_ERR_UNSUPPORTED after filling the outputs
+ * (that term is not differentiated). */
+arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every);
+arp_status arp_tape_end(arp_sim* sim);
+arp_status arp_tape_steps(const arp_sim* sim, uint64_t* steps);
+/* `dl_dstate`: dL/d(state after the last recorded step), 8 floats per mobile
+ * particle in caller order (dx, dy, dz, drho, dvx, dvy, dvz, unused).
+ * `grad_state0` receives dL/d(state when the tape began) in the same layout;
+ * `grad_stiffness` (may be NULL) dL/d(normal, shear) per solid in solid-id
+ * order, with the materials' values where no per-solid stiffness is set.  The
+ * handle's current state is unchanged. */
+arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_state0, float* grad_stiffness);
+
 #ifdef __cplusplus
 }
 #endif

@@ -713,10 +713,16 @@ public:
         mat4<T> dev = strain - (trace(strain) * identity<T>()) / T(int(dim));
         return T(int(dim - 1) / int(dim)) * mat_dot(dev, dev);
     }
-    mat4<T> pk2_of(const mat4<T>& def, const mat4<T>& def_rate, const mat4<T>& plastic, const Mat<T>& m) const {
+    // per-solid (normal, shear) stiffness overriding the material's (empty: none)
+    std::vector<T> solid_stiff;
+    mat4<T> pk2_of(const mat4<T>& def, const mat4<T>& def_rate, const mat4<T>& plastic, const Mat<T>& m,
+                   uint32_t s_id) const {
         mat4<T> strain = seth_hill(def, m.strain_order) + plastic;
         mat4<T> rate = seth_hill_rate(def, def_rate, m.strain_order);
-        return hooke(strain, m.normal_stiffness, m.shear_stiffness) + hooke(rate, m.normal_damp, m.shear_damp);
+        const bool own = 2 * size_t(s_id) + 1 < solid_stiff.size();
+        const T n = own ? solid_stiff[2 * s_id] : m.normal_stiffness;
+        const T sh = own ? solid_stiff[2 * s_id + 1] : m.shear_stiffness;
+        return hooke(strain, n, sh) + hooke(rate, m.normal_damp, m.shear_damp);
     }
 
     // solid.rs:276-524
@@ -747,7 +753,7 @@ public:
             const bool elastic = mm.stiff();
             if (!elastic) continue;
             const mat4<T>& def = strains[s_id].F;
-            const mat4<T> pk2 = pk2_of(def, strains[s_id].Fdot, S[s_id].stress, mm);
+            const mat4<T> pk2 = pk2_of(def, strains[s_id].Fdot, S[s_id].stress, mm, s_id);
             const mat4<T> stress = def * transpose(pk2);
             std::vector<vec4<T>> sforce(81);
             for (uint32_t gid = 0; gid < 81; ++gid) {
@@ -768,7 +774,7 @@ public:
                         if (!literal && !(h * h - dot(r, r) > T(0))) continue;  // grad_w == 0
                         const T V2 = m1 / P[p_id2].den;
                         const mat4<T>& def2 = strains[s_id2].F;
-                        const mat4<T> pk2b = pk2_of(def2, strains[s_id2].Fdot, S[s_id2].stress, mm);
+                        const mat4<T> pk2b = pk2_of(def2, strains[s_id2].Fdot, S[s_id2].stress, mm, s_id2);
                         const mat4<T> stress2 = def2 * transpose(pk2b);
                         vec4<T> el_force =
                             ((-V1 * V2) * (stress * correction + stress2 * strains[s_id2].L)) * grad_w(r, h, kconst);
@@ -1028,6 +1034,17 @@ int orc_add_particles(void* h, const arp_particle* p, uint32_t n, const arp_mate
     bool added = false;
     dispatch(h, [&](auto& S) { added = S.add_particles(p, n, *m, offset); });
     if (material_added) *material_added = added ? 1 : 0;
+    return 0;
+}
+
+// Per-solid (normal, shear) stiffness, 2 values per solid id (NULL clears).
+int orc_set_solid_stiffness(void* h, const double* normal_shear, uint32_t ns) {
+    dispatch(h, [&](auto& S) {
+        using TT = std::remove_reference_t<decltype(S.h)>;
+        S.solid_stiff.clear();
+        if (normal_shear)
+            for (uint32_t i = 0; i < 2 * ns; ++i) S.solid_stiff.push_back(TT(normal_shear[i]));
+    });
     return 0;
 }
 

@@ -45,6 +45,7 @@ def lib():
         L.orc_add_particles.argtypes = [vp, vp, ctypes.c_uint32, vp, vp, ctypes.POINTER(ctypes.c_int)]
         L.orc_materials.argtypes = [vp, u32p, vp, ctypes.c_uint32]
         L.orc_interactions.argtypes = [vp, vp]
+        L.orc_set_solid_stiffness.argtypes = [vp, vp, ctypes.c_uint32]
         _L = L
     return _L
 
@@ -105,6 +106,14 @@ class Oracle:
         lib().orc_add_particles(self.h, _p(p), len(p), _p(m), _p(off), ctypes.byref(added))
         self._refresh_counts()
         return bool(added.value)
+
+    def set_solid_stiffness(self, normal_shear):
+        """Per-solid (normal, shear) stiffness overriding the materials' (None clears)."""
+        if normal_shear is None:
+            lib().orc_set_solid_stiffness(self.h, None, 0)
+            return
+        a = np.ascontiguousarray(normal_shear, dtype=np.float64).reshape(-1, 2)
+        lib().orc_set_solid_stiffness(self.h, _p(a), len(a))
 
     def materials(self):
         from arphys.abi import MATERIAL_DTYPE
