@@ -213,6 +213,86 @@ def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
             "note": "working set > L2 (no flush); batch replayed from a CUDA graph; loop = one simulation per scene"}
 
 
+def _time_adjoint(torch, stream, sim, steps, every, loss_grad):
+    """Plain forward, taped forward and backward of `steps` steps from the
+    handle's current state (device time for the forwards, host wall clock
+    around the backward call, which synchronizes)."""
+    import time
+    import numpy as np
+    init = sim.particles().copy()
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_fwd = e0.elapsed_time(e1)
+    sim.set_particles(init)
+    sim.tape_begin(every)
+    e0.record(stream)
+    sim.step(steps)
+    e1.record(stream)
+    torch.cuda.synchronize()
+    t_tape = e0.elapsed_time(e1)
+    grad = np.zeros((sim.n, 8), np.float32)
+    L, gx = loss_grad(sim.particles()["pos"])
+    grad[:, :3] = gx
+    t0 = time.perf_counter()
+    g0, gs = sim.backward(grad)
+    torch.cuda.synchronize()
+    t_bwd = (time.perf_counter() - t0) * 1000.0
+    sim.tape_end()
+    return {"steps": steps, "checkpoint_every": every, "forward_ms": t_fwd, "forward_taped_ms": t_tape,
+            "backward_ms": t_bwd, "adjoint_fwd_ratio": t_bwd / t_fwd, "loss": L,
+            "grad_v0_norm": float(np.linalg.norm(g0[:, 4:7])), "grad_stiffness_norm": float(np.linalg.norm(gs))}
+
+
+def run_adjoint(torch, stream):
+    """Reverse mode on the two differentiation workloads: the 16x16x256 bar
+    (65,536 particles, per-particle E, 400 RK2 steps, checkpoints every 20;
+    gradient of the tip-centroid loss w.r.t. per-particle stiffness and
+    initial velocity) and 64 batched 2D Rayleigh-Taylor scenes (300 RK2 steps,
+    gradient of the heavy/light centroid separation w.r.t. the initial
+    velocities of all scenes, one backward pass for the batch)."""
+    import numpy as np
+    from arphys import FluidSim, scenes
+    sc = scenes.cantilever_bar()
+    sim = FluidSim(sc)
+    sim.init()
+    sim.set_stream(stream.cuda_stream)
+    sim.set_solid_stiffness(sc.meta["stiffness"])
+    init = sim.particles().copy()
+    sim.step(3)  # warm-up
+    sim.set_particles(init)
+    tip, target = sc.meta["tip"], sc.meta["target"]
+    bar = _time_adjoint(torch, stream, sim, 400, 20, lambda pos: scenes.tip_loss(pos, tip, target))
+    bar["workload"] = ("cantilever bar 16x16x256 (65,024 elastic + 512 clamped), per-particle E lognormal("
+                       "ln 1e5, 0.3), nu 0.3, gravity, RK2, dt 1e-4")
+    sim.close()
+    scs = scenes.rayleigh_taylor_batch()
+    batch = FluidSim.batch(scs)
+    batch.init()
+    batch.set_stream(stream.cuda_stream)
+    init = batch.particles().copy()
+    batch.step(3)  # warm-up
+    batch.set_particles(init)
+    offsets = np.cumsum([0] + [s.n for s in scs])
+
+    def sep_grad(pos):
+        g = np.zeros((len(pos), 3))
+        tot = 0.0
+        for k, s in enumerate(scs):
+            L, gk = scenes.separation(pos[offsets[k]:offsets[k + 1]], s.meta["heavy"])
+            g[offsets[k]:offsets[k + 1]] = gk
+            tot += L
+        return tot, g
+    rt = _time_adjoint(torch, stream, batch, 300, 20, sep_grad)
+    rt["workload"] = (f"{len(scs)} 2D Rayleigh-Taylor scenes, {int(offsets[-1])} particles (8,192-131,072 per "
+                      "scene), heavy 1800 over light 1000, RK2, dt 1e-4; loss = sum of heavy/light centroid "
+                      "separations")
+    batch.close()
+    return {"bar": bar, "rayleigh_taylor_batch": rt}
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference's path cannot run here (Rust + OpenGL
     compute shaders, no GL stack), so the CPU restatement of its shaders is
@@ -336,6 +416,8 @@ def run_ours(args, rank, world, local_rank):
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
     }
     line["fluid_launch_shape"] = sim.fluid_variant()
+    if rank == 0 and not args.no_adjoint:
+        line["adjoint"] = run_adjoint(torch, stream)
     if rank == 0 and not args.no_batched:
         line["batched"] = run_batched(torch, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
@@ -354,6 +436,7 @@ def main():
     ap.add_argument("--config", default="c2", choices=["c1", "c2"])
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
+    ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--fluid-variant", type=int, default=None, help="pin the fluid launch shape (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
