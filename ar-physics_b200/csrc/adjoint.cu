@@ -158,97 +158,127 @@ __device__ __forceinline__ float cpot(uint32_t eq, float r, float S, float R0, f
 
 struct PairSide {
     float3 x, v;
-    float d, pt;
+    float d, inv_d, pt;
     float m, visc, bulk;
     uint32_t mat;
     bool elastic;
+};
+// What the two orientations of a pair share: r = x_b - x_a, v_b - v_a, gradW,
+// the contact potential (the interaction matrix is symmetric).
+struct PairGeom {
+    float3 r, vv, g;
+    float gws, c24, inv_denom;  // c24 = 24 k (h^2 - r.r): d gws / d r = c24 r
+    float cp, dcp_over_R;
+    bool contact;
 };
 struct PairGrad {
     float3 F;        // forward force contribution to the self particle
     float3 lr;       // dL/dr, r = x_nbr - x_self
     float3 lvv;      // dL/d(v_nbr - v_self)
-    float ld_self, ld_nbr, lpt_self, lpt_nbr;
+    float ld_self, ld_nbr, lpt;
 };
 
-// The fluid pair term of `self` with neighbor `nbr` (fluid.rs:154-214, as the
-// forward kernel evaluates it) and its vector-Jacobian product for weights
-// wd (on d rho/dt) and wF (on the force sum).  Friction is not included.
-template <int DIM, bool BOUNDARY>
-__device__ __forceinline__ void pair_vjp(const PairSide& a, const PairSide& b, const DevInter& it, float h2, float kc,
-                                         float eps_hh, float wd, float3 wF, PairGrad& o) {
-    float3 r = sub(b.x, a.x), vv = sub(b.v, a.v);
+template <int DIM>
+__device__ __forceinline__ PairGeom make_geom(float3 xa, float3 va, float3 xb, float3 vb, const DevInter& it,
+                                              float h2, float kc, float eps_hh) {
+    PairGeom G;
+    G.r = sub(xb, xa);
+    G.vv = sub(vb, va);
     if (DIM == 2) {
-        r.z = 0.0f;
-        vv.z = 0.0f;
+        G.r.z = 0.0f;
+        G.vv.z = 0.0f;
     }
-    const float r2 = dot(r, r);
+    const float r2 = dot(G.r, G.r);
     const float diff = fmaxf(h2 - r2, 0.0f);
-    const float gws = -6.0f * kc * diff * diff;
-    const float3 g = mul(gws, r);
-    float3 F = make_float3(0.f, 0.f, 0.f), lg = F, lr = F, lvv = F;
-    float ld1 = 0.f, ld2 = 0.f;
-    if (!BOUNDARY) {
-        lvv = add(lvv, mul(wd * b.m, g));
-        lg = add(lg, mul(wd * b.m, vv));
-    }
-    const float mm = a.m * b.m;
-    const float pf = mm * (a.pt + b.pt);
-    F = add(F, mul(pf, g));
-    lg = add(lg, mul(pf, wF));
-    const float lpt = mm * dot(wF, g);
+    G.gws = -6.0f * kc * diff * diff;
+    G.c24 = 24.0f * kc * diff;
+    G.g = mul(G.gws, G.r);
+    G.inv_denom = __fdividef(1.0f, r2 + eps_hh);
+    G.cp = 0.0f;
+    G.dcp_over_R = 0.0f;
+    G.contact = false;
     if (it.potential != ARP_CONTACT_ZERO) {
         const float R = sqrtf(r2);
         float dcp;
-        const float cp = cpot(it.potential, R, it.radius, it.strength, dcp);
-        if (cp != 0.0f) {
-            const float cs = b.m * cp / b.d;
-            F = add(F, mul(cs, g));
-            lg = add(lg, mul(cs, wF));
-            const float lcs = dot(wF, g);
-            ld2 -= lcs * cs / b.d;
-            const float lR = lcs * b.m / b.d * dcp;
-            if (R > 0.0f) lr = add(lr, mul(lR / R, r));
-        }
+        G.cp = cpot(it.potential, R, it.radius, it.strength, dcp);
+        G.contact = G.cp != 0.0f;
+        G.dcp_over_R = R > 0.0f ? __fdividef(dcp, R) : 0.0f;
+    }
+    return G;
+}
+__device__ __forceinline__ PairGeom flipped(const PairGeom& G) {
+    PairGeom H = G;
+    H.r = neg(G.r);
+    H.vv = neg(G.vv);
+    H.g = neg(G.g);
+    return H;
+}
+
+// The fluid pair term of `a` with neighbor `b` (fluid.rs:154-214, as the
+// forward kernel evaluates it) and its vector-Jacobian product for weights
+// wd (on d rho/dt) and wF (on the force sum).  Friction is not included.
+template <int DIM, bool BOUNDARY>
+__device__ __forceinline__ void pair_vjp(const PairGeom& G, const PairSide& a, const PairSide& b, float dampening,
+                                         float wd, float3 wF, PairGrad& o) {
+    const float3 r = G.r, vv = G.vv, g = G.g;
+    float3 F = make_float3(0.f, 0.f, 0.f), lg = F, lr = F, lvv = F;
+    float ld1 = 0.f, ld2 = 0.f;
+    if (!BOUNDARY) {
+        lvv = mul(wd * b.m, g);
+        lg = mul(wd * b.m, vv);
+    }
+    const float mm = a.m * b.m;
+    const float pf = mm * (a.pt + b.pt);
+    F = mul(pf, g);
+    lg = add(lg, mul(pf, wF));
+    const float wg = dot(wF, g);
+    const float lpt = mm * wg;
+    if (G.contact) {
+        const float cs = b.m * G.cp * b.inv_d;
+        F = add(F, mul(cs, g));
+        lg = add(lg, mul(cs, wF));
+        ld2 -= wg * cs * b.inv_d;
+        lr = mul(wg * b.m * b.inv_d * G.dcp_over_R, r);
     }
     if (!BOUNDARY) {
-        const float denom = r2 + eps_hh;
         float ldenom = 0.0f;
         if (!a.elastic) {
             const float fsum = a.visc + b.visc;
             if (fsum != 0.0f) {
                 const float rgw = dot(r, g);
-                const float dd = a.d * b.d * denom;
-                const float t = mm * fsum * rgw / dd;
+                const float idd = a.inv_d * b.inv_d * G.inv_denom;
+                const float t = mm * fsum * rgw * idd;
                 F = sub(F, mul(t, vv));
                 lvv = sub(lvv, mul(t, wF));
                 const float lt = -dot(wF, vv);
-                const float lrgw = lt * mm * fsum / dd;
-                ld1 -= lt * t / a.d;
-                ld2 -= lt * t / b.d;
-                ldenom -= lt * t / denom;
+                const float lrgw = lt * mm * fsum * idd;
+                ld1 -= lt * t * a.inv_d;
+                ld2 -= lt * t * b.inv_d;
+                ldenom -= lt * t * G.inv_denom;
                 lr = add(lr, mul(lrgw, g));
                 lg = add(lg, mul(lrgw, r));
             }
         }
-        const float f_ = a.mat == b.mat ? a.bulk + b.bulk : it.dampening;
+        const float f_ = a.mat == b.mat ? a.bulk + b.bulk : dampening;
         if (f_ != 0.0f) {
             const float vr = dot(vv, r);
-            const float ds = a.d + b.d;
-            const float Q = mm * (f_ * vr / (ds * denom));
+            const float ids = __fdividef(1.0f, a.d + b.d);
+            const float q0 = mm * f_ * ids * G.inv_denom;
+            const float Q = q0 * vr;
             F = sub(F, mul(Q, g));
             lg = sub(lg, mul(Q, wF));
-            const float lQ = -dot(wF, g);
-            const float lvr = lQ * mm * f_ / (ds * denom);
-            ld1 -= lQ * Q / ds;
-            ld2 -= lQ * Q / ds;
-            ldenom -= lQ * Q / denom;
+            const float lQ = -wg;
+            const float lvr = lQ * q0;
+            ld1 -= lQ * Q * ids;
+            ld2 -= lQ * Q * ids;
+            ldenom -= lQ * Q * G.inv_denom;
             lvv = add(lvv, mul(lvr, r));
             lr = add(lr, mul(lvr, vv));
         }
         lr = add(lr, mul(2.0f * ldenom, r));
     }
     // g = gws(r) r, gws = -6 k (h^2 - r.r)^2
-    lr = add(lr, add(mul(gws, lg), mul(24.0f * kc * diff * dot(lg, r), r)));
+    lr = add(lr, add(mul(G.gws, lg), mul(G.c24 * dot(lg, r), r)));
     if (DIM == 2) {
         lr.z = 0.0f;
         lvv.z = 0.0f;
@@ -258,12 +288,28 @@ __device__ __forceinline__ void pair_vjp(const PairSide& a, const PairSide& b, c
     o.lvv = lvv;
     o.ld_self = ld1;
     o.ld_nbr = ld2;
-    o.lpt_self = lpt;
-    o.lpt_nbr = lpt;
+    o.lpt = lpt;
+}
+
+// Per particle of the stage: the weights of its derivative record and its
+// state-equation terms, read by its own thread and by its neighbors':
+// w = (mu_v / rho, mu_rho), e = (p / rho^2, d(p / rho^2)/d rho, 1 / rho).
+__global__ void k_adj_prep(AdjArgs a, Tables T, float4* __restrict__ w, float4* __restrict__ e) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= a.n) return;
+    const float4 xi = a.st.pd[i];
+    const FluidMat fm = T.fmats[__float_as_uint(a.st.vm[i].w)];
+    const float ir = 1.0f / xi.w;
+    const float4 mv = a.mu_vm[i];
+    w[i] = make_float4(mv.x * ir, mv.y * ir, mv.z * ir, a.mu_pd[i].w);
+    float pt, dpt;
+    eos_pt(fm.eos, xi.w, fm.c, fm.d0, pt, dpt);
+    e[i] = make_float4(pt, dpt, ir, 0.0f);
 }
 
 template <int DIM>
-__global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T) {
+__global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const float4* __restrict__ W,
+                                                  const float4* __restrict__ EQ) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const float4 xi = a.st.pd[i], vi = a.st.vm[i];
@@ -272,15 +318,15 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T) {
     const SceneP& P = T.scenes[mm.scene];
     const FluidMat fm = T.fmats[mat];
     const uint32_t sid = a.sid[i];
-    PairSide si{f3(xi), f3(vi), xi.w, 0.0f, fm.mass, fm.visc, fm.bulk, mat, sid != kInvalid && fm.stiff != 0u};
-    float dpt_i;
-    eos_pt(fm.eos, xi.w, fm.c, fm.d0, si.pt, dpt_i);
-    const float4 mup = a.mu_pd[i], muv = a.mu_vm[i];
-    const float wd = mup.w;
-    const float3 wF = mul(1.0f / xi.w, f3(muv));
+    const float4 ei = EQ[i], wi = W[i];
+    const PairSide si{f3(xi), f3(vi), xi.w, ei.z, ei.x, fm.mass, fm.visc, fm.bulk, mat,
+                      sid != kInvalid && fm.stiff != 0u};
+    const float dpt_i = ei.y;
+    const float wd = wi.w;
+    const float3 wF = f3(wi);
     const bool solid_term = a.solid_branch && sid != kInvalid && P.solid_branch;
     float3 lx = make_float3(0.f, 0.f, 0.f);
-    float3 lv = mul(solid_term ? 2.0f : 1.0f, f3(mup));  // dx/dt = v (twice for solids in the solid branch)
+    float3 lv = mul(solid_term ? 2.0f : 1.0f, f3(a.mu_pd[i]));  // dx/dt = v (twice for solids in the solid branch)
     float lrho = 0.0f;
     float3 Fs = make_float3(0.f, 0.f, 0.f);
     const uint32_t li = mat - P.mat_base;
@@ -302,13 +348,16 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T) {
                     const float4 vb = a.bvs[jb];
                     const uint32_t matb = __float_as_uint(vb.w);
                     const FluidMat fb = T.fmats[matb];
-                    const PairSide sb{f3(xb), f3(vb), xb.w, a.bps[jb], fb.mass, fb.visc, fb.bulk, matb, false};
+                    const PairSide sb{f3(xb), f3(vb), xb.w, __fdividef(1.0f, xb.w), a.bps[jb], fb.mass, fb.visc,
+                                      fb.bulk, matb, false};
+                    const DevInter it = row_i[matb - P.mat_base];
+                    const PairGeom G = make_geom<DIM>(si.x, si.v, sb.x, sb.v, it, P.h2, P.kconst, P.eps_hh);
                     PairGrad o;
-                    pair_vjp<DIM, true>(si, sb, row_i[matb - P.mat_base], P.h2, P.kconst, P.eps_hh, wd, wF, o);
+                    pair_vjp<DIM, true>(G, si, sb, it.dampening, wd, wF, o);
                     Fs = add(Fs, o.F);
                     lx = sub(lx, o.lr);
                     lv = sub(lv, o.lvv);
-                    lrho += o.ld_self + o.lpt_self * dpt_i;
+                    lrho += o.ld_self + o.lpt * dpt_i;
                 }
                 for (uint32_t k = a.st.start[c0]; k < a.st.start[c1]; ++k) {
                     const uint32_t j = a.st.perm ? a.st.perm[k] : k;
@@ -320,27 +369,26 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T) {
                     const uint32_t matj = __float_as_uint(vj.w);
                     const FluidMat fj = T.fmats[matj];
                     const uint32_t sidj = a.sid[j];
-                    PairSide sj{f3(xj), f3(vj), xj.w, 0.0f, fj.mass, fj.visc, fj.bulk, matj,
-                                sidj != kInvalid && fj.stiff != 0u};
-                    float dpt_j;
-                    eos_pt(fj.eos, xj.w, fj.c, fj.d0, sj.pt, dpt_j);
+                    const float4 ej = EQ[j], wj = W[j];
+                    const PairSide sj{f3(xj), f3(vj), xj.w, ej.z, ej.x, fj.mass, fj.visc, fj.bulk, matj,
+                                      sidj != kInvalid && fj.stiff != 0u};
+                    const DevInter it = row_i[matj - P.mat_base];  // symmetric: also the neighbor's entry
+                    const PairGeom G = make_geom<DIM>(si.x, si.v, sj.x, sj.v, it, P.h2, P.kconst, P.eps_hh);
                     PairGrad o;
-                    pair_vjp<DIM, false>(si, sj, row_i[matj - P.mat_base], P.h2, P.kconst, P.eps_hh, wd, wF, o);
+                    pair_vjp<DIM, false>(G, si, sj, it.dampening, wd, wF, o);
                     Fs = add(Fs, o.F);
                     lx = sub(lx, o.lr);
                     lv = sub(lv, o.lvv);
-                    lrho += o.ld_self + o.lpt_self * dpt_i;
+                    lrho += o.ld_self + o.lpt * dpt_i;
                     // the neighbor's own pair, in which this particle is the neighbor
-                    const float4 mupj = a.mu_pd[j], muvj = a.mu_vm[j];
-                    const DevInter itj = T.inter[P.inter_base + (matj - P.mat_base) * P.nmat + li];
-                    pair_vjp<DIM, false>(sj, si, itj, P.h2, P.kconst, P.eps_hh, mupj.w, mul(1.0f / xj.w, f3(muvj)), o);
+                    pair_vjp<DIM, false>(flipped(G), sj, si, it.dampening, wj.w, f3(wj), o);
                     lx = add(lx, o.lr);
                     lv = add(lv, o.lvv);
-                    lrho += o.ld_nbr + o.lpt_nbr * dpt_i;
+                    lrho += o.ld_nbr + o.lpt * dpt_i;
                 }
             }
     }
-    lrho -= dot(wF, Fs) / xi.w;  // k_v = F / rho
+    lrho -= dot(wF, Fs) * ei.z;  // k_v = F / rho
     if (DIM == 2) {
         lx.z = 0.0f;
         lv.z = 0.0f;
@@ -661,9 +709,10 @@ int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream
         launches += 2;
     }
     if (a.n > 0) {
-        if (kdim == 2) k_adj_fluid<2><<<nblocks(a.n, kT), kT, 0, st>>>(a, T);
-        else k_adj_fluid<3><<<nblocks(a.n, kT), kT, 0, st>>>(a, T);
-        ++launches;
+        k_adj_prep<<<nblocks(a.n, 256), 256, 0, st>>>(a, T, a.w, a.eq);
+        if (kdim == 2) k_adj_fluid<2><<<nblocks(a.n, kT), kT, 0, st>>>(a, T, a.w, a.eq);
+        else k_adj_fluid<3><<<nblocks(a.n, kT), kT, 0, st>>>(a, T, a.w, a.eq);
+        launches += 2;
     }
     return launches;
 }

@@ -307,6 +307,8 @@ struct AdjArgs {
     float4* lamFd;             // [3*ns] adjoint of dF/dt
     float2* g_stiff;           // [ns] accumulated dL/d(normal, shear) stiffness
     uint32_t* flags;           // bit 0: an active self-contact pair (not differentiated)
+    float4* w;                 // [n] scratch: per-particle weights of the stage
+    float4* eq;                // [n] scratch: per-particle state-equation terms
     uint32_t n, ns;
     int solid_branch;
 };

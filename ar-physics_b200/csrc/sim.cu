@@ -1788,11 +1788,12 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     now.time = sim->time;
     // adjoint buffers: caller order (lc), storage order (ls, out), per stage (lY), stage weights (mu)
     DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, lY_p[kMaxStages], lY_v[kMaxStages];
-    DevBuf<float4> lamF, lamFd;
+    DevBuf<float4> lamF, lamFd, wbuf, ebuf;
     DevBuf<float2> gst;
     DevBuf<uint32_t> flags;
     const size_t nn = std::max(n, 1u);
-    for (DevBuf<float4>* b : {&lc_p, &lc_v, &ls_p, &ls_v, &out_p, &out_v, &mu_p, &mu_v}) CUDA_TRY(b->alloc(nn));
+    for (DevBuf<float4>* b : {&lc_p, &lc_v, &ls_p, &ls_v, &out_p, &out_v, &mu_p, &mu_v, &wbuf, &ebuf})
+        CUDA_TRY(b->alloc(nn));
     for (int q = 0; q < S; ++q) {
         CUDA_TRY(lY_p[q].alloc(nn));
         CUDA_TRY(lY_v[q].alloc(nn));
@@ -1880,6 +1881,8 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.lamFd = lamFd.p;
                 a.g_stiff = gst.p;
                 a.flags = flags.p;
+                a.w = wbuf.p;
+                a.eq = ebuf.p;
                 a.n = n;
                 a.ns = ns;
                 a.solid_branch = sb ? 1 : 0;

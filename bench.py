@@ -220,6 +220,12 @@ def _time_adjoint(torch, stream, sim, steps, every, loss_grad):
     import time
     import numpy as np
     init = sim.particles().copy()
+    # untimed warm-up of the whole reverse pass (first use of the tape's device memory)
+    sim.tape_begin(every)
+    sim.step(steps)
+    sim.backward(np.zeros((sim.n, 8), np.float32))
+    sim.tape_end()
+    sim.set_particles(init)
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
     e0.record(stream)
     sim.step(steps)
