@@ -162,7 +162,18 @@ struct Tape {
     uint32_t every = 1;
     uint64_t steps = 0;                 // steps recorded since the tape began
     std::vector<Checkpoint> ckpts;      // state before step c * every
-    std::vector<StepRecord> recs;       // one segment of recording steps, reused
+};
+// Device memory of the reverse pass, kept by the handle across tapes so that
+// repeated taping and backward passes allocate nothing after the first.
+struct AdjointPool {
+    std::vector<StepRecord> recs;       // one segment of recording steps
+    std::vector<Checkpoint> spare;      // checkpoints of ended tapes, reused
+    DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, w, e;
+    DevBuf<float4> lY_p[kMaxStages], lY_v[kMaxStages];
+    DevBuf<float4> lamF, lamFd;
+    DevBuf<float2> gst;
+    DevBuf<uint32_t> flags;
+    Checkpoint now;
 };
 
 }  // namespace
@@ -253,6 +264,7 @@ struct arp_sim {
     bool have_stiff = false;
     // reverse mode
     std::unique_ptr<Tape> tape;
+    AdjointPool adj;
     StepRecord* rec = nullptr;  // set while a recording step runs
     bool replaying = false;     // steps re-run by the backward pass take no checkpoints
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
@@ -546,6 +558,10 @@ cudaError_t keep(DevBuf<T>& dst, const T* src, size_t count, cudaStream_t st) {
 
 arp_status save_checkpoint(arp_sim* S) {
     Checkpoint c;
+    if (!S->adj.spare.empty()) {
+        c = std::move(S->adj.spare.back());
+        S->adj.spare.pop_back();
+    }
     CUDA_TRY(keep(c.pd, (const float4*)S->Y.pd.p, S->n, S->stream));
     CUDA_TRY(keep(c.vm, (const float4*)S->Y.vm.p, S->n, S->stream));
     CUDA_TRY(keep(c.orig, (const uint32_t*)S->orig.p, S->n, S->stream));
@@ -1742,6 +1758,13 @@ arp_status arp_sim_set_solid_stiffness(arp_sim* sim, const float* normal_shear, 
     return ARP_OK;
 }
 
+// Checkpoints of an ended tape go back to the handle's pool.
+static void retire_tape(arp_sim* sim) {
+    if (!sim->tape) return;
+    for (auto& c : sim->tape->ckpts) sim->adj.spare.push_back(std::move(c));
+    sim->tape.reset();
+}
+
 arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
     ARP_TRY(need_init(sim));
     if (checkpoint_every == 0) return fail(ARP_ERR_INVALID_ARG, "checkpoint interval must be positive");
@@ -1753,6 +1776,7 @@ arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
             return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate contact friction");
     if (sim->tab.stages > kMaxStages) return fail(ARP_ERR_UNSUPPORTED, "more than 4 stages");
     sim->drop_graph();
+    retire_tape(sim);
     sim->tape.reset(new Tape());
     sim->tape->every = checkpoint_every;
     return ARP_OK;
@@ -1760,7 +1784,7 @@ arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
 
 arp_status arp_tape_end(arp_sim* sim) {
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
-    sim->tape.reset();
+    retire_tape(sim);
     return ARP_OK;
 }
 
@@ -1779,29 +1803,33 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     const uint64_t total = tp.steps;
     cudaStream_t st = sim->stream;
     const int S = sim->tab.stages;
+    AdjointPool& P = sim->adj;
     // the forward state is put back when the pass ends
-    Checkpoint now;
+    Checkpoint& now = P.now;
     CUDA_TRY(keep(now.pd, (const float4*)sim->Y.pd.p, n, st));
     CUDA_TRY(keep(now.vm, (const float4*)sim->Y.vm.p, n, st));
     CUDA_TRY(keep(now.orig, (const uint32_t*)sim->orig.p, n, st));
     CUDA_TRY(keep(now.sid, (const uint32_t*)sim->sid.p, n, st));
     now.time = sim->time;
     // adjoint buffers: caller order (lc), storage order (ls, out), per stage (lY), stage weights (mu)
-    DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, lY_p[kMaxStages], lY_v[kMaxStages];
-    DevBuf<float4> lamF, lamFd, wbuf, ebuf;
-    DevBuf<float2> gst;
-    DevBuf<uint32_t> flags;
     const size_t nn = std::max(n, 1u);
-    for (DevBuf<float4>* b : {&lc_p, &lc_v, &ls_p, &ls_v, &out_p, &out_v, &mu_p, &mu_v, &wbuf, &ebuf})
-        CUDA_TRY(b->alloc(nn));
+    auto fit = [](auto& b, size_t count) -> cudaError_t { return b.n >= count ? cudaSuccess : b.alloc(count); };
+    for (DevBuf<float4>* b : {&P.lc_p, &P.lc_v, &P.ls_p, &P.ls_v, &P.out_p, &P.out_v, &P.mu_p, &P.mu_v, &P.w, &P.e})
+        CUDA_TRY(fit(*b, nn));
     for (int q = 0; q < S; ++q) {
-        CUDA_TRY(lY_p[q].alloc(nn));
-        CUDA_TRY(lY_v[q].alloc(nn));
+        CUDA_TRY(fit(P.lY_p[q], nn));
+        CUDA_TRY(fit(P.lY_v[q], nn));
     }
-    CUDA_TRY(lamF.alloc(3 * size_t(std::max(ns, 1u))));
-    CUDA_TRY(lamFd.alloc(3 * size_t(std::max(ns, 1u))));
-    CUDA_TRY(gst.alloc(std::max(ns, 1u)));
-    CUDA_TRY(flags.alloc(1));
+    CUDA_TRY(fit(P.lamF, 3 * size_t(std::max(ns, 1u))));
+    CUDA_TRY(fit(P.lamFd, 3 * size_t(std::max(ns, 1u))));
+    CUDA_TRY(fit(P.gst, std::max(ns, 1u)));
+    CUDA_TRY(fit(P.flags, 1));
+    DevBuf<float4>&lc_p = P.lc_p, &lc_v = P.lc_v, &ls_p = P.ls_p, &ls_v = P.ls_v, &out_p = P.out_p,
+                  &out_v = P.out_v, &mu_p = P.mu_p, &mu_v = P.mu_v, &lamF = P.lamF, &lamFd = P.lamFd;
+    DevBuf<float4>* lY_p = P.lY_p;
+    DevBuf<float4>* lY_v = P.lY_v;
+    DevBuf<float2>& gst = P.gst;
+    DevBuf<uint32_t>& flags = P.flags;
     CUDA_TRY(cudaMemsetAsync(gst.p, 0, std::max(ns, 1u) * sizeof(float2), st));
     CUDA_TRY(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t), st));
     {
@@ -1818,7 +1846,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
         }
     }
     const uint32_t every = tp.every;
-    if (tp.recs.size() < every) tp.recs.resize(every);
+    if (P.recs.size() < every) P.recs.resize(every);
     const uint64_t nseg = (total + every - 1) / every;
     sim->replaying = true;
     arp_status status = ARP_OK;
@@ -1826,12 +1854,12 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
         const uint64_t t0 = seg * every, t1 = std::min<uint64_t>(t0 + every, total);
         status = restore_checkpoint(sim, tp.ckpts[seg]);
         for (uint64_t t = t0; t < t1 && status == ARP_OK; ++t) {
-            sim->rec = &tp.recs[t - t0];
+            sim->rec = &P.recs[t - t0];
             status = do_step(sim);
             sim->rec = nullptr;
         }
         for (uint64_t t = t1; t-- > t0 && status == ARP_OK;) {
-            const StepRecord& R = tp.recs[t - t0];
+            const StepRecord& R = P.recs[t - t0];
             sim->launches += adjoint_gather(n, R.orig.p, lc_p.p, lc_v.p, ls_p.p, ls_v.p, st);
             for (int q = S - 1; q >= 0; --q) {
                 float ca[kMaxStages];
@@ -1881,8 +1909,8 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.lamFd = lamFd.p;
                 a.g_stiff = gst.p;
                 a.flags = flags.p;
-                a.w = wbuf.p;
-                a.eq = ebuf.p;
+                a.w = P.w.p;
+                a.eq = P.e.p;
                 a.n = n;
                 a.ns = ns;
                 a.solid_branch = sb ? 1 : 0;
