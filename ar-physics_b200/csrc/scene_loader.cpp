@@ -8,21 +8,26 @@
 // the material order: boundaries by name, then objects by name.  Arithmetic
 // follows the Rust code's f32/f64 choices; this file is compiled without
 // floating-point contraction so lattice coordinates accumulate exactly as
-// there.  STL regions ("model") are not supported; "on_click" objects are
-// interactive additions and are not part of the initial scene.
+// there.  STL regions ("model", examples/test_mods/mesh.rs) are read as
+// stl_io 0.4 reads them, from paths relative to the working directory as the
+// reference opens them.  "on_click" objects are interactive additions and are
+// not part of the initial scene.
 #include "scene_loader.h"
 
 #include <algorithm>
+#include <array>
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
 #include <fstream>
+#include <functional>
 #include <map>
 #include <memory>
 #include <sstream>
 #include <stdexcept>
 #include <string>
+#include <thread>
 #include <vector>
 
 namespace arp {
@@ -477,10 +482,313 @@ RegionP aabe_border(const RAABE& e, float depth) {  // region.rs:54-63
     return d;
 }
 
+// ---- STL regions (examples/test_mods/mesh.rs) ------------------------------------
+
+// An indexed triangle mesh as `stl_io::read_stl` (stl_io 0.4) returns it:
+// vertices shared by exact value, each face with the normal stored in the file.
+struct IndexedMesh {
+    std::vector<std::array<float, 3>> vertices;
+    struct Face {
+        float normal[3];
+        uint32_t v[3];
+    };
+    std::vector<Face> faces;
+};
+
+IndexedMesh read_stl(const std::string& path) {
+    std::ifstream f(path, std::ios::binary);
+    if (!f) throw ParseError("cannot open STL file " + path);
+    std::stringstream ss;
+    ss << f.rdbuf();
+    const std::string data = ss.str();
+    struct Tri {
+        float n[3], v[3][3];
+    };
+    std::vector<Tri> tris;
+    bool binary = data.size() >= 84;
+    uint32_t count = 0;
+    if (binary) {
+        std::memcpy(&count, data.data() + 80, 4);
+        binary = data.size() == 84 + 50ull * count;  // a binary file has exactly this size
+    }
+    if (binary) {
+        tris.resize(count);
+        for (uint32_t i = 0; i < count; ++i) {
+            const char* r = data.data() + 84 + 50ull * i;
+            std::memcpy(tris[i].n, r, 12);
+            std::memcpy(tris[i].v, r + 12, 36);
+        }
+    } else {
+        if (data.compare(0, 5, "solid") != 0) throw ParseError("not an STL file: " + path);
+        std::istringstream in(data);
+        std::string w;
+        Tri t{};
+        int nv = 0;
+        while (in >> w) {
+            if (w == "normal") {
+                in >> t.n[0] >> t.n[1] >> t.n[2];
+            } else if (w == "vertex") {
+                if (nv >= 3) throw ParseError("STL facet with more than 3 vertices: " + path);
+                in >> t.v[nv][0] >> t.v[nv][1] >> t.v[nv][2];
+                ++nv;
+            } else if (w == "endfacet") {
+                if (nv != 3) throw ParseError("STL facet without 3 vertices: " + path);
+                tris.push_back(t);
+                nv = 0;
+            }
+        }
+    }
+    IndexedMesh m;
+    std::map<std::array<uint32_t, 3>, uint32_t> index;  // by bit pattern
+    for (const Tri& t : tris) {
+        IndexedMesh::Face fc;
+        std::memcpy(fc.normal, t.n, 12);
+        for (int k = 0; k < 3; ++k) {
+            std::array<uint32_t, 3> key;
+            std::memcpy(key.data(), t.v[k], 12);
+            auto it = index.find(key);
+            if (it == index.end()) {
+                it = index.emplace(key, (uint32_t)m.vertices.size()).first;
+                m.vertices.push_back({t.v[k][0], t.v[k][1], t.v[k][2]});
+            }
+            fc.v[k] = it->second;
+        }
+        m.faces.push_back(fc);
+    }
+    if (m.vertices.empty()) throw ParseError("STL file without triangles: " + path);
+    return m;
+}
+
+Box4 point_bound(const IndexedMesh& m) {  // mesh.rs:12-24
+    float mn[3] = {m.vertices[0][0], m.vertices[0][1], m.vertices[0][2]};
+    float mx[3] = {mn[0], mn[1], mn[2]};
+    for (const auto& v : m.vertices)
+        for (int i = 0; i < 3; ++i) {
+            mn[i] = std::fmin(v[i], mn[i]);
+            mx[i] = std::fmax(v[i], mx[i]);
+        }
+    Box4 b;
+    for (int i = 0; i < 3; ++i) {
+        b.min[i] = mn[i];
+        b.dim[i] = mx[i] - mn[i];
+    }
+    b.min[3] = 0.0f;
+    b.dim[3] = 0.0f;
+    return b;
+}
+
+// f32::signum: 1 for +0 and positives, -1 for -0 and negatives, NaN for NaN
+inline float signum(float x) { return std::isnan(x) ? x : std::copysign(1.0f, x); }
+
+// Uniform grid over a box listing the items whose (margin-grown) boxes
+// overlap each cell: a query visits only the items that can pass the exact
+// test, so the result equals a walk over every item.
+struct CullGrid {
+    float lo[3] = {0, 0, 0}, inv[3] = {0, 0, 0};
+    int n[3] = {1, 1, 1};
+    std::vector<uint32_t> start, items;
+    void build(const float mn[3], const float mx[3], int dims, size_t count,
+               const std::function<void(size_t, float*, float*)>& box) {
+        const int g = std::max(1, std::min(dims == 2 ? 512 : 96, (int)std::cbrt((double)count) * (dims == 2 ? 4 : 2)));
+        for (int a = 0; a < 3; ++a) {
+            n[a] = a < dims ? g : 1;
+            lo[a] = mn[a];
+            const float ext = mx[a] - mn[a];
+            inv[a] = ext > 0.0f ? (float)n[a] / ext : 0.0f;
+        }
+        const size_t cells = (size_t)n[0] * n[1] * n[2];
+        std::vector<uint32_t> cnt(cells + 1, 0);
+        auto range = [&](const float* b0, const float* b1, int* c0, int* c1) {
+            for (int a = 0; a < 3; ++a) {
+                c0[a] = std::max(0, std::min(n[a] - 1, (int)std::floor((b0[a] - lo[a]) * inv[a])));
+                c1[a] = std::max(0, std::min(n[a] - 1, (int)std::floor((b1[a] - lo[a]) * inv[a])));
+            }
+        };
+        for (int pass = 0; pass < 2; ++pass) {
+            if (pass == 1) {
+                start.assign(cells + 1, 0);
+                for (size_t c = 0; c < cells; ++c) start[c + 1] = start[c] + cnt[c];
+                items.assign(start[cells], 0);
+                std::fill(cnt.begin(), cnt.end(), 0);
+            }
+            for (size_t i = 0; i < count; ++i) {
+                float b0[3], b1[3];
+                box(i, b0, b1);
+                int c0[3], c1[3];
+                range(b0, b1, c0, c1);
+                for (int z = c0[2]; z <= c1[2]; ++z)
+                    for (int y = c0[1]; y <= c1[1]; ++y)
+                        for (int x = c0[0]; x <= c1[0]; ++x) {
+                            const size_t c = ((size_t)z * n[1] + y) * n[0] + x;
+                            if (pass == 1) items[start[c] + cnt[c]] = (uint32_t)i;
+                            ++cnt[c];
+                        }
+            }
+        }
+    }
+    // items of the cell holding p (points outside the grid clamp to its border cells)
+    std::pair<const uint32_t*, const uint32_t*> query(const float* p) const {
+        size_t c = 0, mul = 1;
+        for (int a = 0; a < 3; ++a) {
+            const int i = std::max(0, std::min(n[a] - 1, (int)std::floor((p[a] - lo[a]) * inv[a])));
+            c += (size_t)i * mul;
+            mul *= (size_t)n[a];
+        }
+        return {items.data() + start[c], items.data() + start[c + 1]};
+    }
+};
+
+struct RMesh : Region {  // mesh.rs:26-77: parity of the faces above the point whose xy triangle holds it
+    IndexedMesh mesh;
+    CullGrid grid;  // over xy: a face is visited only when p lies in its xy box
+    Box4 bound() const override { return point_bound(mesh); }
+    void index() {
+        const Box4 b = point_bound(mesh);
+        const float margin = 1e-4f * std::max(b.dim[0], b.dim[1]) + 1e-6f;
+        const float mn[3] = {b.min[0] - margin, b.min[1] - margin, 0.0f};
+        const float mx[3] = {b.min[0] + b.dim[0] + margin, b.min[1] + b.dim[1] + margin, 0.0f};
+        grid.build(mn, mx, 2, mesh.faces.size(), [&](size_t i, float* b0, float* b1) {
+            const auto& f = mesh.faces[i];
+            for (int a = 0; a < 2; ++a) {
+                float lo = mesh.vertices[f.v[0]][a], hi = lo;
+                for (int k = 1; k < 3; ++k) {
+                    lo = std::fmin(lo, mesh.vertices[f.v[k]][a]);
+                    hi = std::fmax(hi, mesh.vertices[f.v[k]][a]);
+                }
+                b0[a] = lo - margin;
+                b1[a] = hi + margin;
+            }
+            b0[2] = b1[2] = 0.0f;
+        });
+    }
+    bool contains(const float p[4]) const override {
+        if (p[3] != 0.0f) return false;
+        bool inside = false;
+        const float q[3] = {p[0], p[1], 0.0f};
+        const auto span = grid.query(q);
+        for (const uint32_t* it = span.first; it != span.second; ++it) {
+            const auto& f = mesh.faces[*it];
+            const auto& v0 = mesh.vertices[f.v[0]];
+            const auto& v1 = mesh.vertices[f.v[1]];
+            const auto& v2 = mesh.vertices[f.v[2]];
+            const bool above = v0[2] >= p[2] || v1[2] >= p[2] || v2[2] >= p[2];
+            if (!above) continue;
+            const float s1[2] = {v1[0] - v0[0], v1[1] - v0[1]};
+            const float s2[2] = {v2[0] - v0[0], v2[1] - v0[1]};
+            const float d[2] = {p[0] - v0[0], p[1] - v0[1]};
+            float a = s1[0] * s2[1] - s1[1] * s2[0];
+            const float sg = signum(a);
+            const float s = sg * (d[0] * s2[1] - d[1] * s2[0]);
+            const float t = sg * (s1[0] * d[1] - s1[1] * d[0]);
+            a = std::fabs(a);
+            if (s >= 0.0f && s <= a && t >= 0.0f && t <= a && s + t <= a) inside = !inside;
+        }
+        return inside;
+    }
+};
+
+struct RSurface : Region {  // mesh.rs:79-138: within `border` of a vertex or of a face
+    IndexedMesh mesh;
+    float border = 0.0f;
+    // a vertex or a face is visited only when p lies in its box grown by the border
+    CullGrid vgrid, fgrid;
+    void index() {
+        Box4 b = bound();
+        const float ext = std::max({b.dim[0], b.dim[1], b.dim[2]});
+        const float margin = border + 1e-4f * ext + 1e-6f;
+        const float mn[3] = {b.min[0] - margin, b.min[1] - margin, b.min[2] - margin};
+        const float mx[3] = {b.min[0] + b.dim[0] + margin, b.min[1] + b.dim[1] + margin,
+                             b.min[2] + b.dim[2] + margin};
+        vgrid.build(mn, mx, 3, mesh.vertices.size(), [&](size_t i, float* b0, float* b1) {
+            for (int a = 0; a < 3; ++a) {
+                b0[a] = mesh.vertices[i][a] - margin;
+                b1[a] = mesh.vertices[i][a] + margin;
+            }
+        });
+        fgrid.build(mn, mx, 3, mesh.faces.size(), [&](size_t i, float* b0, float* b1) {
+            const auto& f = mesh.faces[i];
+            for (int a = 0; a < 3; ++a) {
+                float lo = mesh.vertices[f.v[0]][a], hi = lo;
+                for (int k = 1; k < 3; ++k) {
+                    lo = std::fmin(lo, mesh.vertices[f.v[k]][a]);
+                    hi = std::fmax(hi, mesh.vertices[f.v[k]][a]);
+                }
+                b0[a] = lo - margin;
+                b1[a] = hi + margin;
+            }
+        });
+    }
+    Box4 bound() const override {
+        Box4 b = point_bound(mesh);
+        for (int i = 0; i < 3; ++i) {
+            b.min[i] -= border;
+            b.dim[i] += border * 2.0f;
+        }
+        return b;
+    }
+    static float dot3(const float* a, const float* b) { return a[0] * b[0] + a[1] * b[1] + a[2] * b[2]; }
+    static void cross3(const float* a, const float* b, float* o) {
+        o[0] = a[1] * b[2] - a[2] * b[1];
+        o[1] = a[2] * b[0] - a[0] * b[2];
+        o[2] = a[0] * b[1] - a[1] * b[0];
+    }
+    static void sub3(const float* a, const float* b, float* o) {
+        o[0] = a[0] - b[0];
+        o[1] = a[1] - b[1];
+        o[2] = a[2] - b[2];
+    }
+    bool contains(const float p[4]) const override {
+        const auto vs = vgrid.query(p);
+        for (const uint32_t* it = vs.first; it != vs.second; ++it) {
+            float d[3];
+            sub3(p, mesh.vertices[*it].data(), d);
+            if (dot3(d, d) <= border * border) return true;
+        }
+        const auto fs = fgrid.query(p);
+        for (const uint32_t* it = fs.first; it != fs.second; ++it) {
+            const auto& f = mesh.faces[*it];
+            const float* n = f.normal;
+            const float* a = mesh.vertices[f.v[0]].data();
+            const float* b = mesh.vertices[f.v[1]].data();
+            const float* c = mesh.vertices[f.v[2]].data();
+            float d[3];
+            sub3(p, a, d);
+            if (std::fabs(dot3(d, n)) <= std::sqrt(dot3(n, n)) * border) {
+                float s1[3], s2[3], s3[3], s4[3], d2[3], n1[3], n2[3], n3[3];
+                sub3(b, a, s1);
+                sub3(c, a, s2);
+                sub3(c, b, s3);
+                sub3(a, b, s4);
+                sub3(p, b, d2);
+                cross3(s1, n, n1);
+                cross3(s2, n, n2);
+                cross3(s3, n, n3);
+                if (signum(dot3(d, n1)) == signum(dot3(s2, n1)) && signum(dot3(d, n2)) == signum(dot3(s1, n2)) &&
+                    signum(dot3(d2, n3)) == signum(dot3(s4, n3)))
+                    return true;
+            }
+        }
+        return false;
+    }
+};
+
 RegionP parse_region_from_mat(const Table& t);
 
 RegionP parse_base(const Table& t) {  // config.rs:180-239
-    if (get(t, "model")) throw Unsupported("STL regions (\"model\") are not supported");
+    if (const TVal* mv = get(t, "model"); mv && mv->kind == TVal::Str) {
+        const TVal* bv = get(t, "border");
+        if (bv && bv->kind == TVal::Float) {  // .and_then(as_float): an integer border is no border
+            auto r = std::make_shared<RSurface>();
+            r->mesh = read_stl(mv->s);
+            r->border = (float)bv->num;
+            r->index();
+            return r;
+        }
+        auto r = std::make_shared<RMesh>();
+        r->mesh = read_stl(mv->s);
+        r->index();
+        return r;
+    }
     const TVal* border_v = get(t, "border");
     if (border_v && !border_v->is_num()) throw ParseError("border must be a number");
     float dim[4] = {0, 0, 0, 0}, mn[4] = {0, 0, 0, 0};
@@ -623,23 +931,16 @@ void gen_particles(const Region& region, float packing, float kernel_h, arp_mate
     const float start_density = mat.start_den;
     const float sq2 = std::sqrt(2.0f), sq3 = std::sqrt(3.0f), sq8 = std::sqrt(8.0f);
     float offset2 = 0.0f;
-    const uint64_t kLimit = 1ull << 31;
+    const uint64_t kLimit = 1ull << 28;
+    std::vector<std::array<float, 4>> sites;  // every lattice site of the bound, in walk order
     for (;;) {
         float offset = 0.0f;
         pos[1] = bound.min[1] + offset2;
         for (;;) {
             pos[0] = bound.min[0] + (offset + offset2);
             for (;;) {
-                if (++num_in_box > kLimit) throw ParseError("a region seeds more than 2^31 lattice sites");
-                if (region.contains(pos)) {
-                    arp_particle p{};
-                    for (int i = 0; i < 4; ++i) p.pos[i] = pos[i];
-                    if (velf) velf->at(pos, p.vel);
-                    p.den = start_density;
-                    p.mat = mat_id;
-                    p.solid_id = 0xFFFFFFFFu;
-                    out.push_back(p);
-                }
+                if (++num_in_box > kLimit) throw ParseError("a region spans more than 2^28 lattice sites");
+                sites.push_back({pos[0], pos[1], pos[2], pos[3]});
                 pos[0] += h;
                 if (pos[0] - bound.min[0] > bound.dim[0] || bound.dim[0] == 0.0f) break;
             }
@@ -650,6 +951,27 @@ void gen_particles(const Region& region, float packing, float kernel_h, arp_mate
         pos[2] += h / sq3;
         offset2 = offset2 == 0.0f ? h / sq8 : 0.0f;
         if (pos[2] - bound.min[2] > bound.dim[2] || bound.dim[2] == 0.0f) break;
+    }
+    // the region test of every site, on all host threads (the reference tests
+    // its sites on worker threads too, material_region/mod.rs:79-103)
+    std::vector<uint8_t> keep(sites.size(), 0);
+    const size_t nt = std::max<size_t>(1, std::min<size_t>(std::thread::hardware_concurrency(),
+                                                           (sites.size() + 4095) / 4096));
+    std::vector<std::thread> pool;
+    for (size_t t = 0; t < nt; ++t)
+        pool.emplace_back([&, t] {
+            for (size_t k = t; k < sites.size(); k += nt) keep[k] = region.contains(sites[k].data()) ? 1 : 0;
+        });
+    for (auto& th : pool) th.join();
+    for (size_t k = 0; k < sites.size(); ++k) {
+        if (!keep[k]) continue;
+        arp_particle p{};
+        for (int i = 0; i < 4; ++i) p.pos[i] = sites[k][i];
+        if (velf) velf->at(sites[k].data(), p.vel);
+        p.den = start_density;
+        p.mat = mat_id;
+        p.solid_id = 0xFFFFFFFFu;
+        out.push_back(p);
     }
     double content = 1.0;  // the f64 product of the nonzero extents, then times the density
     for (int i = 0; i < 4; ++i)

@@ -222,10 +222,11 @@ arp_status arp_sim_create_from_toml(const char* path, arp_sim** out);
  * `MaterialRegion::gen_particles`, material_region/mod.rs:56-156): materials in
  * object order (boundaries, then objects, each by name), boundary and mobile
  * particles in that order, the n_materials^2 interaction table with a `given`
- * flag per entry.  STL regions ("model") give ARP_ERR_UNSUPPORTED; objects
- * with "on_click" are interactive additions and are skipped; an integrator
- * name outside the reference's list gives ARP_ERR_PARSE, as does any schema
- * error the reference would panic on. */
+ * flag per entry.  STL regions ("model", examples/test_mods/mesh.rs) are read
+ * from paths relative to the working directory; objects with "on_click" are
+ * interactive additions and are skipped; an integrator name outside the
+ * reference's list gives ARP_ERR_PARSE, as does an unreadable STL file or any
+ * schema error the reference would panic on. */
 typedef struct arp_scene_file arp_scene_file;
 arp_status arp_scene_file_load(const char* path, arp_scene_file** out);
 /* Points `out` at the file's records; valid until arp_scene_file_free. */

@@ -225,9 +225,134 @@ def aabe_border(center, radii, b):  # region.rs:54-63
     return Difference(AABE(center, radii), AABE(center, np.fmax(radii - b, f32(0.0))))
 
 
+# ---- STL regions (examples/test_mods/mesh.rs) ----------------------------------
+
+def read_stl(path):
+    """Vertices (V x 3 f32, shared by exact value) and faces (F x 3 indices,
+    F x 3 stored normals) of a binary or ASCII STL file, as stl_io 0.4 reads it."""
+    data = open(path, "rb").read()
+    tris = None
+    if len(data) >= 84:
+        count = int(np.frombuffer(data, np.uint32, 1, 80)[0])
+        if len(data) == 84 + 50 * count:
+            rec = np.dtype([("n", "<f4", 3), ("v", "<f4", (3, 3)), ("a", "<u2")])
+            arr = np.frombuffer(data, rec, count, 84)
+            tris = (arr["n"].astype(f32), arr["v"].astype(f32))
+    if tris is None:
+        if not data.startswith(b"solid"):
+            raise SceneError("not an STL file")
+        toks = data.split()
+        ns, vs = [], []
+        for k, w in enumerate(toks):
+            if w == b"normal":
+                ns.append([float(x) for x in toks[k + 1:k + 4]])
+            elif w == b"vertex":
+                vs.append([float(x) for x in toks[k + 1:k + 4]])
+        tris = (np.array(ns, f32).reshape(-1, 3), np.array(vs, f32).reshape(-1, 3, 3))
+    normals, verts = tris
+    flat = np.ascontiguousarray(verts.reshape(-1, 3))
+    keys = flat.view(np.uint32)
+    uniq, inv = np.unique(keys, axis=0, return_inverse=True)
+    return uniq.view(f32).reshape(-1, 3), inv.reshape(-1, 3), normals
+
+
+def _signum(x):
+    return np.where(np.isnan(x), x, np.copysign(f32(1.0), x)).astype(f32)
+
+
+def _mesh_bound(V):  # mesh.rs:12-24
+    mn = np.zeros(4, f32)
+    mx = np.zeros(4, f32)
+    mn[:3] = V.min(axis=0)
+    mx[:3] = V.max(axis=0)
+    return mn, mx - mn
+
+
+class Mesh:
+    """mesh.rs:26-77: odd number of faces above the point whose xy triangle
+    holds it."""
+
+    def __init__(self, path):
+        self.V, self.Fi, self.N = read_stl(path)
+
+    def bound(self):
+        return _mesh_bound(self.V)
+
+    def contains(self, P):
+        parity = np.zeros(len(P), np.int64)
+        V, Fi = self.V, self.Fi
+        step = max(1, 4_000_000 // max(len(P), 1))
+        for c in range(0, len(Fi), step):
+            v0, v1, v2 = V[Fi[c:c + step, 0]], V[Fi[c:c + step, 1]], V[Fi[c:c + step, 2]]
+            pz = P[:, None, 2]
+            above = (v0[None, :, 2] >= pz) | (v1[None, :, 2] >= pz) | (v2[None, :, 2] >= pz)
+            s1x, s1y = v1[:, 0] - v0[:, 0], v1[:, 1] - v0[:, 1]
+            s2x, s2y = v2[:, 0] - v0[:, 0], v2[:, 1] - v0[:, 1]
+            dx = P[:, None, 0] - v0[None, :, 0]
+            dy = P[:, None, 1] - v0[None, :, 1]
+            a = s1x * s2y - s1y * s2x
+            sg = _signum(a)
+            sv = sg * (dx * s2y - dy * s2x)
+            tv = sg * (s1x * dy - s1y * dx)
+            a = np.abs(a)
+            hit = above & (sv >= 0) & (sv <= a) & (tv >= 0) & (tv <= a) & ((sv + tv) <= a)
+            parity += hit.sum(axis=1)
+        return (parity % 2 == 1) & (P[:, 3] == 0)
+
+
+class Surface(Mesh):
+    """mesh.rs:79-138: within `border` of a vertex, or of a face inside its
+    edges' prism."""
+
+    def __init__(self, path, border):
+        super().__init__(path)
+        self.border = f32(border)
+
+    def bound(self):
+        mn, dim = _mesh_bound(self.V)
+        mn[:3] = mn[:3] - self.border
+        dim[:3] = dim[:3] + self.border * f32(2.0)
+        return mn, dim
+
+    @staticmethod
+    def _dot(a, b):
+        return (a[..., 0] * b[..., 0] + a[..., 1] * b[..., 1]) + a[..., 2] * b[..., 2]
+
+    @staticmethod
+    def _cross(a, b):
+        return np.stack([a[..., 1] * b[..., 2] - a[..., 2] * b[..., 1], a[..., 2] * b[..., 0] - a[..., 0] * b[..., 2],
+                         a[..., 0] * b[..., 1] - a[..., 1] * b[..., 0]], axis=-1)
+
+    def contains(self, P):
+        P3 = P[:, :3]
+        out = np.zeros(len(P), bool)
+        bb = self.border * self.border
+        step = max(1, 4_000_000 // max(len(P), 1))
+        for c in range(0, len(self.V), step):
+            d = P3[:, None, :] - self.V[None, c:c + step, :]
+            out |= (self._dot(d, d) <= bb).any(axis=1)
+        V, Fi = self.V, self.Fi
+        for c in range(0, len(Fi), step):
+            n = self.N[c:c + step]
+            a, b, cc = V[Fi[c:c + step, 0]], V[Fi[c:c + step, 1]], V[Fi[c:c + step, 2]]
+            d = P3[:, None, :] - a[None]
+            near = np.abs(self._dot(d, n[None])) <= np.sqrt(self._dot(n, n))[None] * self.border
+            s1, s2, s3, s4 = b - a, cc - a, cc - b, a - b
+            d2 = P3[:, None, :] - b[None]
+            n1, n2, n3 = self._cross(s1, n), self._cross(s2, n), self._cross(s3, n)
+            ok = (near & (_signum(self._dot(d, n1[None])) == _signum(self._dot(s2, n1))[None])
+                  & (_signum(self._dot(d, n2[None])) == _signum(self._dot(s1, n2))[None])
+                  & (_signum(self._dot(d2, n3[None])) == _signum(self._dot(s4, n3))[None]))
+            out |= ok.any(axis=1)
+        return out
+
+
 def parse_base(t):  # config.rs:180-239
-    if "model" in t:
-        raise SceneError("STL regions are not supported")
+    if isinstance(t.get("model"), str):
+        b = t.get("border")
+        if isinstance(b, float):  # .and_then(as_float): an integer border is no border
+            return Surface(t["model"], f32(b))
+        return Mesh(t["model"])
     border = f32(_num(t["border"])) if "border" in t else None
     mn = np.zeros(4, f32)
     if isinstance(t.get("dim"), list):
