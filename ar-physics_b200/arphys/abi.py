@@ -64,6 +64,19 @@ class ArpScene(ctypes.Structure):
     ]
 
 
+class ArpView(ctypes.Structure):
+    _fields_ = [("angle", ctypes.c_float), ("pos", ctypes.c_float * 2), ("scale", ctypes.c_float)]
+
+
+class ArpRenderStyle(ctypes.Structure):
+    _fields_ = [
+        ("render_h", ctypes.c_float), ("lighting", ctypes.c_int32), ("light_pos", ctypes.c_float * 3),
+        ("light_color", ctypes.c_float * 3), ("ambient", ctypes.c_float), ("diffuse", ctypes.c_float),
+        ("specular", ctypes.c_float), ("n_materials", ctypes.c_uint32), ("colors", ctypes.c_void_p),
+        ("densities", ctypes.c_void_p),
+    ]
+
+
 class ArpProfile(ctypes.Structure):
     _fields_ = [
         ("steps", ctypes.c_uint64), ("launches", ctypes.c_uint64),
@@ -191,6 +204,9 @@ def load_library():
     sig["arp_scene_file_on_click"] = [ctypes.c_void_p, ctypes.c_uint32, ctypes.POINTER(ctypes.c_void_p), u32p,
                                       ctypes.c_void_p, ctypes.POINTER(ctypes.c_int)]
     sig["arp_sim_set_solid_stiffness"] = [c_sim, ctypes.c_void_p, ctypes.c_uint32]
+    sig["arp_sim_render_rgb24"] = [c_sim, ctypes.POINTER(ArpView), ctypes.POINTER(ArpRenderStyle), ctypes.c_uint32,
+                                   ctypes.c_uint32, ctypes.c_void_p]
+    sig["arp_scene_file_render_settings"] = [ctypes.c_void_p, ctypes.POINTER(ArpView), ctypes.POINTER(ArpRenderStyle)]
     sig["arp_tape_begin"] = [c_sim, ctypes.c_uint32]
     sig["arp_tape_end"] = [c_sim]
     sig["arp_tape_steps"] = [c_sim, ctypes.POINTER(ctypes.c_uint64)]

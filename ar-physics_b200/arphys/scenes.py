@@ -288,6 +288,15 @@ def load_toml(path):
 
         m = sc.n_materials
         inv = {v: k for k, v in reversed(list(INTEGRATOR_IDS.items()))}
+        from .abi import ArpView, ArpRenderStyle
+        view, style = ArpView(), ArpRenderStyle()
+        check(L.arp_scene_file_render_settings(f, ctypes.byref(view), ctypes.byref(style)))
+        render = {"view": dict(angle=view.angle, pos=(view.pos[0], view.pos[1]), scale=view.scale),
+                  "style": dict(render_h=style.render_h, lighting=bool(style.lighting),
+                                light_pos=tuple(style.light_pos), light_color=tuple(style.light_color),
+                                ambient=style.ambient, diffuse=style.diffuse, specular=style.specular,
+                                colors=copy(style.colors, 12 * style.n_materials, np.dtype(np.float32)).reshape(-1, 12),
+                                densities=copy(style.densities, style.n_materials, np.dtype(np.float32)))}
         count = ctypes.c_uint32()
         check(L.arp_scene_file_on_click_count(f, ctypes.byref(count)))
         on_click = []
@@ -308,7 +317,7 @@ def load_toml(path):
             subticks=int(sc.subticks), gravity=float(sc.gravity), alpha=float(sc.artificial_viscocity),
             interactions=copy(sc.interactions, m * m, INTERACTION_DTYPE).reshape(m, m),
             interaction_given=copy(sc.interaction_given, m * m, np.dtype(np.uint8)).reshape(m, m),
-            name=name.value.decode(), meta={"source": str(path), "on_click": on_click})
+            name=name.value.decode(), meta={"source": str(path), "on_click": on_click, "render": render})
     finally:
         L.arp_scene_file_free(f)
 

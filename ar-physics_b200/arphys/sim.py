@@ -250,6 +250,36 @@ class FluidSim:
         check(self._L.arp_tape_backward(self._h, ptr(d), ptr(g), ptr(gs)))
         return g, gs[:self.ns]
 
+    def render(self, width, height, view, style):
+        """One RGB24 frame (renderer.rs recording path) as a (height, width, 3)
+        uint8 array, row 0 at the bottom as glReadnPixels returns it.
+        `view`: dict(angle, pos, scale); `style`: dict(render_h, lighting,
+        light_pos, light_color, ambient, diffuse, specular, colors (M x 12),
+        densities (M))."""
+        from .abi import ArpView, ArpRenderStyle
+        v = ArpView()
+        v.angle = float(view.get("angle", 0.0))
+        v.pos[0], v.pos[1] = (float(x) for x in view.get("pos", (0.0, 0.0)))
+        v.scale = float(view.get("scale", 1.0))
+        colors = np.ascontiguousarray(style["colors"], dtype=np.float32).reshape(-1, 12)
+        dens = np.ascontiguousarray(style["densities"], dtype=np.float32).reshape(-1)
+        st = ArpRenderStyle()
+        st.render_h = float(style["render_h"])
+        st.lighting = int(bool(style.get("lighting", False)))
+        for k in range(3):
+            st.light_pos[k] = float(style.get("light_pos", (-3.0, 3.0, -3.0))[k])
+            st.light_color[k] = float(style.get("light_color", (1.0, 1.0, 1.0))[k])
+        st.ambient = float(style.get("ambient", 1.0))
+        st.diffuse = float(style.get("diffuse", 10.0))
+        st.specular = float(style.get("specular", 0.0))
+        st.n_materials = len(colors)
+        st.colors = ptr(colors)
+        st.densities = ptr(dens)
+        out = np.zeros((height, width, 3), np.uint8)
+        check(self._L.arp_sim_render_rgb24(self._h, ctypes.byref(v), ctypes.byref(st), int(width), int(height),
+                                           ptr(out)))
+        return out
+
     def device_state(self):
         v = ArpDeviceView()
         check(self._L.arp_sim_device_state(self._h, ctypes.byref(v)))

@@ -273,6 +273,37 @@ struct SolidArgs {
 };
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st);
 
+// ---- headless renderer ------------------------------------------------------------
+struct RenderCfg {
+    uint32_t W, H;                 // frame, pixels
+    float s2, vx0, vy0;            // square viewport: size and lower-left corner
+    float S;                       // sprite size, pixels
+    float ca, sa, tx, ty, tz;      // view matrix terms
+    float render_h;
+    float kconst;                  // poly6 constant the fragment shader weighs alpha with
+    int lighting;
+    float light[3], lcol[3], amb, dif, spec;
+    const float4* c1;              // per material: low-density colour
+    const float4* c2;              // colour
+    const float4* c3;              // high-density colour
+    const float* d0;               // ramp centre density
+    uint32_t nmat, nprims, tiles_x, tiles_y;
+};
+// sprites of boundary (prim_base 0) or mobile (prim_base = n_boundary)
+// particles in caller order: PR = (window x, window y, clip w, window z),
+// PC = colour, PP = view-space position
+int render_project(const float4* pd, const float4* vm, const uint32_t* orig, uint32_t n, uint32_t prim_base,
+                   const RenderCfg& c, float4* PR, float4* PC, float4* PP, cudaStream_t st);
+uint32_t render_chunk_size();
+uint32_t render_tile_size();
+int render_bin_count(const float4* PR, const float4* PC, const RenderCfg& c, uint32_t* counts, cudaStream_t st);
+int render_bin_scatter(const float4* PR, const float4* PC, const RenderCfg& c, const uint32_t* start,
+                       uint32_t* fill, uint32_t* list, cudaStream_t st);
+int render_composite(const float4* PR, const float4* PC, const RenderCfg& c, const uint32_t* start,
+                     const uint32_t* list, uint8_t* rgb, cudaStream_t st);
+int render_lit(const float4* PR, const float4* PC, const float4* PP, const RenderCfg& c, unsigned long long* zkey,
+               uint8_t* rgb, cudaStream_t st);
+
 // ---- adjoint (reverse mode of one integrator step) ------------------------------
 // Quantities of one RK stage saved by a recording forward step.
 struct AdjStage {

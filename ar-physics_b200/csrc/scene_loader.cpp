@@ -1036,6 +1036,41 @@ void build_scene(const TVal& root, LoadedScene& out) {
     out.integrator = integrator_id(str_or(top, "integrator", "verlet"));
     const float h = out.h;
     const float alpha = out.alpha;
+    // renderer settings (config.rs:302-323, 466-470)
+    {
+        const TVal* lv = get(top, "lighting");
+        if (lv && lv->kind != TVal::Bool) throw ParseError("lighting must be a boolean");
+        out.lighting = lv ? lv->b : get(top, "light_pos") != nullptr;
+        out.render_h = h * (float)num_or(top, "particle_render_factor", 1.0);
+        float lp[4], lc[4];
+        const float dlp[4] = {-3, 3, -3, 0}, dlc[4] = {1, 1, 1, 0};
+        vec4_or(top, "light_pos", dlp, lp);
+        vec4_or(top, "light_color", dlc, lc);
+        for (int i = 0; i < 3; ++i) {
+            out.light_pos[i] = lp[i];
+            out.light_color[i] = lc[i];
+        }
+        out.ambient = (float)num_or(top, "ambient_brightness", 1.0);
+        out.diffuse = (float)num_or(top, "diffuse_brightness", 10.0);
+        out.specular = (float)num_or(top, "specular_brightness", 0.0);
+        out.view_pos[0] = out.view_pos[1] = 0.0;
+        if (const TVal* vp = get(top, "view_pos")) {
+            if (vp->kind != TVal::Arr) throw ParseError("view_pos must be an array");
+            for (size_t i = 0; i < vp->arr.size() && i < 2; ++i) {
+                if (!vp->arr[i].is_num()) throw ParseError("view_pos must hold numbers");
+                out.view_pos[i] = vp->arr[i].num;
+            }
+        }
+        out.view_scale = num_or(top, "view_scale", 1.0);
+        out.view_angle = num_or(top, "view_angle", 0.0) * (3.14159265358979323846 / 180.0);  // f64::to_radians
+    }
+    // get_colors (config.rs:111-118): color, color_low_density, color_high_density
+    auto colors_of = [&](const Table& t, float* c12) {
+        const float black[4] = {0, 0, 0, 1};
+        vec4_or(t, "color", black, c12);
+        vec4_or(t, "color_low_density", c12, c12 + 4);
+        vec4_or(t, "color_high_density", c12, c12 + 8);
+    };
 
     std::vector<Obj> objs;
     std::map<std::pair<std::string, std::string>, arp_interaction> inter_map;
@@ -1129,6 +1164,9 @@ void build_scene(const TVal& root, LoadedScene& out) {
         std::vector<arp_particle> ps;
         seed(objs[idx], idx, m, ps);
         out.materials.push_back(m);
+        float c12[12];
+        colors_of(*objs[idx].table, c12);
+        out.colors.insert(out.colors.end(), c12, c12 + 12);
         auto& dst = m.immobile ? out.boundary : out.particles;
         dst.insert(dst.end(), ps.begin(), ps.end());
         collect_interactions(objs[idx].name, *objs[idx].table);

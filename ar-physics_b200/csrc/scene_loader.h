@@ -28,6 +28,13 @@ struct LoadedScene {
         bool relative = false;
     };
     std::vector<Addition> on_click;
+    // renderer settings of the file (examples/test_mods/config.rs:302-323)
+    std::vector<float> colors;  // 12 per material: color, color_low_density, color_high_density
+    bool lighting = false;
+    float render_h = 1.0f / 64.0f;
+    float light_pos[3] = {-3, 3, -3}, light_color[3] = {1, 1, 1};
+    float ambient = 1.0f, diffuse = 10.0f, specular = 0.0f;
+    double view_pos[2] = {0, 0}, view_scale = 1.0, view_angle = 0.0;
 
     arp_scene as_scene() const {
         arp_scene s{};

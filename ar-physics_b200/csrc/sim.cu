@@ -265,6 +265,13 @@ struct arp_sim {
     // reverse mode
     std::unique_ptr<Tape> tape;
     AdjointPool adj;
+    struct RenderBufs {
+        DevBuf<float4> PR, PC, PP, c1, c2, c3;
+        DevBuf<float> d0;
+        DevBuf<uint32_t> counts, start, fill, list, bsums;
+        DevBuf<unsigned long long> zkey;
+        DevBuf<uint8_t> rgb;
+    } rbuf;
     StepRecord* rec = nullptr;  // set while a recording step runs
     bool replaying = false;     // steps re-run by the backward pass take no checkpoints
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
@@ -1217,6 +1224,7 @@ arp_status arp_sim_create_from_toml(const char* path, arp_sim** out) {
 
 struct arp_scene_file {
     arp::LoadedScene scene;
+    mutable std::vector<float> densities;  // ramp centres handed out by arp_scene_file_render_settings
 };
 
 arp_status arp_scene_file_load(const char* path, arp_scene_file** out) {
@@ -1258,6 +1266,30 @@ arp_status arp_scene_file_on_click(const arp_scene_file* file, uint32_t index, c
     if (n) *n = (uint32_t)a.particles.size();
     if (material) *material = a.material;
     if (relative) *relative = a.relative ? 1 : 0;
+    return ARP_OK;
+}
+
+arp_status arp_scene_file_render_settings(const arp_scene_file* file, arp_view* view, arp_render_style* style) {
+    if (!file || !view || !style) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    const auto& S = file->scene;
+    view->angle = (float)S.view_angle;
+    view->pos[0] = (float)S.view_pos[0];
+    view->pos[1] = (float)S.view_pos[1];
+    view->scale = (float)S.view_scale;
+    style->render_h = S.render_h;
+    style->lighting = S.lighting ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+        style->light_pos[k] = S.light_pos[k];
+        style->light_color[k] = S.light_color[k];
+    }
+    style->ambient = S.ambient;
+    style->diffuse = S.diffuse;
+    style->specular = S.specular;
+    style->n_materials = (uint32_t)S.materials.size();
+    style->colors = S.colors.data();
+    file->densities.resize(S.materials.size());
+    for (size_t m = 0; m < S.materials.size(); ++m) file->densities[m] = S.materials[m].start_den;
+    style->densities = file->densities.data();
     return ARP_OK;
 }
 
@@ -1738,6 +1770,106 @@ arp_status arp_sim_launch_count(const arp_sim* sim, uint64_t* out) {
     if (!sim || !out) return fail(ARP_ERR_INVALID_ARG, "null argument");
     *out = sim->launches;
     return ARP_OK;
+}
+
+arp_status arp_sim_render_rgb24(arp_sim* sim, const arp_view* view, const arp_render_style* style, uint32_t width,
+                                uint32_t height, uint8_t* out_rgb) {
+    ARP_TRY(need_init(sim));
+    if (!view || !style || !out_rgb || !style->colors || !style->densities)
+        return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (width == 0 || height == 0 || (uint64_t)width * height > (1ull << 28))
+        return fail(ARP_ERR_INVALID_ARG, "frame size must be positive and at most 2^28 pixels");
+    if (style->n_materials < sim->M)
+        return fail(ARP_ERR_INVALID_ARG, "the style has fewer materials than the handle");
+    if (!(style->render_h > 0.0f) || !std::isfinite(style->render_h))
+        return fail(ARP_ERR_INVALID_ARG, "render_h must be positive");
+    cudaStream_t st = sim->stream;
+    auto& R = sim->rbuf;
+    auto fit = [](auto& b, size_t count) -> cudaError_t { return b.n >= count ? cudaSuccess : b.alloc(count); };
+    RenderCfg c{};
+    c.W = width;
+    c.H = height;
+    const uint32_t s2 = std::min(width, height);
+    c.s2 = (float)s2;
+    c.vx0 = (float)((width - s2) / 2);
+    c.vy0 = (float)((height - s2) / 2);
+    c.S = (float)s2 * style->render_h;  // gl::PointSize(s2 * render_h)
+    c.ca = std::cos(view->angle);
+    c.sa = std::sin(view->angle);
+    c.tx = -view->pos[0];
+    c.ty = view->pos[1];  // the matrix holds -trans_y with trans_y = -view_pos[1] (renderer.rs:347)
+    c.tz = -view->scale + 1.0f;
+    c.render_h = style->render_h;
+    c.kconst = norm_const_f32(3, 3.0f);  // normalization_constant(3, 3) in the fragment shader
+    c.lighting = style->lighting ? 1 : 0;
+    for (int k = 0; k < 3; ++k) {
+        c.light[k] = style->light_pos[k];
+        c.lcol[k] = style->light_color[k];
+    }
+    c.amb = style->ambient;
+    c.dif = style->diffuse;
+    c.spec = style->specular;
+    c.nmat = sim->M;
+    c.nprims = sim->nb + sim->n;
+    const uint32_t ts = render_tile_size();
+    c.tiles_x = (width + ts - 1) / ts;
+    c.tiles_y = (height + ts - 1) / ts;
+    {
+        std::vector<float4> h1(sim->M), h2(sim->M), h3(sim->M);
+        for (uint32_t m = 0; m < sim->M; ++m) {
+            const float* q = style->colors + 12 * size_t(m);
+            h2[m] = make_float4(q[0], q[1], q[2], q[3]);
+            h1[m] = make_float4(q[4], q[5], q[6], q[7]);
+            h3[m] = make_float4(q[8], q[9], q[10], q[11]);
+        }
+        CUDA_TRY(fit(R.c1, sim->M));
+        CUDA_TRY(fit(R.c2, sim->M));
+        CUDA_TRY(fit(R.c3, sim->M));
+        CUDA_TRY(fit(R.d0, sim->M));
+        CUDA_TRY(cudaMemcpyAsync(R.c1.p, h1.data(), sim->M * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(R.c2.p, h2.data(), sim->M * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(R.c3.p, h3.data(), sim->M * sizeof(float4), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaMemcpyAsync(R.d0.p, style->densities, sim->M * sizeof(float), cudaMemcpyHostToDevice, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+    }
+    c.c1 = R.c1.p;
+    c.c2 = R.c2.p;
+    c.c3 = R.c3.p;
+    c.d0 = R.d0.p;
+    const size_t np = std::max(c.nprims, 1u);
+    CUDA_TRY(fit(R.PR, np));
+    CUDA_TRY(fit(R.PC, np));
+    CUDA_TRY(fit(R.PP, np));
+    CUDA_TRY(fit(R.rgb, (size_t)width * height * 3));
+    sim->launches += render_project(sim->b_pd.p, sim->b_vm.p, sim->b_orig.p, sim->nb, 0, c, R.PR.p, R.PC.p, R.PP.p, st);
+    sim->launches += render_project(sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->n, sim->nb, c, R.PR.p, R.PC.p, R.PP.p,
+                                    st);
+    if (!c.lighting) {
+        const uint64_t nchunks = (c.nprims + render_chunk_size() - 1) / render_chunk_size();
+        const uint64_t K = std::max<uint64_t>(nchunks, 1) * c.tiles_x * c.tiles_y;
+        if (K + 1 > (1ull << 31)) return fail(ARP_ERR_UNSUPPORTED, "too many sprite bins for this frame size");
+        CUDA_TRY(fit(R.counts, K + 1));
+        CUDA_TRY(fit(R.start, K + 1));
+        CUDA_TRY(fit(R.fill, K + 1));
+        CUDA_TRY(fit(R.bsums, scan_block_sums_needed((uint32_t)(K + 1))));
+        CUDA_TRY(cudaMemsetAsync(R.counts.p, 0, (K + 1) * sizeof(uint32_t), st));
+        CUDA_TRY(cudaMemsetAsync(R.fill.p, 0, (K + 1) * sizeof(uint32_t), st));
+        sim->launches += render_bin_count(R.PR.p, R.PC.p, c, R.counts.p, st);
+        sim->launches += exclusive_scan(R.counts.p, (uint32_t)(K + 1), R.start.p, R.bsums.p, st);
+        uint32_t total = 0;
+        CUDA_TRY(cudaMemcpyAsync(&total, R.start.p + K, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaStreamSynchronize(st));
+        CUDA_TRY(fit(R.list, std::max(total, 1u)));
+        sim->launches += render_bin_scatter(R.PR.p, R.PC.p, c, R.start.p, R.fill.p, R.list.p, st);
+        sim->launches += render_composite(R.PR.p, R.PC.p, c, R.start.p, R.list.p, R.rgb.p, st);
+    } else {
+        CUDA_TRY(fit(R.zkey, (size_t)width * height));
+        CUDA_TRY(cudaMemsetAsync(R.zkey.p, 0xFF, (size_t)width * height * sizeof(unsigned long long), st));
+        sim->launches += render_lit(R.PR.p, R.PC.p, R.PP.p, c, R.zkey.p, R.rgb.p, st);
+    }
+    CUDA_TRY(cudaMemcpyAsync(out_rgb, R.rgb.p, (size_t)width * height * 3, cudaMemcpyDeviceToHost, st));
+    CUDA_TRY(cudaStreamSynchronize(st));
+    return check_launch("render");
 }
 
 arp_status arp_sim_set_solid_stiffness(arp_sim* sim, const float* normal_shear, uint32_t ns) {

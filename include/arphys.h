@@ -373,6 +373,47 @@ arp_status arp_sim_launch_count(const arp_sim* sim, uint64_t* out);
 const char* arp_last_error(void);
 uint32_t arp_abi_version(void);
 
+/* ---- headless rendering (examples/test_mods/renderer.rs) --------------------- */
+
+/* The camera of renderer.rs:338-349: the view matrix rotates by `angle`
+ * (radians) about y, translates by -view_pos and moves by 1 - scale along z;
+ * clip w = z + 1. */
+typedef struct arp_view {
+    float angle;      /* view_angle, in radians */
+    float pos[2];     /* view_pos */
+    float scale;      /* view_scale */
+} arp_view;
+
+/* The shader settings of renderer.rs:189-210.  `colors` holds 12 floats per
+ * material (RGBA of "color", "color_low_density", "color_high_density") and
+ * `densities` the density the colour ramp is centred on (the material's
+ * start density), both indexed by material id. */
+typedef struct arp_render_style {
+    float render_h;            /* kernel_radius * particle_render_factor */
+    int32_t lighting;          /* sphere shading with depth test, else density-ramp splats */
+    float light_pos[3], light_color[3];
+    float ambient, diffuse, specular;
+    uint32_t n_materials;
+    const float* colors;
+    const float* densities;
+} arp_render_style;
+
+/* One frame of the recording path (renderer.rs:305-478) without a graphics API:
+ * boundary particles then mobile particles, each in caller order, drawn as
+ * point sprites of render_h * min(width, height) pixels into a square viewport
+ * centred in the frame, over a white background; without lighting each sprite
+ * is a poly6-weighted disc in the density-ramp colour, composited in draw order
+ * with the blend the reference configures (src*(1-dst.a) + dst*(1-src.a), the
+ * destination alpha staying 0) into 8-bit channels; with lighting the nearest
+ * sprite of each pixel is shaded as a sphere.  `out_rgb` (host) receives
+ * width * height * 3 bytes, rows from bottom to top as glReadnPixels returns
+ * them.  A scene's particles are drawn with global material ids. */
+arp_status arp_sim_render_rgb24(arp_sim* sim, const arp_view* view, const arp_render_style* style, uint32_t width,
+                                uint32_t height, uint8_t* out_rgb);
+/* The view and style a scene file sets (config.rs:302-323,466-470); `colors`
+ * and `densities` point into `file`. */
+arp_status arp_scene_file_render_settings(const arp_scene_file* file, arp_view* view, arp_render_style* style);
+
 /* ---- per-particle stiffness and reverse mode (no counterpart in the reference) -- */
 
 /* Per-solid (normal, shear) stiffness — the Lame pair the reference keeps per
