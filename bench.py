@@ -304,6 +304,31 @@ def run_adjoint(torch, stream):
     return {"bar": bar, "rayleigh_taylor_batch": rt}
 
 
+def run_render(torch, sim, sc):
+    """One 1920x1080 frame of the benchmark state (the demo's --record path),
+    splat and lit, host wall clock around the call (frame read back to host)."""
+    import time
+    import numpy as np
+    m = len(sc.materials)
+    colors = np.tile(np.array([0.2, 0.4, 0.9, 1.0, 0.1, 0.1, 0.6, 1.0, 0.9, 0.9, 1.0, 1.0], np.float32), (m, 1))
+    b, d = sc.bounds_min, sc.bounds_dim
+    view = dict(angle=0.4, pos=(b[0] + 0.5 * d[0], -(b[1] + 0.5 * d[1])), scale=1.0)
+    out = {"width": 1920, "height": 1080, "particles": int(sc.n + sc.nb)}
+    for lit in (False, True):
+        style = dict(render_h=sc.h, lighting=lit, colors=colors,
+                     densities=sc.materials["start_den"].astype(np.float32))
+        sim.render(1920, 1080, view, style)  # warm-up (buffers)
+        t = []
+        for _ in range(3):
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            img = sim.render(1920, 1080, view, style)
+            t.append((time.perf_counter() - t0) * 1000.0)
+        out["lit_ms" if lit else "splat_ms"] = min(t)
+        out["lit_drawn_pixels" if lit else "splat_drawn_pixels"] = int(np.count_nonzero((img != 255).any(axis=2)))
+    return out
+
+
 def run_reference(args, rank, world):
     """The reference arm: the reference's path cannot run here (Rust + OpenGL
     compute shaders, no GL stack), so the CPU restatement of its shaders is
@@ -427,6 +452,8 @@ def run_ours(args, rank, world, local_rank):
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
     }
     line["fluid_launch_shape"] = sim.fluid_variant()
+    if rank == 0 and not args.no_render:
+        line["render"] = run_render(torch, sim, sc)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint(torch, stream)
     if rank == 0 and not args.no_batched:
@@ -448,6 +475,7 @@ def main():
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--no-batched", action="store_true")
     ap.add_argument("--no-adjoint", action="store_true")
+    ap.add_argument("--no-render", action="store_true")
     ap.add_argument("--fluid-variant", type=int, default=None, help="pin the fluid launch shape (profiling)")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
