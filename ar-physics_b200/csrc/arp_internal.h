@@ -230,6 +230,7 @@ struct SolidRefList {
     uint32_t* nbr;   // [nnz] solid id | 0x80000000 when same material
     float4* gw;      // [nnz] grad_w(X_j - X_i).xyz, w = vol0 of j
     uint32_t nnz;
+    float4* dk;      // [nnz] X_j - X_i and the kernel W(X_j - X_i) (hourglass term)
 };
 // Reference-neighbor lists: counts per solid (pass 1), then after an
 // exclusive scan of the counts into rl.off, the entries and L (pass 2).

@@ -275,7 +275,7 @@ struct arp_sim {
     StepRecord* rec = nullptr;  // set while a recording step runs
     bool replaying = false;     // steps re-run by the backward pass take no checkpoints
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
-    DevBuf<float4> rl_gw;
+    DevBuf<float4> rl_gw, rl_dk;
     uint32_t rl_nnz = 0;
     DevBuf<DevStats> d_stats;
 
@@ -533,8 +533,9 @@ arp_status do_init(arp_sim* S) {
         CUDA_TRY(cudaStreamSynchronize(st));
         CUDA_TRY(S->rl_nbr.alloc(std::max(nnz, 1u)));
         CUDA_TRY(S->rl_gw.alloc(std::max(nnz, 1u)));
+        CUDA_TRY(S->rl_dk.alloc(std::max(nnz, 1u)));
         S->rl_nnz = nnz;
-        SolidRefList rl{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, nnz};
+        SolidRefList rl{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, nnz, S->rl_dk.p};
         S->launches += ref_lists_fill(S->ref.p, S->mat_of_solid.p, ns, S->gb, S->tables, rl, S->L.p, st);
         CUDA_TRY(cudaStreamSynchronize(st));
         ARP_TRY(check_launch("reference neighbor lists"));
@@ -691,7 +692,7 @@ arp_status do_step(arp_sim* S) {
             a.slot_of = S->slot_of.p;
             a.ref = S->ref.p;
             a.L = S->L.p;
-            a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz};
+            a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz, S->rl_dk.p};
             a.ep = cur_ep;
             a.ep0 = S->ep.p;
             a.ep_next = last ? S->ep_t.p : S->ep_s[s % 2].p;
@@ -2035,7 +2036,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.bps = sim->bps.p;
                 a.ref = sim->ref.p;
                 a.L = sim->L.p;
-                a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz};
+                a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz, sim->rl_dk.p};
                 a.stiff = sim->have_stiff ? sim->stiff.p : nullptr;
                 a.lamF = lamF.p;
                 a.lamFd = lamFd.p;

@@ -83,7 +83,8 @@ __global__ void k_ref_count(const float4* __restrict__ ref, const uint32_t* __re
 
 __global__ void k_ref_fill(const float4* __restrict__ ref, const uint32_t* __restrict__ mat_of, uint32_t ns,
                            const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, Tables T,
-                           const uint32_t* __restrict__ off, uint32_t* __restrict__ nbr, float4* __restrict__ gw) {
+                           const uint32_t* __restrict__ off, uint32_t* __restrict__ nbr, float4* __restrict__ gw,
+                           float4* __restrict__ dk) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     uint32_t w = off[i];
@@ -95,6 +96,7 @@ __global__ void k_ref_fill(const float4* __restrict__ ref, const uint32_t* __res
         const uint32_t mj = mat_of[j];
         nbr[w] = j | (mj == mi ? kSameMat : 0u);
         gw[w] = make_float4(s * dX.x, s * dX.y, s * dX.z, mats[mj].vol0);
+        dk[w] = make_float4(dX.x, dX.y, dX.z, P.kconst * diff * diff * diff);
         ++w;
     });
 }
@@ -401,7 +403,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
         const float4 g = a.rl.gw[k];
         const float4 xj = a.sx[j];
         const float d2 = xj.w;
-        const float V2 = m1 / d2;
+        const float V2 = __fdividef(m1, d2);  // GLSL division carries 2.5 ulp; the 2-ulp hardware quotient is used
         const float s = -V1 * V2;
         const float4 Aj0 = a.A[3 * j], Aj1 = a.A[3 * j + 1], Aj2 = a.A[3 * j + 2];
         const float4 c0 = make_float4(s * (Ai0.x + Aj0.x), s * (Ai0.y + Aj0.y), s * (Ai0.z + Aj0.z), 0.f);
@@ -413,8 +415,8 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
         if (P.dim >= 3) fz += (c0.z * g.x + c1.z * g.y) + c2.z * g.z;
         if (in_stencil(a.sc[j], ci)) {
             const float3 dx = sub3(xj, xi);
-            const float3 dX = sub3(a.ref[j], Xi);
-            const float diff = P.h2 - dot3(dX, dX);
+            const float4 dk = a.rl.dk[k];  // X_j - X_i and W(X_j - X_i), fixed with the reference list
+            const float3 dX = make_float3(dk.x, dk.y, dk.z);
             const float l = sqrtf(dot3(dx, dx));
             const float4 Fj0 = a.F[3 * j], Fj1 = a.F[3 * j + 1], Fj2 = a.F[3 * j + 2];
             const float ex = ((0.5f * (Fi0.x + Fj0.x)) * dX.x + (0.5f * (Fi1.x + Fj1.x)) * dX.y) +
@@ -423,15 +425,15 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
                              (0.5f * (Fi2.y + Fj2.y)) * dX.z - dx.y;
             const float ez = ((0.5f * (Fi0.z + Fj0.z)) * dX.x + (0.5f * (Fi1.z + Fj1.z)) * dX.y) +
                              (0.5f * (Fi2.z + Fj2.z)) * dX.z - dx.z;
-            const float kern = P.kconst * diff * diff * diff;
-            const float sh = (((100000000.0f * m1 * m1 / (d1 * d2)) *
-                               (0.5f * ((ex * dx.x + ey * dx.y) + ez * dx.z) / (l + P.hg_h))) *
-                              (1.0f / (l * l + P.eps_hh))) *
+            const float kern = dk.w;
+            const float sh = ((__fdividef(100000000.0f * m1 * m1, d1 * d2) *
+                               __fdividef(0.5f * ((ex * dx.x + ey * dx.y) + ez * dx.z), l + P.hg_h)) *
+                              __fdividef(1.0f, l * l + P.eps_hh)) *
                              kern;
             const float den = l + P.eps_h;
-            fx -= (sh * dx.x) / den;
-            fy -= (sh * dx.y) / den;
-            fz -= (sh * dx.z) / den;
+            fx -= __fdividef(sh * dx.x, den);
+            fy -= __fdividef(sh * dx.y, den);
+            fz -= __fdividef(sh * dx.z, den);
         }
     }
     // Self-contact (solid.rs:428,445-450): same-material neighbors in the
@@ -485,7 +487,7 @@ int ref_lists_count(const float4* ref, const uint32_t* mat_of, uint32_t ns, cons
 int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const GridBuffers& gb, const Tables& T,
                    SolidRefList& rl, float4* L, cudaStream_t st) {
     k_ref_fill<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, gb.start, gb.perm, T, rl.off, rl.nbr,
-                                                              rl.gw);
+                                                              rl.gw, rl.dk);
     k_ref_L<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, rl.off, rl.nbr, rl.gw, T, L);
     return 2;
 }
