@@ -26,6 +26,10 @@ namespace arp {
 namespace {
 
 constexpr int kThreads = 128;
+#ifndef ARP_SOLID_LANES
+#define ARP_SOLID_LANES 2
+#endif
+constexpr int kSolidLanes = ARP_SOLID_LANES;  // threads per solid in the stress and force kernels
 constexpr uint32_t kSameMat = 0x80000000u;
 
 inline uint32_t blocks_for(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / (uint32_t)t; }
@@ -225,10 +229,23 @@ __global__ void k_solid_gather(const float4* __restrict__ pd, const float4* __re
 // log-series, square-root and inverse paths are compiled out.
 // PLASTIC: some solid material is plastic; otherwise the plastic strain is
 // zero throughout and its buffers are neither read nor written.
-template <bool ORDER2, bool PLASTIC>
+// LANES threads share one solid: they walk its reference list with stride
+// LANES and combine their partial sums with shuffles (a fixed order, so the
+// result is deterministic); lane 0 finishes the particle.
+template <int LANES>
+__device__ __forceinline__ float group_sum(float v) {
+    const uint32_t lane = threadIdx.x & 31u;
+    const uint32_t mask = (LANES == 32 ? 0xFFFFFFFFu : ((1u << LANES) - 1u)) << (lane & ~(uint32_t)(LANES - 1));
+#pragma unroll
+    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, LANES);
+    return v;
+}
+
+template <bool ORDER2, bool PLASTIC, int LANES>
 __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T, StageCoefs c) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.ns) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / LANES, lane = t % LANES;
+    if (i >= a.ns) return;  // whole groups leave together
     const float4 xi = a.sx[i];
     const float4 vi = a.sv[i];
     const DevMat mm = T.mats[__float_as_uint(vi.w)];
@@ -238,7 +255,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
     // strain.rs:139-160: F = sum V dx (x) (L gradW), Fdot likewise with dv
     float F[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     float Fd[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
-    for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
+    for (uint32_t k = a.rl.off[i] + lane; k < a.rl.off[i + 1]; k += LANES) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMat;
         const float4 g = a.rl.gw[k];
         const float3 dx = sub3(a.sx[j], xi);
@@ -253,6 +270,16 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
                 F[cc][r] += g.w * (x[r] * gr[cc]);
                 Fd[cc][r] += g.w * (v[r] * gr[cc]);
             }
+    }
+    if (LANES > 1) {
+#pragma unroll
+        for (int cc = 0; cc < 3; ++cc)
+#pragma unroll
+            for (int r = 0; r < 3; ++r) {
+                F[cc][r] = group_sum<LANES>(F[cc][r]);
+                Fd[cc][r] = group_sum<LANES>(Fd[cc][r]);
+            }
+        if (lane != 0) return;
     }
     M4 Fm = m4_zero(), Fdm = m4_zero(), Lm = m4_zero(), EP;
 #pragma unroll
@@ -377,9 +404,11 @@ __device__ __forceinline__ bool in_stencil(uint2 a, uint2 b) {
            dz <= 1;
 }
 
+template <int LANES>
 __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.ns) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / LANES, lane = t % LANES;
+    if (i >= a.ns) return;  // whole groups leave together
     const float4 xi = a.sx[i];
     const uint32_t mat = __float_as_uint(a.sv[i].w);
     const DevMat mm = T.mats[mat];
@@ -396,7 +425,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
     // (solid.rs:343-374) and, when the neighbor also sits in the current
     // 3x3x3 cells, hourglass control (solid.rs:430-443; kernel(dX) is
     // non-zero exactly for these pairs).
-    for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
+    for (uint32_t k = a.rl.off[i] + lane; k < a.rl.off[i + 1]; k += LANES) {
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMat)) continue;
         const uint32_t j = e & ~kSameMat;
@@ -435,6 +464,12 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
             fy -= __fdividef(sh * dx.y, den);
             fz -= __fdividef(sh * dx.z, den);
         }
+    }
+    if (LANES > 1) {
+        fx = group_sum<LANES>(fx);
+        fy = group_sum<LANES>(fy);
+        fz = group_sum<LANES>(fz);
+        if (lane != 0) return;
     }
     // Self-contact (solid.rs:428,445-450): same-material neighbors in the
     // current cells whose reference distance exceeds r_cut.  Skipped when
@@ -496,12 +531,13 @@ int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaS
     if (a.ns == 0) return 0;
     cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
     k_solid_gather<<<blocks_for(a.ns, 256), 256, 0, st>>>(a.pd, a.vm, a.coord, a.slot_of, a.ns, a.sx, a.sv, a.sc);
-    const uint32_t blocks = blocks_for(a.ns, kThreads);
-    if (a.all_order2 && !a.any_plastic) k_solid_stress<true, false><<<blocks, kThreads, 0, st>>>(a, T, c);
-    else if (a.all_order2) k_solid_stress<true, true><<<blocks, kThreads, 0, st>>>(a, T, c);
-    else if (!a.any_plastic) k_solid_stress<false, false><<<blocks, kThreads, 0, st>>>(a, T, c);
-    else k_solid_stress<false, true><<<blocks, kThreads, 0, st>>>(a, T, c);
-    k_solid_forces<<<blocks, kThreads, 0, st>>>(a, T);
+    constexpr int L = kSolidLanes;
+    const uint32_t blocks = blocks_for(a.ns * L, kThreads);
+    if (a.all_order2 && !a.any_plastic) k_solid_stress<true, false, L><<<blocks, kThreads, 0, st>>>(a, T, c);
+    else if (a.all_order2) k_solid_stress<true, true, L><<<blocks, kThreads, 0, st>>>(a, T, c);
+    else if (!a.any_plastic) k_solid_stress<false, false, L><<<blocks, kThreads, 0, st>>>(a, T, c);
+    else k_solid_stress<false, true, L><<<blocks, kThreads, 0, st>>>(a, T, c);
+    k_solid_forces<L><<<blocks, kThreads, 0, st>>>(a, T);
     return 3;
 }
 
