@@ -25,6 +25,8 @@ import sys
 import tempfile
 import time
 
+import numpy as np
+
 ROOT = os.path.dirname(os.path.abspath(__file__))
 sys.path.insert(0, os.path.join(ROOT, "ar-physics_b200"))
 sys.path.insert(0, ROOT)
@@ -142,6 +144,33 @@ def config_of(sc, name):
         "particles": int(sc.n + sc.nb), "mobile": int(sc.n), "solids": ns, "boundary": int(sc.nb),
         "integrator": sc.integrator, "l2": "flushed between timed steps (256 MiB write)",
     }
+
+
+def step_roofline(sc, stages, step_ms, peak):
+    """Whole-step algorithmic bytes: per mobile particle 96 B per stage plus
+    96 B for the grid build, per solid 196 B per stage (reference position,
+    L, F written and read, plastic strain read and written), per boundary
+    particle 16 B per stage."""
+    ns = sc.n_solids()
+    per_step = sc.n * (96.0 * stages + 96.0) + ns * 196.0 * stages + sc.nb * 16.0 * stages
+    gbs = per_step / (step_ms / 1000.0) / 1e9
+    return {"alg_bytes_per_step": per_step, "achieved": gbs, "unit": "GB/s", "frac": gbs / peak,
+            "formula": "n*(96*S+96) + n_solid*196*S + n_boundary*16*S, S = stages per step"}
+
+
+def pair_rate(sc, stages, fluid_ms_per_step):
+    """Fluid pair interactions per second: ordered pairs (i mobile, j mobile or
+    boundary, j != i, |x_j - x_i| < h) in the initial state, counted with a
+    k-d tree outside the timed region, times the stages of a step, over the
+    fluid kernel's time per step."""
+    from scipy.spatial import cKDTree
+    d = sc.dim
+    mob = sc.particles["pos"][:, :d].astype(np.float64)
+    allp = np.concatenate([mob, sc.boundary["pos"][:, :d].astype(np.float64)])
+    r = float(sc.h) * (1.0 - 1e-6)  # lattice pairs sit exactly at |r| = h, where W = 0
+    pairs = int(cKDTree(mob).count_neighbors(cKDTree(allp), r)) - len(mob)
+    return {"per_stage": pairs, "per_particle": pairs / max(sc.n, 1),
+            "rate": pairs * stages / (fluid_ms_per_step / 1000.0), "unit": "pair-interactions/s"}
 
 
 def cpu_baseline(sc, max_seconds=20.0, max_steps=5):
@@ -444,6 +473,9 @@ def run_ours(args, rank, world, local_rank):
                 "avg_launch_ms": fluid_ms,
                 "segments_ms_per_step": {k: prof[k] / max(prof["steps"], 1) for k in
                                          ("neighbor_ms", "solid_ms", "fluid_ms")}}
+    stages = fl / max(prof["steps"], 1)
+    roofline["step"] = step_roofline(sc, stages, total_ms / args.steps, peak)
+    roofline["pairs"] = pair_rate(sc, stages, prof["fluid_ms"] / max(prof["steps"], 1))
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,
