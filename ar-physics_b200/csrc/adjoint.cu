@@ -332,15 +332,7 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const flo
     const uint32_t li = mat - P.mat_base;
     const DevInter* row_i = T.inter + P.inter_base + li * P.nmat;
     if (finite3(xi)) {
-        const Grid g = P.grid;
-        const CellCoord cc = cell_coord(xi, g);
-        const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
-        const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
-        const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
-        for (int z = zlo; z <= zhi; ++z)
-            for (int y = ylo; y <= yhi; ++y) {
-                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
+        for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
                 for (uint32_t jb = a.bstart[c0]; jb < a.bstart[c1]; ++jb) {
                     const float4 xb = a.bxs[jb];
                     const float rx = xb.x - xi.x, ry = xb.y - xi.y, rz = DIM == 3 ? xb.z - xi.z : 0.0f;
@@ -386,7 +378,7 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const flo
                     lv = add(lv, o.lvv);
                     lrho += o.ld_nbr + o.lpt * dpt_i;
                 }
-            }
+        });
     }
     lrho -= dot(wF, Fs) * ei.z;  // k_v = F / rho
     if (DIM == 2) {
@@ -521,28 +513,18 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
         const bool maybe = !mm.plastic && (P.contact_slack <= 0.0f || a.st.contact_bound[1] != 0u ||
                                           !(2.0f * U < P.contact_slack));
         if (maybe && finite3(xi)) {
-            const Grid& g = P.grid;
-            const CellCoord cc = cell_coord(xi, g);
-            const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
             bool active = false;
-            for (int dz = -1; dz <= 1 && !active; ++dz) {
-                const int z = cc.z + dz;
-                if (z < 0 || z >= (int)g.sub[2]) continue;
-                for (int dy = -1; dy <= 1 && !active; ++dy) {
-                    const int y = cc.y + dy;
-                    if (y < 0 || y >= (int)g.sub[1]) continue;
-                    const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-                    for (uint32_t k = a.st.start[row + x0]; k < a.st.start[row + x1 + 1] && !active; ++k) {
-                        const uint32_t s2 = a.st.perm ? a.st.perm[k] : k;
-                        if (__float_as_uint(a.st.vm[s2].w) != mat) continue;
-                        const uint32_t sj = a.sid[s2];
-                        if (sj == kInvalid) continue;
-                        const float3 dx = sub(f3(a.st.pd[s2]), f3(xi));
-                        const float3 dX = sub(f3(a.ref[sj]), Xi);
-                        if (dot(dX, dX) > P.rcut2 && dot(dx, dx) < P.rcut2) active = true;
-                    }
+            for_reference_block_rows(xi, P, [&](uint32_t c0, uint32_t c1) {
+                for (uint32_t k = a.st.start[c0]; k < a.st.start[c1] && !active; ++k) {
+                    const uint32_t s2 = a.st.perm ? a.st.perm[k] : k;
+                    if (__float_as_uint(a.st.vm[s2].w) != mat) continue;
+                    const uint32_t sj = a.sid[s2];
+                    if (sj == kInvalid) continue;
+                    const float3 dx = sub(f3(a.st.pd[s2]), f3(xi));
+                    const float3 dX = sub(f3(a.ref[sj]), Xi);
+                    if (dot(dX, dX) > P.rcut2 && dot(dx, dx) < P.rcut2) active = true;
                 }
-            }
+            });
             if (active) atomicOr(a.flags, 1u);
         }
     }

@@ -25,6 +25,14 @@ namespace arp {
 constexpr uint32_t kInvalid = 0xFFFFFFFFu;
 constexpr uint32_t kBucketSlots = 128;  // neighbor_list.rs:45
 constexpr int kMaxMaterials = 32;  // per scene
+// Axes (bit a = axis a) along which the search grid halves the reference
+// cells.  Halving x alone keeps a warp's 32 consecutive particles inside a
+// compact 4h x h x h block (the rows stay x-fastest) while its rows of 5
+// half-width cells hold 5/6 of the candidates of 3 reference cells.
+#ifndef ARP_SEARCH_HALVE
+#define ARP_SEARCH_HALVE 1
+#endif
+constexpr uint32_t kSearchHalve = ARP_SEARCH_HALVE;
 
 // Uniform grid of NeighborList::new (neighbor_list.rs:199-217), one scene.
 struct Grid {
@@ -55,10 +63,25 @@ struct DevInter {
 
 // Scalars of one scene.  Products are rounded exactly as the shaders group
 // them (e.g. EPSILON*h*h = (0.1*h)*h).  A single simulation is a batch of one
-// scene; the cells of scene k are global cells cell_base .. cell_base+ncells.
+// scene.
+//
+// Two grids cover the scene's box.  `grid` is the reference's (cells of at
+// least h); the hourglass and self-contact stencils, the cell statistics and
+// the cell queries of the C ABI use it.  `sgrid`, the search grid, halves the
+// cells along the axes of kSearchHalve that have non-zero extent (sub
+// doubled), so along such an axis a sphere of radius h spans at most 5 cells
+// of width h/2 instead of 3 of width h; particles are sorted by search cell,
+// and the search cells of one reference cell c are 2c and 2c+1 along each
+// halved axis.  Because 2 * (t * sub) is rounded exactly like t * (2 sub),
+// floor(search) >> 1 is the reference cell bit for bit.  Search cells of
+// scene k are global cells cell_base .. cell_base + sgrid.ncells; its
+// reference cells, numbered for the C ABI only, start at ccell_base.
 struct SceneP {
     Grid grid;
+    Grid sgrid;
+    uint32_t halved[3];               // 1 where sgrid halves grid's cells
     uint32_t cell_base;
+    uint32_t ccell_base;
     uint32_t dim;                     // the reference's count of non-zero box axes
     uint32_t mat_base, nmat;          // global material range of the scene
     uint32_t inter_base;              // first entry of its nmat x nmat interaction block
@@ -83,8 +106,9 @@ struct Tables {
     const DevMat* mats;
     const FluidMat* fmats;
     const DevInter* inter;
-    uint32_t ncells;                  // total cells of all scenes (the non-finite bucket follows)
+    uint32_t ncells;                  // total search cells of all scenes (the non-finite bucket follows)
     uint32_t max_nmat;                // largest per-scene material count
+    uint32_t nscenes;
 };
 
 // Health counters written by device code.

@@ -4,10 +4,11 @@
 // fluid.rs:95-336) and the lin_comb stage arithmetic that follows it
 // (src/soft_body/particle_state/particles.rs:8-154).  The shader runs one
 // 81-invocation workgroup per particle (27 cells x 3 strided lanes) with a
-// shared-memory tree reduction; here one thread owns one cell-sorted particle
-// and walks the 3x3(x3) neighborhood as 3 (2D) or 9 (3D) contiguous row
-// ranges of the sorted arrays, so neighbor loads are coalesced across a warp
-// (consecutive threads sit in the same or adjacent cells).
+// shared-memory tree reduction; here one thread owns one particle sorted by
+// search cell (the reference cell halved along x) and walks 3 (2D) or 9 (3D)
+// contiguous x-rows of 5 half-width cells, so neighbor loads are coalesced
+// across a warp (consecutive threads sit in the same or adjacent cells) and
+// 5/6 of the candidates of the 3x3x3 reference cells are tested.
 //
 // Per pair the math is the shader's, term by term: continuity density rate,
 // symmetric pressure force with the equation of state evaluated for both
@@ -234,16 +235,19 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     uint32_t* my = lst;
     uint32_t cnt = 0;
     bool full = false;
-    // pass 1: candidates of the 3x3(x3) cells whose squared distance is
-    // inside h^2 (the same h^2 - r^2 > 0 test as grad_w's max(.., 0))
+    // pass 1: candidates of the search rows whose squared distance is inside
+    // h^2 (r^2 < h^2 is h^2 - r^2 > 0, grad_w's max(.., 0) test: without
+    // flush-to-zero a difference of finite floats is zero only when they are
+    // equal).  The particle itself passes the test and is dropped when the
+    // hits are evaluated, which keeps the index compare out of this loop.
     auto hit = [&](float4 q) {
         const float rx = q.x - xi.x, ry = q.y - xi.y;
-        const float r2 = DIM == 3 ? (rx * rx + ry * ry) + (q.z - xi.z) * (q.z - xi.z) : rx * rx + ry * ry;
-        return K.h2 - r2 > 0.0f;
+        const float r2 = DIM == 3 ? fmaf(q.z - xi.z, q.z - xi.z, fmaf(ry, ry, rx * rx)) : fmaf(ry, ry, rx * rx);
+        return r2 < K.h2;
     };
     auto take = [&](uint32_t j) {
         if (DIRECT) {
-            eval_hit<DIM>(j, s, a, K, acc);
+            if (j != k) eval_hit<DIM>(j, s, a, K, acc);
         } else if (cnt < CAP) {
             my[cnt++ * BLOCK] = j;
         } else {
@@ -251,41 +255,34 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
         }
     };
     if (finite3(xi)) {
-        const Grid g = P.grid;
-        const uint32_t cell_base = P.cell_base;
-        const CellCoord cc = cell_coord(xi, g);
-        const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
-        const int zlo = DIM == 3 ? max(cc.z - 1, 0) : cc.z, zhi = DIM == 3 ? min(cc.z + 1, (int)g.sub[2] - 1) : cc.z;
-        const int ylo = max(cc.y - 1, 0), yhi = min(cc.y + 1, (int)g.sub[1] - 1);
-        for (int z = zlo; z <= zhi && !full; ++z) {
-            for (int y = ylo; y <= yhi && !full; ++y) {
-                const uint32_t row = cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
-                const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
-                for (uint32_t j = bb; j < be; ++j)
-                    if (hit(a.bxs[j])) take(j | kBoundaryBit);
-                const uint32_t jb = a.start[c0], je = a.start[c1];
-                uint32_t j = jb;
-                for (; j + 3u < je; j += 4u) {  // four loads in flight
-                    const float4 q0 = a.xs[j], q1 = a.xs[j + 1u], q2 = a.xs[j + 2u], q3 = a.xs[j + 3u];
-                    const bool h0 = j != k && hit(q0), h1 = j + 1u != k && hit(q1);
-                    const bool h2 = j + 2u != k && hit(q2), h3 = j + 3u != k && hit(q3);
-                    if (h0) take(j);
-                    if (h1) take(j + 1u);
-                    if (h2) take(j + 2u);
-                    if (h3) take(j + 3u);
-                }
-                for (; j < je; ++j)
-                    if (j != k && hit(a.xs[j])) take(j);  // the particle itself contributes exactly zero
+        for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
+            if (full) return;
+            const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
+            for (uint32_t j = bb; j < be; ++j)
+                if (hit(a.bxs[j])) take(j | kBoundaryBit);
+            const uint32_t jb = a.start[c0], je = a.start[c1];
+            uint32_t j = jb;
+            for (; j + 3u < je; j += 4u) {  // four loads in flight
+                const float4 q0 = a.xs[j], q1 = a.xs[j + 1u], q2 = a.xs[j + 2u], q3 = a.xs[j + 3u];
+                const bool h0 = hit(q0), h1 = hit(q1), h2 = hit(q2), h3 = hit(q3);
+                if (h0) take(j);
+                if (h1) take(j + 1u);
+                if (h2) take(j + 2u);
+                if (h3) take(j + 3u);
             }
-        }
+            for (; j < je; ++j)
+                if (hit(a.xs[j])) take(j);
+        });
         if (!DIRECT) {
             if (full) {
                 a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
                 return;
             }
             // pass 2: pair math over the collected hits
-            for (uint32_t e = 0; e < cnt; ++e) eval_hit<DIM>(my[e * BLOCK], s, a, K, acc);
+            for (uint32_t e = 0; e < cnt; ++e) {
+                const uint32_t j = my[e * BLOCK];
+                if (j != k) eval_hit<DIM>(j, s, a, K, acc);
+            }
         }
     }
 

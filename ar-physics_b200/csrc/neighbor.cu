@@ -51,9 +51,14 @@ __global__ void k_cell_keys(const float4* __restrict__ pos, const float4* __rest
     } else {
         const SceneP& sp = T.scenes[scene_of(vm, mat_u32, i, T)];
         const Grid& grid = sp.grid;
-        const CellCoord cc = cell_coord(p, grid);
-        k = sp.cell_base + cell_id(cc, grid);
-        if (coord) coord[i] = make_uint2((uint32_t)cc.x | ((uint32_t)cc.y << 16), (uint32_t)cc.z);
+        const CellCoord fc = cell_coord(p, sp.sgrid);
+        k = sp.cell_base + cell_id(fc, sp.sgrid);
+        if (coord) {
+            // reference cell = search cell >> 1 on halved axes (exact, see SceneP)
+            const uint32_t x = (uint32_t)fc.x >> sp.halved[0], y = (uint32_t)fc.y >> sp.halved[1],
+                           z = (uint32_t)fc.z >> sp.halved[2];
+            coord[i] = make_uint2(x | (y << 16), z);
+        }
         if (stats) {
             // a coordinate on the upper face would hash one past the last cell
             bool face = (grid.dim[0] != 0.0f && p.x == grid.min[0] + grid.dim[0]) ||
@@ -153,16 +158,48 @@ __global__ void k_scatter(const uint32_t* __restrict__ key, const uint32_t* __re
     perm[start[key[i]] + rank[i]] = i;
 }
 
+// Occupancy (mobile + boundary) of the reference cell whose first search
+// cell is global cell c, or 0 when c is not the first search cell of its
+// reference cell.
+__device__ __forceinline__ uint32_t reference_cell_occupancy(uint32_t c, const uint32_t* __restrict__ start,
+                                                             const uint32_t* __restrict__ bstart, const Tables& T) {
+    uint32_t lo = 0, hi = T.nscenes;  // scene with the largest cell_base <= c
+    while (hi - lo > 1) {
+        const uint32_t mid = (lo + hi) >> 1;
+        if (T.scenes[mid].cell_base <= c) lo = mid;
+        else hi = mid;
+    }
+    const SceneP& P = T.scenes[lo];
+    const Grid& g = P.sgrid;
+    const uint32_t l = c - P.cell_base;
+    if ((P.halved[1] | P.halved[2]) == 0u) {
+        // only x halved: sub[0] is even, so x and l have the same parity
+        if (l & P.halved[0]) return 0u;
+    } else {
+        const uint32_t x = l % g.sub[0], y = (l / g.sub[0]) % g.sub[1], z = l / (g.sub[0] * g.sub[1]);
+        if (((x & P.halved[0]) | (y & P.halved[1]) | (z & P.halved[2])) != 0u) return 0u;
+    }
+    uint32_t occ = 0;
+    for (uint32_t dz = 0; dz <= P.halved[2]; ++dz)
+        for (uint32_t dy = 0; dy <= P.halved[1]; ++dy) {
+            const uint32_t r0 = c + dy * g.sub[0] + dz * g.sub[0] * g.sub[1], r1 = r0 + 1u + P.halved[0];
+            occ += start[r1] - start[r0];
+            if (bstart) occ += bstart[r1] - bstart[r0];
+        }
+    return occ;
+}
+
 // Sort each cell's run ascending (insertion sort; runs longer than 256 are
-// left in arrival order, which is still a valid grid).
+// left in arrival order, which is still a valid grid).  With `stats`, also
+// the occupancy counters of the reference cells.
 __global__ void k_sort_runs(const uint32_t* __restrict__ start, uint32_t ncells, uint32_t* __restrict__ perm,
-                            const uint32_t* __restrict__ boundary_start, DevStats* stats) {
+                            const uint32_t* __restrict__ boundary_start, DevStats* stats, Tables T) {
     uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c > ncells) return;  // includes the non-finite bucket at index ncells
     const uint32_t b = start[c], e = start[c + 1];
     const uint32_t len = e - b;
     if (stats && c < ncells) {
-        uint32_t occ = len + (boundary_start ? boundary_start[c + 1] - boundary_start[c] : 0u);
+        const uint32_t occ = reference_cell_occupancy(c, start, boundary_start, T);
         if (occ > 0) atomicMax(&stats->max_cell_occupancy, occ);
         if (occ > kBucketSlots) atomicAdd(&stats->overflow_cells, 1u);
     }
@@ -294,22 +331,12 @@ __global__ void k_count_neighbors(const float4* __restrict__ xs, const float4* _
     uint32_t cnt = 0;
     if (finite3(p)) {
         const SceneP& P = T.scenes[scene_of(vs, nullptr, k, T)];
-        const Grid& g = P.grid;
-        const CellCoord c = cell_coord(p, g);
-        const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, (int)g.sub[0] - 1);
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int z = c.z + dz;
-            if (z < 0 || z >= (int)g.sub[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = c.y + dy;
-                if (y < 0 || y >= (int)g.sub[1]) continue;
-                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
-                if (bstart)
-                    for (uint32_t j = bstart[c0]; j < bstart[c1]; ++j) cnt += within_h_exact(bxs[j], p, P.h2);
-                for (uint32_t j = start[c0]; j < start[c1]; ++j) cnt += within_h_exact(xs[j], p, P.h2);
-            }
-        }
+        // the shader's 3x3(x3) reference cells exactly
+        for_reference_block_rows(p, P, [&](uint32_t c0, uint32_t c1) {
+            if (bstart)
+                for (uint32_t j = bstart[c0]; j < bstart[c1]; ++j) cnt += within_h_exact(bxs[j], p, P.h2);
+            for (uint32_t j = start[c0]; j < start[c1]; ++j) cnt += within_h_exact(xs[j], p, P.h2);
+        });
     }
     out[k] = cnt;
 }
@@ -384,7 +411,7 @@ int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uin
         ++launches;
     }
     k_sort_runs<<<blocks_for(T.ncells + 1, kThreads), kThreads, 0, st>>>(gb.start, T.ncells, gb.perm,
-                                                                         boundary_start, stats);
+                                                                         boundary_start, stats, T);
     ++launches;
     return launches;
 }
@@ -496,7 +523,8 @@ extern "C" arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, co
     if (n > 0) k_rank_noalloc<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, g, cell_start, rank);
     exclusive_scan(cell_start, len, cell_start, tile_sums, st);  // in place: counts become starts
     if (n > 0) k_scatter_noalloc<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, g, cell_start, rank, perm);
-    k_sort_runs<<<blocks_for(g.ncells + 1, kThreads), kThreads, 0, st>>>(cell_start, g.ncells, perm, nullptr, nullptr);
+    k_sort_runs<<<blocks_for(g.ncells + 1, kThreads), kThreads, 0, st>>>(cell_start, g.ncells, perm, nullptr, nullptr,
+                                                                         Tables{});
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(ARP_ERR_CUDA, std::string("grid build launch: ") + cudaGetErrorString(e));
     return ARP_OK;

@@ -214,7 +214,8 @@ struct arp_sim {
     bool any_stiff_immobile = false;
     bool all_order2 = true;  // every stiff material uses strain order 2
     bool any_plastic = false;  // some stiff material is plastic
-    uint32_t ncells = 0;     // cells of all scenes
+    uint32_t ncells = 0;     // search cells of all scenes
+    uint32_t nccells = 0;    // reference cells of all scenes (the C ABI's cell numbering)
     uint32_t max_nmat = 0;
     Tables tables{};
     std::vector<uint32_t> scene_of_material;
@@ -397,6 +398,16 @@ arp_status scene_params(arp_sim::SceneHost& H, uint32_t dim) {
     }
     if (nc > (1ull << 30)) return fail(ARP_ERR_UNSUPPORTED, "a scene's grid has more than 2^30 cells");
     P.grid.ncells = (uint32_t)nc;
+    // search grid: the kSearchHalve axes of non-zero extent halved (the w axis is not hashed)
+    P.sgrid = P.grid;
+    uint64_t snc = 1;
+    for (int a = 0; a < 3; ++a) {
+        P.halved[a] = H.bounds.dim[a] != 0.0f && (kSearchHalve >> a & 1u) ? 1u : 0u;
+        P.sgrid.sub[a] = P.grid.sub[a] << P.halved[a];
+        snc *= P.sgrid.sub[a];
+    }
+    if (snc > (1ull << 30)) return fail(ARP_ERR_UNSUPPORTED, "a scene's search grid has more than 2^30 cells");
+    P.sgrid.ncells = (uint32_t)snc;
     P.dim = dim;
     P.h = H.h;
     P.h2 = H.h * H.h;
@@ -898,10 +909,12 @@ arp_status append_scene(const arp_scene* sc, arp_sim* S) {
         }
     S->inter.insert(S->inter.end(), block.begin(), block.end());
     ARP_TRY(scene_params(H, dim));
-    if ((uint64_t)S->ncells + H.sp.grid.ncells + 2 > (1ull << 31))
+    if ((uint64_t)S->ncells + H.sp.sgrid.ncells + 2 > (1ull << 31))
         return fail(ARP_ERR_UNSUPPORTED, "the batch's grids have more than 2^31 cells");
     H.sp.cell_base = S->ncells;
-    S->ncells += H.sp.grid.ncells;
+    S->ncells += H.sp.sgrid.ncells;
+    H.sp.ccell_base = S->nccells;
+    S->nccells += H.sp.grid.ncells;
     S->n += H.n;
     S->nb += H.nb;
     S->M += M;
@@ -1044,6 +1057,7 @@ arp_status allocate(arp_sim* S) {
     S->tables.inter = S->d_inter.p;
     S->tables.ncells = S->ncells;
     S->tables.max_nmat = S->max_nmat;
+    S->tables.nscenes = (uint32_t)S->scenes.size();
     return ARP_OK;
 }
 
@@ -1206,7 +1220,7 @@ arp_status arp_sim_scene_range(const arp_sim* sim, uint32_t scene, uint32_t* fir
     if (n_particles) *n_particles = H.n;
     if (first_boundary) *first_boundary = H.b_base;
     if (n_boundary) *n_boundary = H.nb;
-    if (first_cell) *first_cell = H.sp.cell_base;
+    if (first_cell) *first_cell = H.sp.ccell_base;
     if (n_cells) *n_cells = H.sp.grid.ncells;
     return ARP_OK;
 }
@@ -1667,14 +1681,35 @@ arp_status arp_sim_grid(const arp_sim* sim, uint32_t subdivisions[4], uint32_t* 
         for (int a = 0; a < 3; ++a) subdivisions[a] = sim->scenes[0].sp.grid.sub[a];
         subdivisions[3] = 1;
     }
-    if (n_cells) *n_cells = sim->ncells;
+    if (n_cells) *n_cells = sim->nccells;
     return ARP_OK;
+}
+
+// Reference cell (neighbor_list.rs:95) of a position in scene `scene`, in the
+// C ABI's numbering; nccells for a non-finite position.
+static uint32_t ref_cell_key(const arp_sim* S, float4 p, uint32_t scene) {
+    if (!finite3(p)) return S->nccells;
+    const SceneP& P = S->scenes[scene].sp;
+    return P.ccell_base + cell_id(cell_coord(p, P.grid), P.grid);
+}
+
+// CSR of keys (caller order) over nc cells plus the non-finite bucket:
+// start[0..nc+1], members in ascending caller id inside each cell.
+static void cells_csr(const std::vector<uint32_t>& key, uint32_t nc, uint32_t* start_out, uint32_t* members) {
+    std::vector<uint32_t> start(size_t(nc) + 2, 0u);
+    for (uint32_t k : key) ++start[size_t(k) + 1];
+    for (size_t c = 0; c + 1 < start.size(); ++c) start[c + 1] += start[c];
+    if (start_out) std::memcpy(start_out, start.data(), (size_t(nc) + 1) * 4);
+    if (members) {
+        std::vector<uint32_t> fill(start.begin(), start.end() - 1);
+        for (uint32_t i = 0; i < (uint32_t)key.size(); ++i) members[fill[key[i]]++] = i;
+    }
 }
 
 arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_start, uint32_t* members,
                              uint32_t* nbr_count) {
     ARP_TRY(need_init(sim));
-    const uint32_t n = sim->n, nc = sim->ncells;
+    const uint32_t n = sim->n;
     cudaStream_t st = sim->stream;
     sim->launches += build_grid(sim->Y.pd.p, sim->Y.vm.p, nullptr, n, sim->tables, sim->gb, nullptr, nullptr, st);
     sim->launches += gather_sorted(sim->gb.perm, n, sim->Y.pd.p, sim->X.pd.p, sim->Y.vm.p, sim->X.vm.p, nullptr,
@@ -1683,23 +1718,28 @@ arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_sta
     CUDA_TRY(cnt.alloc(n));
     sim->launches += count_neighbors(sim->X.pd.p, sim->X.vm.p, sim->gb.start, n, sim->b_pd.p, sim->b_start.p, sim->tables,
                                      cnt.p, st);
-    std::vector<uint32_t> key(n), perm(n), start(size_t(nc) + 2), orig(n), c(n);
+    std::vector<uint32_t> perm(n), orig(n), c(n);
+    std::vector<float4> pd(n), vm(n);
     if (n) {
-        CUDA_TRY(cudaMemcpyAsync(key.data(), sim->gb.key, n * 4, cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(pd.data(), sim->Y.pd.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(vm.data(), sim->Y.vm.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaMemcpyAsync(perm.data(), sim->gb.perm, n * 4, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaMemcpyAsync(orig.data(), sim->orig.p, n * 4, cudaMemcpyDeviceToHost, st));
         CUDA_TRY(cudaMemcpyAsync(c.data(), cnt.p, n * 4, cudaMemcpyDeviceToHost, st));
     }
-    CUDA_TRY(cudaMemcpyAsync(start.data(), sim->gb.start, (size_t(nc) + 2) * 4, cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
     ARP_TRY(check_launch("neighbors"));
-    if (cell_of)
-        for (uint32_t k = 0; k < n; ++k) cell_of[orig[k]] = key[k] >= nc ? kInvalid : key[k];
-    if (cell_start) std::memcpy(cell_start, start.data(), (size_t(nc) + 1) * 4);
-    if (members) {
-        for (uint32_t k = 0; k < n; ++k) members[k] = orig[perm[k]];
-        for (uint32_t cc = 0; cc <= nc; ++cc) std::sort(members + start[cc], members + start[cc + 1]);
+    // reference cells of the current positions, in caller order
+    const uint32_t nc = sim->nccells;
+    std::vector<uint32_t> key(n);
+    for (uint32_t k = 0; k < n; ++k) {
+        uint32_t m;
+        std::memcpy(&m, &vm[k].w, 4);
+        key[orig[k]] = ref_cell_key(sim, pd[k], sim->scene_of_material[m]);
     }
+    if (cell_of)
+        for (uint32_t i = 0; i < n; ++i) cell_of[i] = key[i] >= nc ? kInvalid : key[i];
+    cells_csr(key, nc, cell_start, members);
     if (nbr_count)
         for (uint32_t k = 0; k < n; ++k) nbr_count[orig[perm[k]]] = c[k];
     return ARP_OK;
@@ -1707,10 +1747,13 @@ arp_status arp_sim_neighbors(arp_sim* sim, uint32_t* cell_of, uint32_t* cell_sta
 
 arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* members) {
     ARP_TRY(need_init(sim));
-    const uint32_t nb = sim->nb, nc = sim->ncells;
-    if (cell_start)
-        CUDA_TRY(cudaMemcpy(cell_start, sim->b_start.p, (size_t(nc) + 1) * 4, cudaMemcpyDeviceToHost));
-    if (members && nb) CUDA_TRY(cudaMemcpy(members, sim->b_orig.p, size_t(nb) * 4, cudaMemcpyDeviceToHost));
+    const uint32_t nb = sim->nb;
+    std::vector<uint32_t> key(nb);
+    for (uint32_t i = 0; i < nb; ++i) {
+        const arp_particle& p = sim->host_boundary[i];
+        key[i] = ref_cell_key(sim, make_float4(p.pos[0], p.pos[1], p.pos[2], p.den), sim->scene_of_material[p.mat]);
+    }
+    cells_csr(key, sim->nccells, cell_start, members);
     return ARP_OK;
 }
 

@@ -44,34 +44,24 @@ __device__ __forceinline__ void pad_unit(M4& C, uint32_t dim) {
         if (i >= dim) C.m[i][i] = 1.0f;
 }
 
-// Walk the 27 reference cells around solid i (ascending cell, ascending
-// solid id inside a cell) and call f(j, dX, diff) for each other solid with
-// h^2 - |dX|^2 > 0.
+// Walk the 27 reference cells around solid i (search-cell rows ascending,
+// ascending solid id inside a search cell) and call f(j, dX, diff) for each
+// other solid with h^2 - |dX|^2 > 0.
 template <class F>
 __device__ __forceinline__ void for_ref_neighbors(uint32_t i, const float4* __restrict__ ref,
                                                   const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm,
                                                   const SceneP& P, F&& f) {
     const float4 xi = ref[i];
     if (!finite3(xi)) return;
-    const Grid& g = P.grid;
-    const CellCoord c = cell_coord(xi, g);
-    const int x0 = max(c.x - 1, 0), x1 = min(c.x + 1, (int)g.sub[0] - 1);
-    for (int dz = -1; dz <= 1; ++dz) {
-        const int z = c.z + dz;
-        if (z < 0 || z >= (int)g.sub[2]) continue;
-        for (int dy = -1; dy <= 1; ++dy) {
-            const int y = c.y + dy;
-            if (y < 0 || y >= (int)g.sub[1]) continue;
-            const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-            for (uint32_t k = start[row + x0]; k < start[row + x1 + 1]; ++k) {
-                const uint32_t j = perm[k];
-                if (j == i) continue;
-                const float3 dX = sub3(ref[j], xi);
-                const float diff = P.h2 - dot3(dX, dX);
-                if (diff > 0.0f) f(j, dX, diff);
-            }
+    for_reference_block_rows(xi, P, [&](uint32_t c0, uint32_t c1) {
+        for (uint32_t k = start[c0]; k < start[c1]; ++k) {
+            const uint32_t j = perm[k];
+            if (j == i) continue;
+            const float3 dX = sub3(ref[j], xi);
+            const float diff = P.h2 - dot3(dX, dX);
+            if (diff > 0.0f) f(j, dX, diff);
         }
-    }
+    });
 }
 
 __global__ void k_ref_count(const float4* __restrict__ ref, const uint32_t* __restrict__ mat_of, uint32_t ns,
@@ -478,34 +468,24 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
     const float U = __uint_as_float(a.contact_bound[0]);
     const bool maybe = !mm.plastic && (P.contact_slack <= 0.0f || a.contact_bound[1] != 0u || !(2.0f * U < P.contact_slack));
     if (maybe && finite3(xi)) {
-        const Grid& g = P.grid;
-        const CellCoord cc = cell_coord(xi, g);
-        const int x0 = max(cc.x - 1, 0), x1 = min(cc.x + 1, (int)g.sub[0] - 1);
-        for (int dz = -1; dz <= 1; ++dz) {
-            const int z = cc.z + dz;
-            if (z < 0 || z >= (int)g.sub[2]) continue;
-            for (int dy = -1; dy <= 1; ++dy) {
-                const int y = cc.y + dy;
-                if (y < 0 || y >= (int)g.sub[1]) continue;
-                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
-                for (uint32_t k = a.start[row + x0]; k < a.start[row + x1 + 1]; ++k) {
-                    if (__float_as_uint(a.vs[k].w) != mat) continue;
-                    const uint32_t sj = a.sid_sorted[k];
-                    if (sj == kInvalid) continue;
-                    const float4 xj = a.xs[k];
-                    const float3 dx = sub3(xj, xi);
-                    const float3 dX = sub3(a.ref[sj], Xi);
-                    const float dXX = dot3(dX, dX), dxx = dot3(dx, dx);
-                    if (!(dXX > P.rcut2 && dxx < P.rcut2)) continue;
-                    const float l = sqrtf(dxx);
-                    const float dr = fmaxf(P.rcut - l, 0.0f);
-                    const float cs = -5000.0f * sqrtf(dr * P.r_geom);
-                    fx += (cs * dx.x) / l;
-                    fy += (cs * dx.y) / l;
-                    fz += (cs * dx.z) / l;
-                }
+        for_reference_block_rows(xi, P, [&](uint32_t c0, uint32_t c1) {
+            for (uint32_t k = a.start[c0]; k < a.start[c1]; ++k) {
+                if (__float_as_uint(a.vs[k].w) != mat) continue;
+                const uint32_t sj = a.sid_sorted[k];
+                if (sj == kInvalid) continue;
+                const float4 xj = a.xs[k];
+                const float3 dx = sub3(xj, xi);
+                const float3 dX = sub3(a.ref[sj], Xi);
+                const float dXX = dot3(dX, dX), dxx = dot3(dx, dx);
+                if (!(dXX > P.rcut2 && dxx < P.rcut2)) continue;
+                const float l = sqrtf(dxx);
+                const float dr = fmaxf(P.rcut - l, 0.0f);
+                const float cs = -5000.0f * sqrtf(dr * P.r_geom);
+                fx += (cs * dx.x) / l;
+                fy += (cs * dx.y) / l;
+                fz += (cs * dx.z) / l;
             }
-        }
+        });
     }
     // solid.rs:492-494 (den term is zero)
     a.ksol[i] = make_float4(__fdiv_rn(fx, d1), __fadd_rn(__fdiv_rn(fy, d1), -P.g), __fdiv_rn(fz, d1), 0.0f);
