@@ -225,8 +225,9 @@ struct FluidArgs {
     const float* ps;         // p / rho^2 of each sorted particle
     const float* bps;        // p / rho^2 of each sorted boundary particle
     const float4* ksol;      // per-solid solid-term acceleration (nullptr when the solid branch is off)
-    uint32_t* overflow;        // [n] particles whose hit list filled up
-    uint32_t* overflow_count;  // their number (cleared before each launch)
+    uint32_t* overflow;        // [2n] two queues: particles whose hit list filled up ([0, n)), and those
+                               // whose list filled up inside one row ([n, 2n))
+    uint32_t* overflow_count;  // [2] their numbers (cleared before each launch)
     uint32_t n;
     int solid_branch;
     int any_stiff_immobile;

@@ -194,17 +194,28 @@ __device__ __forceinline__ void eval_hit(uint32_t j, const Self& s, const FluidA
     }
 }
 
+// How fluid_particle collects and evaluates the hits of a particle.  Every
+// mode sums the pairs in candidate order, so results do not depend on the
+// mode, CAP or the launch shape.
+enum FluidMode {
+    kTwoPass = 0,  // pass 1 fills the list, pass 2 evaluates it; a full list
+                   // queues the particle for kFlush (first overflow queue)
+    kFlush = 1,    // the warp agrees before each row whether some lane's list
+                   // could fill up in it and then evaluates and empties every
+                   // list; a row alone above CAP queues the particle for
+                   // kDirect (second overflow queue)
+    kDirect = 2,   // every hit evaluated during the scan
+};
+
 // Fluid forces and the stage update of sorted particle k.  `lst` is the
 // thread's column of the hit list ([CAP][BLOCK]); `sm`/`si` hold the
-// tables of scene `scene0`.
-// DIRECT: evaluate every hit during the scan (the overflow kernel) instead
-// of through the list; a list that fills up hands the particle to that kernel
-// through the overflow queue and writes nothing.  Either way the pairs are
-// summed in candidate order.
-template <int DIM, int BLOCK, int CAP, bool DIRECT>
+// tables of scene `scene0`.  A particle handed to an overflow queue writes
+// nothing here.  `wmask` (kFlush): the lanes of this warp that run
+// fluid_particle, all of which take part in the per-row vote.
+template <int DIM, int BLOCK, int CAP, int MODE>
 __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, const Tables& T, const StageCoefs& c,
                                                const StageBuffers& b, uint32_t* lst, const FluidMat* sm,
-                                               const DevInter* si, uint32_t scene0) {
+                                               const DevInter* si, uint32_t scene0, unsigned wmask) {
     const float4 xi = a.xs[k];
     const float4 vi = a.vs[k];
     const uint32_t slot = a.perm ? a.perm[k] : k;
@@ -245,6 +256,7 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
         const float r2 = DIM == 3 ? fmaf(q.z - xi.z, q.z - xi.z, fmaf(ry, ry, rx * rx)) : fmaf(ry, ry, rx * rx);
         return r2 < K.h2;
     };
+    constexpr bool DIRECT = MODE == kDirect;
     auto take = [&](uint32_t j) {
         if (DIRECT) {
             if (j != k) eval_hit<DIM>(j, s, a, K, acc);
@@ -254,7 +266,55 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
             full = true;
         }
     };
-    if (finite3(xi)) {
+    // pass 2 over the hits collected so far, in candidate order
+    auto flush = [&]() {
+        for (uint32_t e = 0; e < cnt; ++e) {
+            const uint32_t j = my[e * BLOCK];
+            if (j != k) eval_hit<DIM>(j, s, a, K, acc);
+        }
+        cnt = 0;
+    };
+    if (MODE == kFlush) {
+        // The search rows (x-rows of the search cells within reach, see
+        // for_search_rows) in a fixed order and number for every lane, rows
+        // outside the grid (and every row of a non-finite particle) empty, so
+        // that the warp can vote before each row; the pass after the last row
+        // only evaluates what is left (one call site of the pair math keeps
+        // the registers down).
+        constexpr int RX = 1 + (int)(kSearchHalve & 1u), RY = 1 + (int)(kSearchHalve >> 1 & 1u),
+                      RZ = 1 + (int)(kSearchHalve >> 2 & 1u);
+        constexpr int NY = 2 * RY + 1, NZ = DIM == 3 ? 2 * RZ + 1 : 1;
+        const bool fin = finite3(xi);
+        const Grid& g = P.sgrid;
+        const CellCoord cc = fin ? cell_coord(xi, g) : CellCoord{0, 0, 0};
+        const int x0 = max(cc.x - RX, 0), x1 = min(cc.x + RX, (int)g.sub[0] - 1);
+        for (int r = 0;; ++r) {
+            const bool last = r == NY * NZ;
+            const int y = cc.y - RY + r % NY;
+            const int z = DIM == 3 ? cc.z - RZ + r / NY : cc.z;
+            uint32_t bb = 0, be = 0, jb = 0, je = 0;
+            if (!last && fin && y >= 0 && y < (int)g.sub[1] && z >= 0 && z < (int)g.sub[2]) {
+                const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
+                const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
+                bb = a.bstart[c0];
+                be = a.bstart[c1];
+                jb = a.start[c0];
+                je = a.start[c1];
+            }
+            const bool fl = last || __any_sync(wmask, !full && cnt + (be - bb) + (je - jb) > (uint32_t)CAP);
+            if (fl && !full) flush();
+            if (last) break;
+            if (full) continue;
+            for (uint32_t j = bb; j < be; ++j)
+                if (hit(a.bxs[j])) take(j | kBoundaryBit);
+            for (uint32_t j = jb; j < je; ++j)
+                if (hit(a.xs[j])) take(j);
+        }
+        if (full) {
+            a.overflow[a.n + atomicAdd(a.overflow_count + 1, 1u)] = k;
+            return;
+        }
+    } else if (finite3(xi)) {
         for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
             if (full) return;
             const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
@@ -273,16 +333,12 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
             for (; j < je; ++j)
                 if (hit(a.xs[j])) take(j);
         });
-        if (!DIRECT) {
+        if (MODE == kTwoPass) {
             if (full) {
                 a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
                 return;
             }
-            // pass 2: pair math over the collected hits
-            for (uint32_t e = 0; e < cnt; ++e) {
-                const uint32_t j = my[e * BLOCK];
-                if (j != k) eval_hit<DIM>(j, s, a, K, acc);
-            }
+            flush();  // pass 2
         }
     }
 
@@ -361,7 +417,7 @@ __global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoe
     load_scene_tables(T, scene0, sm, si);
     __syncthreads();
     const uint32_t k = k0 + threadIdx.x;
-    if (k < a.n) fluid_particle<DIM, BLOCK, CAP, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+    if (k < a.n) fluid_particle<DIM, BLOCK, CAP, kTwoPass>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, 0u);
 }
 
 // Persistent form: each block keeps taking the next tile of the cell-sorted,
@@ -391,18 +447,35 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables 
         }
         __syncthreads();
         const uint32_t k = k0 + threadIdx.x;
-        if (k < a.n) fluid_particle<DIM, BLOCK, CAP, false>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0);
+        if (k < a.n) fluid_particle<DIM, BLOCK, CAP, kTwoPass>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, 0u);
         __syncthreads();
     }
 }
 
-// Particles whose hit list filled up, one thread each, evaluating their
-// pairs during the scan.
+// First overflow queue: particles whose hit list filled up, evaluated with
+// list flushes (kFlush), grid-stride over the queue.
+constexpr int kFlushCap = 64;
+template <int DIM>
+__global__ void __launch_bounds__(128) k_fluid_overflow_flush(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    __shared__ uint32_t lst[kFlushCap * 128];
+    const uint32_t cnt = a.overflow_count[0];
+    for (uint32_t i0 = blockIdx.x * 128u; i0 < cnt; i0 += gridDim.x * 128u) {  // uniform per block
+        const uint32_t i = i0 + threadIdx.x;
+        const unsigned wmask = __ballot_sync(0xFFFFFFFFu, i < cnt);  // lanes with a particle
+        if (i < cnt)
+            fluid_particle<DIM, 128, kFlushCap, kFlush>(a.overflow[i], a, T, c, b, lst + threadIdx.x, nullptr,
+                                                         nullptr, kInvalid, wmask);
+    }
+}
+
+// Second overflow queue: particles with more than kFlushCap hits in one row,
+// one thread each, evaluating their pairs during the scan.
 template <int DIM>
 __global__ void __launch_bounds__(128) k_fluid_overflow(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i < *a.overflow_count)
-        fluid_particle<DIM, 128, 1, true>(a.overflow[i], a, T, c, b, nullptr, nullptr, nullptr, kInvalid);
+    const uint32_t cnt = a.overflow_count[1];
+    for (uint32_t i = blockIdx.x * 128u + threadIdx.x; i < cnt; i += gridDim.x * 128u)
+        fluid_particle<DIM, 128, 1, kDirect>(a.overflow[a.n + i], a, T, c, b, nullptr, nullptr, nullptr, kInvalid,
+                                             0u);
 }
 
 template <int DIM, int BLOCK, int CAP>
@@ -416,7 +489,7 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
                              (int)smem);
     }
     const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
-    cudaMemsetAsync(a.overflow_count, 0, sizeof(uint32_t), st);
+    cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
     if (!persistent) {
         k_fluid<DIM, BLOCK, CAP><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
     } else {
@@ -430,8 +503,11 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
         cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
         k_fluid_persistent<DIM, BLOCK, CAP><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
     }
-    // one thread per possible overflowed particle; threads past the count exit
-    k_fluid_overflow<DIM><<<(a.n + 127) / 128, 128, 0, st>>>(a, T, c, b);
+    // the overflow queues: grids of at most 1184 blocks striding over the
+    // queue, which usually is empty
+    const uint32_t oblocks = std::min<uint32_t>(ntiles * BLOCK / 128u + 1u, 1184u);
+    k_fluid_overflow_flush<DIM><<<oblocks, 128, 0, st>>>(a, T, c, b);
+    k_fluid_overflow<DIM><<<oblocks, 128, 0, st>>>(a, T, c, b);
 }
 
 }  // namespace
@@ -449,7 +525,7 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
 #define ARP_FLUID(D, B, C)                                                  \
     if (kdim == D && v.block == B && v.cap == C) {                          \
         launch_variant<D, B, C>(a, T, c, b, pers, tile_counter, st);        \
-        return 2; /* the tile kernel and the overflow kernel */             \
+        return 3; /* the tile kernel and the two overflow kernels */       \
     }
     ARP_FLUID(3, 128, 48) ARP_FLUID(3, 256, 48) ARP_FLUID(3, 128, 96) ARP_FLUID(3, 256, 96)
     ARP_FLUID(2, 128, 48) ARP_FLUID(2, 256, 48) ARP_FLUID(2, 128, 96) ARP_FLUID(2, 256, 96)

@@ -253,7 +253,7 @@ struct arp_sim {
     DevBuf<uint2> g_coord, coord_s;  // grid coordinates per slot; storage-order copy for stage 0
     DevBuf<uint32_t> contact_bound;
     DevBuf<uint32_t> tile_counter;  // work queue of the persistent fluid kernel
-    DevBuf<uint32_t> overflow, overflow_count;  // particles with more hits than the fluid list holds
+    DevBuf<uint32_t> overflow, overflow_count;  // the fluid kernel's two overflow queues (2n entries, 2 counts)
     int fluid_variant = 0;
     uint32_t grid_cap = 0;
     // solids
@@ -1000,8 +1000,8 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->coord_s.alloc(S->solid_branch() ? n : 1));
     CUDA_TRY(S->contact_bound.alloc(2));
     CUDA_TRY(S->tile_counter.alloc(1));
-    CUDA_TRY(S->overflow.alloc(n));
-    CUDA_TRY(S->overflow_count.alloc(1));
+    CUDA_TRY(S->overflow.alloc(2 * n));  // two queues of n entries
+    CUDA_TRY(S->overflow_count.alloc(2));
     CUDA_TRY(S->ep.alloc(4 * ns));
     CUDA_TRY(S->ep_t.alloc(4 * ns));
     CUDA_TRY(S->sx.alloc(ns));

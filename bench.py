@@ -213,6 +213,15 @@ def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
     torch.cuda.synchronize()
     t_batch = e0.elapsed_time(e1) / 1000.0
     variant = batch.fluid_variant()
+    # where a batch step goes: a few more steps, untimed, with the library's
+    # per-segment events (graph replay off: the events sit between launches)
+    batch.set_graph(False)
+    batch.profile_enable(True)
+    batch.step(4)
+    torch.cuda.synchronize()
+    prof = batch.profile_read()
+    batch.profile_enable(False)
+    segments = {k: prof[k] / max(prof["steps"], 1) for k in ("neighbor_ms", "solid_ms", "fluid_ms")}
     batch.close()
     sims = []
     for sc in scs:
@@ -238,7 +247,8 @@ def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
             "scene_steps_per_s": batched, "particle_steps_per_s": parts * steps_batch / t_batch,
             "ms_per_step": t_batch * 1000.0 / steps_batch,
             "per_scene_loop_scene_steps_per_s": loop, "speedup_vs_per_scene_loop": batched / loop,
-            "fluid_launch_shape": variant,
+            "fluid_launch_shape": variant, "segments_ms_per_step": segments,
+            "solids": int(sum(sc.n_solids() for sc in scs)),
             "note": "working set > L2 (no flush); batch replayed from a CUDA graph; loop = one simulation per scene"}
 
 
@@ -509,7 +519,14 @@ def main():
     ap.add_argument("--no-adjoint", action="store_true")
     ap.add_argument("--no-render", action="store_true")
     ap.add_argument("--fluid-variant", type=int, default=None, help="pin the fluid launch shape (profiling)")
+    ap.add_argument("--batched-only", action="store_true",
+                    help="run only the batched-scenes measurement and print its object (profiling)")
     args = ap.parse_args()
+    if args.batched_only:
+        import torch
+        stream = torch.cuda.Stream()
+        print(json.dumps(run_batched(torch, stream, steps_batch=args.steps)), flush=True)
+        return
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
     local_rank = int(os.environ.get("LOCAL_RANK", "0"))

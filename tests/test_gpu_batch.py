@@ -122,3 +122,56 @@ def test_batched_workload_sample_matches_the_oracle():
         for key in ("den", "pos", "vel"):
             e = rel_err(pb[key][first:first + n], r[key])
             assert e < 1e-5, (k, key, e)
+
+
+def dense_block(h_over_s=4.5, n=10, spacing=0.01):
+    """A Tait fluid block whose kernel radius spans 4.5 particle spacings:
+    ~380 neighbors per particle, more than any hit list holds, and more than
+    64 of them inside one search row for the central particles."""
+    s = spacing
+    h = h_over_s * s
+    pos = scenes.lattice((0.1 + 0.5 * s,) * 3, (n, n, n), s)
+    rng = np.random.default_rng(41)
+    pos = pos + rng.uniform(-0.1 * s, 0.1 * s, size=pos.shape).astype(np.float32)
+    mats = np.array([scenes.liquid(1000.0, 20.0, h, 0.1, mass=1000.0 * s ** 3)])
+    p = scenes.particles(pos, 0, 1000.0)
+    p["vel"][:, :3] = rng.normal(0.0, 0.05, size=(len(p), 3)).astype(np.float32)
+    from arphys.abi import PARTICLE_DTYPE
+    return scenes.Scene(particles=p, boundary=np.zeros(0, PARTICLE_DTYPE), materials=mats,
+                        bounds_min=(0.0, 0.0, 0.0, 0.0), bounds_dim=(0.3, 0.3, 0.3, 0.0), h=h,
+                        integrator="midpoint", dt=2e-5, gravity=9.81, name="dense_block")
+
+
+def test_dense_scene_through_both_overflow_queues():
+    """Most hit lists overflow (first queue, evaluated with list flushes)
+    and some particles have more than 64 hits in one search row (second
+    queue, evaluated during the scan); all 8 launch shapes give the same
+    bits and the oracle's result."""
+    sc = dense_block()
+    pos = sc.particles["pos"][:, :3].astype(np.float64)
+    d2 = ((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1)
+    within = (d2 < np.float32(sc.h) ** 2) & ~np.eye(sc.n, dtype=bool)
+    assert np.median(within.sum(1)) > 96  # most lists of 48 or 96 entries overflow
+    sub = int(np.float32(0.3) / np.float32(sc.h))
+    cell = np.floor(pos / 0.3 * sub).astype(int)  # reference cells; the search rows are (y, z) pairs of them
+    i = int(np.argmin(((pos - pos.mean(0)) ** 2).sum(1)))
+    same_row = (cell[:, 1] == cell[i, 1]) & (cell[:, 2] == cell[i, 2])
+    assert (within[i] & same_row).sum() > 64  # the central particle's own row alone overfills the flush list
+    ref = None
+    for v in range(8):
+        sim = FluidSim(sc)
+        sim.init()
+        sim.set_fluid_variant(v)
+        sim.step(4)
+        p = sim.particles().tobytes()
+        if ref is None:
+            ref = p
+            g = sim.particles()
+        assert p == ref, f"variant {v}"
+    o = Oracle(sc)
+    o.step(4)
+    r = o.state()
+    for key in ("den", "pos", "vel"):
+        e = rel_err(g[key], r[key])
+        print(f"dense {key}: rel err {e:.2e}")
+        assert e < 1e-5, (key, e)

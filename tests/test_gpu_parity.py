@@ -145,7 +145,7 @@ def test_profile_and_launch_counters():
     prof = sim.profile_read()
     assert prof["steps"] == 3
     assert prof["stages"] == 12  # RK4
-    assert prof["fluid_launches"] == 24  # per stage: the fused fluid kernel and its overflow kernel
+    assert prof["fluid_launches"] == 36  # per stage: the fused fluid kernel and its two overflow kernels
     assert prof["fluid_ms"] > 0 and prof["neighbor_ms"] > 0
     assert sim.launch_count() - before == prof["launches"]
     st = sim.stats()
