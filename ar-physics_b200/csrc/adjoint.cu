@@ -38,6 +38,16 @@ __device__ __forceinline__ float3 mul(float s, float3 a) { return make_float3(s 
 __device__ __forceinline__ float dot(float3 a, float3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
 __device__ __forceinline__ float3 neg(float3 a) { return make_float3(-a.x, -a.y, -a.z); }
 
+// gradW(X_j - X_i) of a reference pair, as the reference-list build computes
+// it: recomputed from the reference positions (shared by neighboring solids
+// in L1/L2) rather than streamed per list entry.
+__device__ __forceinline__ float3 ref_grad(const float4* __restrict__ ref, uint32_t j, float3 Xi, const SceneP& P) {
+    const float3 dX = sub(f3(ref[j]), Xi);
+    const float diff = P.h2 - ((dX.x * dX.x + dX.y * dX.y) + dX.z * dX.z);
+    const float s = -6.0f * P.kconst * diff * diff;
+    return make_float3(s * dX.x, s * dX.y, s * dX.z);
+}
+
 // 3x3 matrices, row-major: m[r][c]
 struct M3 {
     float m[3][3];
@@ -470,7 +480,7 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMatBit)) continue;
         const uint32_t j = e & ~kSameMatBit;
-        const float3 g = f3(a.rl.gw[k]);
+        const float3 g = ref_grad(a.ref, j, Xi, P);
         const float4 xj = a.st.sx[j];
         const float d2 = xj.w;
         const float c = -V1 * (m1 / d2);
@@ -535,10 +545,10 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
     M3 Fd = m3_zero();
     for (uint32_t k = k0; k < k1; ++k) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMatBit;
-        const float4 g4 = a.rl.gw[k];
-        const float3 G = m3_vec(L, f3(g4));
-        const float3 dv = sub(f3(a.st.sv[j]), f3(vi));
-        m3_add_outer(Fd, g4.w, dv, G);
+        const float4 vj = a.st.sv[j];
+        const float3 G = m3_vec(L, ref_grad(a.ref, j, Xi, P));
+        const float3 dv = sub(f3(vj), f3(vi));
+        m3_add_outer(Fd, a.ref[j].w, dv, G);  // ref.w = V_j
     }
     const uint32_t dim = P.dim;
     M3 E = m3_mul(m3_t(Fi), Fi);
@@ -615,11 +625,12 @@ __global__ void __launch_bounds__(kT) k_adj_strain(AdjArgs a, Tables T) {
     const M3 Li = m3_cols(a.L + 3 * i);
     const M3 lFi = m3_cols(a.lamF + 3 * i), lFdi = m3_cols(a.lamFd + 3 * i);
     const float Vri = mm.vol0;
+    const float3 Xi = f3(a.ref[i]);
     float3 lx = make_float3(0.f, 0.f, 0.f), lv = lx;
     for (uint32_t k = a.rl.off[i]; k < a.rl.off[i + 1]; ++k) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMatBit;
-        const float4 g4 = a.rl.gw[k];
-        const float3 g = f3(g4);
+        const float3 g = ref_grad(a.ref, j, Xi, P);
+        const float4 g4 = make_float4(g.x, g.y, g.z, a.ref[j].w);  // ref.w = V_j
         const float3 G = m3_vec(Li, g);
         lx = sub(lx, mul(g4.w, m3_vec(lFi, G)));
         lv = sub(lv, mul(g4.w, m3_vec(lFdi, G)));

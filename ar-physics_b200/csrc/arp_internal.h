@@ -255,7 +255,6 @@ struct SolidRefList {
     uint32_t* nbr;   // [nnz] solid id | 0x80000000 when same material
     float4* gw;      // [nnz] grad_w(X_j - X_i).xyz, w = vol0 of j
     uint32_t nnz;
-    float4* dk;      // [nnz] X_j - X_i and the kernel W(X_j - X_i) (hourglass term)
 };
 // Reference-neighbor lists: counts per solid (pass 1), then after an
 // exclusive scan of the counts into rl.off, the entries and L (pass 2).
@@ -269,7 +268,7 @@ struct SolidArgs {
     const float4* pd;         // stage state, storage order
     const float4* vm;
     const uint32_t* slot_of;  // solid id -> storage slot
-    const float4* ref;
+    const float4* ref;        // reference positions, w = rest volume m / rho0
     const float4* L;
     SolidRefList rl;
     const float4* ep;         // stage plastic strain (4 per solid)
@@ -356,7 +355,7 @@ struct AdjArgs {
     const float4* bvs;
     const uint32_t* bstart;
     const float* bps;
-    const float4* ref;
+    const float4* ref;         // reference positions, w = rest volume m / rho0
     const float4* L;
     SolidRefList rl;
     const float2* stiff;       // per-solid stiffness override or null

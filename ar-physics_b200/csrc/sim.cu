@@ -276,7 +276,7 @@ struct arp_sim {
     StepRecord* rec = nullptr;  // set while a recording step runs
     bool replaying = false;     // steps re-run by the backward pass take no checkpoints
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
-    DevBuf<float4> rl_gw, rl_dk;
+    DevBuf<float4> rl_gw;
     uint32_t rl_nnz = 0;
     DevBuf<DevStats> d_stats;
 
@@ -522,7 +522,11 @@ arp_status do_init(arp_sim* S) {
             if (s >= kept) S->host_ref[s] = make_float4(p.pos[0], p.pos[1], p.pos[2], 0.0f);
             mos[s] = p.mat;
         }
-        CUDA_TRY(cudaMemcpyAsync(S->ref.p, S->host_ref.data(), ns * sizeof(float4), cudaMemcpyHostToDevice, st));
+        // the device copy carries each solid's rest volume m / rho0 in w, so
+        // one gather of a reference neighbor gives dX and V_j
+        std::vector<float4> ref_dev(S->host_ref);
+        for (uint32_t s = 0; s < ns; ++s) ref_dev[s].w = S->mats[mos[s]].mass / S->mats[mos[s]].start_den;
+        CUDA_TRY(cudaMemcpyAsync(S->ref.p, ref_dev.data(), ns * sizeof(float4), cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemcpyAsync(S->mat_of_solid.p, mos.data(), ns * sizeof(uint32_t), cudaMemcpyHostToDevice, st));
         CUDA_TRY(cudaMemsetAsync(S->ep.p, 0, size_t(ns) * 4 * sizeof(float4), st));
         if (!S->host_ep.empty()) {
@@ -544,9 +548,8 @@ arp_status do_init(arp_sim* S) {
         CUDA_TRY(cudaStreamSynchronize(st));
         CUDA_TRY(S->rl_nbr.alloc(std::max(nnz, 1u)));
         CUDA_TRY(S->rl_gw.alloc(std::max(nnz, 1u)));
-        CUDA_TRY(S->rl_dk.alloc(std::max(nnz, 1u)));
         S->rl_nnz = nnz;
-        SolidRefList rl{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, nnz, S->rl_dk.p};
+        SolidRefList rl{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, nnz};
         S->launches += ref_lists_fill(S->ref.p, S->mat_of_solid.p, ns, S->gb, S->tables, rl, S->L.p, st);
         CUDA_TRY(cudaStreamSynchronize(st));
         ARP_TRY(check_launch("reference neighbor lists"));
@@ -703,7 +706,7 @@ arp_status do_step(arp_sim* S) {
             a.slot_of = S->slot_of.p;
             a.ref = S->ref.p;
             a.L = S->L.p;
-            a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz, S->rl_dk.p};
+            a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz};
             a.ep = cur_ep;
             a.ep0 = S->ep.p;
             a.ep_next = last ? S->ep_t.p : S->ep_s[s % 2].p;
@@ -2079,7 +2082,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.bps = sim->bps.p;
                 a.ref = sim->ref.p;
                 a.L = sim->L.p;
-                a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz, sim->rl_dk.p};
+                a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz};
                 a.stiff = sim->have_stiff ? sim->stiff.p : nullptr;
                 a.lamF = lamF.p;
                 a.lamFd = lamFd.p;

@@ -31,6 +31,11 @@ constexpr int kThreads = 128;
 #endif
 constexpr int kSolidLanes = ARP_SOLID_LANES;  // threads per solid in the stress and force kernels
 constexpr uint32_t kSameMat = 0x80000000u;
+// The stage kernels recompute gradW(dX) and W(dX) of each reference pair from
+// the reference positions (a gather that neighboring solids share in L1/L2)
+// instead of streaming per-entry values from HBM: a list entry costs its
+// 4-byte index.  The stored gradW and volume (rl.gw) serve L and the reverse
+// pass.
 
 inline uint32_t blocks_for(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / (uint32_t)t; }
 
@@ -77,8 +82,7 @@ __global__ void k_ref_count(const float4* __restrict__ ref, const uint32_t* __re
 
 __global__ void k_ref_fill(const float4* __restrict__ ref, const uint32_t* __restrict__ mat_of, uint32_t ns,
                            const uint32_t* __restrict__ start, const uint32_t* __restrict__ perm, Tables T,
-                           const uint32_t* __restrict__ off, uint32_t* __restrict__ nbr, float4* __restrict__ gw,
-                           float4* __restrict__ dk) {
+                           const uint32_t* __restrict__ off, uint32_t* __restrict__ nbr, float4* __restrict__ gw) {
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= ns) return;
     uint32_t w = off[i];
@@ -90,7 +94,6 @@ __global__ void k_ref_fill(const float4* __restrict__ ref, const uint32_t* __res
         const uint32_t mj = mat_of[j];
         nbr[w] = j | (mj == mi ? kSameMat : 0u);
         gw[w] = make_float4(s * dX.x, s * dX.y, s * dX.z, mats[mj].vol0);
-        dk[w] = make_float4(dX.x, dX.y, dX.z, P.kconst * diff * diff * diff);
         ++w;
     });
 }
@@ -242,14 +245,21 @@ __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T
     const SceneP& P = T.scenes[mm.scene];
     if (!P.solid_branch) return;  // a scene with a single solid skips the solid term
     const float4 L0 = a.L[3 * i], L1 = a.L[3 * i + 1], L2 = a.L[3 * i + 2];
+    const float4 Xs = a.ref[i];
     // strain.rs:139-160: F = sum V dx (x) (L gradW), Fdot likewise with dv
     float F[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     float Fd[3][3] = {{0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}, {0.f, 0.f, 0.f}};
     for (uint32_t k = a.rl.off[i] + lane; k < a.rl.off[i + 1]; k += LANES) {
         const uint32_t j = a.rl.nbr[k] & ~kSameMat;
-        const float4 g = a.rl.gw[k];
+        const float4 vj = a.sv[j];
+        // gradW(X_j - X_i) as k_ref_fill computes it; V_j rides in ref.w
+        const float4 Xj = a.ref[j];
+        const float3 dX = sub3(Xj, Xs);
+        const float diff = P.h2 - dot3(dX, dX);
+        const float sg = -6.0f * P.kconst * diff * diff;
+        const float4 g = make_float4(sg * dX.x, sg * dX.y, sg * dX.z, Xj.w);
         const float3 dx = sub3(a.sx[j], xi);
-        const float3 dv = sub3(a.sv[j], vi);
+        const float3 dv = sub3(vj, vi);
         const float gr[3] = {(L0.x * g.x + L1.x * g.y) + L2.x * g.z, (L0.y * g.x + L1.y * g.y) + L2.y * g.z,
                              (L0.z * g.x + L1.z * g.y) + L2.z * g.z};
         const float x[3] = {dx.x, dx.y, dx.z}, v[3] = {dv.x, dv.y, dv.z};
@@ -419,7 +429,11 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMat)) continue;
         const uint32_t j = e & ~kSameMat;
-        const float4 g = a.rl.gw[k];
+        // dX = X_j - X_i, gradW(dX) as k_ref_fill computes it
+        const float3 dX = sub3(a.ref[j], Xi);
+        const float diff = P.h2 - dot3(dX, dX);
+        const float sg = -6.0f * P.kconst * diff * diff;
+        const float3 g = make_float3(sg * dX.x, sg * dX.y, sg * dX.z);
         const float4 xj = a.sx[j];
         const float d2 = xj.w;
         const float V2 = __fdividef(m1, d2);  // GLSL division carries 2.5 ulp; the 2-ulp hardware quotient is used
@@ -434,8 +448,6 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
         if (P.dim >= 3) fz += (c0.z * g.x + c1.z * g.y) + c2.z * g.z;
         if (in_stencil(a.sc[j], ci)) {
             const float3 dx = sub3(xj, xi);
-            const float4 dk = a.rl.dk[k];  // X_j - X_i and W(X_j - X_i), fixed with the reference list
-            const float3 dX = make_float3(dk.x, dk.y, dk.z);
             const float l = sqrtf(dot3(dx, dx));
             const float4 Fj0 = a.F[3 * j], Fj1 = a.F[3 * j + 1], Fj2 = a.F[3 * j + 2];
             const float ex = ((0.5f * (Fi0.x + Fj0.x)) * dX.x + (0.5f * (Fi1.x + Fj1.x)) * dX.y) +
@@ -444,7 +456,7 @@ __global__ void __launch_bounds__(kThreads) k_solid_forces(SolidArgs a, Tables T
                              (0.5f * (Fi2.y + Fj2.y)) * dX.z - dx.y;
             const float ez = ((0.5f * (Fi0.z + Fj0.z)) * dX.x + (0.5f * (Fi1.z + Fj1.z)) * dX.y) +
                              (0.5f * (Fi2.z + Fj2.z)) * dX.z - dx.z;
-            const float kern = dk.w;
+            const float kern = P.kconst * diff * diff * diff;  // W(dX)
             const float sh = ((__fdividef(100000000.0f * m1 * m1, d1 * d2) *
                                __fdividef(0.5f * ((ex * dx.x + ey * dx.y) + ez * dx.z), l + P.hg_h)) *
                               __fdividef(1.0f, l * l + P.eps_hh)) *
@@ -502,7 +514,7 @@ int ref_lists_count(const float4* ref, const uint32_t* mat_of, uint32_t ns, cons
 int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const GridBuffers& gb, const Tables& T,
                    SolidRefList& rl, float4* L, cudaStream_t st) {
     k_ref_fill<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, gb.start, gb.perm, T, rl.off, rl.nbr,
-                                                              rl.gw, rl.dk);
+                                                              rl.gw);
     k_ref_L<<<blocks_for(ns, kThreads), kThreads, 0, st>>>(ref, mat_of, ns, rl.off, rl.nbr, rl.gw, T, L);
     return 2;
 }
