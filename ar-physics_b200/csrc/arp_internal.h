@@ -233,17 +233,19 @@ struct FluidArgs {
     int any_stiff_immobile;
 };
 // Launch shapes of the fluid kernel the autotuner chooses between: threads
-// per block, hit-list capacity, and one tile per block or persistent blocks
-// taking tiles from an atomic work counter.  Every shape evaluates the same
-// pairs in the same order (a particle whose list fills up is finished by the
-// overflow kernel in candidate order), so results do not depend on the
-// choice.
+// per block, hit-list capacity, one tile per block or persistent blocks
+// taking tiles from an atomic work counter, and whether a warp empties its
+// lists by a vote before each search row (suited to dense scenes, where
+// lists overflow).  Every shape evaluates the same pairs in the same order
+// (a particle whose list fills up is finished by an overflow kernel in
+// candidate order), so results do not depend on the choice.
 struct FluidVariant {
     int block;       // threads per block
     int cap;         // hit-list entries per thread
     int persistent;  // tile-queue form
+    int flush;       // warp-voted list flushes (kFlush) instead of pass 1 then pass 2
 };
-constexpr int kNumFluidVariants = 8;
+constexpr int kNumFluidVariants = 10;
 extern const FluidVariant kFluidVariants[kNumFluidVariants];
 // `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,

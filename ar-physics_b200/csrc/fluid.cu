@@ -405,8 +405,8 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     }
 }
 
-// One tile of BLOCK sorted particles per block.
-template <int DIM, int BLOCK, int CAP>
+// One tile of BLOCK sorted particles per block; MODE kTwoPass or kFlush.
+template <int DIM, int BLOCK, int CAP, int MODE>
 __global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
@@ -417,14 +417,15 @@ __global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoe
     load_scene_tables(T, scene0, sm, si);
     __syncthreads();
     const uint32_t k = k0 + threadIdx.x;
-    if (k < a.n) fluid_particle<DIM, BLOCK, CAP, kTwoPass>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, 0u);
+    const unsigned wmask = MODE == kFlush ? __ballot_sync(0xFFFFFFFFu, k < a.n) : 0u;  // lanes with a particle
+    if (k < a.n) fluid_particle<DIM, BLOCK, CAP, MODE>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, wmask);
 }
 
 // Persistent form: each block keeps taking the next tile of the cell-sorted,
 // scene-concatenated order from an atomic work counter, so scenes of very
 // different sizes share the SMs without a tail of idle blocks.  Blocks never
 // wait on each other.
-template <int DIM, int BLOCK, int CAP>
+template <int DIM, int BLOCK, int CAP, int MODE>
 __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
                                                             uint32_t* tile_counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
@@ -447,7 +448,8 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables 
         }
         __syncthreads();
         const uint32_t k = k0 + threadIdx.x;
-        if (k < a.n) fluid_particle<DIM, BLOCK, CAP, kTwoPass>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, 0u);
+        const unsigned wmask = MODE == kFlush ? __ballot_sync(0xFFFFFFFFu, k < a.n) : 0u;  // lanes with a particle
+        if (k < a.n) fluid_particle<DIM, BLOCK, CAP, MODE>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, wmask);
         __syncthreads();
     }
 }
@@ -478,30 +480,31 @@ __global__ void __launch_bounds__(128) k_fluid_overflow(FluidArgs a, Tables T, S
                                              0u);
 }
 
-template <int DIM, int BLOCK, int CAP>
+template <int DIM, int BLOCK, int CAP, int MODE>
 void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, bool persistent,
                     uint32_t* tile_counter, cudaStream_t st) {
     const size_t smem = sizeof(uint32_t) * CAP * BLOCK + sizeof(FluidMat) * T.max_nmat +
                         sizeof(DevInter) * T.max_nmat * T.max_nmat;
     if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_fluid<DIM, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_fluid_persistent<DIM, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(k_fluid<DIM, BLOCK, CAP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_fluid_persistent<DIM, BLOCK, CAP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
     }
     const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
     cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
     if (!persistent) {
-        k_fluid<DIM, BLOCK, CAP><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
+        k_fluid<DIM, BLOCK, CAP, MODE><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
     } else {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, BLOCK, CAP>, BLOCK, smem);
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, BLOCK, CAP, MODE>, BLOCK,
+                                                      smem);
         per_sm = per_sm > 0 ? per_sm : 1;
         int sms = 148;
         int dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
         cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
-        k_fluid_persistent<DIM, BLOCK, CAP><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
+        k_fluid_persistent<DIM, BLOCK, CAP, MODE><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
     }
     // the overflow queues: grids of at most 1184 blocks striding over the
     // queue, which usually is empty
@@ -513,8 +516,9 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
 }  // namespace
 
 const FluidVariant kFluidVariants[kNumFluidVariants] = {
-    {128, 48, 0}, {256, 48, 0}, {128, 48, 1}, {256, 48, 1},
-    {128, 96, 0}, {256, 96, 0}, {128, 96, 1}, {256, 96, 1},
+    {128, 48, 0, 0}, {256, 48, 0, 0}, {128, 48, 1, 0}, {256, 48, 1, 0},
+    {128, 96, 0, 0}, {256, 96, 0, 0}, {128, 96, 1, 0}, {256, 96, 1, 0},
+    {128, 48, 0, 1}, {128, 48, 1, 1},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -522,13 +526,14 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
     if (a.n == 0) return 0;
     const FluidVariant v = kFluidVariants[variant < 0 || variant >= kNumFluidVariants ? 0 : variant];
     const bool pers = v.persistent != 0;
-#define ARP_FLUID(D, B, C)                                                  \
-    if (kdim == D && v.block == B && v.cap == C) {                          \
-        launch_variant<D, B, C>(a, T, c, b, pers, tile_counter, st);        \
+#define ARP_FLUID(D, B, C, M)                                               \
+    if (kdim == D && v.block == B && v.cap == C && v.flush == M) {          \
+        launch_variant<D, B, C, M>(a, T, c, b, pers, tile_counter, st);     \
         return 3; /* the tile kernel and the two overflow kernels */       \
     }
-    ARP_FLUID(3, 128, 48) ARP_FLUID(3, 256, 48) ARP_FLUID(3, 128, 96) ARP_FLUID(3, 256, 96)
-    ARP_FLUID(2, 128, 48) ARP_FLUID(2, 256, 48) ARP_FLUID(2, 128, 96) ARP_FLUID(2, 256, 96)
+    ARP_FLUID(3, 128, 48, 0) ARP_FLUID(3, 256, 48, 0) ARP_FLUID(3, 128, 96, 0) ARP_FLUID(3, 256, 96, 0)
+    ARP_FLUID(2, 128, 48, 0) ARP_FLUID(2, 256, 48, 0) ARP_FLUID(2, 128, 96, 0) ARP_FLUID(2, 256, 96, 0)
+    ARP_FLUID(3, 128, 48, 1) ARP_FLUID(2, 128, 48, 1)
 #undef ARP_FLUID
     return 0;
 }

@@ -257,13 +257,14 @@ arp_status arp_sim_update(arp_sim* sim);
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps);
 /* Time every launch shape of the fluid kernel (128 or 256 threads per block,
  * 48 or 96 listed neighbors per thread, one tile per block or persistent
- * blocks on a tile queue) on the current
+ * blocks on a tile queue, lists evaluated after the scan or emptied whenever
+ * a warp's next row could overfill one) on the current
  * state and keep the fastest; arp_sim_init does this once per (dimension,
  * particle count, h/spacing) bucket and reuses the choice afterwards.  The
  * shapes evaluate identical arithmetic, so results do not depend on it. */
 arp_status arp_sim_autotune(arp_sim* sim, int* variant);
 arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent);
-/* Pin the fluid kernel's launch shape (0 .. 7). */
+/* Pin the fluid kernel's launch shape (0 .. 9). */
 arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant);
 /* Replay pairs of steps from a CUDA graph captured on the handle's stream
  * (captured on first use and again after the stream changes; profiling

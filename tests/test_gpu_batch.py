@@ -89,7 +89,7 @@ def test_graph_replay_matches_plain_steps():
 def test_fluid_launch_shapes_give_identical_results():
     sc = scenes.small_fluid_bar_3d(seed=21)
     ref = None
-    for v in range(8):
+    for v in range(10):
         sim = FluidSim(sc)
         sim.init()
         sim.set_fluid_variant(v)
@@ -145,7 +145,7 @@ def dense_block(h_over_s=4.5, n=10, spacing=0.01):
 def test_dense_scene_through_both_overflow_queues():
     """Most hit lists overflow (first queue, evaluated with list flushes)
     and some particles have more than 64 hits in one search row (second
-    queue, evaluated during the scan); all 8 launch shapes give the same
+    queue, evaluated during the scan); all 10 launch shapes give the same
     bits and the oracle's result."""
     sc = dense_block()
     pos = sc.particles["pos"][:, :3].astype(np.float64)
@@ -158,7 +158,7 @@ def test_dense_scene_through_both_overflow_queues():
     same_row = (cell[:, 1] == cell[i, 1]) & (cell[:, 2] == cell[i, 2])
     assert (within[i] & same_row).sum() > 64  # the central particle's own row alone overfills the flush list
     ref = None
-    for v in range(8):
+    for v in range(10):
         sim = FluidSim(sc)
         sim.init()
         sim.set_fluid_variant(v)
