@@ -201,8 +201,9 @@ class FluidSim:
     def synchronize(self):
         check(self._L.arp_sim_synchronize(self._h))
 
-    def profile_enable(self, on=True):
-        check(self._L.arp_sim_profile_enable(self._h, int(bool(on))))
+    def profile_enable(self, on=True, every=1):
+        """Per-segment CUDA-event timing on one step in every `every`."""
+        check(self._L.arp_sim_profile_enable(self._h, int(every) if on else 0))
 
     def profile_read(self):
         p = ArpProfile()

@@ -295,8 +295,10 @@ struct arp_sim {
         graph_stream = nullptr;
     }
 
-    // profiling
-    bool profiling = false;
+    // profiling: events around the segments of one step in every prof_every
+    bool prof_on = false;
+    uint32_t prof_every = 1, prof_phase = 0;
+    bool profiling = false;  // the current step records events
     std::vector<cudaEvent_t> ev_free;
     struct Mark {
         cudaEvent_t e[4];
@@ -618,6 +620,7 @@ arp_status do_step(arp_sim* S) {
     S->time += S->dt_sub;
     const uint32_t* bstart = S->b_start.p;
     uint64_t l0 = S->launches;
+    S->profiling = S->prof_on && S->prof_phase++ % S->prof_every == 0;
 
     // 1. sort y0 into cell order
     arp_sim::Mark mk{};
@@ -1360,14 +1363,14 @@ arp_status capture_graph(arp_sim* S) {
     S->drop_graph();
     const float t0 = S->time;
     const uint64_t l0 = S->launches;
-    const bool prof = S->profiling;
-    S->profiling = false;
+    const bool prof = S->prof_on;
+    S->prof_on = false;
     CUDA_TRY(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
     arp_status st = do_step(S);
     if (st == ARP_OK) st = do_step(S);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(S->stream, &g);
-    S->profiling = prof;
+    S->prof_on = prof;
     S->time = t0;
     S->graph_launches = S->launches - l0;
     S->launches = l0;
@@ -1389,7 +1392,7 @@ arp_status capture_graph(arp_sim* S) {
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
     ARP_TRY(need_init(sim));
     uint32_t i = 0;
-    if (sim->use_graph && !sim->profiling && !sim->tape && nsteps >= 2) {
+    if (sim->use_graph && !sim->prof_on && !sim->tape && nsteps >= 2) {
         if (!sim->graph_exec || sim->graph_stream != sim->stream) ARP_TRY(capture_graph(sim));
         for (; i + 2 <= nsteps; i += 2) {
             CUDA_TRY(cudaGraphLaunch(sim->graph_exec, sim->stream));
@@ -1776,8 +1779,12 @@ arp_status arp_sim_synchronize(arp_sim* sim) {
 
 arp_status arp_sim_profile_enable(arp_sim* sim, int enable) {
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (enable < 0) return fail(ARP_ERR_INVALID_ARG, "enable must be 0 or a sampling period >= 1");
     if (!enable) harvest_marks(sim);
-    sim->profiling = enable != 0;
+    sim->prof_on = enable != 0;
+    sim->prof_every = enable > 0 ? (uint32_t)enable : 1u;
+    sim->prof_phase = 0;
+    sim->profiling = false;
     return ARP_OK;
 }
 

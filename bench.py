@@ -34,6 +34,7 @@ sys.path.insert(0, ROOT)
 METRIC = "particle-steps/s at 1M (vs HBM roofline); batched scenes/s; adjoint/fwd ratio"
 UNIT = "particle-steps/s"
 L2_FLUSH_BYTES = 256 << 20
+PROFILE_EVERY = 10  # timed steps per step carrying the segment events
 
 
 def load_peaks():
@@ -424,7 +425,10 @@ def run_ours(args, rank, world, local_rank):
     if dist:
         torch.distributed.barrier()
     torch.cuda.synchronize()
-    sim.profile_enable(True)
+    # the fluid kernel's launch times for the roofline: the library's CUDA
+    # events around its segments on every PROFILE_EVERY-th timed step (an
+    # event between two launches costs the step a few microseconds)
+    sim.profile_enable(True, every=PROFILE_EVERY)
     sim.profile_read()
     l0 = sim.launch_count()
     clk = ClockSampler(local_rank)

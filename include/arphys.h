@@ -364,6 +364,11 @@ arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, const arp_aab
  * to the handle's own stream. */
 arp_status arp_sim_set_stream(arp_sim* sim, void* stream);
 arp_status arp_sim_synchronize(arp_sim* sim);
+/* Per-segment timing (grid build, solid, fluid) with CUDA events between the
+ * launches of a step.  enable = 0 stops it; enable = N >= 1 records the events
+ * on one step in every N (1: every step; each event costs the step a few
+ * microseconds, so a long timed run samples); arp_sim_profile_read reports
+ * the sampled steps only. */
 arp_status arp_sim_profile_enable(arp_sim* sim, int enable);
 arp_status arp_sim_profile_read(arp_sim* sim, arp_profile* out);
 arp_status arp_sim_stats(arp_sim* sim, arp_stats* out);

@@ -150,6 +150,13 @@ def test_profile_and_launch_counters():
     assert sim.launch_count() - before == prof["launches"]
     st = sim.stats()
     assert st["nonfinite_positions"] == 0 and st["max_cell_occupancy"] > 0
+    # sampled: events on one step in every 3
+    sim.profile_enable(True, every=3)
+    sim.step(7)
+    prof = sim.profile_read()
+    assert prof["steps"] == 3 and prof["stages"] == 12  # steps 1, 4 and 7 of the 7
+    assert prof["fluid_ms"] > 0
+    sim.profile_enable(False)
 
 
 def test_state_round_trip_and_validation():
