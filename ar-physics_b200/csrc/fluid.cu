@@ -405,9 +405,18 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
     }
 }
 
-// One tile of BLOCK sorted particles per block; MODE kTwoPass or kFlush.
+// The flush form keeps the row loop's state live around the pair math; left
+// alone the compiler gives it 92 registers (5 blocks of 128 per SM), and
+// holding it to 7 blocks (72 registers, a few spilled) ran the batched
+// workload's fluid kernel 7 % faster.  The two-pass form keeps the
+// compiler's own choice (72 registers at 128 threads; an explicit minimum of
+// one block raises it to 80).
+constexpr int kFlushMinBlocks = 7;
+
+// One tile of BLOCK sorted particles per block.
 template <int DIM, int BLOCK, int CAP, int MODE>
-__global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+__device__ __forceinline__ void fluid_tile(const FluidArgs& a, const Tables& T, const StageCoefs& c,
+                                           const StageBuffers& b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
     FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * BLOCK);
@@ -426,8 +435,8 @@ __global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoe
 // different sizes share the SMs without a tail of idle blocks.  Blocks never
 // wait on each other.
 template <int DIM, int BLOCK, int CAP, int MODE>
-__global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
-                                                            uint32_t* tile_counter) {
+__device__ __forceinline__ void fluid_tiles_persistent(const FluidArgs& a, const Tables& T, const StageCoefs& c,
+                                                       const StageBuffers& b, uint32_t* tile_counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
     FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * BLOCK);
@@ -454,11 +463,47 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables 
     }
 }
 
+template <int DIM, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    fluid_tile<DIM, BLOCK, CAP, kTwoPass>(a, T, c, b);
+}
+template <int DIM, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
+                                                            uint32_t* tile_counter) {
+    fluid_tiles_persistent<DIM, BLOCK, CAP, kTwoPass>(a, T, c, b, tile_counter);
+}
+template <int DIM, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK, kFlushMinBlocks * 128 / BLOCK)
+    k_fluid_flush(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    fluid_tile<DIM, BLOCK, CAP, kFlush>(a, T, c, b);
+}
+template <int DIM, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK, kFlushMinBlocks * 128 / BLOCK)
+    k_fluid_flush_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b, uint32_t* tile_counter) {
+    fluid_tiles_persistent<DIM, BLOCK, CAP, kFlush>(a, T, c, b, tile_counter);
+}
+
+// The kernels of one launch shape (only the used ones are instantiated).
+template <int DIM, int BLOCK, int CAP, int MODE>
+struct FluidKernels {
+    static constexpr auto tile_kernel() {
+        if constexpr (MODE == kFlush) return k_fluid_flush<DIM, BLOCK, CAP>;
+        else return k_fluid<DIM, BLOCK, CAP>;
+    }
+    static constexpr auto persistent_kernel() {
+        if constexpr (MODE == kFlush) return k_fluid_flush_persistent<DIM, BLOCK, CAP>;
+        else return k_fluid_persistent<DIM, BLOCK, CAP>;
+    }
+    static constexpr auto tile = tile_kernel();
+    static constexpr auto persistent = persistent_kernel();
+};
+
 // First overflow queue: particles whose hit list filled up, evaluated with
 // list flushes (kFlush), grid-stride over the queue.
 constexpr int kFlushCap = 64;
 template <int DIM>
-__global__ void __launch_bounds__(128) k_fluid_overflow_flush(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+__global__ void __launch_bounds__(128, kFlushMinBlocks) k_fluid_overflow_flush(FluidArgs a, Tables T, StageCoefs c,
+                                                                                StageBuffers b) {
     __shared__ uint32_t lst[kFlushCap * 128];
     const uint32_t cnt = a.overflow_count[0];
     for (uint32_t i0 = blockIdx.x * 128u; i0 < cnt; i0 += gridDim.x * 128u) {  // uniform per block
@@ -486,17 +531,18 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
     const size_t smem = sizeof(uint32_t) * CAP * BLOCK + sizeof(FluidMat) * T.max_nmat +
                         sizeof(DevInter) * T.max_nmat * T.max_nmat;
     if (smem > 48 * 1024) {
-        cudaFuncSetAttribute(k_fluid<DIM, BLOCK, CAP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-        cudaFuncSetAttribute(k_fluid_persistent<DIM, BLOCK, CAP, MODE>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaFuncSetAttribute(FluidKernels<DIM, BLOCK, CAP, MODE>::tile, cudaFuncAttributeMaxDynamicSharedMemorySize,
                              (int)smem);
+        cudaFuncSetAttribute(FluidKernels<DIM, BLOCK, CAP, MODE>::persistent,
+                             cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
     cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
     if (!persistent) {
-        k_fluid<DIM, BLOCK, CAP, MODE><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
+        FluidKernels<DIM, BLOCK, CAP, MODE>::tile<<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
     } else {
         int per_sm = 0;
-        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_fluid_persistent<DIM, BLOCK, CAP, MODE>, BLOCK,
+        cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, FluidKernels<DIM, BLOCK, CAP, MODE>::persistent, BLOCK,
                                                       smem);
         per_sm = per_sm > 0 ? per_sm : 1;
         int sms = 148;
@@ -504,7 +550,7 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
         cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
-        k_fluid_persistent<DIM, BLOCK, CAP, MODE><<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
+        FluidKernels<DIM, BLOCK, CAP, MODE>::persistent<<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
     }
     // the overflow queues: grids of at most 1184 blocks striding over the
     // queue, which usually is empty
