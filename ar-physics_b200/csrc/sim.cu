@@ -280,18 +280,26 @@ struct arp_sim {
     uint32_t rl_nnz = 0;
     DevBuf<DevStats> d_stats;
 
-    // CUDA graph of two integrator steps (every buffer swap of a step is
-    // undone by the next, so the captured pointers stay valid)
+    // CUDA graphs of one integrator step.  A step swaps the caller-id and
+    // solid-id buffers (and the plastic strain's when it changes), so the
+    // steps alternate between two sets of buffer pointers; a graph is kept
+    // for each set, keyed by its pointers, and replayed with the step's
+    // host-side effects applied by hand.
+    struct StepGraph {
+        cudaGraph_t g = nullptr;
+        cudaGraphExec_t exec = nullptr;
+        const void* sig[4] = {nullptr, nullptr, nullptr, nullptr};
+        uint64_t launches = 0;  // kernels per replay
+    };
     bool use_graph = false;
-    cudaGraph_t graph = nullptr;
-    cudaGraphExec_t graph_exec = nullptr;
+    StepGraph graphs[2];
     cudaStream_t graph_stream = nullptr;
-    uint64_t graph_launches = 0;  // kernels per replay
     void drop_graph() {
-        if (graph_exec) cudaGraphExecDestroy(graph_exec);
-        if (graph) cudaGraphDestroy(graph);
-        graph_exec = nullptr;
-        graph = nullptr;
+        for (auto& x : graphs) {
+            if (x.exec) cudaGraphExecDestroy(x.exec);
+            if (x.g) cudaGraphDestroy(x.g);
+            x = StepGraph{};
+        }
         graph_stream = nullptr;
     }
 
@@ -1357,30 +1365,43 @@ arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, i
     return ARP_OK;
 }
 
-// Capture two steps into a graph on the handle's stream.  Host-side effects
-// of the captured steps (time, launch count) are applied per replay instead.
-arp_status capture_graph(arp_sim* S) {
-    S->drop_graph();
-    const float t0 = S->time;
+// The buffer pointers a step's launches depend on and swaps.
+static void step_signature(const arp_sim* S, const void* sig[4]) {
+    sig[0] = S->Y.pd.p;
+    sig[1] = S->orig.p;
+    sig[2] = S->sid.p;
+    sig[3] = S->ep.p;
+}
+
+// Capture one step on the handle's stream into the graph slot `k`; the host
+// side of the step (buffer swaps, time, launch count) happens here, so the
+// caller launches the graph once to run the step it stands for.
+arp_status capture_step_graph(arp_sim* S, int k) {
+    arp_sim::StepGraph& G = S->graphs[k];
+    if (G.exec) cudaGraphExecDestroy(G.exec);
+    if (G.g) cudaGraphDestroy(G.g);
+    G = arp_sim::StepGraph{};
+    step_signature(S, G.sig);
     const uint64_t l0 = S->launches;
     const bool prof = S->prof_on;
     S->prof_on = false;
     CUDA_TRY(cudaStreamBeginCapture(S->stream, cudaStreamCaptureModeThreadLocal));
     arp_status st = do_step(S);
-    if (st == ARP_OK) st = do_step(S);
     cudaGraph_t g = nullptr;
     cudaError_t e = cudaStreamEndCapture(S->stream, &g);
     S->prof_on = prof;
-    S->time = t0;
-    S->graph_launches = S->launches - l0;
-    S->launches = l0;
+    G.launches = S->launches - l0;
     if (st != ARP_OK) {
         if (g) cudaGraphDestroy(g);
+        S->drop_graph();
         return st;
     }
-    if (e != cudaSuccess) return fail(ARP_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
-    S->graph = g;
-    e = cudaGraphInstantiate(&S->graph_exec, g, 0);
+    if (e != cudaSuccess) {
+        S->drop_graph();
+        return fail(ARP_ERR_CUDA, std::string("cudaStreamEndCapture: ") + cudaGetErrorString(e));
+    }
+    G.g = g;
+    e = cudaGraphInstantiate(&G.exec, g, 0);
     if (e != cudaSuccess) {
         S->drop_graph();
         return fail(ARP_ERR_CUDA, std::string("cudaGraphInstantiate: ") + cudaGetErrorString(e));
@@ -1389,19 +1410,43 @@ arp_status capture_graph(arp_sim* S) {
     return ARP_OK;
 }
 
+// One step from a graph: replay the graph captured for the current buffer
+// pointers (capturing it first if there is none) and apply the step's host
+// side: the buffer swaps of do_step, time and launch count.
+arp_status graph_step(arp_sim* S) {
+    if (S->graph_stream != S->stream) S->drop_graph();
+    const void* sig[4];
+    step_signature(S, sig);
+    int k = -1, free_slot = -1;
+    for (int q = 0; q < 2; ++q) {
+        const auto& G = S->graphs[q];
+        if (G.exec && std::equal(sig, sig + 4, G.sig)) k = q;
+        if (!G.exec && free_slot < 0) free_slot = q;
+    }
+    if (k < 0) {  // capture; do_step's host side happens during the capture
+        k = free_slot >= 0 ? free_slot : 0;
+        const float t = S->time;
+        ARP_TRY(capture_step_graph(S, k));
+        S->time = t;
+    } else {
+        std::swap(S->orig, S->orig_r);
+        std::swap(S->sid, S->sid_r);
+        if (S->solid_branch() && S->any_plastic) std::swap(S->ep, S->ep_t);
+        S->launches += S->graphs[k].launches;
+    }
+    CUDA_TRY(cudaGraphLaunch(S->graphs[k].exec, S->stream));
+    S->time += S->dt_sub;
+    if (S->prof_on) S->prof_phase++;  // a step not sampled by the profiler
+    return ARP_OK;
+}
+
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
     ARP_TRY(need_init(sim));
-    uint32_t i = 0;
-    if (sim->use_graph && !sim->prof_on && !sim->tape && nsteps >= 2) {
-        if (!sim->graph_exec || sim->graph_stream != sim->stream) ARP_TRY(capture_graph(sim));
-        for (; i + 2 <= nsteps; i += 2) {
-            CUDA_TRY(cudaGraphLaunch(sim->graph_exec, sim->stream));
-            sim->time += sim->dt_sub;
-            sim->time += sim->dt_sub;
-            sim->launches += sim->graph_launches;
-        }
+    for (uint32_t i = 0; i < nsteps; ++i) {
+        const bool sampled = sim->prof_on && sim->prof_phase % sim->prof_every == 0;
+        if (sim->use_graph && !sim->tape && !sampled) ARP_TRY(graph_step(sim));
+        else ARP_TRY(do_step(sim));
     }
-    for (; i < nsteps; ++i) ARP_TRY(do_step(sim));
     return ARP_OK;
 }
 

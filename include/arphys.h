@@ -266,9 +266,11 @@ arp_status arp_sim_autotune(arp_sim* sim, int* variant);
 arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent);
 /* Pin the fluid kernel's launch shape (0 .. 9). */
 arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant);
-/* Replay pairs of steps from a CUDA graph captured on the handle's stream
- * (captured on first use and again after the stream changes; profiling
- * disables replay).  Off by default. */
+/* Replay each step from a CUDA graph captured on the handle's stream (two
+ * graphs, one for each of the two buffer sets consecutive steps alternate
+ * between; captured on first use and again after the stream or the buffers
+ * change).  Steps sampled by arp_sim_profile_enable and steps on a tape run
+ * as plain launches.  Off by default. */
 arp_status arp_sim_set_graph(arp_sim* sim, int enable);
 
 /* ---- queries (FluidSim accessors, src/soft_body/mod.rs:168-178) ------------ */

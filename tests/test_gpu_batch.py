@@ -78,12 +78,41 @@ def test_graph_replay_matches_plain_steps():
     b.init()
     b.set_graph(True)
     a.step(9)
-    b.step(9)  # four graph replays of two steps plus one plain step
+    b.step(9)  # nine graph replays, alternating between the two buffer sets
     assert a.particles().tobytes() == b.particles().tobytes()
     assert abs(a.time() - b.time()) == 0
     b.step(4)
     a.step(4)
     assert a.particles().tobytes() == b.particles().tobytes()
+
+
+def test_single_step_graphs_match_plain_steps():
+    """Graph replay one step at a time (a graph for each of the two buffer
+    sets the steps alternate between), mixed with plain steps sampled by the
+    profiler, gives the plain steps' bits, time and launch count; a plastic
+    solid exercises the plastic-strain buffer swap."""
+    sc = scenes.cantilever_bar(n=(4, 8, 4))
+    sc.materials["plastic"][1] = 1
+    sc.materials["yield_strength"][1] = 1.0
+    a = FluidSim(sc)
+    a.init()
+    b = FluidSim(sc)
+    b.init()
+    b.set_graph(True)
+    for k in (1, 1, 3, 2, 1):
+        a.step(k)
+        b.step(k)
+        assert a.particles().tobytes() == b.particles().tobytes()
+        assert a.solids().tobytes() == b.solids().tobytes()
+        assert a.time() == b.time()
+    b.profile_enable(True, every=3)
+    a.step(5)
+    b.step(5)
+    assert b.profile_read()["steps"] == 2  # the first and the fourth of the five ran plain
+    b.profile_enable(False)
+    assert a.particles().tobytes() == b.particles().tobytes()
+    assert a.solids().tobytes() == b.solids().tobytes()
+    assert a.launch_count() == b.launch_count()
 
 
 def test_fluid_launch_shapes_give_identical_results():
