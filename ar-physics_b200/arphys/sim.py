@@ -179,7 +179,7 @@ class FluidSim:
         return start, members[:self.nb]
 
     def set_graph(self, on=True):
-        """Replay pairs of steps from a captured CUDA graph."""
+        """Replay each step from a captured CUDA graph (one per alternating buffer set)."""
         check(self._L.arp_sim_set_graph(self._h, int(bool(on))))
 
     def autotune(self):
