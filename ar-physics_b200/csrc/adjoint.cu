@@ -21,12 +21,17 @@
 // strain orders other than 2 (refused), self-contact (flagged when a pair is
 // active).
 #include "grid.cuh"
+#include "warp.cuh"
 
 namespace arp {
 
 namespace {
 
 constexpr int kT = 128;
+#ifndef ARP_ADJ_SOLID_LANES
+#define ARP_ADJ_SOLID_LANES 4
+#endif
+constexpr int kAdjSolidLanes = ARP_ADJ_SOLID_LANES;  // threads per solid in k_adj_solid
 constexpr uint32_t kSameMatBit = 0x80000000u;
 
 inline uint32_t nblocks(uint32_t n, int t) { return (n + (uint32_t)t - 1u) / (uint32_t)t; }
@@ -457,9 +462,14 @@ __device__ __forceinline__ bool in_stencil2(uint2 a, uint2 b) {
            dz <= 1;
 }
 
+// LANES threads share one solid: both reference-list loops are split over
+// them with stride LANES, their partial sums combined by group_sum; lane 0
+// finishes the particle.
+template <int LANES>
 __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.ns) return;
+    const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
+    const uint32_t i = t / LANES, lane = t % LANES;
+    if (i >= a.ns) return;  // whole groups leave together
     const float4 xi = a.st.sx[i], vi = a.st.sv[i];
     const uint32_t mat = __float_as_uint(vi.w);
     const DevMat mm = T.mats[mat];
@@ -476,7 +486,7 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
     float3 lx = make_float3(0.f, 0.f, 0.f), fs = lx;
     float lrho = 0.0f;
     const uint32_t k0 = a.rl.off[i], k1 = a.rl.off[i + 1];
-    for (uint32_t k = k0; k < k1; ++k) {
+    for (uint32_t k = k0 + lane; k < k1; k += LANES) {
         const uint32_t e = a.rl.nbr[k];
         if (!(e & kSameMatBit)) continue;
         const uint32_t j = e & ~kSameMatBit;
@@ -517,6 +527,30 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
             lrho += o.ldb;
         }
     }
+    // dF/dt of the stage, recomputed from the reference list
+    const M3 L = m3_cols(a.L + 3 * i);
+    M3 Fd = m3_zero();
+    for (uint32_t k = k0 + lane; k < k1; k += LANES) {
+        const uint32_t j = a.rl.nbr[k] & ~kSameMatBit;
+        const float4 vj = a.st.sv[j];
+        const float3 G = m3_vec(L, ref_grad(a.ref, j, Xi, P));
+        const float3 dv = sub(f3(vj), f3(vi));
+        m3_add_outer(Fd, a.ref[j].w, dv, G);  // ref.w = V_j
+    }
+    if (LANES > 1) {
+#pragma unroll
+        for (int r = 0; r < 3; ++r)
+#pragma unroll
+            for (int c = 0; c < 3; ++c) {
+                lA.m[r][c] = group_sum<LANES>(lA.m[r][c]);
+                lFh.m[r][c] = group_sum<LANES>(lFh.m[r][c]);
+                Fd.m[r][c] = group_sum<LANES>(Fd.m[r][c]);
+            }
+        lx = make_float3(group_sum<LANES>(lx.x), group_sum<LANES>(lx.y), group_sum<LANES>(lx.z));
+        fs = make_float3(group_sum<LANES>(fs.x), group_sum<LANES>(fs.y), group_sum<LANES>(fs.z));
+        lrho = group_sum<LANES>(lrho);
+        if (lane != 0) return;
+    }
     // self-contact (solid.rs:445-450) is not differentiated: flag an active pair
     {
         const float U = __uint_as_float(a.st.contact_bound[0]);
@@ -541,15 +575,6 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
     lrho -= dot(w, fs) / d1;  // k_v = f / rho - g
     // stress chain (order 2): E = (F^T F - I)/2, dE/dt = (dF^T F + F^T dF)/2,
     // S = Hooke(E; n, s) + Hooke(dE/dt; n_d, s_d), sigma = F S^T, A = sigma L
-    const M3 L = m3_cols(a.L + 3 * i);
-    M3 Fd = m3_zero();
-    for (uint32_t k = k0; k < k1; ++k) {
-        const uint32_t j = a.rl.nbr[k] & ~kSameMatBit;
-        const float4 vj = a.st.sv[j];
-        const float3 G = m3_vec(L, ref_grad(a.ref, j, Xi, P));
-        const float3 dv = sub(f3(vj), f3(vi));
-        m3_add_outer(Fd, a.ref[j].w, dv, G);  // ref.w = V_j
-    }
     const uint32_t dim = P.dim;
     M3 E = m3_mul(m3_t(Fi), Fi);
 #pragma unroll
@@ -697,7 +722,7 @@ __global__ void k_adj_perm(uint32_t n, const uint32_t* __restrict__ orig, const 
 int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st) {
     int launches = 0;
     if (a.solid_branch && a.ns > 0) {
-        k_adj_solid<<<nblocks(a.ns, kT), kT, 0, st>>>(a, T);
+        k_adj_solid<kAdjSolidLanes><<<nblocks(a.ns * kAdjSolidLanes, kT), kT, 0, st>>>(a, T);
         k_adj_strain<<<nblocks(a.ns, kT), kT, 0, st>>>(a, T);
         launches += 2;
     }

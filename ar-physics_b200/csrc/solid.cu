@@ -20,6 +20,7 @@
 //     current 3x3x3 cells (k_solid_forces).  A_j is read, not recomputed.
 #include "grid.cuh"
 #include "mat4.cuh"
+#include "warp.cuh"
 
 namespace arp {
 
@@ -223,16 +224,8 @@ __global__ void k_solid_gather(const float4* __restrict__ pd, const float4* __re
 // PLASTIC: some solid material is plastic; otherwise the plastic strain is
 // zero throughout and its buffers are neither read nor written.
 // LANES threads share one solid: they walk its reference list with stride
-// LANES and combine their partial sums with shuffles (a fixed order, so the
-// result is deterministic); lane 0 finishes the particle.
-template <int LANES>
-__device__ __forceinline__ float group_sum(float v) {
-    const uint32_t lane = threadIdx.x & 31u;
-    const uint32_t mask = (LANES == 32 ? 0xFFFFFFFFu : ((1u << LANES) - 1u)) << (lane & ~(uint32_t)(LANES - 1));
-#pragma unroll
-    for (int o = LANES / 2; o > 0; o >>= 1) v += __shfl_xor_sync(mask, v, o, LANES);
-    return v;
-}
+// LANES and combine their partial sums with shuffles (group_sum: a fixed
+// order, so the result is deterministic); lane 0 finishes the particle.
 
 template <bool ORDER2, bool PLASTIC, int LANES>
 __global__ void __launch_bounds__(kThreads) k_solid_stress(SolidArgs a, Tables T, StageCoefs c) {

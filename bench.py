@@ -297,7 +297,7 @@ def _time_adjoint(torch, stream, sim, steps, every, loss_grad):
                       "(it synchronizes), including dL/dy upload and gradient download"}
 
 
-def run_adjoint(torch, stream):
+def run_adjoint(torch, stream, bar_steps=400, rt_steps=300, only=None):
     """Reverse mode on the two differentiation workloads: the 16x16x256 bar
     (65,536 particles, per-particle E, 400 RK2 steps, checkpoints every 20;
     gradient of the tip-centroid loss w.r.t. per-particle stiffness and
@@ -306,6 +306,9 @@ def run_adjoint(torch, stream):
     velocities of all scenes, one backward pass for the batch)."""
     import numpy as np
     from arphys import FluidSim, scenes
+    out = {}
+    if only not in (None, "bar"):
+        return out | run_adjoint_rt(torch, stream, rt_steps)
     sc = scenes.cantilever_bar()
     sim = FluidSim(sc)
     sim.init()
@@ -315,10 +318,20 @@ def run_adjoint(torch, stream):
     sim.step(3)  # warm-up
     sim.set_particles(init)
     tip, target = sc.meta["tip"], sc.meta["target"]
-    bar = _time_adjoint(torch, stream, sim, 400, 20, lambda pos: scenes.tip_loss(pos, tip, target))
+    bar = _time_adjoint(torch, stream, sim, bar_steps, 20, lambda pos: scenes.tip_loss(pos, tip, target))
     bar["workload"] = ("cantilever bar 16x16x256 (65,024 elastic + 512 clamped), per-particle E lognormal("
                        "ln 1e5, 0.3), nu 0.3, gravity, RK2, dt 1e-4")
     sim.close()
+    out["bar"] = bar
+    if only == "bar":
+        return out
+    return out | run_adjoint_rt(torch, stream, rt_steps)
+
+
+def run_adjoint_rt(torch, stream, steps):
+    """The batched Rayleigh-Taylor part of run_adjoint."""
+    import numpy as np
+    from arphys import FluidSim, scenes
     scs = scenes.rayleigh_taylor_batch()
     batch = FluidSim.batch(scs)
     batch.init()
@@ -336,12 +349,12 @@ def run_adjoint(torch, stream):
             g[offsets[k]:offsets[k + 1]] = gk
             tot += L
         return tot, g
-    rt = _time_adjoint(torch, stream, batch, 300, 20, sep_grad)
+    rt = _time_adjoint(torch, stream, batch, steps, 20, sep_grad)
     rt["workload"] = (f"{len(scs)} 2D Rayleigh-Taylor scenes, {int(offsets[-1])} particles (8,192-131,072 per "
                       "scene), heavy 1800 over light 1000, RK2, dt 1e-4; loss = sum of heavy/light centroid "
                       "separations")
     batch.close()
-    return {"bar": bar, "rayleigh_taylor_batch": rt}
+    return {"rayleigh_taylor_batch": rt}
 
 
 def run_render(torch, sim, sc):
@@ -527,7 +540,18 @@ def main():
     ap.add_argument("--fluid-variant", type=int, default=None, help="pin the fluid launch shape (profiling)")
     ap.add_argument("--batched-only", action="store_true",
                     help="run only the batched-scenes measurement and print its object (profiling)")
+    ap.add_argument("--adjoint-only", choices=["bar", "rt", "both"], default=None,
+                    help="run only the reverse-mode measurement and print its object (profiling)")
+    ap.add_argument("--adjoint-steps", type=int, default=None,
+                    help="steps of each reverse-mode workload (default: 400 for the bar, 300 for the batch)")
     args = ap.parse_args()
+    if args.adjoint_only:
+        import torch
+        stream = torch.cuda.Stream()
+        n = args.adjoint_steps
+        print(json.dumps(run_adjoint(torch, stream, n or 400, n or 300,
+                                     None if args.adjoint_only == "both" else args.adjoint_only)), flush=True)
+        return
     if args.batched_only:
         import torch
         stream = torch.cuda.Stream()
