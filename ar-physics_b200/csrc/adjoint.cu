@@ -308,11 +308,15 @@ __device__ __forceinline__ void pair_vjp(const PairGeom& G, const PairSide& a, c
 
 // Per particle of the stage: the weights of its derivative record and its
 // state-equation terms, read by its own thread and by its neighbors':
-// w = (mu_v / rho, mu_rho), e = (p / rho^2, d(p / rho^2)/d rho, 1 / rho).
+// w = (mu_v / rho, mu_rho), e = (p / rho^2, d(p / rho^2)/d rho, 1 / rho);
+// and the positions in cell order for the neighbor scan.  Thread k is cell
+// position k.
 __global__ void k_adj_prep(AdjArgs a, Tables T, float4* __restrict__ w, float4* __restrict__ e) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= a.n) return;
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= a.n) return;
+    const uint32_t i = a.st.perm ? a.st.perm[k] : k;
     const float4 xi = a.st.pd[i];
+    a.xs[k] = xi;
     const FluidMat fm = T.fmats[__float_as_uint(a.st.vm[i].w)];
     const float ir = 1.0f / xi.w;
     const float4 mv = a.mu_vm[i];
@@ -322,9 +326,13 @@ __global__ void k_adj_prep(AdjArgs a, Tables T, float4* __restrict__ w, float4* 
     e[i] = make_float4(pt, dpt, ir, 0.0f);
 }
 
+constexpr int kAdjCap = 48;                   // hit-list entries per thread of k_adj_fluid
+constexpr uint32_t kHitBoundary = 0x80000000u;  // list entry of a boundary particle
+
 template <int DIM>
 __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const float4* __restrict__ W,
                                                   const float4* __restrict__ EQ) {
+    __shared__ uint32_t lst[kAdjCap * kT];
     const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
     if (i >= a.n) return;
     const float4 xi = a.st.pd[i], vi = a.st.vm[i];
@@ -346,54 +354,78 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const flo
     float3 Fs = make_float3(0.f, 0.f, 0.f);
     const uint32_t li = mat - P.mat_base;
     const DevInter* row_i = T.inter + P.inter_base + li * P.nmat;
+    // Two passes, as in the forward kernel: the scan lists the hits (cell
+    // positions; boundary ones flagged) in shared memory, then the pair VJPs
+    // run over the list with nearly full warps.  A particle with more hits
+    // than the list holds scans again for the next kAdjCap of them (the pair
+    // math stays at one call site); the pairs are taken in scan order.
+    uint32_t* my = lst + threadIdx.x;
+    auto eval = [&](uint32_t h) {
+        if (h & kHitBoundary) {
+            const uint32_t jb = h & ~kHitBoundary;
+            const float4 xb = a.bxs[jb];
+            const float4 vb = a.bvs[jb];
+            const uint32_t matb = __float_as_uint(vb.w);
+            const FluidMat fb = T.fmats[matb];
+            const PairSide sb{f3(xb), f3(vb), xb.w, __fdividef(1.0f, xb.w), a.bps[jb], fb.mass, fb.visc,
+                              fb.bulk, matb, false};
+            const DevInter it = row_i[matb - P.mat_base];
+            const PairGeom G = make_geom<DIM>(si.x, si.v, sb.x, sb.v, it, P.h2, P.kconst, P.eps_hh);
+            PairGrad o;
+            pair_vjp<DIM, true>(G, si, sb, it.dampening, wd, wF, o);
+            Fs = add(Fs, o.F);
+            lx = sub(lx, o.lr);
+            lv = sub(lv, o.lvv);
+            lrho += o.ld_self + o.lpt * dpt_i;
+        } else {
+            const uint32_t j = a.st.perm ? a.st.perm[h] : h;
+            if (j == i) return;
+            const float4 xj = a.st.pd[j];
+            const float4 vj = a.st.vm[j];
+            const uint32_t matj = __float_as_uint(vj.w);
+            const FluidMat fj = T.fmats[matj];
+            const uint32_t sidj = a.sid[j];
+            const float4 ej = EQ[j], wj = W[j];
+            const PairSide sj{f3(xj), f3(vj), xj.w, ej.z, ej.x, fj.mass, fj.visc, fj.bulk, matj,
+                              sidj != kInvalid && fj.stiff != 0u};
+            const DevInter it = row_i[matj - P.mat_base];  // symmetric: also the neighbor's entry
+            const PairGeom G = make_geom<DIM>(si.x, si.v, sj.x, sj.v, it, P.h2, P.kconst, P.eps_hh);
+            PairGrad o;
+            pair_vjp<DIM, false>(G, si, sj, it.dampening, wd, wF, o);
+            Fs = add(Fs, o.F);
+            lx = sub(lx, o.lr);
+            lv = sub(lv, o.lvv);
+            lrho += o.ld_self + o.lpt * dpt_i;
+            // the neighbor's own pair, in which this particle is the neighbor
+            pair_vjp<DIM, false>(flipped(G), sj, si, it.dampening, wj.w, f3(wj), o);
+            lx = add(lx, o.lr);
+            lv = add(lv, o.lvv);
+            lrho += o.ld_nbr + o.lpt * dpt_i;
+        }
+    };
     if (finite3(xi)) {
-        for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
+        for (uint32_t done = 0;;) {
+            uint32_t total = 0, cnt = 0;  // hits seen in this scan, hits listed
+            auto take = [&](uint32_t h) {
+                if (total >= done && cnt < (uint32_t)kAdjCap) my[cnt++ * kT] = h;
+                ++total;
+            };
+            for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
                 for (uint32_t jb = a.bstart[c0]; jb < a.bstart[c1]; ++jb) {
                     const float4 xb = a.bxs[jb];
                     const float rx = xb.x - xi.x, ry = xb.y - xi.y, rz = DIM == 3 ? xb.z - xi.z : 0.0f;
-                    if (!(P.h2 - (rx * rx + ry * ry + rz * rz) > 0.0f)) continue;
-                    const float4 vb = a.bvs[jb];
-                    const uint32_t matb = __float_as_uint(vb.w);
-                    const FluidMat fb = T.fmats[matb];
-                    const PairSide sb{f3(xb), f3(vb), xb.w, __fdividef(1.0f, xb.w), a.bps[jb], fb.mass, fb.visc,
-                                      fb.bulk, matb, false};
-                    const DevInter it = row_i[matb - P.mat_base];
-                    const PairGeom G = make_geom<DIM>(si.x, si.v, sb.x, sb.v, it, P.h2, P.kconst, P.eps_hh);
-                    PairGrad o;
-                    pair_vjp<DIM, true>(G, si, sb, it.dampening, wd, wF, o);
-                    Fs = add(Fs, o.F);
-                    lx = sub(lx, o.lr);
-                    lv = sub(lv, o.lvv);
-                    lrho += o.ld_self + o.lpt * dpt_i;
+                    if (P.h2 - (rx * rx + ry * ry + rz * rz) > 0.0f) take(jb | kHitBoundary);
                 }
                 for (uint32_t k = a.st.start[c0]; k < a.st.start[c1]; ++k) {
-                    const uint32_t j = a.st.perm ? a.st.perm[k] : k;
-                    if (j == i) continue;
-                    const float4 xj = a.st.pd[j];
+                    const float4 xj = a.xs[k];
                     const float rx = xj.x - xi.x, ry = xj.y - xi.y, rz = DIM == 3 ? xj.z - xi.z : 0.0f;
-                    if (!(P.h2 - (rx * rx + ry * ry + rz * rz) > 0.0f)) continue;
-                    const float4 vj = a.st.vm[j];
-                    const uint32_t matj = __float_as_uint(vj.w);
-                    const FluidMat fj = T.fmats[matj];
-                    const uint32_t sidj = a.sid[j];
-                    const float4 ej = EQ[j], wj = W[j];
-                    const PairSide sj{f3(xj), f3(vj), xj.w, ej.z, ej.x, fj.mass, fj.visc, fj.bulk, matj,
-                                      sidj != kInvalid && fj.stiff != 0u};
-                    const DevInter it = row_i[matj - P.mat_base];  // symmetric: also the neighbor's entry
-                    const PairGeom G = make_geom<DIM>(si.x, si.v, sj.x, sj.v, it, P.h2, P.kconst, P.eps_hh);
-                    PairGrad o;
-                    pair_vjp<DIM, false>(G, si, sj, it.dampening, wd, wF, o);
-                    Fs = add(Fs, o.F);
-                    lx = sub(lx, o.lr);
-                    lv = sub(lv, o.lvv);
-                    lrho += o.ld_self + o.lpt * dpt_i;
-                    // the neighbor's own pair, in which this particle is the neighbor
-                    pair_vjp<DIM, false>(flipped(G), sj, si, it.dampening, wj.w, f3(wj), o);
-                    lx = add(lx, o.lr);
-                    lv = add(lv, o.lvv);
-                    lrho += o.ld_nbr + o.lpt * dpt_i;
+                    if (P.h2 - (rx * rx + ry * ry + rz * rz) > 0.0f) take(k);
                 }
-        });
+            });
+            for (uint32_t e = 0; e < cnt; ++e) eval(my[e * kT]);
+            done += cnt;
+            if (done >= total) break;
+        }
     }
     lrho -= dot(wF, Fs) * ei.z;  // k_v = F / rho
     if (DIM == 2) {

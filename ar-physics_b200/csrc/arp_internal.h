@@ -367,6 +367,7 @@ struct AdjArgs {
     uint32_t* flags;           // bit 0: an active self-contact pair (not differentiated)
     float4* w;                 // [n] scratch: per-particle weights of the stage
     float4* eq;                // [n] scratch: per-particle state-equation terms
+    float4* xs;                // [n] scratch: the stage positions in cell order
     uint32_t n, ns;
     int solid_branch;
 };

@@ -168,7 +168,7 @@ struct Tape {
 struct AdjointPool {
     std::vector<StepRecord> recs;       // one segment of recording steps
     std::vector<Checkpoint> spare;      // checkpoints of ended tapes, reused
-    DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, w, e;
+    DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, w, e, xs;
     DevBuf<float4> lY_p[kMaxStages], lY_v[kMaxStages];
     DevBuf<float4> lamF, lamFd;
     DevBuf<float2> gst;
@@ -2045,7 +2045,8 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     // adjoint buffers: caller order (lc), storage order (ls, out), per stage (lY), stage weights (mu)
     const size_t nn = std::max(n, 1u);
     auto fit = [](auto& b, size_t count) -> cudaError_t { return b.n >= count ? cudaSuccess : b.alloc(count); };
-    for (DevBuf<float4>* b : {&P.lc_p, &P.lc_v, &P.ls_p, &P.ls_v, &P.out_p, &P.out_v, &P.mu_p, &P.mu_v, &P.w, &P.e})
+    for (DevBuf<float4>* b :
+         {&P.lc_p, &P.lc_v, &P.ls_p, &P.ls_v, &P.out_p, &P.out_v, &P.mu_p, &P.mu_v, &P.w, &P.e, &P.xs})
         CUDA_TRY(fit(*b, nn));
     for (int q = 0; q < S; ++q) {
         CUDA_TRY(fit(P.lY_p[q], nn));
@@ -2142,6 +2143,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.flags = flags.p;
                 a.w = P.w.p;
                 a.eq = P.e.p;
+                a.xs = P.xs.p;
                 a.n = n;
                 a.ns = ns;
                 a.solid_branch = sb ? 1 : 0;
