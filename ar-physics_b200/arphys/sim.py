@@ -246,7 +246,7 @@ class FluidSim:
         state); states are (n, 8) float arrays (x, y, z, rho, vx, vy, vz, 0) in
         caller order.  Returns (grad_state0 (n, 8), grad_stiffness (ns, 2))."""
         d = np.ascontiguousarray(dl_dstate, dtype=np.float32).reshape(self.n, 8)
-        g = np.zeros((self.n, 8), np.float32)
+        g = np.empty((self.n, 8), np.float32)  # written in full by the library
         gs = np.zeros((max(self.ns, 1), 2), np.float32)
         check(self._L.arp_tape_backward(self._h, ptr(d), ptr(g), ptr(gs)))
         return g, gs[:self.ns]

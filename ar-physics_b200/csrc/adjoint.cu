@@ -811,4 +811,37 @@ int adjoint_scatter(uint32_t n, const uint32_t* orig, const float4* in_pd, const
     return 1;
 }
 
+namespace {
+// The C ABI's state gradients are 8 floats per particle (x, y, z, rho, vx,
+// vy, vz, unused); on the device they are two float4 arrays.
+__global__ void k_adj_unpack(uint32_t n, const float4* __restrict__ in2, float4* __restrict__ p,
+                             float4* __restrict__ v) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    p[i] = in2[2 * i];
+    const float4 b = in2[2 * i + 1];
+    v[i] = make_float4(b.x, b.y, b.z, 0.0f);
+}
+__global__ void k_adj_pack(uint32_t n, const float4* __restrict__ p, const float4* __restrict__ v,
+                           float4* __restrict__ out2) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    out2[2 * i] = p[i];
+    const float4 b = v[i];
+    out2[2 * i + 1] = make_float4(b.x, b.y, b.z, 0.0f);
+}
+}  // namespace
+
+int adjoint_unpack(uint32_t n, const float4* in2, float4* p, float4* v, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_adj_unpack<<<nblocks(n, 256), 256, 0, st>>>(n, in2, p, v);
+    return 1;
+}
+
+int adjoint_pack(uint32_t n, const float4* p, const float4* v, float4* out2, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_adj_pack<<<nblocks(n, 256), 256, 0, st>>>(n, p, v, out2);
+    return 1;
+}
+
 }  // namespace arp

@@ -386,5 +386,9 @@ int adjoint_gather(uint32_t n, const uint32_t* orig, const float4* in_pd, const 
                    float4* out_vm, cudaStream_t st);
 int adjoint_scatter(uint32_t n, const uint32_t* orig, const float4* in_pd, const float4* in_vm, float4* out_pd,
                     float4* out_vm, cudaStream_t st);
+// 8 floats per particle (x, y, z, rho, vx, vy, vz, unused) <-> two float4
+// arrays, the unused one written and read as 0.
+int adjoint_unpack(uint32_t n, const float4* in2, float4* p, float4* v, cudaStream_t st);
+int adjoint_pack(uint32_t n, const float4* p, const float4* v, float4* out2, cudaStream_t st);
 
 }  // namespace arp

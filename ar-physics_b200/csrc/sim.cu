@@ -169,6 +169,7 @@ struct AdjointPool {
     std::vector<StepRecord> recs;       // one segment of recording steps
     std::vector<Checkpoint> spare;      // checkpoints of ended tapes, reused
     DevBuf<float4> lc_p, lc_v, ls_p, ls_v, out_p, out_v, mu_p, mu_v, w, e, xs;
+    DevBuf<float4> io;  // [2n] the caller's 8-float-per-particle gradients, on the device
     DevBuf<float4> lY_p[kMaxStages], lY_v[kMaxStages];
     DevBuf<float4> lamF, lamFd;
     DevBuf<float2> gst;
@@ -2056,6 +2057,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     CUDA_TRY(fit(P.lamFd, 3 * size_t(std::max(ns, 1u))));
     CUDA_TRY(fit(P.gst, std::max(ns, 1u)));
     CUDA_TRY(fit(P.flags, 1));
+    CUDA_TRY(fit(P.io, 2 * nn));
     DevBuf<float4>&lc_p = P.lc_p, &lc_v = P.lc_v, &ls_p = P.ls_p, &ls_v = P.ls_v, &out_p = P.out_p,
                   &out_v = P.out_v, &mu_p = P.mu_p, &mu_v = P.mu_v, &lamF = P.lamF, &lamFd = P.lamFd;
     DevBuf<float4>* lY_p = P.lY_p;
@@ -2064,18 +2066,9 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     DevBuf<uint32_t>& flags = P.flags;
     CUDA_TRY(cudaMemsetAsync(gst.p, 0, std::max(ns, 1u) * sizeof(float2), st));
     CUDA_TRY(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t), st));
-    {
-        std::vector<float4> hp(nn), hv(nn);
-        for (uint32_t i = 0; i < n; ++i) {
-            const float* d = dl_dstate + 8 * size_t(i);
-            hp[i] = make_float4(d[0], d[1], d[2], d[3]);
-            hv[i] = make_float4(d[4], d[5], d[6], 0.0f);
-        }
-        if (n) {
-            CUDA_TRY(cudaMemcpyAsync(lc_p.p, hp.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
-            CUDA_TRY(cudaMemcpyAsync(lc_v.p, hv.data(), n * sizeof(float4), cudaMemcpyHostToDevice, st));
-            CUDA_TRY(cudaStreamSynchronize(st));
-        }
+    if (n) {  // one copy of the caller's array, split on the device
+        CUDA_TRY(cudaMemcpyAsync(P.io.p, dl_dstate, n * 2 * sizeof(float4), cudaMemcpyHostToDevice, st));
+        sim->launches += adjoint_unpack(n, P.io.p, lc_p.p, lc_v.p, st);
     }
     const uint32_t every = tp.every;
     if (P.recs.size() < every) P.recs.resize(every);
@@ -2168,26 +2161,16 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     ARP_TRY(status);
     ARP_TRY(restore_checkpoint(sim, now));
     ARP_TRY(check_launch("adjoint"));
-    std::vector<float4> hp(nn), hv(nn);
-    std::vector<float2> hg(std::max(ns, 1u));
     uint32_t hflags = 0;
-    if (n) {
-        CUDA_TRY(cudaMemcpyAsync(hp.data(), lc_p.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
-        CUDA_TRY(cudaMemcpyAsync(hv.data(), lc_v.p, n * sizeof(float4), cudaMemcpyDeviceToHost, st));
+    if (n) {  // interleaved on the device, one copy into the caller's array
+        sim->launches += adjoint_pack(n, lc_p.p, lc_v.p, P.io.p, st);
+        CUDA_TRY(cudaMemcpyAsync(grad_state0, P.io.p, n * 2 * sizeof(float4), cudaMemcpyDeviceToHost, st));
     }
-    if (ns) CUDA_TRY(cudaMemcpyAsync(hg.data(), gst.p, ns * sizeof(float2), cudaMemcpyDeviceToHost, st));
+    // float2 (normal, shear) per solid is the caller's layout
+    if (ns && grad_stiffness)
+        CUDA_TRY(cudaMemcpyAsync(grad_stiffness, gst.p, ns * sizeof(float2), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(&hflags, flags.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
-    for (uint32_t i = 0; i < n; ++i) {
-        float* d = grad_state0 + 8 * size_t(i);
-        d[0] = hp[i].x; d[1] = hp[i].y; d[2] = hp[i].z; d[3] = hp[i].w;
-        d[4] = hv[i].x; d[5] = hv[i].y; d[6] = hv[i].z; d[7] = 0.0f;
-    }
-    if (grad_stiffness)
-        for (uint32_t q = 0; q < ns; ++q) {
-            grad_stiffness[2 * q] = hg[q].x;
-            grad_stiffness[2 * q + 1] = hg[q].y;
-        }
     if (hflags & 1u) return fail(ARP_ERR_UNSUPPORTED, "a self-contact pair was active; it is not differentiated");
     return ARP_OK;
 }
