@@ -400,8 +400,10 @@ int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uin
                GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st) {
     int launches = 0;
     if (n > 0) {
-        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, vm, mat_u32, n, T, gb.key, gb.rank, gb.count,
-                                                                  gb.coord, stats);
+        // a single scene needs no material to find the scene: skip that read
+        const bool one = T.nscenes == 1;
+        k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, one ? nullptr : vm, one ? nullptr : mat_u32, n,
+                                                                  T, gb.key, gb.rank, gb.count, gb.coord, stats);
         ++launches;
     }
     // cells, the non-finite bucket, and the total
