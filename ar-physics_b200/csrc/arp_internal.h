@@ -185,9 +185,22 @@ int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* 
 // Gather a state into sorted order (out[k] = in[perm[k]]) and evaluate the
 // pressure term p / rho^2 of every gathered particle (fluid.rs:131-138,
 // :270-271).  Any pointer pair may be null.
+// Solid-order copies a gather writes on the side: for a gathered particle
+// whose solid id (sid_of_slot at its source slot) is valid, sx/sv/sc[sid] =
+// its state and cell coordinates, and slot_of[sid] = its new index (when
+// slot_of is given).
+struct SolidScatter {
+    const uint32_t* sid_of_slot = nullptr;
+    const uint2* coord_of_slot = nullptr;
+    float4* sx = nullptr;
+    float4* sv = nullptr;
+    uint2* sc = nullptr;
+    uint32_t* slot_of = nullptr;
+};
 int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* pd_out, const float4* vm_in,
                  float4* vm_out, const uint32_t* a_in, uint32_t* a_out, const uint32_t* b_in, uint32_t* b_out,
-                 const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st);
+                 const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st,
+                 const SolidScatter& sol = SolidScatter{});
 
 // Particle records (caller order) to structure of arrays in caller order, and
 // back from cell order into caller order (the state exchange of the C ABI).
@@ -202,8 +215,6 @@ int soa_to_records(const float4* pd, const float4* vm, const uint32_t* orig, con
 int check_records(const arp_particle* in, uint32_t n, const uint32_t* mat_of, const DevMat* mats, float pos_w,
                   uint32_t* flag, cudaStream_t st);
 
-// slot_of[sid[k]] = k for solid slots.
-int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st);
 // Neighbor counts within h of each sorted particle (mobile + boundary),
 // computed with separately rounded float products for bit-exact output.
 int count_neighbors(const float4* xs, const float4* vs, const uint32_t* start, uint32_t n, const float4* bxs,
@@ -267,9 +278,6 @@ int ref_lists_fill(const float4* ref, const uint32_t* mat_of_solid, uint32_t ns,
                    const Tables& T, SolidRefList& rl, float4* L, cudaStream_t st);
 
 struct SolidArgs {
-    const float4* pd;         // stage state, storage order
-    const float4* vm;
-    const uint32_t* slot_of;  // solid id -> storage slot
     const float4* ref;        // reference positions, w = rest volume m / rho0
     const float4* L;
     SolidRefList rl;
@@ -284,7 +292,6 @@ struct SolidArgs {
     float4* F;                // [3*ns] deformation gradient columns (stage scratch)
     float4* A;                // [3*ns] sigma * L columns (stage scratch)
     float4* ksol;             // [ns] solid-term acceleration
-    const uint2* coord;       // storage-order packed cell coordinates of the stage grid
     uint32_t* contact_bound;  // [2] max |u_i - u_0| bits, outside-box flag (cleared per stage)
     const float4* xs;         // sorted stage positions (current-neighbor loop)
     const float4* vs;

@@ -249,7 +249,7 @@ __global__ void k_gather_state(const uint32_t* __restrict__ perm, uint32_t n, co
                                uint32_t* __restrict__ a_out, const uint32_t* __restrict__ b_in,
                                uint32_t* __restrict__ b_out, const uint2* __restrict__ c_in,
                                uint2* __restrict__ c_out, float* __restrict__ ps_out,
-                               const DevMat* __restrict__ mats) {
+                               const DevMat* __restrict__ mats, SolidScatter sol) {
     uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
     if (k >= n) return;
     const uint32_t s = perm ? perm[k] : k;
@@ -257,6 +257,15 @@ __global__ void k_gather_state(const uint32_t* __restrict__ perm, uint32_t n, co
     const float4 vm = vm_in[s];
     if (pd_out) pd_out[k] = pd;
     if (vm_out) vm_out[k] = vm;
+    if (sol.sx) {
+        const uint32_t sid = sol.sid_of_slot[s];
+        if (sid != kInvalid) {
+            sol.sx[sid] = pd;
+            sol.sv[sid] = vm;
+            sol.sc[sid] = sol.coord_of_slot[s];
+            if (sol.slot_of) sol.slot_of[sid] = k;
+        }
+    }
     if (a_out) a_out[k] = a_in[s];
     if (b_out) b_out[k] = b_in[s];
     if (c_out) c_out[k] = c_in[s];
@@ -307,13 +316,6 @@ __global__ void k_soa_to_records(const float4* __restrict__ pd, const float4* __
     r[0] = make_float4(p.w, __uint_as_float(m.local), __uint_as_float(sk == kInvalid ? sk : sk - m.solid_base), 0.0f);
     r[1] = make_float4(p.x, p.y, p.z, pos_w);
     r[2] = make_float4(v.x, v.y, v.z, 0.0f);
-}
-
-__global__ void k_index_solids(const uint32_t* __restrict__ sid, uint32_t n, uint32_t* __restrict__ slot_of) {
-    uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
-    if (k >= n) return;
-    const uint32_t s = sid[k];
-    if (s != kInvalid) slot_of[s] = k;
 }
 
 __device__ __forceinline__ bool within_h_exact(float4 q, float4 p, float h2) {
@@ -439,10 +441,11 @@ int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* 
 
 int gather_state(const uint32_t* perm, uint32_t n, const float4* pd_in, float4* pd_out, const float4* vm_in,
                  float4* vm_out, const uint32_t* a_in, uint32_t* a_out, const uint32_t* b_in, uint32_t* b_out,
-                 const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st) {
+                 const uint2* c_in, uint2* c_out, float* ps_out, const DevMat* mats, cudaStream_t st,
+                 const SolidScatter& sol) {
     if (n == 0) return 0;
     k_gather_state<<<blocks_for(n, kThreads), kThreads, 0, st>>>(perm, n, pd_in, pd_out, vm_in, vm_out, a_in, a_out,
-                                                                 b_in, b_out, c_in, c_out, ps_out, mats);
+                                                                 b_in, b_out, c_in, c_out, ps_out, mats, sol);
     return 1;
 }
 
@@ -464,12 +467,6 @@ int soa_to_records(const float4* pd, const float4* vm, const uint32_t* orig, con
                    float pos_w, const DevMat* mats, arp_particle* out, cudaStream_t st) {
     if (n == 0) return 0;
     k_soa_to_records<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pd, vm, orig, sid, n, pos_w, mats, out);
-    return 1;
-}
-
-int index_solids(const uint32_t* sid, uint32_t n, uint32_t* slot_of, cudaStream_t st) {
-    if (n == 0) return 0;
-    k_index_solids<<<blocks_for(n, kThreads), kThreads, 0, st>>>(sid, n, slot_of);
     return 1;
 }
 

@@ -251,7 +251,7 @@ struct arp_sim {
     // grid scratch
     GridBuffers gb{};
     DevBuf<uint32_t> g_key, g_rank, g_count, g_start, g_perm, g_bsums;
-    DevBuf<uint2> g_coord, coord_s;  // grid coordinates per slot; storage-order copy for stage 0
+    DevBuf<uint2> g_coord;  // grid coordinates per slot
     DevBuf<uint32_t> contact_bound;
     DevBuf<uint32_t> tile_counter;  // work queue of the persistent fluid kernel
     DevBuf<uint32_t> overflow, overflow_count;  // the fluid kernel's two overflow queues (2n entries, 2 counts)
@@ -635,13 +635,21 @@ arp_status do_step(arp_sim* S) {
     arp_sim::Mark mk{};
     mark(S, mk, 0);
     S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
+    // the stage-0 solid copies and the solid -> slot map come out of the same gather
+    SolidScatter sol0;
+    if (ns) {
+        sol0.sid_of_slot = S->sid.p;
+        sol0.coord_of_slot = S->gb.coord;
+        sol0.sx = S->sx.p;
+        sol0.sv = S->sv.p;
+        sol0.sc = S->sc.p;
+        sol0.slot_of = S->slot_of.p;
+    }
     S->launches += gather_state(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
-                                S->orig_r.p, S->sid.p, S->sid_r.p, sb ? S->gb.coord : nullptr,
-                                sb ? S->coord_s.p : nullptr, S->ps.p, S->d_mats.p, st);
+                                S->orig_r.p, S->sid.p, S->sid_r.p, nullptr, nullptr, S->ps.p, S->d_mats.p, st, sol0);
     std::swap(S->Y, S->T);
     std::swap(S->orig, S->orig_r);
     std::swap(S->sid, S->sid_r);
-    if (ns) S->launches += index_solids(S->sid.p, n, S->slot_of.p, st);
     if (R) {
         CUDA_TRY(keep(R->orig, (const uint32_t*)S->orig.p, n, st));
         CUDA_TRY(keep(R->sid, (const uint32_t*)S->sid.p, n, st));
@@ -690,9 +698,17 @@ arp_status do_step(arp_sim* S) {
             if (S->profiling && s > 0) mark(S, mk, 0);
             l0 = S->launches;
             S->launches += build_grid(cur_pd, cur_vm, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
+            SolidScatter sol;  // this stage's solid copies
+            if (sb && ns) {
+                sol.sid_of_slot = S->sid.p;
+                sol.coord_of_slot = S->gb.coord;
+                sol.sx = S->sx.p;
+                sol.sv = S->sv.p;
+                sol.sc = S->sc.p;
+            }
             S->launches += gather_state(S->gb.perm, n, cur_pd, S->X.pd.p, cur_vm, S->X.vm.p, sb ? S->sid.p : nullptr,
                                         sb ? S->sid_sorted.p : nullptr, nullptr, nullptr, nullptr, nullptr, S->ps.p,
-                                        S->d_mats.p, st);
+                                        S->d_mats.p, st, sol);
             nl += S->launches - l0;
         }
         const float4* xs = s == 0 ? S->Y.pd.p : S->X.pd.p;
@@ -713,9 +729,6 @@ arp_status do_step(arp_sim* S) {
         uint64_t sl = 0;
         if (sb) {
             SolidArgs a{};
-            a.pd = cur_pd;
-            a.vm = cur_vm;
-            a.slot_of = S->slot_of.p;
             a.ref = S->ref.p;
             a.L = S->L.p;
             a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz};
@@ -730,7 +743,6 @@ arp_status do_step(arp_sim* S) {
             a.F = S->F.p;
             a.A = S->A.p;
             a.ksol = S->ksol.p;
-            a.coord = s == 0 ? S->coord_s.p : S->gb.coord;  // storage-order coordinates of this stage's grid
             a.contact_bound = S->contact_bound.p;
             a.xs = xs;
             a.vs = vs;
@@ -1012,7 +1024,6 @@ arp_status allocate(arp_sim* S) {
     CUDA_TRY(S->F.alloc(3 * ns));
     CUDA_TRY(S->A.alloc(3 * ns));
     CUDA_TRY(S->ksol.alloc(ns));
-    CUDA_TRY(S->coord_s.alloc(S->solid_branch() ? n : 1));
     CUDA_TRY(S->contact_bound.alloc(2));
     CUDA_TRY(S->tile_counter.alloc(1));
     CUDA_TRY(S->overflow.alloc(2 * n));  // two queues of n entries

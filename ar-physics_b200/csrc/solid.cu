@@ -205,20 +205,6 @@ __device__ __forceinline__ float4 add4(float4 a, float4 b) {
     return make_float4(__fadd_rn(a.x, b.x), __fadd_rn(a.y, b.y), __fadd_rn(a.z, b.z), __fadd_rn(a.w, b.w));
 }
 
-// The stage state of every solid in solid-id order (position, velocity, cell
-// coordinates), so that the per-neighbor reads of the two solid kernels are
-// direct and local: reference neighbors have nearby solid ids.
-__global__ void k_solid_gather(const float4* __restrict__ pd, const float4* __restrict__ vm,
-                               const uint2* __restrict__ coord, const uint32_t* __restrict__ slot_of, uint32_t ns,
-                               float4* __restrict__ sx, float4* __restrict__ sv, uint2* __restrict__ sc) {
-    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
-    if (i >= ns) return;
-    const uint32_t slot = slot_of[i];
-    sx[i] = pd[slot];
-    sv[i] = vm[slot];
-    sc[i] = coord[slot];
-}
-
 // ORDER2: every solid material uses strain order 2 (Green-Lagrange), so the
 // log-series, square-root and inverse paths are compiled out.
 // PLASTIC: some solid material is plastic; otherwise the plastic strain is
@@ -515,7 +501,7 @@ int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st) {
     if (a.ns == 0) return 0;
     cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
-    k_solid_gather<<<blocks_for(a.ns, 256), 256, 0, st>>>(a.pd, a.vm, a.coord, a.slot_of, a.ns, a.sx, a.sv, a.sc);
+    // a.sx, a.sv, a.sc were written by the stage's gather (gather_state)
     constexpr int L = kSolidLanes;
     const uint32_t blocks = blocks_for(a.ns * L, kThreads);
     if (a.all_order2 && !a.any_plastic) k_solid_stress<true, false, L><<<blocks, kThreads, 0, st>>>(a, T, c);
@@ -523,7 +509,7 @@ int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaS
     else if (!a.any_plastic) k_solid_stress<false, false, L><<<blocks, kThreads, 0, st>>>(a, T, c);
     else k_solid_stress<false, true, L><<<blocks, kThreads, 0, st>>>(a, T, c);
     k_solid_forces<L><<<blocks, kThreads, 0, st>>>(a, T);
-    return 3;
+    return 2;
 }
 
 }  // namespace arp
