@@ -170,8 +170,16 @@ struct GridBuffers {
 // cell.  Returns the number of kernel launches issued.
 // The scene of item i is mats[material].scene, the material read from
 // vm[i].w (bits) when vm is given, else from mat_u32[i].
+// Counters a stage's later kernels start from zero (the fluid kernel's
+// overflow counts and tile counter, the self-contact gate): the grid build's
+// first kernel clears them, which saves a memset per counter per stage.
+struct StageCounters {
+    uint32_t* p[3] = {nullptr, nullptr, nullptr};
+    uint32_t n[3] = {0, 0, 0};  // words at each pointer (at most 2)
+};
 int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uint32_t n, const Tables& T,
-               GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st);
+               GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st,
+               const StageCounters& zero = StageCounters{});
 
 // Exclusive scan of `len` counts into out (len entries); clears `count`.
 int exclusive_scan(uint32_t* count, uint32_t len, uint32_t* out, uint32_t* block_sums, cudaStream_t st);
@@ -242,6 +250,7 @@ struct FluidArgs {
     uint32_t n;
     int solid_branch;
     int any_stiff_immobile;
+    int counters_cleared;  // the stage's grid build cleared overflow_count and the tile counter
 };
 // Launch shapes of the fluid kernel the autotuner chooses between: threads
 // per block, hit-list capacity, one tile per block or persistent blocks
@@ -304,6 +313,7 @@ struct SolidArgs {
     uint32_t ns;
     int all_order2;           // every solid material has strain_order 2
     int any_plastic;          // some solid material is plastic; otherwise the plastic strain stays zero
+    int counters_cleared;     // the stage's grid build cleared contact_bound
 };
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st);
 

@@ -537,7 +537,7 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
                              cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
     }
     const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
-    cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
+    if (!a.counters_cleared) cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
     if (!persistent) {
         FluidKernels<DIM, BLOCK, CAP, MODE>::tile<<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
     } else {
@@ -549,7 +549,7 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
         int dev = 0;
         if (cudaGetDevice(&dev) == cudaSuccess) cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
         const uint32_t blocks = std::min<uint32_t>(ntiles, (uint32_t)(sms * per_sm));
-        cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
+        if (!a.counters_cleared) cudaMemsetAsync(tile_counter, 0, sizeof(uint32_t), st);
         FluidKernels<DIM, BLOCK, CAP, MODE>::persistent<<<blocks, BLOCK, smem, st>>>(a, T, c, b, tile_counter);
     }
     // the overflow queues: grids of at most 1184 blocks striding over the

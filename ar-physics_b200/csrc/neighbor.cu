@@ -39,8 +39,10 @@ __device__ __forceinline__ uint32_t scene_of(const float4* vm, const uint32_t* m
 __global__ void k_cell_keys(const float4* __restrict__ pos, const float4* __restrict__ vm,
                             const uint32_t* __restrict__ mat_u32, uint32_t n, Tables T, uint32_t* __restrict__ key,
                             uint32_t* __restrict__ rank, uint32_t* __restrict__ count, uint2* __restrict__ coord,
-                            DevStats* stats) {
+                            DevStats* stats, StageCounters zero) {
     uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < 3 && zero.p[i])
+        for (uint32_t q = 0; q < zero.n[i]; ++q) zero.p[i][q] = 0u;
     if (i >= n) return;
     float4 p = pos[i];
     uint32_t k;
@@ -127,28 +129,32 @@ __global__ void k_scan_tiles(uint32_t* count, uint32_t len, uint32_t* out, uint3
     if (threadIdx.x == 0) block_sums[blockIdx.x] = last_total;
 }
 
-// One block: exclusive scan of the tile totals in chunks, carrying the sum.
-__global__ void k_scan_sums(uint32_t* __restrict__ sums, uint32_t nb) {
-    __shared__ uint32_t carry;
-    if (threadIdx.x == 0) carry = 0;
+// Adds to each tile of the scan the sum of the totals of the tiles before it;
+// each block (one tile of kScanTile items) sums those totals itself, a block
+// reduction over at most a few hundred values, so no separate pass scans them.
+__global__ void k_scan_add(uint32_t* out, uint32_t len, const uint32_t* __restrict__ sums) {
+    __shared__ uint32_t warp_part[kScanThreads / 32];
+    __shared__ uint32_t prefix;
+    uint32_t part = 0;
+    for (uint32_t t = threadIdx.x; t < blockIdx.x; t += blockDim.x) part += sums[t];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) part += __shfl_xor_sync(0xffffffffu, part, o);
+    if ((threadIdx.x & 31) == 0) warp_part[threadIdx.x >> 5] = part;
     __syncthreads();
-    for (uint32_t base = 0; base < nb; base += blockDim.x) {
-        uint32_t idx = base + threadIdx.x;
-        uint32_t v = idx < nb ? sums[idx] : 0u;
-        uint32_t excl;
-        block_excl_scan(v, excl);
-        __shared__ uint32_t chunk_total;
-        if (threadIdx.x == blockDim.x - 1) chunk_total = excl + v;
-        if (idx < nb) sums[idx] = carry + excl;
-        __syncthreads();
-        if (threadIdx.x == 0) carry += chunk_total;
-        __syncthreads();
+    if (threadIdx.x == 0) {
+        uint32_t p = 0;
+        for (uint32_t w = 0; w < blockDim.x / 32; ++w) p += warp_part[w];
+        prefix = p;
     }
-}
-
-__global__ void k_scan_add(uint32_t* __restrict__ out, uint32_t len, const uint32_t* __restrict__ sums) {
-    const uint32_t idx = blockIdx.x * blockDim.x + threadIdx.x;
-    if (idx < len) out[idx] += sums[idx / kScanTile];
+    __syncthreads();
+    const uint32_t add = prefix;
+    if (add == 0u) return;
+    const uint32_t base = blockIdx.x * kScanTile;
+#pragma unroll
+    for (int j = 0; j < kScanItems; ++j) {
+        const uint32_t idx = base + (uint32_t)j * blockDim.x + threadIdx.x;
+        if (idx < len) out[idx] += add;
+    }
 }
 
 __global__ void k_scatter(const uint32_t* __restrict__ key, const uint32_t* __restrict__ rank, uint32_t n,
@@ -399,13 +405,15 @@ cudaError_t noalloc_scratch(uint32_t** out) {
 }  // namespace
 
 int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uint32_t n, const Tables& T,
-               GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st) {
+               GridBuffers& gb, DevStats* stats, const uint32_t* boundary_start, cudaStream_t st,
+               const StageCounters& zero) {
     int launches = 0;
     if (n > 0) {
         // a single scene needs no material to find the scene: skip that read
         const bool one = T.nscenes == 1;
         k_cell_keys<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, one ? nullptr : vm, one ? nullptr : mat_u32, n,
-                                                                  T, gb.key, gb.rank, gb.count, gb.coord, stats);
+                                                                  T, gb.key, gb.rank, gb.count, gb.coord, stats,
+                                                                  zero);
         ++launches;
     }
     // cells, the non-finite bucket, and the total
@@ -425,9 +433,8 @@ uint32_t scan_block_sums_needed(uint32_t len) { return blocks_for(len, kScanTile
 int exclusive_scan(uint32_t* count, uint32_t len, uint32_t* out, uint32_t* block_sums, cudaStream_t st) {
     const uint32_t tiles = blocks_for(len, kScanTile);
     k_scan_tiles<<<tiles, kScanThreads, 0, st>>>(count, len, out, block_sums);
-    k_scan_sums<<<1, kScanThreads, 0, st>>>(block_sums, tiles);
-    k_scan_add<<<blocks_for(len, kThreads), kThreads, 0, st>>>(out, len, block_sums);
-    return 3;
+    k_scan_add<<<tiles, kScanThreads, 0, st>>>(out, len, block_sums);
+    return 2;
 }
 
 int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* a_out, const float4* b_in,

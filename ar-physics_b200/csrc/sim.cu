@@ -634,7 +634,17 @@ arp_status do_step(arp_sim* S) {
     // 1. sort y0 into cell order
     arp_sim::Mark mk{};
     mark(S, mk, 0);
-    S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
+    // each stage's grid build clears the counters the stage's kernels start from
+    StageCounters zero;
+    zero.p[0] = S->overflow_count.p;
+    zero.n[0] = 2;
+    zero.p[1] = S->tile_counter.p;
+    zero.n[1] = 1;
+    if (sb) {
+        zero.p[2] = S->contact_bound.p;
+        zero.n[2] = 2;
+    }
+    S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st, zero);
     // the stage-0 solid copies and the solid -> slot map come out of the same gather
     SolidScatter sol0;
     if (ns) {
@@ -697,7 +707,7 @@ arp_status do_step(arp_sim* S) {
         if (s > 0) {
             if (S->profiling && s > 0) mark(S, mk, 0);
             l0 = S->launches;
-            S->launches += build_grid(cur_pd, cur_vm, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st);
+            S->launches += build_grid(cur_pd, cur_vm, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st, zero);
             SolidScatter sol;  // this stage's solid copies
             if (sb && ns) {
                 sol.sid_of_slot = S->sid.p;
@@ -744,6 +754,7 @@ arp_status do_step(arp_sim* S) {
             a.A = S->A.p;
             a.ksol = S->ksol.p;
             a.contact_bound = S->contact_bound.p;
+            a.counters_cleared = n > 0 ? 1 : 0;
             a.xs = xs;
             a.vs = vs;
             a.start = S->gb.start;
@@ -787,6 +798,7 @@ arp_status do_step(arp_sim* S) {
         f.solid_branch = sb ? 1 : 0;
         f.overflow = S->overflow.p;
         f.overflow_count = S->overflow_count.p;
+        f.counters_cleared = 1;  // by this stage's grid build
         f.any_stiff_immobile = S->any_stiff_immobile ? 1 : 0;
         B.next_pd = next_pd;
         B.next_vm = next_vm;

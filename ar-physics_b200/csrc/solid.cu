@@ -500,7 +500,7 @@ int ref_lists_fill(const float4* ref, const uint32_t* mat_of, uint32_t ns, const
 
 int launch_solid(const SolidArgs& a, const Tables& T, const StageCoefs& c, cudaStream_t st) {
     if (a.ns == 0) return 0;
-    cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
+    if (!a.counters_cleared) cudaMemsetAsync(a.contact_bound, 0, 2 * sizeof(uint32_t), st);
     // a.sx, a.sv, a.sc were written by the stage's gather (gather_state)
     constexpr int L = kSolidLanes;
     const uint32_t blocks = blocks_for(a.ns * L, kThreads);
