@@ -99,6 +99,8 @@ def test_single_step_graphs_match_plain_steps():
     b = FluidSim(sc)
     b.init()
     b.set_graph(True)
+    # launches counted from here: only the first handle of a scene shape runs the autotuner at init
+    la, lb = a.launch_count(), b.launch_count()
     for k in (1, 1, 3, 2, 1):
         a.step(k)
         b.step(k)
@@ -112,7 +114,7 @@ def test_single_step_graphs_match_plain_steps():
     b.profile_enable(False)
     assert a.particles().tobytes() == b.particles().tobytes()
     assert a.solids().tobytes() == b.solids().tobytes()
-    assert a.launch_count() == b.launch_count()
+    assert a.launch_count() - la == b.launch_count() - lb
 
 
 def test_fluid_launch_shapes_give_identical_results():
