@@ -33,6 +33,13 @@ constexpr int kMaxMaterials = 32;  // per scene
 #define ARP_SEARCH_HALVE 1
 #endif
 constexpr uint32_t kSearchHalve = ARP_SEARCH_HALVE;
+// A scene whose particles have at least this many neighbors within h,
+// estimated as (h / spacing)^dim, also halves y: its rows of 5 x 5 half
+// cells hold ~40 % fewer candidates than 5 x 3, which outweighs the grid's
+// four times as many cells (the batched workload: 23.0 k -> 25.8 k scene
+// steps/s with every scene halved so; the 1M workload, (h/s)^3 = 8, loses 4 %
+// that way and keeps x alone).
+constexpr double kDenseNeighbors = 10.0;
 
 // Uniform grid of NeighborList::new (neighbor_list.rs:199-217), one scene.
 struct Grid {
@@ -68,8 +75,8 @@ struct DevInter {
 // Two grids cover the scene's box.  `grid` is the reference's (cells of at
 // least h); the hourglass and self-contact stencils, the cell statistics and
 // the cell queries of the C ABI use it.  `sgrid`, the search grid, halves the
-// cells along the axes of kSearchHalve that have non-zero extent (sub
-// doubled), so along such an axis a sphere of radius h spans at most 5 cells
+// cells along the axes of kSearchHalve that have non-zero extent, and along y
+// too in a dense scene (kDenseNeighbors) (sub doubled), so along such an axis a sphere of radius h spans at most 5 cells
 // of width h/2 instead of 3 of width h; particles are sorted by search cell,
 // and the search cells of one reference cell c are 2c and 2c+1 along each
 // halved axis.  Because 2 * (t * sub) is rounded exactly like t * (2 sub),

@@ -281,19 +281,22 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
         // that the warp can vote before each row; the pass after the last row
         // only evaluates what is left (one call site of the pair math keeps
         // the registers down).
-        constexpr int RX = 1 + (int)(kSearchHalve & 1u), RY = 1 + (int)(kSearchHalve >> 1 & 1u),
-                      RZ = 1 + (int)(kSearchHalve >> 2 & 1u);
+        // (y reach: 2 rows for every lane, as dense scenes halve y; a lane
+        // whose scene does not skips the outer two as empty)
+        constexpr int RY = 2, RZ = 1 + (int)(kSearchHalve >> 2 & 1u);
         constexpr int NY = 2 * RY + 1, NZ = DIM == 3 ? 2 * RZ + 1 : 1;
         const bool fin = finite3(xi);
         const Grid& g = P.sgrid;
         const CellCoord cc = fin ? cell_coord(xi, g) : CellCoord{0, 0, 0};
-        const int x0 = max(cc.x - RX, 0), x1 = min(cc.x + RX, (int)g.sub[0] - 1);
+        const int rx = 1 + (int)P.halved[0], ry = 1 + (int)P.halved[1];
+        const int x0 = max(cc.x - rx, 0), x1 = min(cc.x + rx, (int)g.sub[0] - 1);
         for (int r = 0;; ++r) {
             const bool last = r == NY * NZ;
-            const int y = cc.y - RY + r % NY;
+            const int dy = r % NY - RY;
+            const int y = cc.y + dy;
             const int z = DIM == 3 ? cc.z - RZ + r / NY : cc.z;
             uint32_t bb = 0, be = 0, jb = 0, je = 0;
-            if (!last && fin && y >= 0 && y < (int)g.sub[1] && z >= 0 && z < (int)g.sub[2]) {
+            if (!last && fin && abs(dy) <= ry && y >= 0 && y < (int)g.sub[1] && z >= 0 && z < (int)g.sub[2]) {
                 const uint32_t row = P.cell_base + (uint32_t)y * g.sub[0] + (uint32_t)z * g.sub[0] * g.sub[1];
                 const uint32_t c0 = row + (uint32_t)x0, c1 = row + (uint32_t)x1 + 1u;
                 bb = a.bstart[c0];

@@ -194,6 +194,7 @@ struct arp_sim {
                                   // placeholder solid entry 0 (particles.rs:502), so solids added
                                   // later are numbered from 1 and count one more
         bool flat_z;              // every particle shares one z and moves in the plane
+        bool dense = false;       // the search grid halves y as well as x (see scene_params)
         arp_aabb bounds;
         float h, gravity, alpha;
         SceneP sp;
@@ -413,7 +414,8 @@ arp_status scene_params(arp_sim::SceneHost& H, uint32_t dim) {
     P.sgrid = P.grid;
     uint64_t snc = 1;
     for (int a = 0; a < 3; ++a) {
-        P.halved[a] = H.bounds.dim[a] != 0.0f && (kSearchHalve >> a & 1u) ? 1u : 0u;
+        const bool halve = (kSearchHalve >> a & 1u) || (a == 1 && H.dense);
+        P.halved[a] = H.bounds.dim[a] != 0.0f && halve ? 1u : 0u;
         P.sgrid.sub[a] = P.grid.sub[a] << P.halved[a];
         snc *= P.sgrid.sub[a];
     }
@@ -947,6 +949,16 @@ arp_status append_scene(const arp_scene* sc, arp_sim* S) {
             block[size_t(j) * M + i] = x;
         }
     S->inter.insert(S->inter.end(), block.begin(), block.end());
+    // particles within h of a particle, ~ (h / s)^dim with s = (m / rho0)^(1/dim) the mean spacing
+    if (sc->n_particles > 0 && dim > 0) {
+        double vol = 0.0;
+        for (uint32_t i = 0; i < sc->n_particles; ++i) {
+            const arp_material& m = mats[sc->particles[i].mat];
+            vol += m.start_den > 0.0f ? (double)m.mass / (double)m.start_den : 0.0;
+        }
+        const double s = std::pow(vol / sc->n_particles, 1.0 / dim);
+        H.dense = s > 0.0 && std::pow((double)H.h / s, (double)dim) >= kDenseNeighbors;
+    }
     ARP_TRY(scene_params(H, dim));
     if ((uint64_t)S->ncells + H.sp.sgrid.ncells + 2 > (1ull << 31))
         return fail(ARP_ERR_UNSUPPORTED, "the batch's grids have more than 2^31 cells");
