@@ -204,16 +204,19 @@ enum FluidMode {
                    // could fill up in it and then evaluates and empties every
                    // list; a row alone above CAP queues the particle for
                    // kDirect (second overflow queue)
-    kDirect = 2,   // every hit evaluated during the scan
+    kDirect = 2,   // every hit evaluated during the scan (a row above even the
+                   // second queue's list)
 };
 
 // Fluid forces and the stage update of sorted particle k.  `lst` is the
 // thread's column of the hit list ([CAP][BLOCK]); `sm`/`si` hold the
 // tables of scene `scene0`.  A particle handed to an overflow queue writes
 // nothing here.  `wmask` (kFlush): the lanes of this warp that run
-// fluid_particle, all of which take part in the per-row vote.
-template <int DIM, int BLOCK, int CAP, int MODE>
-__device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, const Tables& T, const StageCoefs& c,
+// fluid_particle, all of which take part in the per-row vote.  QUEUE false
+// (kFlush): a particle whose row holds more than CAP hits is not queued; the
+// call returns false, having written nothing, and the caller finishes it.
+template <int DIM, int BLOCK, int CAP, int MODE, bool QUEUE = true>
+__device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, const Tables& T, const StageCoefs& c,
                                                const StageBuffers& b, uint32_t* lst, const FluidMat* sm,
                                                const DevInter* si, uint32_t scene0, unsigned wmask) {
     const float4 xi = a.xs[k];
@@ -314,8 +317,9 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
                 if (hit(a.xs[j])) take(j);
         }
         if (full) {
+            if (!QUEUE) return false;
             a.overflow[a.n + atomicAdd(a.overflow_count + 1, 1u)] = k;
-            return;
+            return true;
         }
     } else if (finite3(xi)) {
         for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
@@ -339,7 +343,7 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
         if (MODE == kTwoPass) {
             if (full) {
                 a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
-                return;
+                return true;
             }
             flush();  // pass 2
         }
@@ -406,6 +410,7 @@ __device__ __forceinline__ void fluid_particle(uint32_t k, const FluidArgs& a, c
         b.next_pd[slot] = comb(y0p, tp, false);
         b.next_vm[slot] = comb(y0v, tv, true);
     }
+    return true;
 }
 
 // The flush form keeps the row loop's state live around the pair math; left
@@ -518,14 +523,26 @@ __global__ void __launch_bounds__(128, kFlushMinBlocks) k_fluid_overflow_flush(F
     }
 }
 
-// Second overflow queue: particles with more than kFlushCap hits in one row,
-// one thread each, evaluating their pairs during the scan.
+// Second overflow queue: particles with more hits in one row than the list
+// that queued them holds.  The same flushing scan with lists of kWideCap
+// entries (64 threads per block, 40 KB of shared memory); a particle with
+// even more hits in one row is finished by its own thread evaluating its
+// pairs during the scan.
+constexpr int kWideCap = 160;
 template <int DIM>
-__global__ void __launch_bounds__(128) k_fluid_overflow(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+__global__ void __launch_bounds__(64) k_fluid_overflow(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    __shared__ uint32_t lst[kWideCap * 64];
     const uint32_t cnt = a.overflow_count[1];
-    for (uint32_t i = blockIdx.x * 128u + threadIdx.x; i < cnt; i += gridDim.x * 128u)
-        fluid_particle<DIM, 128, 1, kDirect>(a.overflow[a.n + i], a, T, c, b, nullptr, nullptr, nullptr, kInvalid,
-                                             0u);
+    for (uint32_t i0 = blockIdx.x * 64u; i0 < cnt; i0 += gridDim.x * 64u) {  // uniform per block
+        const uint32_t i = i0 + threadIdx.x;
+        const unsigned wmask = __ballot_sync(0xFFFFFFFFu, i < cnt);  // lanes with a particle
+        if (i < cnt) {
+            const uint32_t k = a.overflow[a.n + i];
+            if (!fluid_particle<DIM, 64, kWideCap, kFlush, false>(k, a, T, c, b, lst + threadIdx.x, nullptr,
+                                                                   nullptr, kInvalid, wmask))
+                fluid_particle<DIM, 64, 1, kDirect>(k, a, T, c, b, nullptr, nullptr, nullptr, kInvalid, 0u);
+        }
+    }
 }
 
 template <int DIM, int BLOCK, int CAP, int MODE>
@@ -559,7 +576,7 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
     // queue, which usually is empty
     const uint32_t oblocks = std::min<uint32_t>(ntiles * BLOCK / 128u + 1u, 1184u);
     k_fluid_overflow_flush<DIM><<<oblocks, 128, 0, st>>>(a, T, c, b);
-    k_fluid_overflow<DIM><<<oblocks, 128, 0, st>>>(a, T, c, b);
+    k_fluid_overflow<DIM><<<2u * oblocks, 64, 0, st>>>(a, T, c, b);
 }
 
 }  // namespace

@@ -156,9 +156,10 @@ def test_batched_workload_sample_matches_the_oracle():
 
 
 def dense_block(h_over_s=4.5, n=10, spacing=0.01):
-    """A Tait fluid block whose kernel radius spans 4.5 particle spacings:
-    ~380 neighbors per particle, more than any hit list holds, and more than
-    64 of them inside one search row for the central particles."""
+    """A Tait fluid block whose kernel radius spans `h_over_s` particle
+    spacings: at 4.5, ~380 neighbors per particle, more than any hit list
+    holds, and more than 64 of them inside one search row for the central
+    particles; at 6.5, more than 160 in one row."""
     s = spacing
     h = h_over_s * s
     pos = scenes.lattice((0.1 + 0.5 * s,) * 3, (n, n, n), s)
@@ -173,12 +174,13 @@ def dense_block(h_over_s=4.5, n=10, spacing=0.01):
                         integrator="midpoint", dt=2e-5, gravity=9.81, name="dense_block")
 
 
-def test_dense_scene_through_both_overflow_queues():
-    """Most hit lists overflow (first queue, evaluated with list flushes)
-    and some particles have more than 64 hits in one search row (second
-    queue, evaluated during the scan); all 10 launch shapes give the same
-    bits and the oracle's result."""
-    sc = dense_block()
+@pytest.mark.parametrize("h_over_s,row_hits_above", [(4.5, 64), (6.5, 160)])
+def test_dense_scene_through_the_overflow_queues(h_over_s, row_hits_above):
+    """Most hit lists overflow (first queue, evaluated with list flushes);
+    some particles have more hits in one search row than 64 (second queue,
+    flushing lists of 160) or than 160 (evaluated during the scan); all 10
+    launch shapes give the same bits and the oracle's result."""
+    sc = dense_block(h_over_s=h_over_s)
     pos = sc.particles["pos"][:, :3].astype(np.float64)
     d2 = ((pos[:, None, :] - pos[None, :, :]) ** 2).sum(-1)
     within = (d2 < np.float32(sc.h) ** 2) & ~np.eye(sc.n, dtype=bool)
@@ -188,7 +190,7 @@ def test_dense_scene_through_both_overflow_queues():
     cell = np.floor(pos / 0.3 * np.array([2 * sub, 2 * sub, sub])).astype(int)
     row_hits = max(int((within[i] & (cell[:, 1] == cell[i, 1]) & (cell[:, 2] == cell[i, 2])).sum())
                    for i in range(sc.n))
-    assert row_hits > 64  # some particle's row alone overfills the flush list
+    assert row_hits > row_hits_above  # some particle's row alone overfills that list
     ref = None
     for v in range(10):
         sim = FluidSim(sc)
