@@ -8,7 +8,7 @@ the AABB, kernel radius, integrator, time step, subticks and gravity.
 Material constructors follow src/soft_body/material_region/material.rs:61-121
 and the TOML mapping of examples/test_mods/config.rs:351-391 (bulk_visc =
 alpha * h * c, state equation inferred from the keys given).  Masses follow
-the reference's rule (material_region/mod.rs:316-323): start density times
+the reference's rule (material_region/mod.rs:144-149): start density times
 the lattice cell volume.
 
 The benchmark workloads are the five configurations the benchmark is quoted

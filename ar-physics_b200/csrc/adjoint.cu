@@ -125,7 +125,7 @@ __device__ __forceinline__ float3 mask_dim(float3 v, uint32_t dim) {
     return make_float3(v.x, dim >= 2 ? v.y : 0.0f, dim >= 3 ? v.z : 0.0f);
 }
 
-// p / rho^2 of a state equation (fluid.rs:131-138) and its derivative in rho
+// p / rho^2 of a state equation (fluid.rs:45-52) and its derivative in rho
 __device__ __forceinline__ void eos_pt(uint32_t eq, float rho, float c, float d0, float& pt, float& dpt) {
     float p = 0.0f, dp = 0.0f;
     if (eq == ARP_EOS_CONSTANT) {

@@ -198,7 +198,7 @@ int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* 
                   float4* b_out, const uint32_t* c_in, uint32_t* c_out, const uint32_t* d_in, uint32_t* d_out,
                   cudaStream_t st);
 // Gather a state into sorted order (out[k] = in[perm[k]]) and evaluate the
-// pressure term p / rho^2 of every gathered particle (fluid.rs:131-138,
+// pressure term p / rho^2 of every gathered particle (fluid.rs:45-52,
 // :270-271).  Any pointer pair may be null.
 // Solid-order copies a gather writes on the side: for a gathered particle
 // whose solid id (sid_of_slot at its source slot) is valid, sx/sv/sc[sid] =

@@ -1,7 +1,7 @@
 // fluid.cu -- fluid forces with the Runge-Kutta stage update fused at the tail.
 //
 // Replaces the reference's `fluid_forces` shader (src/soft_body/shaders/
-// fluid.rs:95-336) and the lin_comb stage arithmetic that follows it
+// fluid.rs:95-251) and the lin_comb stage arithmetic that follows it
 // (src/soft_body/particle_state/particles.rs:8-154).  The shader runs one
 // 81-invocation workgroup per particle (27 cells x 3 strided lanes) with a
 // shared-memory tree reduction; here one thread owns one particle sorted by
@@ -36,7 +36,7 @@ __device__ __forceinline__ float pow7(float x) {
     return x6 * x;
 }
 
-// fluid.rs:140-153 (called with radius and strength in the shader's order)
+// fluid.rs:54-67 (called with radius and strength in the shader's order)
 __device__ __forceinline__ float contact_potential(uint32_t eq, float r, float strength, float r0) {
     switch (eq) {
         case ARP_CONTACT_CONSTANT: return r <= r0 ? strength : 0.0f;
@@ -101,7 +101,7 @@ __device__ __forceinline__ void pair(const Self& s, float4 xj, float4 vj, float 
             const float cs = m2.mass * cp / d2;
             const float cx = cs * gx, cy = cs * gy, cz = cs * gz;
             if ((s.elastic || elastic2 || BOUNDARY) && s.mat != mat2) {
-                // fluid.rs:278-285: friction along the normalised tangential velocity
+                // fluid.rs:192-199: friction along the normalised tangential velocity
                 const float ix = rx / r2, iy = ry / r2, iz = rz / r2;
                 const float cr = DIM == 3 ? (cx * rx + cy * ry) + cz * rz : cx * rx + cy * ry;
                 const float nx = ix * cr, ny = iy * cr, nz = iz * cr;
@@ -182,7 +182,7 @@ __device__ __forceinline__ void eval_hit(uint32_t j, const Self& s, const FluidA
         const uint32_t mat2 = __float_as_uint(vj.w);
         bool elastic2 = false;
         if (a.any_stiff_immobile && s.mt[mat2].stiff) {
-            // fluid.rs:227: the boundary index reads the mobile array's solid id
+            // fluid.rs:141: the boundary index reads the mobile array's solid id
             elastic2 = a.sid_of_boundary_index[a.borig[jb]] != kInvalid;
         }
         pair<DIM, true>(s, xj, vj, a.bps[jb], mat2, elastic2, K, acc);
@@ -349,7 +349,7 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
         }
     }
 
-    // derivative record (fluid.rs:329-333), plus the solid term when active
+    // derivative record (fluid.rs:243-247), plus the solid term when active
     float4 kpd = make_float4(vi.x, vi.y, vi.z, acc.den);
     float4 kvm = make_float4(__fdiv_rn(acc.f.x, s.d1), __fadd_rn(__fdiv_rn(acc.f.y, s.d1), -g_acc),
                              __fdiv_rn(acc.f.z, s.d1), 0.0f);

@@ -10,8 +10,10 @@
 //   2. exclusive scan of the histogram (warp-shuffle block scan, block sums,
 //      offsets), which also clears the histogram for the next build;
 //   3. scatter to perm[start[key] + rank];
-//   4. sort each cell's run by slot so the order is deterministic; this also
-//      records the largest occupancy and cells over the reference's 128.
+//   4. sort each cell's run by slot so the order is deterministic for every
+//      run length (short runs by one thread, long runs by the whole block);
+//      this also records the largest occupancy and cells over the
+//      reference's 128.
 // Memory traffic per particle: 16 B position read, 4+4 B key/rank write and
 // read, 4 B perm write, 4+4 B perm read/write in the run sort.
 #include <algorithm>
@@ -195,29 +197,111 @@ __device__ __forceinline__ uint32_t reference_cell_occupancy(uint32_t c, const u
     return occ;
 }
 
-// Sort each cell's run ascending (insertion sort; runs longer than 256 are
-// left in arrival order, which is still a valid grid).  With `stats`, also
-// the occupancy counters of the reference cells.
-__global__ void k_sort_runs(const uint32_t* __restrict__ start, uint32_t ncells, uint32_t* __restrict__ perm,
-                            const uint32_t* __restrict__ boundary_start, DevStats* stats, Tables T) {
-    uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
-    if (c > ncells) return;  // includes the non-finite bucket at index ncells
-    const uint32_t b = start[c], e = start[c + 1];
-    const uint32_t len = e - b;
-    if (stats && c < ncells) {
-        const uint32_t occ = reference_cell_occupancy(c, start, boundary_start, T);
-        if (occ > 0) atomicMax(&stats->max_cell_occupancy, occ);
-        if (occ > kBucketSlots) atomicAdd(&stats->overflow_cells, 1u);
+constexpr uint32_t kShortRun = 128;  // runs up to this length: insertion sort by their own thread
+
+// Block-wide reductions (blockDim.x == kThreads); every thread gets the result.
+template <class Op>
+__device__ __forceinline__ uint32_t block_reduce(uint32_t v, Op op) {
+    __shared__ uint32_t part[kThreads / 32];
+#pragma unroll
+    for (int o = 16; o > 0; o >>= 1) v = op(v, __shfl_xor_sync(0xffffffffu, v, o));
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = v;
+    __syncthreads();
+    uint32_t r = part[0];
+    for (int w = 1; w < kThreads / 32; ++w) r = op(r, part[w]);
+    __syncthreads();  // part[] is reused by the next call
+    return r;
+}
+
+// Sorts one long run perm[b, e) ascending with the whole block: stable
+// one-bit LSD radix passes over (v - min), ping-ponging through tmp[b, e).
+// The run's values are distinct slots, and a run of a cell-ordered state
+// spans few slots, so log2(max - min + 1) passes suffice.
+__device__ void block_sort_run(uint32_t* perm, uint32_t* tmp, uint32_t b, uint32_t e) {
+    __shared__ uint32_t chunk_zeros;
+    const uint32_t L = e - b;
+    uint32_t lo = 0xFFFFFFFFu, hi = 0u;
+    for (uint32_t i = threadIdx.x; i < L; i += kThreads) {
+        const uint32_t v = perm[b + i];
+        lo = min(lo, v);
+        hi = max(hi, v);
     }
-    if (len < 2 || len > 256) return;
-    for (uint32_t i = b + 1; i < e; ++i) {
-        uint32_t v = perm[i];
-        uint32_t j = i;
-        while (j > b && perm[j - 1] > v) {
-            perm[j] = perm[j - 1];
-            --j;
+    lo = block_reduce(lo, [](uint32_t x, uint32_t y) { return min(x, y); });
+    hi = block_reduce(hi, [](uint32_t x, uint32_t y) { return max(x, y); });
+    const uint32_t span = hi - lo;
+    const int bits = span ? 32 - __clz(span) : 0;
+    uint32_t* src = perm + b;
+    uint32_t* dst = tmp + b;
+    for (int bit = 0; bit < bits; ++bit) {
+        uint32_t z = 0;
+        for (uint32_t i = threadIdx.x; i < L; i += kThreads) z += (((src[i] - lo) >> bit) & 1u) ^ 1u;
+        z = block_reduce(z, [](uint32_t x, uint32_t y) { return x + y; });
+        uint32_t zbase = 0, obase = z;
+        for (uint32_t c0 = 0; c0 < L; c0 += kThreads) {
+            const uint32_t i = c0 + threadIdx.x;
+            const uint32_t v = i < L ? src[i] : 0u;
+            const uint32_t f = i < L ? ((((v - lo) >> bit) & 1u) ^ 1u) : 0u;
+            uint32_t excl;
+            block_excl_scan(f, excl);
+            if (threadIdx.x == kThreads - 1) chunk_zeros = excl + f;
+            __syncthreads();
+            const uint32_t cz = chunk_zeros;
+            if (i < L) dst[f ? zbase + excl : obase + (threadIdx.x - excl)] = v;
+            zbase += cz;
+            obase += min((uint32_t)kThreads, L - c0) - cz;
+            __syncthreads();  // chunk_zeros and the scan's shared totals are reused
         }
-        perm[j] = v;
+        __syncthreads();  // dst complete before the next pass reads it
+        uint32_t* t = src;
+        src = dst;
+        dst = t;
+    }
+    if (src != perm + b)
+        for (uint32_t i = threadIdx.x; i < L; i += kThreads) perm[b + i] = src[i];
+    __syncthreads();
+}
+
+// Sort each cell's run ascending, so the order inside a cell never depends
+// on the arrival order of the histogram's atomics: runs of at most kShortRun
+// by an insertion sort on their own thread, longer runs by the whole block
+// (block_sort_run, through the scratch `tmp`, free once the scatter has run).
+// With `stats`, also the occupancy counters of the reference cells.
+__global__ void __launch_bounds__(kThreads) k_sort_runs(const uint32_t* __restrict__ start, uint32_t ncells,
+                                                        uint32_t* __restrict__ perm, uint32_t* __restrict__ tmp,
+                                                        const uint32_t* __restrict__ boundary_start, DevStats* stats,
+                                                        Tables T) {
+    __shared__ uint32_t long_cells[kThreads];
+    __shared__ uint32_t nlong;
+    if (threadIdx.x == 0) nlong = 0;
+    __syncthreads();
+    const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
+    if (c <= ncells) {  // includes the non-finite bucket at index ncells
+        const uint32_t b = start[c], e = start[c + 1];
+        const uint32_t len = e - b;
+        if (stats && c < ncells) {
+            const uint32_t occ = reference_cell_occupancy(c, start, boundary_start, T);
+            if (occ > 0) atomicMax(&stats->max_cell_occupancy, occ);
+            if (occ > kBucketSlots) atomicAdd(&stats->overflow_cells, 1u);
+        }
+        if (len > kShortRun) {
+            long_cells[atomicAdd(&nlong, 1u)] = c;
+        } else if (len >= 2) {
+            for (uint32_t i = b + 1; i < e; ++i) {
+                uint32_t v = perm[i];
+                uint32_t j = i;
+                while (j > b && perm[j - 1] > v) {
+                    perm[j] = perm[j - 1];
+                    --j;
+                }
+                perm[j] = v;
+            }
+        }
+    }
+    __syncthreads();
+    const uint32_t cnt = nlong;
+    for (uint32_t q = 0; q < cnt; ++q) {
+        const uint32_t lc = long_cells[q];
+        block_sort_run(perm, tmp, start[lc], start[lc + 1]);
     }
 }
 
@@ -235,7 +319,7 @@ __global__ void k_gather(const uint32_t* __restrict__ perm, uint32_t n, const fl
 }
 
 __device__ __forceinline__ float eos_pressure(uint32_t eq, float density, float c, float d0) {
-    switch (eq) {  // fluid.rs:131-138, x^7 by products
+    switch (eq) {  // fluid.rs:45-52, x^7 by products
         case ARP_EOS_CONSTANT: return c * c;
         case ARP_EOS_IDEAL_GAS: return c * c * (density - d0);
         case ARP_EOS_TAIT: {
@@ -422,7 +506,7 @@ int build_grid(const float4* pos, const float4* vm, const uint32_t* mat_u32, uin
         k_scatter<<<blocks_for(n, kThreads), kThreads, 0, st>>>(gb.key, gb.rank, n, gb.start, gb.perm);
         ++launches;
     }
-    k_sort_runs<<<blocks_for(T.ncells + 1, kThreads), kThreads, 0, st>>>(gb.start, T.ncells, gb.perm,
+    k_sort_runs<<<blocks_for(T.ncells + 1, kThreads), kThreads, 0, st>>>(gb.start, T.ncells, gb.perm, gb.rank,
                                                                          boundary_start, stats, T);
     ++launches;
     return launches;
@@ -507,7 +591,12 @@ extern "C" arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, co
             return set_error(ARP_ERR_INVALID_ARG, "bounds must be finite with non-negative extent");
         g.min[a] = bounds->min[a];
         g.dim[a] = bounds->dim[a];
-        g.sub[a] = (uint32_t)std::max(1.0f, bounds->dim[a] / kernel_radius);  // neighbor_list.rs:201-206
+        // neighbor_list.rs:201-206; the quotient is range-checked in float
+        // before the conversion (a huge dim / h would not fit in 32 bits)
+        const float q = std::max(1.0f, bounds->dim[a] / kernel_radius);
+        if (!(q <= (float)kNoAllocMaxCells))
+            return set_error(ARP_ERR_CAPACITY, "arp_grid_build_noalloc: the grid exceeds the 4194302-cell maximum");
+        g.sub[a] = (uint32_t)q;
         nc *= g.sub[a];
     }
     if (nc > kNoAllocMaxCells)
@@ -529,8 +618,8 @@ extern "C" arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, co
     if (n > 0) k_rank_noalloc<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, g, cell_start, rank);
     exclusive_scan(cell_start, len, cell_start, tile_sums, st);  // in place: counts become starts
     if (n > 0) k_scatter_noalloc<<<blocks_for(n, kThreads), kThreads, 0, st>>>(pos, n, g, cell_start, rank, perm);
-    k_sort_runs<<<blocks_for(g.ncells + 1, kThreads), kThreads, 0, st>>>(cell_start, g.ncells, perm, nullptr, nullptr,
-                                                                         Tables{});
+    k_sort_runs<<<blocks_for(g.ncells + 1, kThreads), kThreads, 0, st>>>(cell_start, g.ncells, perm, rank, nullptr,
+                                                                         nullptr, Tables{});
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_error(ARP_ERR_CUDA, std::string("grid build launch: ") + cudaGetErrorString(e));
     return ARP_OK;

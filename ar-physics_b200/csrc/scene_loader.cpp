@@ -2,7 +2,7 @@
 //
 // Restates examples/test_mods/config.rs:62-474 (the schema and its defaults),
 // src/soft_body/material_region/region.rs:21-272 (AABB, AABE, Transformed,
-// Difference, Union, Intersection) and material_region/mod.rs:230-329
+// Difference, Union, Intersection) and material_region/mod.rs:56-155
 // (hex/HCP lattice seeding and the mass rule) on top of a small TOML reader.
 // Tables iterate in sorted key order as toml 0.5's BTreeMap does, which fixes
 // the material order: boundaries by name, then objects by name.  Arithmetic
@@ -904,7 +904,7 @@ RegionP parse_region_from_mat(const Table& t) {  // config.rs:242-252
     throw ParseError("material has no region table and no union, difference or intersection array");
 }
 
-// ---- seeding (material_region/mod.rs:230-329) --------------------------------
+// ---- seeding (material_region/mod.rs:56-155) --------------------------------
 
 struct Velocity {
     float vel[4] = {0, 0, 0, 0};

@@ -79,7 +79,7 @@ bool make_tableau(int id, Tableau& t) {
     }
 }
 
-// kernel.rs:280-286 and :335-338, in f32 as the Rust code evaluates them
+// kernel.rs:5-11 and :60-63, in f32 as the Rust code evaluates them
 float volume_nball_f32(uint32_t n, float r) {
     if (n == 0) return 1.0f;
     if (n == 1) return 2.0f * r;
@@ -393,7 +393,7 @@ void harvest_marks(arp_sim* S) {
     S->marks.clear();
 }
 
-// Scalars and grid of one scene (neighbor_list.rs:201-206, kernel.rs:335-338,
+// Scalars and grid of one scene (neighbor_list.rs:201-206, kernel.rs:60-63,
 // the shader constants of fluid.rs / solid.rs).
 arp_status scene_params(arp_sim::SceneHost& H, uint32_t dim) {
     SceneP& P = H.sp;
@@ -404,6 +404,9 @@ arp_status scene_params(arp_sim::SceneHost& H, uint32_t dim) {
     uint64_t nc = 1;
     for (int a = 0; a < 4; ++a) {
         const float q = std::max(1.0f, H.bounds.dim[a] / H.h);
+        // range-checked in float: a quotient past 2^30 would not convert to a
+        // meaningful cell count
+        if (!(q <= 1073741824.0f)) return fail(ARP_ERR_UNSUPPORTED, "a scene's grid has more than 2^30 cells");
         const uint32_t sub = (uint32_t)q;
         if (a < 3) P.grid.sub[a] = sub;
         nc *= sub;

@@ -124,7 +124,7 @@ static bool make_tableau(int id, Tableau& t) {
     }
 }
 
-// kernel.rs:280-286 (volume_nball) and :335-338 (poly6 norm_const), evaluated
+// kernel.rs:5-11 (volume_nball) and :60-63 (poly6 norm_const), evaluated
 // left to right in T as the Rust code does in f32.
 template <class T> static T volume_nball(uint32_t n, T r) {
     if (n == 0) return T(1);
@@ -470,7 +470,7 @@ public:
     uint32_t bucket_index(const int b[3]) const {
         return uint32_t(b[0]) + uint32_t(b[1]) * sub[0] + uint32_t(b[2]) * sub[0] * sub[1];
     }
-    // local_bucket_pos (fluid.rs:175-179) for invocation gid of a 9x3x3 group
+    // local_bucket_pos (fluid.rs:89-93) for invocation gid of a 9x3x3 group
     bool local_bucket(uint32_t bucket, uint32_t gid, int out[3]) const {
         if (bucket == INVALID) return false;
         uint32_t lx = gid % 9, ly = (gid / 9) % 3, lz = gid / 27;
@@ -484,7 +484,7 @@ public:
         return idx < p.size() ? p[idx].solid_id : INVALID;  // Q2: boundary index read from the mobile array
     }
 
-    // ternary reduction of the 81 shared slots (fluid.rs:312-327)
+    // ternary reduction of the 81 shared slots (fluid.rs:226-241)
     template <class V> static V reduce81(std::vector<V>& s) {
         uint32_t shadow = 81;
         while (shadow % 3 == 0) {
@@ -495,7 +495,7 @@ public:
         return s[0];
     }
 
-    // fluid.rs:181-336
+    // fluid.rs:95-251
     void fluid_forces(const State<T>& y, std::vector<Particle<T>>& out) const {
         const auto& P = y.p;
         const T hh_eps = T(0.1f) * h * h;

@@ -86,3 +86,24 @@ def test_null_handle_calls_fail_cleanly(lib):
     assert lib.arp_sim_time(None, ctypes.byref(t)) == 1
     assert lib.arp_sim_step(None, 1) == 1
     assert lib.arp_sim_destroy(None) == 0
+
+
+def test_noalloc_grid_rejects_a_grid_too_large_to_index(lib):
+    """A kernel radius tiny against the box would make dim / h overflow a
+    32-bit cell count; the call refuses it before touching the device."""
+    from arphys.abi import ArpAABB
+    b = ArpAABB()
+    for i in range(3):
+        b.dim[i] = 1.0
+    dummy = ctypes.c_void_p(256)  # never dereferenced: the size checks come first
+    for h in (1e-12, 2.0 ** -32, 1e-3):
+        code = lib.arp_grid_build_noalloc(dummy, 16, ctypes.byref(b), ctypes.c_float(h), dummy, 1 << 22, dummy, None)
+        assert code == 10, (h, lib.arp_last_error())
+        assert b"4194302" in lib.arp_last_error()
+
+
+def test_scene_with_a_grid_too_large_to_index_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.h = 1e-12
+    code, _, msg = _create(lib, sc)
+    assert code == 6 and "2^30" in msg

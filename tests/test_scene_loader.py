@@ -20,9 +20,11 @@ from oracle import scene_oracle
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 SCENES = sorted(glob.glob(os.path.join(HERE, "golden", "scenes", "*.toml")))
-# The reference's own example scenes, read as data when its tree is mounted
-# next to this one; the tests that use them skip otherwise.
-REFERENCE_EXAMPLES = sorted(glob.glob("/root/reference/examples/*.toml"))
+# The reference's own example scenes, read as data from the directory named by
+# ARP_REFERENCE_EXAMPLES (the reference's `examples/`); the tests that use them
+# skip when it is unset or holds no scenes.
+_EXAMPLES_DIR = os.environ.get("ARP_REFERENCE_EXAMPLES", "")
+REFERENCE_EXAMPLES = sorted(glob.glob(os.path.join(_EXAMPLES_DIR, "*.toml"))) if _EXAMPLES_DIR else []
 
 f32 = np.float32
 

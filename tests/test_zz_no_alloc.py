@@ -62,6 +62,51 @@ def test_noalloc_grid_matches_the_handle_entry_point():
         np.testing.assert_array_equal(perm, ref["members"])
 
 
+def _expected_grid(pos, bmin, bdim, h):
+    """The grid a stable counting sort gives: cell of every particle by the
+    reference's hash (every operation rounded to f32), members ascending."""
+    f32 = np.float32
+    sub = [max(1, int(max(f32(1.0), f32(bdim[a]) / f32(h)))) for a in range(3)]
+    nc = sub[0] * sub[1] * sub[2]
+    p = pos[:, :3].astype(np.float32)
+    finite = np.isfinite(p).all(axis=1)
+    key = np.full(len(p), nc, np.int64)
+    c = np.zeros((len(p), 3), np.int64)
+    with np.errstate(invalid="ignore"):
+        for a in range(3):
+            t = (p[:, a] - f32(bmin[a])) / f32(bdim[a])
+            t = np.clip(t, f32(0.0), f32(1.0)) * f32(sub[a])
+            c[:, a] = np.minimum(np.floor(np.where(finite, t, 0)).astype(np.int64), sub[a] - 1)
+    key[finite] = (c[:, 0] + c[:, 1] * sub[0] + c[:, 2] * sub[0] * sub[1])[finite]
+    perm = np.argsort(key, kind="stable").astype(np.uint32)
+    start = np.searchsorted(key[perm], np.arange(nc + 2)).astype(np.uint32)
+    return nc, start, perm
+
+
+def test_noalloc_grid_orders_long_runs():
+    """Cells holding far more particles than one thread sorts (thousands in
+    one cell, a long non-finite run) still list their members ascending, the
+    same on every call."""
+    torch = pytest.importorskip("torch")
+    lib = load_library()
+    rng = np.random.default_rng(8)
+    parts = [np.array([0.2, 0.3, 0.4]) + 0.1 * rng.uniform(0.05, 0.95, size=(3000, 3)),
+             np.array([0.5, 0.5, 0.5]) + 0.1 * rng.uniform(0.05, 0.95, size=(700, 3)),
+             rng.uniform(0.0, 1.0, size=(1500, 3)),
+             np.full((300, 3), np.nan)]
+    xyz = np.concatenate(parts)[rng.permutation(5500)]
+    pos = np.zeros((len(xyz), 4), np.float32)
+    pos[:, :3] = xyz
+    sc = scenes.Scene(particles=None, boundary=None, materials=None, bounds_min=(0.0, 0.0, 0.0, 0.0),
+                      bounds_dim=(1.0, 1.0, 1.0, 0.0), h=0.1)
+    nc, start_ref, perm_ref = _expected_grid(pos, sc.bounds_min, sc.bounds_dim, sc.h)
+    assert np.diff(start_ref).max() >= 3000
+    for call in range(2):
+        start, perm = _noalloc_grid(lib, torch, pos, sc, nc)
+        np.testing.assert_array_equal(start, start_ref)
+        np.testing.assert_array_equal(perm, perm_ref)
+
+
 def test_noalloc_grid_rejects_sizes_beyond_its_maximum():
     lib = load_library()
     sc = scenes.small_fluid_bar_3d()
