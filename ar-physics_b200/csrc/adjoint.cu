@@ -656,9 +656,12 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
     m3_acc(lF, lFh);
     m3_store_cols(lF, a.lamF + 3 * i);
     m3_store_cols(lFd, a.lamFd + 3 * i);
-    float2 gsum = a.g_stiff[i];
-    gsum.x += gn;
-    gsum.y += gs;
+    // summed over every stage of every step in double: the per-stage terms
+    // change sign as the bar oscillates, and a float sum would lose the
+    // difference to rounding
+    double2 gsum = a.g_stiff[i];
+    gsum.x += (double)gn;
+    gsum.y += (double)gs;
     a.g_stiff[i] = gsum;
     float4 lp = a.lam_pd[slot];
     lp.x += lx.x;

@@ -138,6 +138,7 @@ struct StageCoefs {
     float c_self;       // a[stage+1][stage] * dt (unused when last)
     float c_acc;        // b[stage] * dt
     int acc_first;      // 1 when no earlier stage contributed to acc
+    int kick;           // 1: a velocity-Verlet kick, which leaves positions as they are
 };
 
 struct StageBuffers {
@@ -199,7 +200,7 @@ int gather_sorted(const uint32_t* perm, uint32_t n, const float4* a_in, float4* 
                   cudaStream_t st);
 // Gather a state into sorted order (out[k] = in[perm[k]]) and evaluate the
 // pressure term p / rho^2 of every gathered particle (fluid.rs:45-52,
-// :270-271).  Any pointer pair may be null.
+// :128,165).  Any pointer pair may be null.
 // Solid-order copies a gather writes on the side: for a gathered particle
 // whose solid id (sid_of_slot at its source slot) is valid, sx/sv/sc[sid] =
 // its state and cell coordinates, and slot_of[sid] = its new index (when
@@ -277,6 +278,14 @@ extern const FluidVariant kFluidVariants[kNumFluidVariants];
 // `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
                  int variant, uint32_t* tile_counter, cudaStream_t st);
+
+// Velocity Verlet's kick and drift, in storage order: v' = v + (dt/2) a,
+// rho' = rho + (dt/2) drho/dt, x' = x + dt v' from the derivative record
+// (fpd, fvm) of the previous force evaluation; and the kick of a 4-float4
+// per-solid field (the plastic strain).  Return the launches issued.
+int verlet_kick_drift(const float4* pd, const float4* vm, const float4* fpd, const float4* fvm, uint32_t n, float half,
+                      float full, float4* out_pd, float4* out_vm, cudaStream_t st);
+int verlet_kick4(const float4* e, const float4* k4, uint32_t count, float half, float4* out, cudaStream_t st);
 
 // ---- solids (solid.cu) ------------------------------------------------------
 struct SolidRefList {
@@ -387,7 +396,7 @@ struct AdjArgs {
     const float2* stiff;       // per-solid stiffness override or null
     float4* lamF;              // [3*ns] adjoint of F (columns), scratch
     float4* lamFd;             // [3*ns] adjoint of dF/dt
-    float2* g_stiff;           // [ns] accumulated dL/d(normal, shear) stiffness
+    double2* g_stiff;          // [ns] accumulated dL/d(normal, shear) stiffness
     uint32_t* flags;           // bit 0: an active self-contact pair (not differentiated)
     float4* w;                 // [n] scratch: per-particle weights of the stage
     float4* eq;                // [n] scratch: per-particle state-equation terms

@@ -387,7 +387,13 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
         accv = b.acc_vm[slot];
     }
     if (c.last) {
-        b.next_pd[slot] = comb(y0p, accp, false);
+        float4 np = comb(y0p, accp, false);
+        if (c.kick) {  // a velocity-Verlet kick moves no particle: positions come from the drift
+            np.x = y0p.x;
+            np.y = y0p.y;
+            np.z = y0p.z;
+        }
+        b.next_pd[slot] = np;
         b.next_vm[slot] = comb(y0v, accv, true);
     } else {
         float4 tp = make_float4(0.f, 0.f, 0.f, 0.f), tv = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -579,7 +585,47 @@ void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, co
     k_fluid_overflow<DIM><<<2u * oblocks, 64, 0, st>>>(a, T, c, b);
 }
 
+// Velocity Verlet, first half of a step (kick, then drift), in storage
+// order: v' = v + (dt/2) a, rho' = rho + (dt/2) drho/dt, x' = x + dt v', with
+// (a, drho/dt) the derivative record kept from the previous force evaluation
+// (its position part is not used).  Each sum is formed as y + (0 + c k), the
+// order of the stage epilogue.
+__global__ void k_verlet_kick_drift(const float4* __restrict__ pd, const float4* __restrict__ vm,
+                                    const float4* __restrict__ fpd, const float4* __restrict__ fvm, uint32_t n,
+                                    float half, float full, float4* __restrict__ out_pd, float4* __restrict__ out_vm) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 p = pd[k], v = vm[k], fp = fpd[k], fv = fvm[k];
+    const float4 z = make_float4(0.f, 0.f, 0.f, 0.f);
+    const float4 vh = comb(v, axpy(half, fv, z), true);  // w holds the material bits
+    const float rho = __fadd_rn(p.w, __fadd_rn(0.0f, __fmul_rn(half, fp.w)));
+    const float4 dx = axpy(full, make_float4(vh.x, vh.y, vh.z, 0.0f), z);
+    out_pd[k] = make_float4(__fadd_rn(p.x, dx.x), __fadd_rn(p.y, dx.y), __fadd_rn(p.z, dx.z), rho);
+    out_vm[k] = vh;
+}
+
+// The kick of the plastic strain (4 float4 per solid): e' = e + (0 + c k).
+__global__ void k_verlet_kick4(const float4* __restrict__ e, const float4* __restrict__ k4, uint32_t count, float half,
+                               float4* __restrict__ out) {
+    const uint32_t i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= count) return;
+    out[i] = comb(e[i], axpy(half, k4[i], make_float4(0.f, 0.f, 0.f, 0.f)), false);
+}
+
 }  // namespace
+
+int verlet_kick_drift(const float4* pd, const float4* vm, const float4* fpd, const float4* fvm, uint32_t n, float half,
+                      float full, float4* out_pd, float4* out_vm, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_verlet_kick_drift<<<(n + 255) / 256, 256, 0, st>>>(pd, vm, fpd, fvm, n, half, full, out_pd, out_vm);
+    return 1;
+}
+
+int verlet_kick4(const float4* e, const float4* k4, uint32_t count, float half, float4* out, cudaStream_t st) {
+    if (count == 0) return 0;
+    k_verlet_kick4<<<(count + 255) / 256, 256, 0, st>>>(e, k4, count, half, out);
+    return 1;
+}
 
 const FluidVariant kFluidVariants[kNumFluidVariants] = {
     {128, 48, 0, 0}, {256, 48, 0, 0}, {128, 48, 1, 0}, {256, 48, 1, 0},

@@ -71,6 +71,8 @@ bool make_tableau(int id, Tableau& t) {
         case ARP_INT_RK4:
             t.stages = 4; t.a[1][0] = 0.5; t.a[2][1] = 0.5; t.a[3][2] = 1;
             t.b[0] = 1.0 / 6.0; t.b[1] = 1.0 / 3.0; t.b[2] = 1.0 / 3.0; t.b[3] = 1.0 / 6.0; return true;
+        case ARP_INT_VERLET:  // one force evaluation per step; b[0] = 1/2 is the closing kick
+            t.stages = 1; t.b[0] = 0.5; return true;
         case ARP_INT_RK_3_8:
             t.stages = 4; t.a[1][0] = 1.0 / 3.0; t.a[2][0] = -1.0 / 3.0; t.a[2][1] = 1;
             t.a[3][0] = 1; t.a[3][1] = -1; t.a[3][2] = 1;
@@ -172,7 +174,7 @@ struct AdjointPool {
     DevBuf<float4> io;  // [2n] the caller's 8-float-per-particle gradients, on the device
     DevBuf<float4> lY_p[kMaxStages], lY_v[kMaxStages];
     DevBuf<float4> lamF, lamFd;
-    DevBuf<float2> gst;
+    DevBuf<double2> gst;
     DevBuf<uint32_t> flags;
     Checkpoint now;
 };
@@ -240,6 +242,13 @@ struct arp_sim {
     DevBuf<DevInter> d_inter;
     // mobile state: Y (y0), T (reorder target / y_new), S[2] (stage states)
     StateBuf Y, T, S[2], X, acc, kst[4];
+    // velocity Verlet: the derivative record of the last force evaluation
+    // (storage order of Y) and its plastic-strain rates (solid-id order);
+    // invalid until a force evaluation at the current state has run
+    StateBuf vforce;
+    DevBuf<float4> ep_force;
+    bool vforce_valid = false;
+    bool verlet() const { return integrator == ARP_INT_VERLET; }
     DevBuf<uint32_t> orig, orig_r, sid, sid_r, sid_sorted, slot_of;
     DevBuf<float> ps, bps;  // p / rho^2 of sorted particles / boundary particles
     DevBuf<arp_particle> records;      // device copy of caller-order Particle records (state exchange)
@@ -571,6 +580,7 @@ arp_status do_init(arp_sim* S) {
         ARP_TRY(check_launch("reference neighbor lists"));
     }
     CUDA_TRY(cudaMemsetAsync(S->d_stats.p, 0, sizeof(DevStats), st));
+    S->vforce_valid = false;
     S->initialized = true;
     return ARP_OK;
 }
@@ -621,20 +631,28 @@ arp_status restore_checkpoint(arp_sim* S, const Checkpoint& c) {
     return ARP_OK;
 }
 
-arp_status do_step(arp_sim* S) {
+// One integrator step.  With `prime` (velocity Verlet only) it instead
+// evaluates the forces at the current state and keeps their derivative
+// record for the next step's kick, the force evaluation of the reference's
+// init_with_vel (src/soft_body/mod.rs:213-233): the state is re-sorted into
+// cell order but not advanced, and no time passes.
+arp_status do_step(arp_sim* S, bool prime = false) {
     cudaStream_t st = S->stream;
     const uint32_t n = S->n, ns = S->ns;
     const Tableau& tab = S->tab;
     const bool sb = S->solid_branch();
-    if (S->tape && !S->replaying) {
+    const bool verlet = S->verlet();
+    if (S->tape && !S->replaying && !prime) {
         if (S->tape->steps % S->tape->every == 0) ARP_TRY(save_checkpoint(S));
         S->tape->steps++;
     }
-    StepRecord* R = S->rec;
-    S->time += S->dt_sub;
+    StepRecord* R = prime ? nullptr : S->rec;
+    if (!prime) S->time += S->dt_sub;
     const uint32_t* bstart = S->b_start.p;
     uint64_t l0 = S->launches;
-    S->profiling = S->prof_on && S->prof_phase++ % S->prof_every == 0;
+    S->profiling = !prime && S->prof_on && S->prof_phase++ % S->prof_every == 0;
+    // velocity Verlet: (dt/2) as the stage epilogue's coefficient b[0] dt
+    const float half = (float)(tab.b[0] * (double)S->dt_sub);
 
     // 1. sort y0 into cell order
     arp_sim::Mark mk{};
@@ -649,7 +667,17 @@ arp_status do_step(arp_sim* S) {
         zero.p[2] = S->contact_bound.p;
         zero.n[2] = 2;
     }
-    S->launches += build_grid(S->Y.pd.p, S->Y.vm.p, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st, zero);
+    // velocity Verlet kicks and drifts first (storage order, into X); the grid
+    // and the force evaluation then see the drifted state
+    const float4* src_pd = S->Y.pd.p;
+    const float4* src_vm = S->Y.vm.p;
+    if (verlet && !prime) {
+        S->launches += verlet_kick_drift(S->Y.pd.p, S->Y.vm.p, S->vforce.pd.p, S->vforce.vm.p, n, half, S->dt_sub,
+                                         S->X.pd.p, S->X.vm.p, st);
+        src_pd = S->X.pd.p;
+        src_vm = S->X.vm.p;
+    }
+    S->launches += build_grid(src_pd, src_vm, nullptr, n, S->tables, S->gb, S->d_stats.p, bstart, st, zero);
     // the stage-0 solid copies and the solid -> slot map come out of the same gather
     SolidScatter sol0;
     if (ns) {
@@ -660,8 +688,8 @@ arp_status do_step(arp_sim* S) {
         sol0.sc = S->sc.p;
         sol0.slot_of = S->slot_of.p;
     }
-    S->launches += gather_state(S->gb.perm, n, S->Y.pd.p, S->T.pd.p, S->Y.vm.p, S->T.vm.p, S->orig.p,
-                                S->orig_r.p, S->sid.p, S->sid_r.p, nullptr, nullptr, S->ps.p, S->d_mats.p, st, sol0);
+    S->launches += gather_state(S->gb.perm, n, src_pd, S->T.pd.p, src_vm, S->T.vm.p, S->orig.p, S->orig_r.p,
+                                S->sid.p, S->sid_r.p, nullptr, nullptr, S->ps.p, S->d_mats.p, st, sol0);
     std::swap(S->Y, S->T);
     std::swap(S->orig, S->orig_r);
     std::swap(S->sid, S->sid_r);
@@ -681,8 +709,13 @@ arp_status do_step(arp_sim* S) {
     const float4* cur_pd = S->Y.pd.p;
     const float4* cur_vm = S->Y.vm.p;
     const float4* cur_ep = S->ep.p;
+    const float4* ep_base = S->ep.p;  // the step's y0 of the plastic strain
+    if (verlet && !prime && sb && S->any_plastic) {
+        S->launches += verlet_kick4(S->ep.p, S->ep_force.p, 4 * ns, half, S->ep_s[0].p, st);
+        ep_base = cur_ep = S->ep_s[0].p;
+    }
     for (int s = 0; s < tab.stages; ++s) {
-        const bool last = s == tab.stages - 1;
+        const bool last = !prime && s == tab.stages - 1;
         StageCoefs c{};
         c.stage = s;
         c.last = last ? 1 : 0;
@@ -694,14 +727,15 @@ arp_status do_step(arp_sim* S) {
         c.c_prev0 = cp[0];
         c.c_prev1 = cp[1];
         c.c_prev2 = cp[2];
-        c.c_acc = (float)(tab.b[s] * (double)S->dt_sub);
+        c.c_acc = prime ? 0.0f : (float)(tab.b[s] * (double)S->dt_sub);
         c.acc_first = acc_started ? 0 : 1;
+        c.kick = verlet ? 1 : 0;
         if (c.c_acc != 0.0f) acc_started = true;
         bool store_k = false;
         for (int t = s + 2; t < tab.stages; ++t)
             if (tab.a[t][s] != 0.0) store_k = true;
-        B.store_pd = store_k ? S->kst[s].pd.p : nullptr;
-        B.store_vm = store_k ? S->kst[s].vm.p : nullptr;
+        B.store_pd = verlet ? S->vforce.pd.p : store_k ? S->kst[s].pd.p : nullptr;
+        B.store_vm = verlet ? S->vforce.vm.p : store_k ? S->kst[s].vm.p : nullptr;
         B.prev0_pd = cp[0] != 0.f ? S->kst[0].pd.p : nullptr;
         B.prev0_vm = cp[0] != 0.f ? S->kst[0].vm.p : nullptr;
         B.prev1_pd = cp[1] != 0.f ? S->kst[1].pd.p : nullptr;
@@ -748,10 +782,10 @@ arp_status do_step(arp_sim* S) {
             a.L = S->L.p;
             a.rl = SolidRefList{S->rl_off.p, S->rl_nbr.p, S->rl_gw.p, S->rl_nnz};
             a.ep = cur_ep;
-            a.ep0 = S->ep.p;
+            a.ep0 = ep_base;
             a.ep_next = last ? S->ep_t.p : S->ep_s[s % 2].p;
             a.ep_acc = S->ep_acc.p;
-            a.ep_store = store_k ? S->ep_kst[s].p : nullptr;
+            a.ep_store = verlet ? S->ep_force.p : store_k ? S->ep_kst[s].p : nullptr;
             a.ep_prev0 = cp[0] != 0.f ? S->ep_kst[0].p : nullptr;
             a.ep_prev1 = cp[1] != 0.f ? S->ep_kst[1].p : nullptr;
             a.ep_prev2 = cp[2] != 0.f ? S->ep_kst[2].p : nullptr;
@@ -823,8 +857,11 @@ arp_status do_step(arp_sim* S) {
         cur_pd = next_pd;
         cur_vm = next_vm;
     }
-    std::swap(S->Y, S->T);
-    if (sb && S->any_plastic) std::swap(S->ep, S->ep_t);  // without plastic materials ep stays zero
+    if (!prime) {
+        std::swap(S->Y, S->T);
+        if (sb && S->any_plastic) std::swap(S->ep, S->ep_t);  // without plastic materials ep stays zero
+    }
+    if (verlet) S->vforce_valid = true;
     if (S->profiling) S->prof_steps++;
     return check_launch("step");
 }
@@ -842,8 +879,6 @@ arp_status append_scene(const arp_scene* sc, arp_sim* S) {
     if (!(sc->kernel_radius > 0.0f) || !std::isfinite(sc->kernel_radius))
         return fail(ARP_ERR_INVALID_ARG, "kernel_radius must be positive");
     if (!std::isfinite(sc->timestep)) return fail(ARP_ERR_INVALID_ARG, "timestep must be finite");
-    if (sc->integrator == ARP_INT_VERLET)
-        return fail(ARP_ERR_UNSUPPORTED, "the velocity-Verlet integrator is not implemented; use an RK tableau");
     Tableau tab;
     if (!make_tableau(sc->integrator, tab)) return fail(ARP_ERR_INVALID_ARG, "unknown integrator id");
     if (sc->bounds.dim[3] > 0.0f) return fail(ARP_ERR_UNSUPPORTED, "4-dimensional boxes are not supported");
@@ -1014,6 +1049,10 @@ arp_status allocate(arp_sim* S) {
     if (S->tab.stages > 2) ARP_TRY(alloc_state(S->S[1], n));
     ARP_TRY(alloc_state(S->X, n));
     ARP_TRY(alloc_state(S->acc, n));
+    if (S->verlet()) {
+        ARP_TRY(alloc_state(S->vforce, n));
+        CUDA_TRY(S->ep_force.alloc(4 * ns));
+    }
     for (int j = 0; j < S->tab.stages; ++j) {
         bool needed = false;
         for (int t = j + 2; t < S->tab.stages; ++t)
@@ -1157,6 +1196,11 @@ arp_status run_autotune(arp_sim* S, bool force) {
     std::swap(S->Y, S->T);
     std::swap(S->orig, S->orig_r);
     std::swap(S->sid, S->sid_r);
+    if (S->verlet() && S->vforce_valid) {  // the carried force record follows the reorder
+        S->launches += gather_sorted(S->gb.perm, n, S->vforce.pd.p, S->X.pd.p, S->vforce.vm.p, S->X.vm.p, nullptr,
+                                     nullptr, nullptr, nullptr, st);
+        std::swap(S->vforce, S->X);
+    }
     const Tableau& tab = S->tab;
     const bool last = tab.stages == 1;
     StageCoefs c{};
@@ -1482,6 +1526,9 @@ arp_status graph_step(arp_sim* S) {
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
     ARP_TRY(need_init(sim));
     for (uint32_t i = 0; i < nsteps; ++i) {
+        // velocity Verlet starts from a force evaluation at the current state
+        // (plain launches: it is not part of the step a graph replays)
+        if (sim->verlet() && !sim->vforce_valid) ARP_TRY(do_step(sim, true));
         const bool sampled = sim->prof_on && sim->prof_phase % sim->prof_every == 0;
         if (sim->use_graph && !sim->tape && !sampled) ARP_TRY(graph_step(sim));
         else ARP_TRY(do_step(sim));
@@ -1629,6 +1676,7 @@ arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t 
         if (flag & 2u) return fail(ARP_ERR_UNSUPPORTED, "w components must keep their values");
         sim->launches += records_to_soa(sim->records.p, n, sim->sid_of_caller_d.p, sim->mat_of_caller_d.p,
                                         sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, st);
+        sim->vforce_valid = false;  // a new state: velocity Verlet evaluates its forces again
         CUDA_TRY(cudaStreamSynchronize(st));
         ARP_TRY(check_launch("set_particles"));
     }
@@ -2045,6 +2093,7 @@ arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
         if (it.potential != ARP_CONTACT_ZERO && it.friction != 0.0f)
             return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate contact friction");
     if (sim->tab.stages > kMaxStages) return fail(ARP_ERR_UNSUPPORTED, "more than 4 stages");
+    if (sim->verlet()) return fail(ARP_ERR_UNSUPPORTED, "the adjoint differentiates Runge-Kutta steps only");
     sim->drop_graph();
     retire_tape(sim);
     sim->tape.reset(new Tape());
@@ -2100,9 +2149,9 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                   &out_v = P.out_v, &mu_p = P.mu_p, &mu_v = P.mu_v, &lamF = P.lamF, &lamFd = P.lamFd;
     DevBuf<float4>* lY_p = P.lY_p;
     DevBuf<float4>* lY_v = P.lY_v;
-    DevBuf<float2>& gst = P.gst;
+    DevBuf<double2>& gst = P.gst;
     DevBuf<uint32_t>& flags = P.flags;
-    CUDA_TRY(cudaMemsetAsync(gst.p, 0, std::max(ns, 1u) * sizeof(float2), st));
+    CUDA_TRY(cudaMemsetAsync(gst.p, 0, std::max(ns, 1u) * sizeof(double2), st));
     CUDA_TRY(cudaMemsetAsync(flags.p, 0, sizeof(uint32_t), st));
     if (n) {  // one copy of the caller's array, split on the device
         CUDA_TRY(cudaMemcpyAsync(P.io.p, dl_dstate, n * 2 * sizeof(float4), cudaMemcpyHostToDevice, st));
@@ -2204,11 +2253,16 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
         sim->launches += adjoint_pack(n, lc_p.p, lc_v.p, P.io.p, st);
         CUDA_TRY(cudaMemcpyAsync(grad_state0, P.io.p, n * 2 * sizeof(float4), cudaMemcpyDeviceToHost, st));
     }
-    // float2 (normal, shear) per solid is the caller's layout
+    // accumulated in double; float2 (normal, shear) per solid is the caller's layout
+    std::vector<double2> gst_host(grad_stiffness ? ns : 0);
     if (ns && grad_stiffness)
-        CUDA_TRY(cudaMemcpyAsync(grad_stiffness, gst.p, ns * sizeof(float2), cudaMemcpyDeviceToHost, st));
+        CUDA_TRY(cudaMemcpyAsync(gst_host.data(), gst.p, ns * sizeof(double2), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaMemcpyAsync(&hflags, flags.p, sizeof(uint32_t), cudaMemcpyDeviceToHost, st));
     CUDA_TRY(cudaStreamSynchronize(st));
+    for (uint32_t q = 0; q < gst_host.size(); ++q) {
+        grad_stiffness[2 * q] = (float)gst_host[q].x;
+        grad_stiffness[2 * q + 1] = (float)gst_host[q].y;
+    }
     if (hflags & 1u) return fail(ARP_ERR_UNSUPPORTED, "a self-contact pair was active; it is not differentiated");
     return ARP_OK;
 }

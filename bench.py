@@ -174,30 +174,48 @@ def pair_rate(sc, stages, fluid_ms_per_step):
             "rate": pairs * stages / (fluid_ms_per_step / 1000.0), "unit": "pair-interactions/s"}
 
 
-def cpu_baseline(sc, max_seconds=20.0, max_steps=5):
-    """The CPU oracle on all host cores: full-size steps until ~max_seconds."""
+def oracle_sample(config, steps, warmup, max_seconds=60.0):
+    """The CPU oracle (the float restatement of the reference's shaders) on
+    all host cores: `warmup` untimed full-size steps (the first fills the
+    boundary and reference buckets), then up to `steps` timed steps, one
+    oracle step call each, stopping early after `max_seconds`.  Both the
+    reference arm and the cpu_baseline leg run this, each in a process that
+    has not loaded torch, so they time the same thing the same way."""
     from oracle import oracle as orc
+    sc = make_scene(config)
     cores = os.cpu_count() or 1
     orc.set_threads(cores)
     o = orc.Oracle(sc, 32)
-    o.step(1)  # first step fills the boundary and reference buckets
-    t0 = time.perf_counter()
-    steps = 0
-    while steps < max_steps and time.perf_counter() - t0 < max_seconds:
+    for _ in range(max(1, warmup)):
         o.step(1)
-        steps += 1
+    t0 = time.perf_counter()
+    done = 0
+    while done < steps and time.perf_counter() - t0 < max_seconds:
+        o.step(1)
+        done += 1
     dt = time.perf_counter() - t0
     parts = sc.n + sc.nb
-    return {"value": parts * steps / dt, "unit": UNIT, "cores": cores, "kind": "port",
-            "sample": f"{steps} full RK steps of the {parts}-particle scene after 1 untimed step "
-                      f"(C++ oracle, float, OpenMP x{cores})", "seconds": dt}
+    return {"value": parts * done / dt, "unit": UNIT, "cores": cores, "kind": "port",
+            "sample": f"{done} full RK steps of the {parts}-particle scene after {max(1, warmup)} untimed "
+                      f"step(s) (C++ oracle, float, OpenMP x{cores}); the reference's Rust/OpenGL path cannot "
+                      f"run here", "seconds": dt, "steps": done}
 
 
-def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
+def cpu_baseline(config, steps=5, warmup=1):
+    """oracle_sample in a fresh interpreter (this process has loaded torch,
+    whose OpenMP runtime would otherwise be the one the oracle runs on)."""
+    r = subprocess.run([sys.executable, os.path.abspath(__file__), "--oracle-sample", config, str(steps),
+                        str(warmup)], capture_output=True, text=True, check=True)
+    return json.loads(r.stdout.strip().splitlines()[-1])
+
+
+def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20):
     """256 independent scenes (2,048-65,536 particles each, own h, fluid
     blocks and elastic blocks): stepped as one batch (one set of launches per
-    stage, replayed from a CUDA graph) and as a loop over 256 separate
-    simulations, both on one GPU."""
+    stage) and as a loop over 256 separate simulations, both on one GPU and
+    both replaying each step from a CUDA graph.  The batch is timed over the
+    configuration's 200 steps with the autotuner's launch shape; every
+    persistent tile-queue shape of the fluid kernel is timed beside it."""
     from arphys import FluidSim, scenes
     scs = scenes.batched_scenes()
     parts = int(sum(sc.n + sc.nb for sc in scs))
@@ -205,15 +223,34 @@ def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
     batch.init()
     batch.set_stream(stream.cuda_stream)
     batch.set_graph(True)
+    init = batch.particles().copy()
     batch.step(4)
     torch.cuda.synchronize()
     e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    batch.set_particles(init)
     e0.record(stream)
     batch.step(steps_batch)
     e1.record(stream)
     torch.cuda.synchronize()
     t_batch = e0.elapsed_time(e1) / 1000.0
     variant = batch.fluid_variant()
+    # the persistent (scene, cell-tile) work-queue shapes, same state, same steps each
+    shapes = {}
+    for v in range(10):
+        batch.set_fluid_variant(v)
+        vi = batch.fluid_variant()
+        if not vi["persistent"]:
+            continue
+        batch.set_particles(init)
+        batch.step(2)  # captures this shape's step graphs
+        batch.set_particles(init)
+        e0.record(stream)
+        batch.step(steps_variant)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        shapes[str(v)] = dict(vi, ms_per_step=e0.elapsed_time(e1) / steps_variant)
+    batch.set_fluid_variant(variant["variant"])
+    best_pers = min(shapes, key=lambda k: shapes[k]["ms_per_step"]) if shapes else None
     # where a batch step goes: a few more steps, untimed, with the library's
     # per-segment events (graph replay off: the events sit between launches)
     batch.set_graph(False)
@@ -229,9 +266,10 @@ def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
         sim = FluidSim(sc)
         sim.init()
         sim.set_stream(stream.cuda_stream)
+        sim.set_graph(True)
         sims.append(sim)
     for sim in sims:
-        sim.step(1)
+        sim.step(2)  # captures each simulation's step graphs
     torch.cuda.synchronize()
     e0.record(stream)
     for _ in range(rounds_loop):
@@ -244,16 +282,19 @@ def run_batched(torch, stream, steps_batch=40, rounds_loop=4):
         sim.close()
     batched = len(scs) * steps_batch / t_batch
     loop = len(scs) * rounds_loop / t_loop
-    return {"scenes": len(scs), "particles": parts, "integrator": "rk2",
+    return {"scenes": len(scs), "particles": parts, "integrator": "rk2", "steps": steps_batch,
             "scene_steps_per_s": batched, "particle_steps_per_s": parts * steps_batch / t_batch,
             "ms_per_step": t_batch * 1000.0 / steps_batch,
             "per_scene_loop_scene_steps_per_s": loop, "speedup_vs_per_scene_loop": batched / loop,
-            "fluid_launch_shape": variant, "segments_ms_per_step": segments,
+            "fluid_launch_shape": variant, "persistent_shapes": shapes, "best_persistent_shape": best_pers,
+            "segments_ms_per_step": segments,
             "solids": int(sum(sc.n_solids() for sc in scs)),
-            "note": "working set > L2 (no flush); batch replayed from a CUDA graph; loop = one simulation per scene"}
+            "note": ("no L2 flush: the batch's state (~%d MB) is larger than L2; both the batch and the "
+                     "per-scene loop (%d rounds of one step per simulation) replay CUDA graphs"
+                     % (parts * 32 * 4 // (1 << 20), rounds_loop))}
 
 
-def _time_adjoint(torch, stream, sim, steps, every, loss_grad):
+def _time_adjoint(torch, stream, sim, steps, every, loss_grad, stiff=None):
     """Plain forward, taped forward and backward of `steps` steps from the
     handle's current state (device time for the forwards, host wall clock
     around the backward call, which synchronizes)."""
@@ -301,7 +342,14 @@ def _time_adjoint(torch, stream, sim, steps, every, loss_grad):
         t_bwd.append((time.perf_counter() - t0) * 1000.0)
     sim.tape_end()
     t_mean = sum(t_bwd) / len(t_bwd)
-    return {"steps": steps, "checkpoint_every": every, "forward_ms": t_fwd, "forward_plain_launches_ms": t_plain,
+    live = {}
+    if stiff is not None:
+        # dL/d(ln E) per particle: E scales both Lame parameters
+        dlne = (gs.astype(np.float64) * stiff.astype(np.float64)).sum(axis=1)
+        live = {"grad_lnE_norm": float(np.linalg.norm(dlne)),
+                "grad_lnE_norm_over_loss": float(np.linalg.norm(dlne) / max(abs(L), 1e-300)),
+                "grad_lnE_nonzero_particles": int(np.count_nonzero(np.abs(dlne) > 1e-6 * np.abs(dlne).max()))}
+    return live | {"steps": steps, "checkpoint_every": every, "forward_ms": t_fwd, "forward_plain_launches_ms": t_plain,
             "forward_taped_ms": t_tape,
             "backward_ms": t_mean, "backward_ms_each": t_bwd, "adjoint_fwd_ratio": t_mean / t_fwd, "loss": L,
             "grad_v0_norm": float(np.linalg.norm(g0[:, 4:7])), "grad_stiffness_norm": float(np.linalg.norm(gs)),
@@ -322,7 +370,7 @@ def run_adjoint(torch, stream, bar_steps=400, rt_steps=300, only=None):
     out = {}
     if only not in (None, "bar"):
         return out | run_adjoint_rt(torch, stream, rt_steps)
-    sc = scenes.cantilever_bar()
+    sc = scenes.cantilever_bar(v_sigma=0.05)
     sim = FluidSim(sc)
     sim.init()
     sim.set_stream(stream.cuda_stream)
@@ -331,9 +379,17 @@ def run_adjoint(torch, stream, bar_steps=400, rt_steps=300, only=None):
     sim.step(3)  # warm-up
     sim.set_particles(init)
     tip, target = sc.meta["tip"], sc.meta["target"]
-    bar = _time_adjoint(torch, stream, sim, bar_steps, 20, lambda pos: scenes.tip_loss(pos, tip, target))
+    bar = _time_adjoint(torch, stream, sim, bar_steps, 20, lambda pos: scenes.tip_loss(pos, tip, target),
+                        stiff=sc.meta["stiffness"])
     bar["workload"] = ("cantilever bar 16x16x256 (65,024 elastic + 512 clamped), per-particle E lognormal("
-                       "ln 1e5, 0.3), nu 0.3, gravity, RK2, dt 1e-4")
+                       "ln 1e5, 0.3), nu 0.3, gravity, seeded initial velocities N(0, 0.05 m/s) per component, "
+                       "RK2, dt 1e-4")
+    if not bar["grad_lnE_norm_over_loss"] > 1e-6:
+        # the elastic wave from the clamp crosses only ~0.46 m of the 2.54 m bar
+        # in 400 steps, so the tip loss depends on E only through the motion
+        # the initial velocity field starts near the tip; a zero gradient
+        # means the workload is not the one meant
+        raise RuntimeError(f"stiffness gradient of the bar workload is zero ({bar['grad_lnE_norm']:.3e})")
     sim.close()
     out["bar"] = bar
     if only == "bar":
@@ -398,29 +454,19 @@ def run_render(torch, sim, sc):
 def run_reference(args, rank, world):
     """The reference arm: the reference's path cannot run here (Rust + OpenGL
     compute shaders, no GL stack), so the CPU restatement of its shaders is
-    timed on the host cores, rank 0 only."""
+    timed on the host cores, rank 0 only (oracle_sample, the same harness as
+    the cpu_baseline leg)."""
     if rank != 0:
         return
     sc = make_scene(args.config)
-    from oracle import oracle as orc
-    cores = os.cpu_count() or 1
-    orc.set_threads(cores)
-    o = orc.Oracle(sc, 32)
-    for _ in range(args.warmup):
-        o.step(1)
-    t0 = time.perf_counter()
-    o.step(args.steps)
-    dt = time.perf_counter() - t0
-    parts = sc.n + sc.nb
-    v = parts * args.steps / dt
+    cb = oracle_sample(args.config, args.steps, args.warmup)
+    v = cb["value"]
     line = {
-        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": args.steps,
-        "warmup": args.warmup, "ms_per_step": dt * 1000 / args.steps, "higher_is_better": True,
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": world, "steps": cb["steps"],
+        "warmup": args.warmup, "ms_per_step": cb["seconds"] * 1000 / max(cb["steps"], 1), "higher_is_better": True,
         "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded)",
-        "config": config_of(sc, args.config),
-        "cpu_baseline": {"value": v, "unit": UNIT, "cores": cores, "kind": "port",
-                         "sample": f"{args.steps} full RK steps after {args.warmup} warm-up steps (C++ oracle, "
-                                   f"float, OpenMP x{cores}); the reference's Rust/OpenGL path cannot run here"},
+        "config": dict(config_of(sc, args.config), parallelism=f"replicas x{world}"),
+        "cpu_baseline": cb,
         "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
     }
     print(json.dumps(line), flush=True)
@@ -533,7 +579,7 @@ def run_ours(args, rank, world, local_rank):
     if rank == 0 and not args.no_batched:
         line["batched"] = run_batched(torch, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        line["cpu_baseline"] = cpu_baseline(sc)
+        line["cpu_baseline"] = cpu_baseline(args.config)
     if rank == 0:
         print(json.dumps(line), flush=True)
     sim.close()
@@ -557,7 +603,13 @@ def main():
                     help="run only the reverse-mode measurement and print its object (profiling)")
     ap.add_argument("--adjoint-steps", type=int, default=None,
                     help="steps of each reverse-mode workload (default: 400 for the bar, 300 for the batch)")
+    ap.add_argument("--oracle-sample", nargs=3, metavar=("CONFIG", "STEPS", "WARMUP"), default=None,
+                    help="time the CPU oracle alone and print its object (the cpu_baseline leg runs this)")
     args = ap.parse_args()
+    if args.oracle_sample:
+        c, k, w = args.oracle_sample
+        print(json.dumps(oracle_sample(c, int(k), int(w))), flush=True)
+        return
     if args.adjoint_only:
         import torch
         stream = torch.cuda.Stream()

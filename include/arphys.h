@@ -71,7 +71,7 @@ typedef enum arp_integrator {
     ARP_INT_HEUN3 = 5,     /* "heun3" */
     ARP_INT_RK4 = 6,       /* "rk4" */
     ARP_INT_RK_3_8 = 7,    /* "rk_3_8" */
-    ARP_INT_VERLET = 8     /* "verlet": not implemented, rejected with ARP_ERR_UNSUPPORTED */
+    ARP_INT_VERLET = 8     /* "verlet": velocity Verlet, kick-drift-kick (see arp_sim_step) */
 } arp_integrator;
 
 /* `Material`, std430, 80 bytes (src/soft_body/material_region/material.rs:11-28).
@@ -253,7 +253,22 @@ arp_status arp_sim_destroy(arp_sim* sim);
  * of timestep/subticks. */
 arp_status arp_sim_update(arp_sim* sim);
 /* `nsteps` integrator steps of timestep/subticks (update() without the
- * subtick grouping). */
+ * subtick grouping).
+ * Velocity Verlet (ARP_INT_VERLET; the reference's default integrator,
+ * examples/test_mods/config.rs:451) is taken as the textbook kick-drift-kick
+ * over the derivative record f = (drho/dt, a) of the force evaluation
+ * (src/soft_body/shaders/mod.rs:11-86), with dt' = timestep/subticks:
+ *   v' = v + (dt'/2) a_n, rho' = rho + (dt'/2) drho_n/dt, x_{n+1} = x + dt' v',
+ *   f_{n+1} = f(x_{n+1}, v', rho'),
+ *   v_{n+1} = v' + (dt'/2) a_{n+1}, rho_{n+1} = rho' + (dt'/2) drho_{n+1}/dt
+ * (the plastic strain is kicked like the density).  Positions move only in
+ * the drift, with the velocity closure of FluidSim::update (state.velocity(),
+ * src/soft_body/mod.rs:256), so the position part of f is not used.  f_n is
+ * carried from the previous step; the first step after init, set_particles
+ * or add_particles first evaluates f at the current state, as init_with_vel
+ * does in FluidSim::init (src/soft_body/mod.rs:213-233).  The scheme inside
+ * the un-vendored crate numerical-integration is not observable, so this is
+ * a stated assumption, like the Runge-Kutta tableaus. */
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps);
 /* Time every launch shape of the fluid kernel (128 or 256 threads per block,
  * 48 or 96 listed neighbors per thread, one tile per block or persistent

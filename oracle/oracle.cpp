@@ -103,6 +103,7 @@ static bool make_tableau(int id, Tableau& t) {
     switch (id) {
         case ARP_INT_EULER: t.stages = 1; t.b[0] = 1; return true;
         case ARP_INT_MIDPOINT: t.stages = 2; t.a[1][0] = 0.5; t.b[1] = 1; return true;
+        case ARP_INT_VERLET: t.stages = 1; t.b[0] = 0.5; return true;  // see step_verlet
         case ARP_INT_HEUN2: t.stages = 2; t.a[1][0] = 1; t.b[0] = 0.5; t.b[1] = 0.5; return true;
         case ARP_INT_RALSTON:
             t.stages = 2; t.a[1][0] = 2.0 / 3.0; t.b[0] = 0.25; t.b[1] = 0.75; return true;
@@ -192,6 +193,10 @@ public:
     uint32_t subticks = 1;
     float time = 0;
     bool literal = false;  // evaluate every candidate pair, no cut-off shortcut
+    // velocity Verlet: the derivative record of the last force evaluation
+    bool verlet = false;
+    State<T> fcarry;
+    bool fvalid = false;
 
     // neighbor buckets (neighbor_list.rs:147-160)
     std::vector<Bucket> buckets;
@@ -203,6 +208,7 @@ public:
         if (!sc) return "null scene";
         if (sc->n_materials == 0 || !sc->materials) return "no materials";
         if (!make_tableau(sc->integrator, tab)) return "unsupported integrator";
+        verlet = sc->integrator == ARP_INT_VERLET;
         M = sc->n_materials;
         for (uint32_t i = 0; i < M; ++i) {
             const arp_material& m = sc->materials[i];
@@ -327,6 +333,7 @@ public:
     // next step because the particle count grew (neighbor_list.rs:226-235).
     bool add_particles(const arp_particle* in, uint32_t n, const arp_material& m, const float* offset) {
         if (n == 0) return false;
+        fvalid = false;  // a new state: velocity Verlet evaluates its forces again
         const bool stiff = m.normal_stiffness != 0.0f || m.shear_stiffness != 0.0f;
         uint32_t id = M;
         if (!stiff)
@@ -913,7 +920,55 @@ public:
         }
     }
 
+    // Velocity Verlet as the textbook kick-drift-kick over the force closure's
+    // derivative record f (the velocity closure state.velocity() of
+    // src/soft_body/mod.rs:256 moves the positions, so f's position part is
+    // not used); f at the initial state comes from the force evaluation of
+    // init_with_vel (src/soft_body/mod.rs:213-233).  The scheme inside the
+    // un-vendored numerical-integration crate is not observable: this is the
+    // stated assumption the library implements too.  Sums are formed as
+    // y + (0 + c k), the order combine() uses.
+    void step_verlet() {
+        time += dt_sub;
+        if (!fvalid) {
+            compute_forces(st, fcarry);
+            fvalid = true;
+        }
+        const T half = coef(0.5), full = coef(1.0);
+        State<T> y = st;
+        const size_t np = st.p.size(), ns = st.s.size();
+        for (size_t i = 0; i < np; ++i) {
+            T z = 0;
+            vec4<T> zv;
+            y.p[i].den = st.p[i].den + (z + half * fcarry.p[i].den);
+            y.p[i].vel = st.p[i].vel + (zv + half * fcarry.p[i].vel);
+            y.p[i].pos = st.p[i].pos + (zv + full * y.p[i].vel);
+        }
+        for (size_t i = 0; i < ns; ++i) {
+            mat4<T> zm;
+            y.s[i].stress = st.s[i].stress + (zm + half * fcarry.s[i].stress);
+        }
+        State<T> f;
+        compute_forces(y, f);
+        for (size_t i = 0; i < np; ++i) {
+            T z = 0;
+            vec4<T> zv;
+            y.p[i].den = y.p[i].den + (z + half * f.p[i].den);
+            y.p[i].vel = y.p[i].vel + (zv + half * f.p[i].vel);
+        }
+        for (size_t i = 0; i < ns; ++i) {
+            mat4<T> zm;
+            y.s[i].stress = y.s[i].stress + (zm + half * f.s[i].stress);
+        }
+        st = std::move(y);
+        fcarry = std::move(f);
+    }
+
     void step() {
+        if (verlet) {
+            step_verlet();
+            return;
+        }
         time += dt_sub;
         std::vector<State<T>> ks(tab.stages);
         State<T> y;
@@ -1074,6 +1129,7 @@ int orc_set_state(void* h, const double* den, const double* pos, const double* v
     dispatch(h, [&](auto& S) {
         using TT = std::remove_reference_t<decltype(S.st.p[0].den)>;
         auto& P = S.st.p;
+        S.fvalid = false;
         for (size_t i = 0; i < P.size(); ++i) {
             if (den) P[i].den = TT(den[i]);
             for (int c = 0; c < 4; ++c) {

@@ -33,3 +33,53 @@ def oracle_csr(buckets, n, ncells):
         members[start[c]:start[c + 1]] = np.sort(contents[c, bc + rc:bc + rc + cn])
         bmembers[bstart[c]:bstart[c + 1]] = np.sort(contents[c, :bc])
     return start, members, bstart, bmembers
+
+
+def load_seeded_scene(name):
+    """A seeded scene fixture of tests/golden/scenes_seeded (written by
+    tests/golden/make_scene_fixtures.py from the reference's example files)."""
+    import os
+    from arphys import scenes
+    z = np.load(os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scenes_seeded", name + ".npz"))
+    h, dt, g, alpha = (float(x) for x in z["scalars"])
+    return scenes.Scene(particles=z["particles"], boundary=z["boundary"], materials=z["materials"],
+                        bounds_min=tuple(float(x) for x in z["bounds_min"]),
+                        bounds_dim=tuple(float(x) for x in z["bounds_dim"]), h=h, integrator=str(z["integrator"]),
+                        dt=dt, subticks=int(z["subticks"]), gravity=g, alpha=alpha, interactions=z["interactions"],
+                        interaction_given=z["interaction_given"], name=str(z["name"]))
+
+
+def _oracle_loss(task):
+    """One FP64 oracle run for a finite difference: the scene stepped `steps`
+    times from the given per-solid stiffness and initial velocity (set in
+    double precision, so a small perturbation is not rounded to f32), and the
+    loss of the final positions: ("tip", caller ids, target) for the squared
+    distance of their centroid to the target, ("points", targets) for the
+    summed squared distances to per-particle targets."""
+    sc, steps, stiff, vel, loss = task
+    from oracle.oracle import Oracle, lib
+    lib().orc_set_threads(1)
+    o = Oracle(sc, 64)
+    if stiff is not None:
+        o.set_solid_stiffness(np.ascontiguousarray(stiff, np.float64))
+    if vel is not None:
+        v = np.zeros((sc.n, 4))
+        v[:, :3] = vel
+        o.set_state(vel=v)
+    o.step(steps)
+    pos = o.state()["pos"][:, :3]
+    if loss[0] == "tip":
+        d = pos[loss[1]].mean(axis=0) - np.asarray(loss[2], np.float64)
+        return float(d @ d)
+    d = pos - loss[1]
+    return float(np.sum(d * d))
+
+
+def oracle_losses(tasks, processes=None):
+    """_oracle_loss over many tasks in a pool of spawned processes (spawned,
+    not forked: the parent holds a CUDA context)."""
+    import multiprocessing as mp
+    import os
+    procs = processes or max(1, min(32, os.cpu_count() or 1, len(tasks)))
+    with mp.get_context("spawn").Pool(procs) as pool:
+        return pool.map(_oracle_loss, tasks, chunksize=1)

@@ -53,13 +53,6 @@ def test_null_scene_is_rejected(lib):
     assert b"null" in lib.arp_last_error()
 
 
-def test_verlet_is_reported_unsupported(lib):
-    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
-    sc.integrator = "verlet"
-    code, _, msg = _create(lib, sc)
-    assert code == 6 and "Verlet" in msg
-
-
 def test_four_dimensional_box_is_rejected(lib):
     sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
     sc.bounds_dim = (0.2, 0.2, 0.0, 0.1)

@@ -12,7 +12,7 @@ import numpy as np
 import pytest
 
 from arphys import FluidSim, scenes
-from oracle.oracle import Oracle
+from helpers import oracle_losses
 
 pytestmark = pytest.mark.gpu
 
@@ -23,18 +23,10 @@ def state_grad(n, gpos):
     return g
 
 
-def oracle_loss(sc, steps, stiff=None, vel=None, loss=None):
-    sc2 = scenes.Scene(**{**sc.__dict__, "particles": sc.particles.copy()})
-    if vel is not None:
-        sc2.particles["vel"][:, :3] = vel
-    o = Oracle(sc2, 64)
-    if stiff is not None:
-        o.set_solid_stiffness(stiff)
-    o.step(steps)
-    return loss(o.state()["pos"])
-
-
-def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4):
+def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4, eps_vel=1e-4):
+    """The GPU gradient along each direction, and the FP64 oracle's central
+    difference (L(p + e d) - L(p - e d)) / 2e along the same direction.
+    `loss` is ("tip", ids, target) or ("points", targets)."""
     stiff = sc.meta.get("stiffness")
     sim = FluidSim(sc)
     sim.init()
@@ -43,46 +35,65 @@ def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1
     sim.tape_begin(every)
     sim.step(steps)
     before = sim.particles().copy()
-    L, gx = loss(sim.particles()["pos"], True)
+    pos = sim.particles()["pos"][:, :3].astype(np.float64)
+    gx = np.zeros((sc.n, 3))
+    if loss[0] == "tip":
+        d = pos[loss[1]].mean(axis=0) - np.asarray(loss[2], np.float64)
+        L = float(d @ d)
+        gx[loss[1]] = 2.0 * d / len(loss[1])
+    else:
+        d = pos - loss[1]
+        L = float(np.sum(d * d))
+        gx = 2.0 * d
     g0, gs = sim.backward(state_grad(sc.n, gx))
     after = sim.particles()
     assert before.tobytes() == after.tobytes()  # the forward state is put back
-    out = []
-    v0 = sc.particles["vel"][:, :3].astype(np.float64)
-    for d in directions_stiff:
-        adj = float(np.sum(gs.astype(np.float64) * stiff.astype(np.float64) * d[:, None]))
-        e = eps_rel
-        lp = oracle_loss(sc, steps, stiff=stiff.astype(np.float64) * (1 + e * d[:, None]), loss=loss)
-        lm = oracle_loss(sc, steps, stiff=stiff.astype(np.float64) * (1 - e * d[:, None]), loss=loss)
-        out.append(("stiffness", adj, (lp - lm) / (2 * e)))
-    for d in directions_vel:
-        adj = float(np.sum(g0[:, 4:7].astype(np.float64) * d))
-        e = eps_rel
-        lp = oracle_loss(sc, steps, stiff=None if stiff is None else stiff.astype(np.float64), vel=v0 + e * d,
-                         loss=loss)
-        lm = oracle_loss(sc, steps, stiff=None if stiff is None else stiff.astype(np.float64), vel=v0 - e * d,
-                         loss=loss)
-        out.append(("velocity", adj, (lp - lm) / (2 * e)))
     sim.tape_end()
+    v0 = sc.particles["vel"][:, :3].astype(np.float64)
+    s64 = None if stiff is None else stiff.astype(np.float64)
+    tasks, adj = [], []
+    for d in directions_stiff:
+        adj.append(("stiffness", float(np.sum(gs.astype(np.float64) * s64 * d[:, None]))))
+        tasks += [(sc, steps, s64 * (1 + eps_rel * d[:, None]), None, loss),
+                  (sc, steps, s64 * (1 - eps_rel * d[:, None]), None, loss)]
+    for d in directions_vel:
+        adj.append(("velocity", float(np.sum(g0[:, 4:7].astype(np.float64) * d))))
+        tasks += [(sc, steps, s64, v0 + eps_vel * d, loss), (sc, steps, s64, v0 - eps_vel * d, loss)]
+    ls = oracle_losses(tasks)
+    out = []
+    for q, (kind, a) in enumerate(adj):
+        e = eps_rel if kind == "stiffness" else eps_vel
+        out.append((kind, a, (ls[2 * q] - ls[2 * q + 1]) / (2 * e)))
     return L, out
 
 
+def report(res, tol):
+    """Per-direction relative error |adj - fd| / |fd|; returns the worst."""
+    worst = 0.0
+    for kind in ("stiffness", "velocity"):
+        rows = [(a, f) for k, a, f in res if k == kind]
+        if not rows:
+            continue
+        errs = [abs(a - f) / max(abs(f), 1e-300) for a, f in rows]
+        mags = [abs(f) for _, f in rows]
+        print(f"{kind}: {len(rows)} directions, |fd| {min(mags):.3e} .. {max(mags):.3e}, "
+              f"rel err median {np.median(errs):.2e} max {max(errs):.2e} (bound {tol:.0e})")
+        worst = max(worst, max(errs))
+    return worst
+
+
 def test_cantilever_bar_gradients_match_fp64_finite_differences():
-    sc = scenes.cantilever_bar(n=(4, 16, 4), v_sigma=0.2, target_offset=(0.002, -0.02, 0.001))
-    tip, target = sc.meta["tip"], sc.meta["target"]
-
-    def loss(pos, want_grad=False):
-        L, g = scenes.tip_loss(pos, tip, target)
-        return (L, g) if want_grad else L
-
+    """The differentiation workload's bar at reduced size (4 x 32 x 4 sites,
+    clamped base, lognormal E, gravity, RK2, checkpoints every 20) from a seeded
+    random initial velocity field: the gradients of the tip-centroid loss with
+    respect to the per-particle stiffness and the initial velocities along 32
+    seeded directions each agree with FP64 central differences within 1e-4."""
+    sc = scenes.cantilever_bar(n=(4, 32, 4), v_sigma=0.05, target_offset=(0.002, -0.02, 0.001))
     rng = np.random.default_rng(44)
-    ds = [rng.normal(size=sc.n) for _ in range(3)]
-    dv = [rng.normal(size=(sc.n, 3)) for _ in range(3)]
-    L, res = fd_check(sc, 200, 20, loss, ds, dv)
-    for kind, adj, fd in res:
-        err = abs(adj - fd) / max(abs(fd), 1e-30)
-        print(f"{kind}: adjoint {adj:.6e} fd64 {fd:.6e} rel err {err:.2e}")
-        assert err < 2e-3, (kind, adj, fd)
+    ds = [rng.normal(size=sc.n) for _ in range(32)]
+    dv = [rng.normal(size=(sc.n, 3)) for _ in range(32)]
+    L, res = fd_check(sc, 200, 20, ("tip", sc.meta["tip"], sc.meta["target"]), ds, dv)
+    assert report(res, 1e-4) < 1e-4
 
 
 def test_fluid_gradients_match_fp64_finite_differences():
@@ -91,22 +102,13 @@ def test_fluid_gradients_match_fp64_finite_differences():
     sc.particles["vel"][:, :2] = rng.normal(0.0, 0.2, size=(sc.n, 2)).astype(np.float32)
     target = (sc.particles["pos"][:, :3] + rng.normal(0.0, 0.002, size=(sc.n, 3))).astype(np.float64)
     target[:, 2] = 0.0
-
-    def loss(pos, want_grad=False):
-        d = pos[:, :3].astype(np.float64) - target
-        L = float(np.sum(d * d))
-        return (L, 2.0 * d) if want_grad else L
-
     dv = []
-    for _ in range(3):
+    for _ in range(32):
         d = rng.normal(size=(sc.n, 3))
         d[:, 2] = 0.0
         dv.append(d)
-    L, res = fd_check(sc, 20, 5, loss, [], dv)
-    for kind, adj, fd in res:
-        err = abs(adj - fd) / max(abs(fd), 1e-30)
-        print(f"{kind}: adjoint {adj:.6e} fd64 {fd:.6e} rel err {err:.2e}")
-        assert err < 2e-3, (kind, adj, fd)
+    L, res = fd_check(sc, 20, 5, ("points", target), [], dv)
+    assert report(res, 1e-4) < 1e-4
 
 
 def test_tape_refuses_plastic_materials_and_backward_without_tape():

@@ -1,0 +1,96 @@
+"""Velocity Verlet (the reference's default integrator,
+examples/test_mods/config.rs:451; selected at examples/test.rs:167) on the GPU
+against the oracle's kick-drift-kick restatement: synthetic fluid and
+fluid + solid scenes, and the reference's own Verlet scenes as seeded by the
+scene loader (fixtures under tests/golden/scenes_seeded).  State within 1e-5
+norm-wise relative error of the float oracle after the stated steps; the
+error against the double oracle is printed beside it."""
+import numpy as np
+import pytest
+
+from arphys import FluidSim, scenes
+from oracle.oracle import Oracle
+from helpers import load_seeded_scene, rel_err
+
+pytestmark = pytest.mark.gpu
+
+
+def compare(sc, steps, tol=1e-5, graph=False):
+    sim = FluidSim(sc)
+    sim.init()
+    if graph:
+        sim.set_graph(True)
+    sim.step(steps)
+    g = sim.particles()
+    o32, o64 = Oracle(sc, 32), Oracle(sc, 64)
+    o32.step(steps)
+    o64.step(steps)
+    r32, r64 = o32.state(), o64.state()
+    assert abs(sim.time() - o32.time) < 1e-6
+    for key in ("den", "pos", "vel"):
+        e = rel_err(g[key], r32[key])
+        e64 = rel_err(g[key], r64[key])
+        print(f"{sc.name} {key}: vs f32 oracle {e:.2e}, vs f64 oracle {e64:.2e}")
+        assert e < tol, (sc.name, key, e)
+    return sim
+
+
+def test_verlet_dam_break_matches_oracle():
+    sc = scenes.dam_break_2d(nx=48, ny=48, box=(0.96, 0.64), integrator="verlet")
+    compare(sc, 100)
+
+
+def test_verlet_fluid_and_solid_match_oracle():
+    sc = scenes.small_fluid_bar_3d(integrator="verlet")
+    compare(sc, 60)
+
+
+def test_verlet_graph_replay_matches_plain_steps():
+    sc = scenes.small_fluid_bar_3d(integrator="verlet")
+    a = FluidSim(sc)
+    a.init()
+    a.step(7)
+    b = FluidSim(sc)
+    b.init()
+    b.set_graph(True)
+    b.step(7)
+    assert a.particles().tobytes() == b.particles().tobytes()
+    assert a.time() == b.time()
+
+
+def test_verlet_restarts_from_a_new_state():
+    """After set_particles the first step evaluates the forces at the new
+    state again, as the oracle does after its state is replaced."""
+    sc = scenes.dam_break_2d(nx=16, ny=16, box=(0.32, 0.32), integrator="verlet")
+    sim = FluidSim(sc)
+    sim.init()
+    sim.step(5)
+    p = sim.particles().copy()
+    p["vel"][:, 0] += np.float32(0.05)
+    sim.set_particles(p)
+    sim.step(5)
+    o = Oracle(sc, 32)
+    o.step(5)
+    s = o.state()
+    o.set_state(den=s["den"], pos=s["pos"], vel=s["vel"] + np.array([0.05, 0, 0, 0]))
+    o.step(5)
+    r = o.state()
+    for key in ("den", "pos", "vel"):
+        assert rel_err(sim.particles()[key], r[key]) < 1e-5, key
+
+
+@pytest.mark.parametrize("name,steps", [("cloth", 40), ("solid_test_3D", 60), ("spinning_ball", 60),
+                                        ("container_buckling", 40)])
+def test_reference_verlet_scenes_match_oracle(name, steps):
+    sc = load_seeded_scene(name)
+    assert sc.integrator == "verlet"
+    compare(sc, steps)
+
+
+def test_tape_refuses_verlet():
+    sc = scenes.cantilever_bar(n=(4, 8, 4), integrator="verlet")
+    sim = FluidSim(sc)
+    sim.init()
+    with pytest.raises(Exception) as e:
+        sim.tape_begin(4)
+    assert e.value.code == 6

@@ -114,7 +114,7 @@ def test_neighbor_buckets_match_brute_force():
     assert cnt == sc.n
 
 
-@pytest.mark.parametrize("integ", ["euler", "midpoint", "heun2", "ralston", "rk3", "heun3", "rk4", "rk_3_8"])
+@pytest.mark.parametrize("integ", ["euler", "midpoint", "heun2", "ralston", "rk3", "heun3", "rk4", "rk_3_8", "verlet"])
 def test_free_fall_is_integrated_exactly(integ):
     """An isolated particle feels only gravity; any consistent tableau
     integrates x(t) = x0 + v0 t - g t^2 / 2 exactly for order >= 2."""

@@ -278,15 +278,12 @@ integrator = "rk2"
     assert set(np.unique(sc.particles["mat"])) == {1, 2, 3}
 
 
-def test_defaults_scene_loads_and_verlet_is_rejected_at_create():
+def test_defaults_scene_loads_with_the_verlet_default():
     path = os.path.join(HERE, "golden", "scenes", "defaults.toml")
     sc = scenes.load_toml(path)
-    assert sc.name == "Fluid Test" and sc.integrator == "verlet"
+    assert sc.name == "Fluid Test" and sc.integrator == "verlet"  # config.rs:451
     assert f32(sc.h) == f32(1.0 / 64.0) and f32(sc.dt) == f32(0.01)
     assert sc.bounds_min[:2] == (-1.0, -1.0) and sc.bounds_dim[:2] == (2.0, 2.0)
-    with pytest.raises(ArpError) as e:
-        FluidSim.from_toml(path)
-    assert e.value.code == 6
 
 
 @pytest.mark.parametrize("text,code,needle", [
