@@ -191,6 +191,7 @@ def load_library():
     sig["arp_sim_set_graph"] = [c_sim, ctypes.c_int]
     sig["arp_sim_autotune"] = [c_sim, ctypes.POINTER(ctypes.c_int)]
     sig["arp_sim_set_fluid_variant"] = [c_sim, ctypes.c_int]
+    sig["arp_fluid_variant_count"] = []
     sig["arp_sim_fluid_variant"] = [c_sim, ctypes.POINTER(ctypes.c_int), ctypes.POINTER(ctypes.c_int),
                                      ctypes.POINTER(ctypes.c_int)]
     sig["arp_sim_scene_range"] = [c_sim, ctypes.c_uint32, u32p, u32p, u32p, u32p, u32p, u32p]

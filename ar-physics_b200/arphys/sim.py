@@ -187,6 +187,12 @@ class FluidSim:
         check(self._L.arp_sim_autotune(self._h, ctypes.byref(v)))
         return v.value
 
+    @staticmethod
+    def fluid_variant_count():
+        """Number of launch shapes of the fluid kernel."""
+        from .abi import load_library
+        return int(load_library().arp_fluid_variant_count())
+
     def set_fluid_variant(self, v):
         check(self._L.arp_sim_set_fluid_variant(self._h, int(v)))
 

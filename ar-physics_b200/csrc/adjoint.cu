@@ -4,22 +4,20 @@
 // (one (x, rho) and one (v) float4 per particle), these kernels accumulate
 // lam_Y += J_f(Y)^T mu, hand-derived term by term from the forward kernels:
 //   * k_adj_solid   elastic force (solid.rs:343-374), hourglass control
-//                   (solid.rs:430-443) and the order-2 stress chain
+//                   (solid.rs:430-443) and the stress chain of any strain order
 //                   F, dF/dt -> E, dE/dt -> S (Hooke) -> sigma = F S^T -> A = sigma L
 //                   (strain.rs:139-160, solid.rs:147-204,334-341), plus the
 //                   gradient of the per-solid (normal, shear) stiffness;
 //   * k_adj_strain  F and dF/dt as sums over the reference neighbors;
 //   * k_adj_fluid   every fluid pair term (continuity, pressure with the
 //                   state equation, contact potential, viscosity, artificial
-//                   viscosity; fluid.rs:154-247) and dx/dt = v.
+//                   viscosity, friction; fluid.rs:154-247) and dx/dt = v.
 // Neighbor sets (hits within h, reference lists, the current-cell condition
 // of the hourglass term) are those of the recorded forward stage and are not
 // differentiated.  Each particle gathers the contributions of its own pairs
 // and of its neighbors' pairs (pairwise-symmetric gathers): no atomics, each
-// thread writes only its own particle.  Not differentiated: friction (the
-// tape refuses interactions with a friction coefficient), plastic flow and
-// strain orders other than 2 (refused), self-contact (flagged when a pair is
-// active).
+// thread writes only its own particle.  Not differentiated: plastic flow
+// (refused), self-contact (flagged when a pair is active).
 #include "grid.cuh"
 #include "warp.cuh"
 
@@ -111,14 +109,6 @@ __device__ __forceinline__ void m3_acc(M3& a, const M3& b) {
     for (int i = 0; i < 3; ++i)
 #pragma unroll
         for (int j = 0; j < 3; ++j) a.m[i][j] += b.m[i][j];
-}
-__device__ __forceinline__ M3 m3_sym(const M3& a) {
-    M3 r;
-#pragma unroll
-    for (int i = 0; i < 3; ++i)
-#pragma unroll
-        for (int j = 0; j < 3; ++j) r.m[i][j] = 0.5f * (a.m[i][j] + a.m[j][i]);
-    return r;
 }
 
 __device__ __forceinline__ float3 mask_dim(float3 v, uint32_t dim) {
@@ -231,10 +221,11 @@ __device__ __forceinline__ PairGeom flipped(const PairGeom& G) {
 
 // The fluid pair term of `a` with neighbor `b` (fluid.rs:154-214, as the
 // forward kernel evaluates it) and its vector-Jacobian product for weights
-// wd (on d rho/dt) and wF (on the force sum).  Friction is not included.
+// wd (on d rho/dt) and wF (on the force sum), friction (fluid.rs:192-199)
+// included.
 template <int DIM, bool BOUNDARY>
 __device__ __forceinline__ void pair_vjp(const PairGeom& G, const PairSide& a, const PairSide& b, float dampening,
-                                         float wd, float3 wF, PairGrad& o) {
+                                         float friction, float wd, float3 wF, PairGrad& o) {
     const float3 r = G.r, vv = G.vv, g = G.g;
     float3 F = make_float3(0.f, 0.f, 0.f), lg = F, lr = F, lvv = F;
     float ld1 = 0.f, ld2 = 0.f;
@@ -254,6 +245,36 @@ __device__ __forceinline__ void pair_vjp(const PairGeom& G, const PairSide& a, c
         lg = add(lg, mul(cs, wF));
         ld2 -= wg * cs * b.inv_d;
         lr = mul(wg * b.m * b.inv_d * G.dcp_over_R, r);
+        if (friction != 0.0f && (a.elastic || b.elastic || BOUNDARY) && a.mat != b.mat) {
+            // forward: the normal force r (cs g.r) / r.r = cs gws r has length
+            // N = |cs gws| R; the tangential velocity u = vv - r (vv.r) / r.r
+            // gives t = u / |u|, and the force gains friction N t (the second
+            // normalize of the shader leaves t as it is)
+            const float r2 = dot(r, r);
+            const float sv = dot(vv, r) / r2;
+            const float3 u = sub(vv, mul(sv, r));
+            const float ul = sqrtf(dot(u, u));
+            const float3 t = mul(1.0f / ul, u);
+            if (isfinite(t.x) && isfinite(t.y) && isfinite(t.z)) {
+                const float R = sqrtf(r2);
+                const float acs = fabsf(cs), ags = fabsf(G.gws);
+                const float N = acs * ags * R;
+                F = add(F, mul(friction * N, t));
+                const float wt = dot(wF, t);
+                // through t = u / |u| and u = (I - r r^T / r.r) vv
+                const float3 lu = mul(friction * N / ul, sub(wF, mul(wt, t)));
+                const float lur = dot(lu, r);
+                lvv = add(lvv, sub(lu, mul(lur / r2, r)));
+                lr = add(lr, sub(mul(-sv, lu), mul(lur / r2, sub(vv, mul(2.0f * sv, r)))));
+                // through N: |cs| ~ 1/rho_b; dN/dR from cp(R), gws(R) (d gws/dR = c24 R) and R
+                const float lN = friction * wt;
+                ld2 -= lN * N * b.inv_d;
+                const float dcs = copysignf(b.m * b.inv_d * G.dcp_over_R * R, cs);
+                const float dgs = copysignf(G.c24 * R, G.gws);
+                const float dN = dcs * ags * R + acs * dgs * R + acs * ags;
+                lr = add(lr, mul(lN * dN / R, r));
+            }
+        }
     }
     if (!BOUNDARY) {
         float ldenom = 0.0f;
@@ -372,7 +393,7 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const flo
             const DevInter it = row_i[matb - P.mat_base];
             const PairGeom G = make_geom<DIM>(si.x, si.v, sb.x, sb.v, it, P.h2, P.kconst, P.eps_hh);
             PairGrad o;
-            pair_vjp<DIM, true>(G, si, sb, it.dampening, wd, wF, o);
+            pair_vjp<DIM, true>(G, si, sb, it.dampening, it.friction, wd, wF, o);
             Fs = add(Fs, o.F);
             lx = sub(lx, o.lr);
             lv = sub(lv, o.lvv);
@@ -391,13 +412,13 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const flo
             const DevInter it = row_i[matj - P.mat_base];  // symmetric: also the neighbor's entry
             const PairGeom G = make_geom<DIM>(si.x, si.v, sj.x, sj.v, it, P.h2, P.kconst, P.eps_hh);
             PairGrad o;
-            pair_vjp<DIM, false>(G, si, sj, it.dampening, wd, wF, o);
+            pair_vjp<DIM, false>(G, si, sj, it.dampening, it.friction, wd, wF, o);
             Fs = add(Fs, o.F);
             lx = sub(lx, o.lr);
             lv = sub(lv, o.lvv);
             lrho += o.ld_self + o.lpt * dpt_i;
             // the neighbor's own pair, in which this particle is the neighbor
-            pair_vjp<DIM, false>(flipped(G), sj, si, it.dampening, wj.w, f3(wj), o);
+            pair_vjp<DIM, false>(flipped(G), sj, si, it.dampening, it.friction, wj.w, f3(wj), o);
             lx = add(lx, o.lr);
             lv = add(lv, o.lvv);
             lrho += o.ld_nbr + o.lpt * dpt_i;
@@ -442,6 +463,205 @@ __global__ void __launch_bounds__(kT) k_adj_fluid(AdjArgs a, Tables T, const flo
     lw.z += lv.z;
     a.lam_pd[i] = lp;
     a.lam_vm[i] = lw;
+}
+
+// ---- Seth-Hill strain of any order and its VJP (3x3: the padded fourth axis,
+// where C = 1, stays out of every matrix function) --------------------------
+__device__ __forceinline__ M3 m3_ident() {
+    M3 r = m3_zero();
+    r.m[0][0] = r.m[1][1] = r.m[2][2] = 1.0f;
+    return r;
+}
+__device__ __forceinline__ M3 m3_scale(float s, const M3& a) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = s * a.m[i][j];
+    return r;
+}
+__device__ __forceinline__ M3 m3_add(const M3& a, const M3& b) {
+    M3 r = a;
+    m3_acc(r, b);
+    return r;
+}
+__device__ __forceinline__ M3 m3_sub(const M3& a, const M3& b) {
+    M3 r;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) r.m[i][j] = a.m[i][j] - b.m[i][j];
+    return r;
+}
+__device__ inline M3 m3_inv(const M3& a) {  // adjugate over determinant
+    const float (&m)[3][3] = a.m;
+    M3 c;
+    c.m[0][0] = m[1][1] * m[2][2] - m[1][2] * m[2][1];
+    c.m[0][1] = m[0][2] * m[2][1] - m[0][1] * m[2][2];
+    c.m[0][2] = m[0][1] * m[1][2] - m[0][2] * m[1][1];
+    c.m[1][0] = m[1][2] * m[2][0] - m[1][0] * m[2][2];
+    c.m[1][1] = m[0][0] * m[2][2] - m[0][2] * m[2][0];
+    c.m[1][2] = m[0][2] * m[1][0] - m[0][0] * m[1][2];
+    c.m[2][0] = m[1][0] * m[2][1] - m[1][1] * m[2][0];
+    c.m[2][1] = m[0][1] * m[2][0] - m[0][0] * m[2][1];
+    c.m[2][2] = m[0][0] * m[1][1] - m[0][1] * m[1][0];
+    const float det = m[0][0] * c.m[0][0] + m[0][1] * c.m[1][0] + m[0][2] * c.m[2][0];
+    return m3_scale(1.0f / det, c);
+}
+__device__ inline M3 m3_pow(const M3& c, int m) {
+    M3 r = m3_ident();
+    for (int i = 0; i < m; ++i) r = m3_mul(r, c);
+    return r;
+}
+// Denman-Beavers square root, the iteration of solid.rs:119-133
+__device__ inline M3 m3_sqrt_db(const M3& c) {
+    M3 Y = c, Z = m3_ident();
+    for (int i = 0; i < 15; ++i) {
+        const M3 Yn = m3_scale(0.5f, m3_add(Y, m3_inv(Z)));
+        const M3 Zn = m3_scale(0.5f, m3_add(Z, m3_inv(Y)));
+        Y = Yn;
+        Z = Zn;
+    }
+    return Y;
+}
+// X with R X + X R = W (R symmetric): the VJP of the square root, whose
+// differential solves R dR + dR R = dC (the operator is self-adjoint for a
+// symmetric R).  A 9 x 9 system, Gaussian elimination with partial pivoting.
+__device__ inline M3 lyap_solve(const M3& R, const M3& W) {
+    float A[9][10];
+#pragma unroll
+    for (int p = 0; p < 9; ++p)
+#pragma unroll
+        for (int q = 0; q < 10; ++q) A[p][q] = 0.0f;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) {
+            const int p = 3 * r + c;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                A[p][3 * k + c] += R.m[r][k];
+                A[p][3 * r + k] += R.m[k][c];
+            }
+            A[p][9] = W.m[r][c];
+        }
+    for (int col = 0; col < 9; ++col) {
+        int piv = col;
+        for (int p = col + 1; p < 9; ++p)
+            if (fabsf(A[p][col]) > fabsf(A[piv][col])) piv = p;
+        if (piv != col)
+            for (int q = 0; q < 10; ++q) {
+                const float t = A[col][q];
+                A[col][q] = A[piv][q];
+                A[piv][q] = t;
+            }
+        const float inv = 1.0f / A[col][col];
+        for (int p = col + 1; p < 9; ++p) {
+            const float f = A[p][col] * inv;
+            for (int q = col; q < 10; ++q) A[p][q] -= f * A[col][q];
+        }
+    }
+    float x[9];
+    for (int p = 8; p >= 0; --p) {
+        float t = A[p][9];
+        for (int q = p + 1; q < 9; ++q) t -= A[p][q] * x[q];
+        x[p] = t / A[p][p];
+    }
+    M3 X;
+#pragma unroll
+    for (int r = 0; r < 3; ++r)
+#pragma unroll
+        for (int c = 0; c < 3; ++c) X.m[r][c] = x[3 * r + c];
+    return X;
+}
+// d/dC of C^m against weight W: sum_k C^k W C^(m-1-k) (C symmetric)
+__device__ inline M3 m3_pow_vjp(const M3& C, int m, const M3& W) {
+    M3 g = m3_zero();
+    for (int k = 0; k < m; ++k) m3_acc(g, m3_mul(m3_mul(m3_pow(C, k), W), m3_pow(C, m - 1 - k)));
+    return g;
+}
+// E = seth_hill(C, two_m) (solid.rs:147-168; C padded with ones)
+__device__ inline M3 sh_forward(const M3& C, int two_m) {
+    if (two_m == 0) {  // 0.5 * the 5-term log series of solid.rs:105-116
+        const M3 D = m3_sub(C, m3_ident());
+        M3 sum = m3_zero(), Dk = m3_ident();
+        for (int i = 1; i <= 5; ++i) {
+            Dk = m3_mul(Dk, D);
+            m3_acc(sum, m3_scale((i & 1 ? 1.0f : -1.0f) / (float)i, Dk));
+        }
+        return m3_scale(0.5f, sum);
+    }
+    const int a = two_m < 0 ? -two_m : two_m;
+    M3 M = m3_pow(C, a >> 1);
+    if (a & 1) M = m3_mul(M, m3_sqrt_db(C));
+    if (two_m < 0) M = m3_inv(M);
+    return m3_scale(1.0f / (float)two_m, m3_sub(M, m3_ident()));
+}
+// dL/dC of E = seth_hill(C, two_m) for the weight W on E
+__device__ inline M3 sh_vjp(const M3& C, int two_m, const M3& W) {
+    if (two_m == 0) {
+        const M3 D = m3_sub(C, m3_ident());
+        const M3 hw = m3_scale(0.5f, W);
+        M3 g = m3_zero();
+        for (int i = 1; i <= 5; ++i) m3_acc(g, m3_scale((i & 1 ? 1.0f : -1.0f) / (float)i, m3_pow_vjp(D, i, hw)));
+        return g;
+    }
+    const int a = two_m < 0 ? -two_m : two_m, m = a >> 1;
+    const M3 Pm = m3_pow(C, m);
+    const M3 Rt = (a & 1) ? m3_sqrt_db(C) : m3_ident();
+    const M3 Q = m3_mul(Pm, Rt);
+    M3 lQ = m3_scale(1.0f / (float)two_m, W);
+    if (two_m < 0) {  // M = Q^-1: dL/dQ = -Q^-T W' Q^-T
+        const M3 Qi = m3_inv(Q);
+        lQ = m3_scale(-1.0f, m3_mul(m3_mul(m3_t(Qi), lQ), m3_t(Qi)));
+    }
+    M3 g = m3_pow_vjp(C, m, m3_mul(lQ, m3_t(Rt)));
+    if (a & 1) m3_acc(g, lyap_solve(Rt, m3_mul(m3_t(Pm), lQ)));
+    return g;
+}
+// Ed = seth_hill_rate(C, dC, two_m) (solid.rs:170-204): 0.5 dC C^-1 for order
+// 0, else (1/two_m) sum_i C^i dC C^(m-1-i) (the square-root part is not
+// differentiated in time there, the shader's TODO), conjugated by -C^-1 for
+// negative orders
+__device__ inline M3 sh_rate_forward(const M3& C, const M3& dC, int two_m) {
+    if (two_m == 0) return m3_mul(m3_scale(0.5f, dC), m3_inv(C));
+    const int a = two_m < 0 ? -two_m : two_m, m = a >> 1;
+    M3 rate = m3_zero();
+    for (int i = 0; i < m; ++i) m3_acc(rate, m3_mul(m3_mul(m3_pow(C, i), dC), m3_pow(C, m - 1 - i)));
+    rate = m3_scale(1.0f / (float)two_m, rate);
+    if (two_m < 0) {
+        const M3 iC = m3_inv(C);
+        return m3_scale(-1.0f, m3_mul(m3_mul(iC, rate), iC));
+    }
+    return rate;
+}
+__device__ inline void sh_rate_vjp(const M3& C, const M3& dC, int two_m, const M3& W, M3& lC, M3& ldC) {
+    if (two_m == 0) {  // 0.5 dC Ci
+        const M3 Ci = m3_inv(C);
+        ldC = m3_scale(0.5f, m3_mul(W, m3_t(Ci)));
+        const M3 lCi = m3_scale(0.5f, m3_mul(m3_t(dC), W));
+        lC = m3_scale(-1.0f, m3_mul(m3_mul(m3_t(Ci), lCi), m3_t(Ci)));
+        return;
+    }
+    const int a = two_m < 0 ? -two_m : two_m, m = a >> 1;
+    M3 lX = m3_scale(1.0f / (float)two_m, W);
+    lC = m3_zero();
+    if (two_m < 0) {  // Ed = -Ci X Ci, X = rate / two_m
+        const M3 Ci = m3_inv(C);
+        M3 X = m3_zero();
+        for (int i = 0; i < m; ++i) m3_acc(X, m3_mul(m3_mul(m3_pow(C, i), dC), m3_pow(C, m - 1 - i)));
+        X = m3_scale(1.0f / (float)two_m, X);
+        const M3 lCi = m3_scale(-1.0f, m3_add(m3_mul(W, m3_t(m3_mul(X, Ci))), m3_mul(m3_t(m3_mul(Ci, X)), W)));
+        lC = m3_scale(-1.0f, m3_mul(m3_mul(m3_t(Ci), lCi), m3_t(Ci)));
+        lX = m3_scale(-1.0f / (float)two_m, m3_mul(m3_mul(m3_t(Ci), W), m3_t(Ci)));
+    }
+    ldC = m3_zero();
+    for (int i = 0; i < m; ++i) {
+        const M3 Pi = m3_pow(C, i), Pj = m3_pow(C, m - 1 - i);
+        m3_acc(ldC, m3_mul(m3_mul(m3_t(Pi), lX), m3_t(Pj)));
+        m3_acc(lC, m3_pow_vjp(C, i, m3_mul(lX, m3_t(m3_mul(dC, Pj)))));
+        m3_acc(lC, m3_pow_vjp(C, m - 1 - i, m3_mul(m3_t(m3_mul(Pi, dC)), lX)));
+    }
 }
 
 // Hourglass pair term of `self` (solid.rs:430-443 as k_solid_forces evaluates
@@ -497,7 +717,9 @@ __device__ __forceinline__ bool in_stencil2(uint2 a, uint2 b) {
 // LANES threads share one solid: both reference-list loops are split over
 // them with stride LANES, their partial sums combined by group_sum; lane 0
 // finishes the particle.
-template <int LANES>
+// GENERAL: some solid material has a strain order other than 2 (the log
+// series, square roots and inverses are compiled out otherwise).
+template <int LANES, bool GENERAL>
 __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t i = t / LANES, lane = t % LANES;
@@ -605,20 +827,25 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
         }
     }
     lrho -= dot(w, fs) / d1;  // k_v = f / rho - g
-    // stress chain (order 2): E = (F^T F - I)/2, dE/dt = (dF^T F + F^T dF)/2,
+    // stress chain: C = F^T F (padded with ones past dim), dC = dF^T F + F^T dF,
+    // E = seth_hill(C), dE/dt = seth_hill_rate(C, dC) (any strain order),
     // S = Hooke(E; n, s) + Hooke(dE/dt; n_d, s_d), sigma = F S^T, A = sigma L
     const uint32_t dim = P.dim;
-    M3 E = m3_mul(m3_t(Fi), Fi);
-#pragma unroll
-    for (int q = 0; q < 3; ++q) E.m[q][q] -= 1.0f;
-#pragma unroll
-    for (int r = 0; r < 3; ++r)
-#pragma unroll
-        for (int c = 0; c < 3; ++c) E.m[r][c] *= 0.5f;
+    const int two_m = mm.strain_order;
+    M3 C = m3_mul(m3_t(Fi), Fi);
 #pragma unroll
     for (int q = 0; q < 3; ++q)
-        if ((uint32_t)q >= dim) E.m[q][q] = 0.0f;  // padded axes: C = 1 there
-    const M3 Ed = m3_sym(m3_mul(m3_t(Fd), Fi));
+        if ((uint32_t)q >= dim) C.m[q][q] = 1.0f;
+    const M3 Rfd = m3_mul(m3_t(Fd), Fi);
+    const M3 dC = m3_add(Rfd, m3_t(Rfd));
+    M3 E, Ed;
+    if (!GENERAL || two_m == 2) {
+        E = m3_scale(0.5f, m3_sub(C, m3_ident()));
+        Ed = m3_scale(0.5f, dC);
+    } else {
+        E = sh_forward(C, two_m);
+        Ed = sh_rate_forward(C, dC, two_m);
+    }
     const float2 lm = a.stiff ? a.stiff[i] : make_float2(mm.lam, mm.mu);
     float trE = 0.f, trEd = 0.f;
 #pragma unroll
@@ -650,9 +877,24 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
             gs += 2.0f * lS.m[r][c] * E.m[r][c];
         }
     const float gn = trE * trS;
-    m3_acc(lF, m3_mul(Fi, m3_sym(lE)));
-    m3_acc(lF, m3_mul(Fd, m3_sym(lEd)));
-    const M3 lFd = m3_mul(Fi, m3_sym(lEd));
+    M3 lC, ldC;
+    if (!GENERAL || two_m == 2) {
+        lC = m3_scale(0.5f, lE);
+        ldC = m3_scale(0.5f, lEd);
+    } else {
+        lC = sh_vjp(C, two_m, lE);
+        M3 lC2;
+        sh_rate_vjp(C, dC, two_m, lEd, lC2, ldC);
+        m3_acc(lC, lC2);
+    }
+#pragma unroll
+    for (int q = 0; q < 3; ++q)
+        if ((uint32_t)q >= dim) lC.m[q][q] = 0.0f;  // the padded ones do not depend on F
+    // C = F^T F; dC = R + R^T with R = dF^T F
+    const M3 lR = m3_add(ldC, m3_t(ldC));
+    m3_acc(lF, m3_mul(Fi, m3_add(lC, m3_t(lC))));
+    m3_acc(lF, m3_mul(Fd, lR));
+    const M3 lFd = m3_mul(Fi, m3_t(lR));
     m3_acc(lF, lFh);
     m3_store_cols(lF, a.lamF + 3 * i);
     m3_store_cols(lFd, a.lamFd + 3 * i);
@@ -757,7 +999,10 @@ __global__ void k_adj_perm(uint32_t n, const uint32_t* __restrict__ orig, const 
 int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st) {
     int launches = 0;
     if (a.solid_branch && a.ns > 0) {
-        k_adj_solid<kAdjSolidLanes><<<nblocks(a.ns * kAdjSolidLanes, kT), kT, 0, st>>>(a, T);
+        if (a.all_order2)
+            k_adj_solid<kAdjSolidLanes, false><<<nblocks(a.ns * kAdjSolidLanes, kT), kT, 0, st>>>(a, T);
+        else
+            k_adj_solid<kAdjSolidLanes, true><<<nblocks(a.ns * kAdjSolidLanes, kT), kT, 0, st>>>(a, T);
         k_adj_strain<<<nblocks(a.ns, kT), kT, 0, st>>>(a, T);
         launches += 2;
     }

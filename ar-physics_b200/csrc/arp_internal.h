@@ -272,8 +272,9 @@ struct FluidVariant {
     int cap;         // hit-list entries per thread
     int persistent;  // tile-queue form
     int flush;       // warp-voted list flushes (kFlush) instead of pass 1 then pass 2
+    int staged;      // candidates staged in shared memory per tile before the scan
 };
-constexpr int kNumFluidVariants = 10;
+constexpr int kNumFluidVariants = 12;
 extern const FluidVariant kFluidVariants[kNumFluidVariants];
 // `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -403,6 +404,7 @@ struct AdjArgs {
     float4* xs;                // [n] scratch: the stage positions in cell order
     uint32_t n, ns;
     int solid_branch;
+    int all_order2;            // every solid material has strain order 2
 };
 // One stage VJP: lam_{Y_s} += J_f(Y_s)^T mu_s (+ stiffness gradients).  Returns launches.
 int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st);

@@ -194,6 +194,104 @@ __device__ __forceinline__ void eval_hit(uint32_t j, const Self& s, const FluidA
     }
 }
 
+// The derivative record of one particle (fluid.rs:243-247, plus the solid
+// term when active) and the Runge-Kutta stage epilogue: the store of k, the
+// b-weighted accumulator and the next stage state, in storage slot `slot`.
+__device__ __forceinline__ void stage_epilogue(const FluidArgs& a, const StageCoefs& c, const StageBuffers& b,
+                                               uint32_t slot, uint32_t sid, float4 vi, const Acc& acc, float d1,
+                                               float g_acc, bool solid_scene) {
+    float4 kpd = make_float4(vi.x, vi.y, vi.z, acc.den);
+    float4 kvm = make_float4(__fdiv_rn(acc.f.x, d1), __fadd_rn(__fdiv_rn(acc.f.y, d1), -g_acc),
+                             __fdiv_rn(acc.f.z, d1), 0.0f);
+    if (a.solid_branch && sid != kInvalid && solid_scene) {
+        const float4 ks = a.ksol[sid];
+        kpd.x = __fadd_rn(kpd.x, vi.x);
+        kpd.y = __fadd_rn(kpd.y, vi.y);
+        kpd.z = __fadd_rn(kpd.z, vi.z);
+        kvm.x = __fadd_rn(kvm.x, ks.x);
+        kvm.y = __fadd_rn(kvm.y, ks.y);
+        kvm.z = __fadd_rn(kvm.z, ks.z);
+    }
+
+    // Runge-Kutta stage epilogue
+    if (b.store_pd) {
+        b.store_pd[slot] = kpd;
+        b.store_vm[slot] = kvm;
+    }
+    const float4 y0p = b.y0_pd[slot];
+    const float4 y0v = b.y0_vm[slot];
+    float4 accp = make_float4(0.f, 0.f, 0.f, 0.f), accv = make_float4(0.f, 0.f, 0.f, 0.f);
+    if (c.c_acc != 0.0f) {
+        if (!c.acc_first) {
+            accp = b.acc_pd[slot];
+            accv = b.acc_vm[slot];
+        }
+        accp = axpy(c.c_acc, kpd, accp);
+        accv = axpy(c.c_acc, kvm, accv);
+        if (!c.last) {
+            b.acc_pd[slot] = accp;
+            b.acc_vm[slot] = accv;
+        }
+    } else if (c.last) {
+        accp = b.acc_pd[slot];
+        accv = b.acc_vm[slot];
+    }
+    if (c.last) {
+        float4 np = comb(y0p, accp, false);
+        if (c.kick) {  // a velocity-Verlet kick moves no particle: positions come from the drift
+            np.x = y0p.x;
+            np.y = y0p.y;
+            np.z = y0p.z;
+        }
+        b.next_pd[slot] = np;
+        b.next_vm[slot] = comb(y0v, accv, true);
+    } else {
+        float4 tp = make_float4(0.f, 0.f, 0.f, 0.f), tv = make_float4(0.f, 0.f, 0.f, 0.f);
+        if (c.c_prev0 != 0.0f) {
+            tp = axpy(c.c_prev0, b.prev0_pd[slot], tp);
+            tv = axpy(c.c_prev0, b.prev0_vm[slot], tv);
+        }
+        if (c.c_prev1 != 0.0f) {
+            tp = axpy(c.c_prev1, b.prev1_pd[slot], tp);
+            tv = axpy(c.c_prev1, b.prev1_vm[slot], tv);
+        }
+        if (c.c_prev2 != 0.0f) {
+            tp = axpy(c.c_prev2, b.prev2_pd[slot], tp);
+            tv = axpy(c.c_prev2, b.prev2_vm[slot], tv);
+        }
+        if (c.c_self != 0.0f) {
+            tp = axpy(c.c_self, kpd, tp);
+            tv = axpy(c.c_self, kvm, tv);
+        }
+        b.next_pd[slot] = comb(y0p, tp, false);
+        b.next_vm[slot] = comb(y0v, tv, true);
+    }
+}
+
+// The particle's own fields and table pointers for the pair loop; returns
+// its scene.  `sm`/`si` hold the tables of scene `scene0`.
+__device__ __forceinline__ const SceneP& init_self(uint32_t k, float4 xi, float4 vi, uint32_t sid, const FluidArgs& a,
+                                                   const Tables& T, const FluidMat* sm, const DevInter* si,
+                                                   uint32_t scene0, Self& s) {
+    s.x = make_float3(xi.x, xi.y, xi.z);
+    s.v = make_float3(vi.x, vi.y, vi.z);
+    s.mat = __float_as_uint(vi.w);
+    const uint32_t scene = T.mats[s.mat].scene;
+    const SceneP& P = T.scenes[scene];
+    const uint32_t li = s.mat - P.mat_base;
+    // pre-offset so that [global id] lands on the scene's entry
+    s.mt = (scene == scene0 ? sm : T.fmats + P.mat_base) - P.mat_base;
+    s.it = (scene == scene0 ? si : T.inter + P.inter_base) + li * P.nmat - P.mat_base;
+    s.d1 = xi.w;
+    const FluidMat m1 = s.mt[s.mat];
+    s.m1 = m1.mass;
+    s.f1 = m1.visc;
+    s.bf1 = m1.bulk;
+    s.elastic = sid != kInvalid && m1.stiff;
+    s.pterm1 = a.ps[k];
+    return P;
+}
+
 // How fluid_particle collects and evaluates the hits of a particle.  Every
 // mode sums the pairs in candidate order, so results do not depend on the
 // mode, CAP or the launch shape.
@@ -224,24 +322,9 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
     const uint32_t slot = a.perm ? a.perm[k] : k;
     const uint32_t sid = a.sid[slot];
     Self s;
-    s.x = make_float3(xi.x, xi.y, xi.z);
-    s.v = make_float3(vi.x, vi.y, vi.z);
-    s.mat = __float_as_uint(vi.w);
-    const uint32_t scene = T.mats[s.mat].scene;
-    const SceneP& P = T.scenes[scene];
+    const SceneP& P = init_self(k, xi, vi, sid, a, T, sm, si, scene0, s);
     const PairK K{P.h2, P.kconst, P.eps_hh};
     const float g_acc = P.g;
-    const uint32_t li = s.mat - P.mat_base;
-    // pre-offset so that [global id] lands on the scene's entry
-    s.mt = (scene == scene0 ? sm : T.fmats + P.mat_base) - P.mat_base;
-    s.it = (scene == scene0 ? si : T.inter + P.inter_base) + li * P.nmat - P.mat_base;
-    s.d1 = xi.w;
-    const FluidMat m1 = s.mt[s.mat];
-    s.m1 = m1.mass;
-    s.f1 = m1.visc;
-    s.bf1 = m1.bulk;
-    s.elastic = sid != kInvalid && m1.stiff;
-    s.pterm1 = a.ps[k];
 
     Acc acc;
     acc.den = 0.0f;
@@ -349,73 +432,7 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
         }
     }
 
-    // derivative record (fluid.rs:243-247), plus the solid term when active
-    float4 kpd = make_float4(vi.x, vi.y, vi.z, acc.den);
-    float4 kvm = make_float4(__fdiv_rn(acc.f.x, s.d1), __fadd_rn(__fdiv_rn(acc.f.y, s.d1), -g_acc),
-                             __fdiv_rn(acc.f.z, s.d1), 0.0f);
-    if (a.solid_branch && sid != kInvalid && P.solid_branch) {
-        const float4 ks = a.ksol[sid];
-        kpd.x = __fadd_rn(kpd.x, vi.x);
-        kpd.y = __fadd_rn(kpd.y, vi.y);
-        kpd.z = __fadd_rn(kpd.z, vi.z);
-        kvm.x = __fadd_rn(kvm.x, ks.x);
-        kvm.y = __fadd_rn(kvm.y, ks.y);
-        kvm.z = __fadd_rn(kvm.z, ks.z);
-    }
-
-    // Runge-Kutta stage epilogue
-    if (b.store_pd) {
-        b.store_pd[slot] = kpd;
-        b.store_vm[slot] = kvm;
-    }
-    const float4 y0p = b.y0_pd[slot];
-    const float4 y0v = b.y0_vm[slot];
-    float4 accp = make_float4(0.f, 0.f, 0.f, 0.f), accv = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (c.c_acc != 0.0f) {
-        if (!c.acc_first) {
-            accp = b.acc_pd[slot];
-            accv = b.acc_vm[slot];
-        }
-        accp = axpy(c.c_acc, kpd, accp);
-        accv = axpy(c.c_acc, kvm, accv);
-        if (!c.last) {
-            b.acc_pd[slot] = accp;
-            b.acc_vm[slot] = accv;
-        }
-    } else if (c.last) {
-        accp = b.acc_pd[slot];
-        accv = b.acc_vm[slot];
-    }
-    if (c.last) {
-        float4 np = comb(y0p, accp, false);
-        if (c.kick) {  // a velocity-Verlet kick moves no particle: positions come from the drift
-            np.x = y0p.x;
-            np.y = y0p.y;
-            np.z = y0p.z;
-        }
-        b.next_pd[slot] = np;
-        b.next_vm[slot] = comb(y0v, accv, true);
-    } else {
-        float4 tp = make_float4(0.f, 0.f, 0.f, 0.f), tv = make_float4(0.f, 0.f, 0.f, 0.f);
-        if (c.c_prev0 != 0.0f) {
-            tp = axpy(c.c_prev0, b.prev0_pd[slot], tp);
-            tv = axpy(c.c_prev0, b.prev0_vm[slot], tv);
-        }
-        if (c.c_prev1 != 0.0f) {
-            tp = axpy(c.c_prev1, b.prev1_pd[slot], tp);
-            tv = axpy(c.c_prev1, b.prev1_vm[slot], tv);
-        }
-        if (c.c_prev2 != 0.0f) {
-            tp = axpy(c.c_prev2, b.prev2_pd[slot], tp);
-            tv = axpy(c.c_prev2, b.prev2_vm[slot], tv);
-        }
-        if (c.c_self != 0.0f) {
-            tp = axpy(c.c_self, kpd, tp);
-            tv = axpy(c.c_self, kvm, tv);
-        }
-        b.next_pd[slot] = comb(y0p, tp, false);
-        b.next_vm[slot] = comb(y0v, tv, true);
-    }
+    stage_epilogue(a, c, b, slot, sid, vi, acc, s.d1, g_acc, P.solid_branch != 0u);
     return true;
 }
 
@@ -551,6 +568,200 @@ __global__ void __launch_bounds__(64) k_fluid_overflow(FluidArgs a, Tables T, St
     }
 }
 
+// ---- staged form -----------------------------------------------------------
+// One tile of BLOCK consecutive cell-sorted particles per block, with the
+// candidates of the tile staged in shared memory before the scan.  The tile's
+// particles lie in a few x-rows of search cells ("own rows"); for each own row
+// the NY x NZ neighbor rows it reaches are windows of contiguous cells, and
+// the positions of each window (a contiguous range of the sorted state) are
+// copied into shared memory once per block, instead of each thread reading
+// every candidate through L1 (a tile's particles share most candidates).
+// The scan then reads candidates from shared memory in the order the global
+// scan visits them (rows z-major, then y, cells ascending; boundary
+// candidates first in each row, read from global memory), so the pairs are
+// summed in the same order and the results are the same bits.  A tile with
+// more own rows than kMaxOwnRows or more candidates than kStageSlots sends its
+// particles to the first overflow queue.
+constexpr int kStageSlots = 1536;   // staged positions per block (24 KB)
+constexpr int kMaxOwnRows = 4;
+constexpr int kStageRY = 2;         // y reach of a dense scene (x-halved scenes use 1)
+constexpr int kStageRZ = 1 + (int)(kSearchHalve >> 2 & 1u);
+constexpr int kStageNY = 2 * kStageRY + 1;
+
+template <int DIM>
+struct StageShape {
+    static constexpr int NZ = DIM == 3 ? 2 * kStageRZ + 1 : 1;
+    static constexpr int NQ = kStageNY * NZ;   // windows per own row
+    static constexpr int NW = kMaxOwnRows * NQ;
+};
+
+// Shared-memory bytes of a staged launch.
+template <int DIM, int BLOCK, int CAP>
+constexpr size_t staged_smem_fixed() {
+    return 16 * (size_t)kStageSlots + sizeof(uint32_t) * (size_t)CAP * BLOCK;
+}
+
+template <int DIM, int BLOCK, int CAP>
+__global__ void __launch_bounds__(BLOCK) k_fluid_staged(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
+    using SS = StageShape<DIM>;
+    static_assert(BLOCK >= SS::NW && BLOCK % 32 == 0, "one thread per window");
+    extern __shared__ __align__(16) unsigned char smem_raw[];
+    float4* stg = reinterpret_cast<float4*>(smem_raw);
+    uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw + 16 * (size_t)kStageSlots);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(lst + CAP * BLOCK);
+    DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
+    __shared__ uint32_t s_row[BLOCK];          // global row id (first cell of the x-row) of each thread, or invalid
+    __shared__ uint32_t s_heads[BLOCK / 32];   // own-row heads per warp
+    __shared__ uint32_t r_scene[kMaxOwnRows], r_base[kMaxOwnRows], r_xa[kMaxOwnRows], r_xb[kMaxOwnRows];
+    __shared__ int r_y[kMaxOwnRows], r_z[kMaxOwnRows];
+    __shared__ uint32_t w_gstart[SS::NW], w_off[SS::NW + 1];
+    __shared__ uint32_t s_nrows;
+
+    const uint32_t k0 = blockIdx.x * BLOCK;
+    const uint32_t k = k0 + threadIdx.x;
+    const uint32_t scene0 = T.mats[__float_as_uint(a.vs[min(k0, a.n - 1u)].w)].scene;
+    load_scene_tables(T, scene0, sm, si);
+
+    // own rows: consecutive threads of one x-row of search cells
+    const bool valid = k < a.n;
+    float4 xi = make_float4(0.f, 0.f, 0.f, 0.f), vi = xi;
+    CellCoord cc{0, 0, 0};
+    uint32_t row = kInvalid;
+    const SceneP* Pp = nullptr;
+    if (valid) {
+        xi = a.xs[k];
+        vi = a.vs[k];
+        Pp = &T.scenes[T.mats[__float_as_uint(vi.w)].scene];
+        if (finite3(xi)) {
+            const Grid& g = Pp->sgrid;
+            cc = cell_coord(xi, g);
+            row = Pp->cell_base + (uint32_t)cc.y * g.sub[0] + (uint32_t)cc.z * g.sub[0] * g.sub[1];
+        }
+    }
+    s_row[threadIdx.x] = row;
+    __syncthreads();
+    const bool head = row != kInvalid && (threadIdx.x == 0 || s_row[threadIdx.x - 1] != row);
+    const bool tail = row != kInvalid && (threadIdx.x == BLOCK - 1 || s_row[threadIdx.x + 1] != row);
+    const uint32_t lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+    const unsigned hb = __ballot_sync(0xFFFFFFFFu, head);
+    if (lane == 0) s_heads[warp] = __popc(hb);
+    __syncthreads();
+    uint32_t before = 0, nrows = 0;
+    for (uint32_t w = 0; w < BLOCK / 32; ++w) {
+        before += w < warp ? s_heads[w] : 0u;
+        nrows += s_heads[w];
+    }
+    // own-row index of this thread (rows are contiguous runs of threads)
+    const int rho = row == kInvalid ? -1 : (int)(before + __popc(hb & ((2u << lane) - 1u))) - 1;
+    if (head && rho < kMaxOwnRows) {
+        r_scene[rho] = T.mats[__float_as_uint(vi.w)].scene;
+        r_base[rho] = row;
+        r_y[rho] = cc.y;
+        r_z[rho] = cc.z;
+        r_xa[rho] = (uint32_t)cc.x;
+    }
+    if (tail && rho < kMaxOwnRows) r_xb[rho] = (uint32_t)cc.x;
+    if (threadIdx.x == 0) s_nrows = nrows;
+    __syncthreads();
+
+    // windows: own row r, neighbor row q = (dz + RZ) * NY + (dy + RY)
+    const uint32_t nwin = min(nrows, (uint32_t)kMaxOwnRows) * SS::NQ;
+    if (threadIdx.x < nwin) {
+        const uint32_t r = threadIdx.x / SS::NQ, q = threadIdx.x % SS::NQ;
+        const SceneP& P = T.scenes[r_scene[r]];
+        const Grid& g = P.sgrid;
+        const int dy = (int)(q % kStageNY) - kStageRY;
+        const int dz = DIM == 3 ? (int)(q / kStageNY) - kStageRZ : 0;
+        const int y = r_y[r] + dy, z = r_z[r] + dz;
+        const int ry = 1 + (int)P.halved[1], rx = 1 + (int)P.halved[0];
+        uint32_t wstart = 0, wlen = 0;
+        if (abs(dy) <= ry && y >= 0 && y < (int)g.sub[1] && z >= 0 && z < (int)g.sub[2]) {
+            const uint32_t rb = r_base[r] + (uint32_t)(dy * (int)g.sub[0]) + (uint32_t)(dz * (int)(g.sub[0] * g.sub[1]));
+            const uint32_t x0 = (uint32_t)max((int)r_xa[r] - rx, 0);
+            const uint32_t x1 = (uint32_t)min((int)r_xb[r] + rx, (int)g.sub[0] - 1);
+            wstart = a.start[rb + x0];
+            wlen = a.start[rb + x1 + 1u] - wstart;
+        }
+        w_gstart[threadIdx.x] = wstart;
+        w_off[threadIdx.x + 1] = wlen;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {  // at most NW (<= 60) windows: a serial prefix sum
+        uint32_t t = 0;
+        w_off[0] = 0;
+        for (uint32_t w = 1; w <= nwin; ++w) {
+            t += w_off[w];
+            w_off[w] = t;
+        }
+    }
+    __syncthreads();
+    const uint32_t total = w_off[nwin];
+    const bool staged = s_nrows <= (uint32_t)kMaxOwnRows && total <= (uint32_t)kStageSlots;
+    if (!staged) {
+        // too many rows or candidates for the staging area: the first overflow
+        // queue (global-memory scan with list flushes) takes the tile
+        if (valid) a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
+        return;
+    }
+    for (uint32_t w = 0; w < nwin; ++w) {
+        const uint32_t o = w_off[w], len = w_off[w + 1] - o, gs = w_gstart[w];
+        for (uint32_t i = threadIdx.x; i < len; i += BLOCK) stg[o + i] = a.xs[gs + i];
+    }
+    __syncthreads();
+    if (!valid) return;
+
+    const uint32_t slot = a.perm ? a.perm[k] : k;
+    const uint32_t sid = a.sid[slot];
+    Self s;
+    const SceneP& P = init_self(k, xi, vi, sid, a, T, sm, si, scene0, s);
+    const PairK K{P.h2, P.kconst, P.eps_hh};
+    Acc acc;
+    acc.den = 0.0f;
+    acc.f = make_float3(0.0f, 0.0f, 0.0f);
+    uint32_t* my = lst + threadIdx.x;
+    uint32_t cnt = 0;
+    bool full = false;
+    auto hit = [&](float4 q) {
+        const float rx = q.x - xi.x, ry = q.y - xi.y;
+        const float r2 = DIM == 3 ? fmaf(q.z - xi.z, q.z - xi.z, fmaf(ry, ry, rx * rx)) : fmaf(ry, ry, rx * rx);
+        return r2 < K.h2;
+    };
+    auto take = [&](uint32_t j) {
+        if (cnt < CAP) my[cnt++ * BLOCK] = j;
+        else full = true;
+    };
+    if (rho >= 0) {
+        const Grid& g = P.sgrid;
+        const int rx = 1 + (int)P.halved[0], ry = 1 + (int)P.halved[1];
+        const uint32_t x0 = (uint32_t)max(cc.x - rx, 0), x1 = (uint32_t)min(cc.x + rx, (int)g.sub[0] - 1);
+        for (int q = 0; q < SS::NQ; ++q) {
+            const int dy = q % kStageNY - kStageRY;
+            const int dz = DIM == 3 ? q / kStageNY - kStageRZ : 0;
+            const int y = cc.y + dy, z = cc.z + dz;
+            if (abs(dy) > ry || y < 0 || y >= (int)g.sub[1] || z < 0 || z >= (int)g.sub[2]) continue;
+            const uint32_t rb = row + (uint32_t)(dy * (int)g.sub[0]) + (uint32_t)(dz * (int)(g.sub[0] * g.sub[1]));
+            const uint32_t c0 = rb + x0, c1 = rb + x1 + 1u;
+            const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
+            for (uint32_t j = bb; j < be; ++j)
+                if (hit(a.bxs[j])) take(j | kBoundaryBit);
+            const uint32_t w = (uint32_t)rho * SS::NQ + (uint32_t)q;
+            const uint32_t jb = a.start[c0], je = a.start[c1];
+            const int shift = (int)w_off[w] - (int)w_gstart[w];  // global index -> staging slot
+            for (uint32_t j = jb; j < je; ++j)
+                if (hit(stg[(int)j + shift])) take(j);
+        }
+    }
+    if (full) {
+        a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
+        return;
+    }
+    for (uint32_t e = 0; e < cnt; ++e) {
+        const uint32_t j = my[e * BLOCK];
+        if (j != k) eval_hit<DIM>(j, s, a, K, acc);
+    }
+    stage_epilogue(a, c, b, slot, sid, vi, acc, s.d1, P.g, P.solid_branch != 0u);
+}
+
 template <int DIM, int BLOCK, int CAP, int MODE>
 void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, bool persistent,
                     uint32_t* tile_counter, cudaStream_t st) {
@@ -612,6 +823,21 @@ __global__ void k_verlet_kick4(const float4* __restrict__ e, const float4* __res
     out[i] = comb(e[i], axpy(half, k4[i], make_float4(0.f, 0.f, 0.f, 0.f)), false);
 }
 
+template <int DIM, int BLOCK, int CAP>
+int launch_staged(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, cudaStream_t st) {
+    const size_t smem = staged_smem_fixed<DIM, BLOCK, CAP>() + sizeof(FluidMat) * T.max_nmat +
+                        sizeof(DevInter) * T.max_nmat * T.max_nmat;
+    if (smem > 48 * 1024)
+        cudaFuncSetAttribute(k_fluid_staged<DIM, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
+    if (!a.counters_cleared) cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
+    k_fluid_staged<DIM, BLOCK, CAP><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
+    const uint32_t oblocks = std::min<uint32_t>(ntiles * BLOCK / 128u + 1u, 1184u);
+    k_fluid_overflow_flush<DIM><<<oblocks, 128, 0, st>>>(a, T, c, b);
+    k_fluid_overflow<DIM><<<2u * oblocks, 64, 0, st>>>(a, T, c, b);
+    return 3;
+}
+
 }  // namespace
 
 int verlet_kick_drift(const float4* pd, const float4* vm, const float4* fpd, const float4* fvm, uint32_t n, float half,
@@ -628,9 +854,10 @@ int verlet_kick4(const float4* e, const float4* k4, uint32_t count, float half, 
 }
 
 const FluidVariant kFluidVariants[kNumFluidVariants] = {
-    {128, 48, 0, 0}, {256, 48, 0, 0}, {128, 48, 1, 0}, {256, 48, 1, 0},
-    {128, 96, 0, 0}, {256, 96, 0, 0}, {128, 96, 1, 0}, {256, 96, 1, 0},
-    {128, 48, 0, 1}, {128, 48, 1, 1},
+    {128, 48, 0, 0, 0}, {256, 48, 0, 0, 0}, {128, 48, 1, 0, 0}, {256, 48, 1, 0, 0},
+    {128, 96, 0, 0, 0}, {256, 96, 0, 0, 0}, {128, 96, 1, 0, 0}, {256, 96, 1, 0, 0},
+    {128, 48, 0, 1, 0}, {128, 48, 1, 1, 0},
+    {128, 48, 0, 0, 1}, {64, 48, 0, 0, 1},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -638,8 +865,15 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
     if (a.n == 0) return 0;
     const FluidVariant v = kFluidVariants[variant < 0 || variant >= kNumFluidVariants ? 0 : variant];
     const bool pers = v.persistent != 0;
+    if (v.staged) {
+        if (kdim == 3 && v.block == 128) return launch_staged<3, 128, 48>(a, T, c, b, st);
+        if (kdim == 3 && v.block == 64) return launch_staged<3, 64, 48>(a, T, c, b, st);
+        if (kdim == 2 && v.block == 128) return launch_staged<2, 128, 48>(a, T, c, b, st);
+        if (kdim == 2 && v.block == 64) return launch_staged<2, 64, 48>(a, T, c, b, st);
+        return 0;
+    }
 #define ARP_FLUID(D, B, C, M)                                               \
-    if (kdim == D && v.block == B && v.cap == C && v.flush == M) {          \
+    if (kdim == D && v.block == B && v.cap == C && v.flush == M && !v.staged) {  \
         launch_variant<D, B, C, M>(a, T, c, b, pers, tile_counter, st);     \
         return 3; /* the tile kernel and the two overflow kernels */       \
     }

@@ -1439,6 +1439,8 @@ arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant) {
     return ARP_OK;
 }
 
+int arp_fluid_variant_count(void) { return kNumFluidVariants; }
+
 arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent) {
     // (the hit-list capacity of the shape is kFluidVariants[variant].cap)
     if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
@@ -2087,11 +2089,6 @@ arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
     ARP_TRY(need_init(sim));
     if (checkpoint_every == 0) return fail(ARP_ERR_INVALID_ARG, "checkpoint interval must be positive");
     if (sim->any_plastic) return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate plastic flow");
-    if (!sim->all_order2)
-        return fail(ARP_ERR_UNSUPPORTED, "the adjoint differentiates strain order 2 (Green-Lagrange) only");
-    for (const auto& it : sim->inter)
-        if (it.potential != ARP_CONTACT_ZERO && it.friction != 0.0f)
-            return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate contact friction");
     if (sim->tab.stages > kMaxStages) return fail(ARP_ERR_UNSUPPORTED, "more than 4 stages");
     if (sim->verlet()) return fail(ARP_ERR_UNSUPPORTED, "the adjoint differentiates Runge-Kutta steps only");
     sim->drop_graph();
@@ -2227,6 +2224,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.n = n;
                 a.ns = ns;
                 a.solid_branch = sb ? 1 : 0;
+                a.all_order2 = sim->all_order2 ? 1 : 0;
                 sim->launches += launch_adjoint_stage(a, sim->tables, sim->kdim, st);
             }
             const float4* yp[kMaxStages];

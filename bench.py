@@ -236,7 +236,7 @@ def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20
     variant = batch.fluid_variant()
     # the persistent (scene, cell-tile) work-queue shapes, same state, same steps each
     shapes = {}
-    for v in range(10):
+    for v in range(FluidSim.fluid_variant_count()):
         batch.set_fluid_variant(v)
         vi = batch.fluid_variant()
         if not vi["persistent"]:

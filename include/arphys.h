@@ -273,14 +273,17 @@ arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps);
 /* Time every launch shape of the fluid kernel (128 or 256 threads per block,
  * 48 or 96 listed neighbors per thread, one tile per block or persistent
  * blocks on a tile queue, lists evaluated after the scan or emptied whenever
- * a warp's next row could overfill one) on the current
+ * a warp's next row could overfill one, or the tile's candidates staged in
+ * shared memory before the scan, 64 or 128 threads per block) on the current
  * state and keep the fastest; arp_sim_init does this once per (dimension,
  * particle count, h/spacing) bucket and reuses the choice afterwards.  The
  * shapes evaluate identical arithmetic, so results do not depend on it. */
 arp_status arp_sim_autotune(arp_sim* sim, int* variant);
 arp_status arp_sim_fluid_variant(const arp_sim* sim, int* variant, int* block, int* persistent);
-/* Pin the fluid kernel's launch shape (0 .. 9). */
+/* Pin the fluid kernel's launch shape (0 .. arp_fluid_variant_count() - 1). */
 arp_status arp_sim_set_fluid_variant(arp_sim* sim, int variant);
+/* The number of launch shapes of the fluid kernel. */
+int arp_fluid_variant_count(void);
 /* Replay each step from a CUDA graph captured on the handle's stream (two
  * graphs, one for each of the two buffer sets consecutive steps alternate
  * between; captured on first use and again after the stream or the buffers

@@ -22,16 +22,19 @@ def oracle_csr(buckets, n, ncells):
     members ascending inside each cell, plus the boundary section."""
     counts = buckets["counts"].astype(np.int64)
     contents = buckets["contents"]
-    start = np.zeros(ncells + 1, np.int64)
-    start[1:] = np.cumsum(counts[:, 2])
-    members = np.zeros(int(start[-1]), np.uint32)
-    bstart = np.zeros(ncells + 1, np.int64)
-    bstart[1:] = np.cumsum(counts[:, 0])
-    bmembers = np.zeros(int(bstart[-1]), np.uint32)
-    for c in np.nonzero(counts.sum(axis=1))[0]:
-        bc, rc, cn = counts[c]
-        members[start[c]:start[c + 1]] = np.sort(contents[c, bc + rc:bc + rc + cn])
-        bmembers[bstart[c]:bstart[c + 1]] = np.sort(contents[c, :bc])
+    col = np.arange(contents.shape[1])[None, :]
+
+    def section(lo, cnt):
+        mask = (col >= lo[:, None]) & (col < (lo + cnt)[:, None])
+        cell = np.broadcast_to(np.arange(len(counts))[:, None], mask.shape)[mask]
+        vals = contents[mask]
+        order = np.lexsort((vals, cell))  # by cell, ascending id inside a cell
+        start = np.zeros(ncells + 1, np.int64)
+        start[1:] = np.cumsum(cnt)
+        return start, vals[order].astype(np.uint32)
+
+    start, members = section(counts[:, 0] + counts[:, 1], counts[:, 2])
+    bstart, bmembers = section(np.zeros(len(counts), np.int64), counts[:, 0])
     return start, members, bstart, bmembers
 
 
@@ -54,8 +57,9 @@ def _oracle_loss(task):
     times from the given per-solid stiffness and initial velocity (set in
     double precision, so a small perturbation is not rounded to f32), and the
     loss of the final positions: ("tip", caller ids, target) for the squared
-    distance of their centroid to the target, ("points", targets) for the
-    summed squared distances to per-particle targets."""
+    distance of their centroid to the target, ("separation", heavy mask) for
+    the heavy/light centroid separation, ("points", targets) for the summed
+    squared distances to per-particle targets."""
     sc, steps, stiff, vel, loss = task
     from oracle.oracle import Oracle, lib
     lib().orc_set_threads(1)
@@ -71,6 +75,9 @@ def _oracle_loss(task):
     if loss[0] == "tip":
         d = pos[loss[1]].mean(axis=0) - np.asarray(loss[2], np.float64)
         return float(d @ d)
+    if loss[0] == "separation":  # heavy centroid height above the light one's
+        heavy = loss[1]
+        return float(pos[heavy, 1].mean() - pos[~heavy, 1].mean())
     d = pos - loss[1]
     return float(np.sum(d * d))
 

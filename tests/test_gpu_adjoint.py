@@ -111,6 +111,40 @@ def test_fluid_gradients_match_fp64_finite_differences():
     assert report(res, 1e-4) < 1e-4
 
 
+def test_friction_gradients_match_fp64_finite_differences():
+    """Fluid against the walls with a friction coefficient (the interaction of
+    default_between carries the materials' visc sum, interaction.rs:42-50): the
+    friction term of fluid.rs:192-199 is differentiated too."""
+    sc = scenes.dam_break_2d(nx=12, ny=12, box=(0.32, 0.24), integrator="midpoint")
+    sc.materials["visc"][0] = 0.3  # the boundary's friction
+    rng = np.random.default_rng(9)
+    sc.particles["vel"][:, :2] = rng.normal(0.0, 0.2, size=(sc.n, 2)).astype(np.float32)
+    target = (sc.particles["pos"][:, :3] + rng.normal(0.0, 0.002, size=(sc.n, 3))).astype(np.float64)
+    target[:, 2] = 0.0
+    dv = []
+    for _ in range(32):
+        d = rng.normal(size=(sc.n, 3))
+        d[:, 2] = 0.0
+        dv.append(d)
+    L, res = fd_check(sc, 20, 5, ("points", target), [], dv)
+    assert report(res, 1e-4) < 1e-4
+
+
+@pytest.mark.parametrize("order", [0, 1, -2, 3])
+def test_strain_order_gradients_match_fp64_finite_differences(order):
+    """Seth-Hill strains other than Green-Lagrange (solid.rs:105-204): the
+    5-term log series (order 0), the Denman-Beavers square root (odd orders,
+    differentiated through the Sylvester equation of the square root) and
+    inverses (negative orders), with their strain rates."""
+    sc = scenes.cantilever_bar(n=(4, 16, 4), v_sigma=0.1, target_offset=(0.002, -0.02, 0.001))
+    sc.materials["strain_order"][1] = order
+    rng = np.random.default_rng(60 + order)
+    ds = [rng.normal(size=sc.n) for _ in range(8)]
+    dv = [rng.normal(size=(sc.n, 3)) for _ in range(8)]
+    L, res = fd_check(sc, 100, 20, ("tip", sc.meta["tip"], sc.meta["target"]), ds, dv)
+    assert report(res, 1e-4) < 1e-4
+
+
 def test_tape_refuses_plastic_materials_and_backward_without_tape():
     sc = scenes.cantilever_bar(n=(4, 8, 4))
     sc.materials["plastic"][1] = 1

@@ -120,7 +120,7 @@ def test_single_step_graphs_match_plain_steps():
 def test_fluid_launch_shapes_give_identical_results():
     sc = scenes.small_fluid_bar_3d(seed=21)
     ref = None
-    for v in range(10):
+    for v in range(FluidSim.fluid_variant_count()):
         sim = FluidSim(sc)
         sim.init()
         sim.set_fluid_variant(v)
@@ -178,7 +178,7 @@ def dense_block(h_over_s=4.5, n=10, spacing=0.01):
 def test_dense_scene_through_the_overflow_queues(h_over_s, row_hits_above):
     """Most hit lists overflow (first queue, evaluated with list flushes);
     some particles have more hits in one search row than 64 (second queue,
-    flushing lists of 160) or than 160 (evaluated during the scan); all 10
+    flushing lists of 160) or than 160 (evaluated during the scan); all
     launch shapes give the same bits and the oracle's result."""
     sc = dense_block(h_over_s=h_over_s)
     pos = sc.particles["pos"][:, :3].astype(np.float64)
@@ -192,7 +192,7 @@ def test_dense_scene_through_the_overflow_queues(h_over_s, row_hits_above):
                    for i in range(sc.n))
     assert row_hits > row_hits_above  # some particle's row alone overfills that list
     ref = None
-    for v in range(10):
+    for v in range(FluidSim.fluid_variant_count()):
         sim = FluidSim(sc)
         sim.init()
         sim.set_fluid_variant(v)
