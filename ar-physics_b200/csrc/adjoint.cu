@@ -16,8 +16,8 @@
 // of the hourglass term) are those of the recorded forward stage and are not
 // differentiated.  Each particle gathers the contributions of its own pairs
 // and of its neighbors' pairs (pairwise-symmetric gathers): no atomics, each
-// thread writes only its own particle.  Not differentiated: plastic flow
-// (refused), self-contact (flagged when a pair is active).
+// thread writes only its own particle.  Not differentiated: self-contact
+// (flagged when a pair is active).
 #include "grid.cuh"
 #include "warp.cuh"
 
@@ -718,8 +718,11 @@ __device__ __forceinline__ bool in_stencil2(uint2 a, uint2 b) {
 // them with stride LANES, their partial sums combined by group_sum; lane 0
 // finishes the particle.
 // GENERAL: some solid material has a strain order other than 2 (the log
-// series, square roots and inverses are compiled out otherwise).
-template <int LANES, bool GENERAL>
+// series, square roots and inverses are compiled out otherwise).  PLASTIC:
+// some material is plastic; the plastic strain then enters E and its rate
+// (the relaxation towards the Johnson-Cook yield surface, solid.rs:499-517)
+// is differentiated, 4 x 4 as the shader holds them.
+template <int LANES, bool GENERAL, bool PLASTIC>
 __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
     const uint32_t t = blockIdx.x * blockDim.x + threadIdx.x;
     const uint32_t i = t / LANES, lane = t % LANES;
@@ -847,34 +850,113 @@ __global__ void __launch_bounds__(kT) k_adj_solid(AdjArgs a, Tables T) {
         Ed = sh_rate_forward(C, dC, two_m);
     }
     const float2 lm = a.stiff ? a.stiff[i] : make_float2(mm.lam, mm.mu);
+    // 4 x 4 (row, column) as the shader: E4 = E (+ the plastic strain), S4 =
+    // Hooke(E4) + Hooke(dE/dt) with the trace over the first dim axes times the
+    // full 4 x 4 identity; sigma reads only S4's upper 3 x 3 block
+    float E4[4][4], S4[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) E4[r][c] = (r < 3 && c < 3) ? E.m[r][c] : 0.0f;
+    if (PLASTIC) {
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float4 e = a.st.ep[4 * i + c];  // column c
+            E4[0][c] += e.x;
+            E4[1][c] += e.y;
+            E4[2][c] += e.z;
+            E4[3][c] += e.w;
+        }
+    }
     float trE = 0.f, trEd = 0.f;
 #pragma unroll
     for (int q = 0; q < 3; ++q)
         if ((uint32_t)q < dim) {
-            trE += E.m[q][q];
+            trE += E4[q][q];
             trEd += Ed.m[q][q];
         }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c)
+            S4[r][c] = 2.0f * lm.y * E4[r][c] + ((r < 3 && c < 3) ? 2.0f * mm.mu_d * Ed.m[r][c] : 0.0f) +
+                       (r == c ? lm.x * trE + mm.lam_d * trEd : 0.0f);
     M3 S;
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
-        for (int c = 0; c < 3; ++c)
-            S.m[r][c] = 2.0f * lm.y * E.m[r][c] + 2.0f * mm.mu_d * Ed.m[r][c] +
-                        (r == c ? lm.x * trE + mm.lam_d * trEd : 0.0f);
+        for (int c = 0; c < 3; ++c) S.m[r][c] = S4[r][c];
     const M3 lsig = m3_mul(lA, m3_t(L));
     M3 lF = m3_mul(lsig, S);
-    const M3 lS = m3_mul(m3_t(lsig), Fi);
-    const float trS = lS.m[0][0] + lS.m[1][1] + lS.m[2][2];
+    const M3 lS3 = m3_mul(m3_t(lsig), Fi);
+    float lS4[4][4];
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) lS4[r][c] = (r < 3 && c < 3) ? lS3.m[r][c] : 0.0f;
+    if (PLASTIC && mm.plastic) {
+        // rate = ((|S| - Y) / T) S / |S| when Y^2 <= |S|^2; the yield stress Y
+        // is constant (the equivalent strain carries the integer factor
+        // (dim-1)/dim = 0, solid.rs:214); its VJP for the weight mu:
+        // (1/T) ((1 - Y/|S|) mu + (mu:S) Y S / |S|^3)
+        float sn = 0.0f, ms = 0.0f, mu4[4][4];
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            const float4 m = a.mu_ep[4 * i + c];
+            mu4[0][c] = m.x;
+            mu4[1][c] = m.y;
+            mu4[2][c] = m.z;
+            mu4[3][c] = m.w;
+        }
+#pragma unroll
+        for (int r = 0; r < 4; ++r)
+#pragma unroll
+            for (int c = 0; c < 4; ++c) {
+                sn += S4[r][c] * S4[r][c];
+                ms += mu4[r][c] * S4[r][c];
+            }
+        const float Y = (mm.yield_strength + mm.work_hardening * powf(0.0f, mm.work_hardening_exp / 2.0f)) *
+                        (1.0f + mm.kinematic_hardening * logf(1.0f));
+        if (Y * Y <= sn) {
+            const float sl = sqrtf(sn);
+            const float it = 1.0f / mm.relaxation_time;
+            const float c1 = it * (1.0f - Y / sl), c2 = it * ms * Y / (sl * sl * sl);
+#pragma unroll
+            for (int r = 0; r < 4; ++r)
+#pragma unroll
+                for (int c = 0; c < 4; ++c) lS4[r][c] += c1 * mu4[r][c] + c2 * S4[r][c];
+        }
+    }
+    float trS = lS4[0][0] + lS4[1][1] + lS4[2][2] + lS4[3][3];
     M3 lE, lEd;
     float gs = 0.0f;
+    if (PLASTIC) {
+        // E4 = E + plastic strain: its adjoint is the plastic strain's
+#pragma unroll
+        for (int c = 0; c < 4; ++c) {
+            float4 l;
+            float* lc = &l.x;
+#pragma unroll
+            for (int r = 0; r < 4; ++r) lc[r] = 2.0f * lm.y * lS4[r][c] + (r == c && (uint32_t)r < dim ? lm.x * trS : 0.0f);
+            float4 acc = a.lam_ep[4 * i + c];
+            acc.x += l.x;
+            acc.y += l.y;
+            acc.z += l.z;
+            acc.w += l.w;
+            a.lam_ep[4 * i + c] = acc;
+        }
+    }
+#pragma unroll
+    for (int r = 0; r < 4; ++r)
+#pragma unroll
+        for (int c = 0; c < 4; ++c) gs += 2.0f * lS4[r][c] * E4[r][c];
 #pragma unroll
     for (int r = 0; r < 3; ++r)
 #pragma unroll
         for (int c = 0; c < 3; ++c) {
             const bool d = r == c && (uint32_t)r < dim;
-            lE.m[r][c] = 2.0f * lm.y * lS.m[r][c] + (d ? lm.x * trS : 0.0f);
-            lEd.m[r][c] = 2.0f * mm.mu_d * lS.m[r][c] + (d ? mm.lam_d * trS : 0.0f);
-            gs += 2.0f * lS.m[r][c] * E.m[r][c];
+            lE.m[r][c] = 2.0f * lm.y * lS4[r][c] + (d ? lm.x * trS : 0.0f);
+            lEd.m[r][c] = 2.0f * mm.mu_d * lS4[r][c] + (d ? mm.lam_d * trS : 0.0f);
         }
     const float gn = trE * trS;
     M3 lC, ldC;
@@ -979,6 +1061,23 @@ __global__ void k_adj_weights(uint32_t n, float cb, const float4* __restrict__ l
     mv[k] = v;
 }
 
+__global__ void k_adj_weights_all(uint32_t n, float cb, const float4* __restrict__ l, Later L,
+                                  float4* __restrict__ m) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float4 p = axpy4(cb, l[k], make_float4(0.f, 0.f, 0.f, 0.f));
+    for (int t = 0; t < L.n; ++t) p = axpy4(L.c[t], L.pd[t][k], p);
+    m[k] = p;
+}
+
+__global__ void k_adj_sum_all(uint32_t n, const float4* __restrict__ l, Later L, float4* __restrict__ out) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    float4 p = l[k];
+    for (int t = 0; t < L.n; ++t) p = axpy4(1.0f, L.pd[t][k], p);
+    out[k] = p;
+}
+
 __global__ void k_adj_perm(uint32_t n, const uint32_t* __restrict__ orig, const float4* __restrict__ ip,
                            const float4* __restrict__ iv, float4* __restrict__ op, float4* __restrict__ ov,
                            int scatter) {
@@ -999,10 +1098,14 @@ __global__ void k_adj_perm(uint32_t n, const uint32_t* __restrict__ orig, const 
 int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st) {
     int launches = 0;
     if (a.solid_branch && a.ns > 0) {
-        if (a.all_order2)
-            k_adj_solid<kAdjSolidLanes, false><<<nblocks(a.ns * kAdjSolidLanes, kT), kT, 0, st>>>(a, T);
-        else
-            k_adj_solid<kAdjSolidLanes, true><<<nblocks(a.ns * kAdjSolidLanes, kT), kT, 0, st>>>(a, T);
+        const uint32_t nb = nblocks(a.ns * kAdjSolidLanes, kT);
+        if (a.st.ep) {
+            if (a.all_order2) k_adj_solid<kAdjSolidLanes, false, true><<<nb, kT, 0, st>>>(a, T);
+            else k_adj_solid<kAdjSolidLanes, true, true><<<nb, kT, 0, st>>>(a, T);
+        } else {
+            if (a.all_order2) k_adj_solid<kAdjSolidLanes, false, false><<<nb, kT, 0, st>>>(a, T);
+            else k_adj_solid<kAdjSolidLanes, true, false><<<nb, kT, 0, st>>>(a, T);
+        }
         k_adj_strain<<<nblocks(a.ns, kT), kT, 0, st>>>(a, T);
         launches += 2;
     }
@@ -1042,6 +1145,29 @@ int adjoint_step_sum(uint32_t n, const float4* lam_pd, const float4* lam_vm, int
         L.c[t] = 1.0f;
     }
     k_adj_weights<<<nblocks(n, 256), 256, 0, st>>>(n, 1.0f, lam_pd, lam_vm, L, out_pd, out_vm);
+    return 1;
+}
+
+int adjoint_stage_weights_all(uint32_t n, float cb, const float4* lam, int nlater, const float* ca,
+                              const float4* const* lamY, float4* mu, cudaStream_t st) {
+    if (n == 0) return 0;
+    Later L{};
+    L.n = nlater;
+    for (int t = 0; t < nlater; ++t) {
+        L.pd[t] = lamY[t];
+        L.c[t] = ca[t];
+    }
+    k_adj_weights_all<<<nblocks(n, 256), 256, 0, st>>>(n, cb, lam, L, mu);
+    return 1;
+}
+
+int adjoint_step_sum_all(uint32_t n, const float4* lam, int stages, const float4* const* lamY, float4* out,
+                         cudaStream_t st) {
+    if (n == 0) return 0;
+    Later L{};
+    L.n = stages;
+    for (int t = 0; t < stages; ++t) L.pd[t] = lamY[t];
+    k_adj_sum_all<<<nblocks(n, 256), 256, 0, st>>>(n, lam, L, out);
     return 1;
 }
 

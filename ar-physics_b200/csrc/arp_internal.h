@@ -378,6 +378,7 @@ struct AdjStage {
     const float4* sv;
     const uint2* sc;           // [ns] packed cell coordinates
     const uint32_t* contact_bound;  // [2] self-contact gate of the stage
+    const float4* ep;          // [4*ns] plastic strain of the stage (columns), null without plastic materials
 };
 struct AdjArgs {
     AdjStage st;
@@ -405,9 +406,18 @@ struct AdjArgs {
     uint32_t n, ns;
     int solid_branch;
     int all_order2;            // every solid material has strain order 2
+    const float4* mu_ep;       // [4*ns] adjoint of the stage's plastic-strain rate (columns), or null
+    float4* lam_ep;            // [4*ns] adjoint of the stage's plastic strain (accumulated)
 };
 // One stage VJP: lam_{Y_s} += J_f(Y_s)^T mu_s (+ stiffness gradients).  Returns launches.
 int launch_adjoint_stage(const AdjArgs& a, const Tables& T, int kdim, cudaStream_t st);
+// The same weights for a plain array of `n` float4 (the plastic strain:
+// every component kept).
+int adjoint_stage_weights_all(uint32_t n, float cb, const float4* lam, int nlater, const float* ca,
+                              const float4* const* lamY, float4* mu, cudaStream_t st);
+// out = lam + sum_s lamY[s] for a plain array of `n` float4.
+int adjoint_step_sum_all(uint32_t n, const float4* lam, int stages, const float4* const* lamY, float4* out,
+                         cudaStream_t st);
 // mu = cb * lam_next + sum_t ca[t] * lamY[t] over the given later stages.
 int adjoint_stage_weights(uint32_t n, float cb, const float4* lam_pd, const float4* lam_vm, int nlater,
                           const float* ca, const float4* const* lamY_pd, const float4* const* lamY_vm,

@@ -153,10 +153,12 @@ struct StepRecord {
     DevBuf<float4> F[kMaxStages], A[kMaxStages], sx[kMaxStages], sv[kMaxStages];
     DevBuf<uint2> sc[kMaxStages];
     DevBuf<uint32_t> cb[kMaxStages];
+    DevBuf<float4> ep[kMaxStages];                       // plastic strain of each stage (plastic scenes)
     DevBuf<uint32_t> orig, sid, slot_of;                 // of the step (after its reorder)
 };
 struct Checkpoint {
     DevBuf<float4> pd, vm;
+    DevBuf<float4> ep;  // plastic strain (plastic scenes)
     DevBuf<uint32_t> orig, sid;
     float time = 0.0f;
 };
@@ -174,6 +176,7 @@ struct AdjointPool {
     DevBuf<float4> io;  // [2n] the caller's 8-float-per-particle gradients, on the device
     DevBuf<float4> lY_p[kMaxStages], lY_v[kMaxStages];
     DevBuf<float4> lamF, lamFd;
+    DevBuf<float4> lam_ep, out_ep, mu_ep, lY_ep[kMaxStages];  // adjoint of the plastic strain (solid order)
     DevBuf<double2> gst;
     DevBuf<uint32_t> flags;
     Checkpoint now;
@@ -614,6 +617,7 @@ arp_status save_checkpoint(arp_sim* S) {
     CUDA_TRY(keep(c.vm, (const float4*)S->Y.vm.p, S->n, S->stream));
     CUDA_TRY(keep(c.orig, (const uint32_t*)S->orig.p, S->n, S->stream));
     CUDA_TRY(keep(c.sid, (const uint32_t*)S->sid.p, S->n, S->stream));
+    if (S->any_plastic) CUDA_TRY(keep(c.ep, (const float4*)S->ep.p, 4 * size_t(S->ns), S->stream));
     c.time = S->time;
     S->tape->ckpts.push_back(std::move(c));
     return ARP_OK;
@@ -627,6 +631,9 @@ arp_status restore_checkpoint(arp_sim* S, const Checkpoint& c) {
         CUDA_TRY(cudaMemcpyAsync(S->orig.p, c.orig.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, S->stream));
         CUDA_TRY(cudaMemcpyAsync(S->sid.p, c.sid.p, n * sizeof(uint32_t), cudaMemcpyDeviceToDevice, S->stream));
     }
+    if (S->any_plastic && S->ns)
+        CUDA_TRY(cudaMemcpyAsync(S->ep.p, c.ep.p, 4 * size_t(S->ns) * sizeof(float4), cudaMemcpyDeviceToDevice,
+                                 S->stream));
     S->time = c.time;
     return ARP_OK;
 }
@@ -815,6 +822,7 @@ arp_status do_step(arp_sim* S, bool prime = false) {
                 CUDA_TRY(keep(R->sv[s], (const float4*)S->sv.p, ns, st));
                 CUDA_TRY(keep(R->sc[s], (const uint2*)S->sc.p, ns, st));
                 CUDA_TRY(keep(R->cb[s], (const uint32_t*)S->contact_bound.p, 2, st));
+                if (S->any_plastic) CUDA_TRY(keep(R->ep[s], a.ep, 4 * size_t(ns), st));
             }
         }
         mark(S, mk, 2);
@@ -2088,7 +2096,6 @@ static void retire_tape(arp_sim* sim) {
 arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
     ARP_TRY(need_init(sim));
     if (checkpoint_every == 0) return fail(ARP_ERR_INVALID_ARG, "checkpoint interval must be positive");
-    if (sim->any_plastic) return fail(ARP_ERR_UNSUPPORTED, "the adjoint does not differentiate plastic flow");
     if (sim->tab.stages > kMaxStages) return fail(ARP_ERR_UNSUPPORTED, "more than 4 stages");
     if (sim->verlet()) return fail(ARP_ERR_UNSUPPORTED, "the adjoint differentiates Runge-Kutta steps only");
     sim->drop_graph();
@@ -2126,6 +2133,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     CUDA_TRY(keep(now.vm, (const float4*)sim->Y.vm.p, n, st));
     CUDA_TRY(keep(now.orig, (const uint32_t*)sim->orig.p, n, st));
     CUDA_TRY(keep(now.sid, (const uint32_t*)sim->sid.p, n, st));
+    if (sim->any_plastic) CUDA_TRY(keep(now.ep, (const float4*)sim->ep.p, 4 * size_t(ns), st));
     now.time = sim->time;
     // adjoint buffers: caller order (lc), storage order (ls, out), per stage (lY), stage weights (mu)
     const size_t nn = std::max(n, 1u);
@@ -2140,6 +2148,13 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     CUDA_TRY(fit(P.lamF, 3 * size_t(std::max(ns, 1u))));
     CUDA_TRY(fit(P.lamFd, 3 * size_t(std::max(ns, 1u))));
     CUDA_TRY(fit(P.gst, std::max(ns, 1u)));
+    const bool plastic = sim->any_plastic && sim->solid_branch() && ns > 0;
+    const size_t ne = 4 * size_t(std::max(ns, 1u));
+    if (plastic) {
+        for (DevBuf<float4>* b : {&P.lam_ep, &P.out_ep, &P.mu_ep}) CUDA_TRY(fit(*b, ne));
+        for (int q = 0; q < S; ++q) CUDA_TRY(fit(P.lY_ep[q], ne));
+        CUDA_TRY(cudaMemsetAsync(P.lam_ep.p, 0, ne * sizeof(float4), st));  // the loss reads no plastic strain
+    }
     CUDA_TRY(fit(P.flags, 1));
     CUDA_TRY(fit(P.io, 2 * nn));
     DevBuf<float4>&lc_p = P.lc_p, &lc_v = P.lc_v, &ls_p = P.ls_p, &ls_v = P.ls_v, &out_p = P.out_p,
@@ -2184,6 +2199,14 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                     }
                 const float cb = (float)(sim->tab.b[q] * (double)sim->dt_sub);
                 sim->launches += adjoint_stage_weights(n, cb, ls_p.p, ls_v.p, nl, ca, lp, lv, mu_p.p, mu_v.p, st);
+                if (plastic) {  // the same weights for the plastic strain's record
+                    const float4* le[kMaxStages];
+                    int ne_later = 0;
+                    for (int u = q + 1; u < S; ++u)
+                        if (sim->tab.a[u][q] != 0.0) le[ne_later++] = P.lY_ep[u].p;
+                    sim->launches += adjoint_stage_weights_all(4 * ns, cb, P.lam_ep.p, ne_later, ca, le, P.mu_ep.p, st);
+                    CUDA_TRY(cudaMemsetAsync(P.lY_ep[q].p, 0, 4 * size_t(ns) * sizeof(float4), st));
+                }
                 if (n) {
                     cudaMemsetAsync(lY_p[q].p, 0, n * sizeof(float4), st);
                     cudaMemsetAsync(lY_v[q].p, 0, n * sizeof(float4), st);
@@ -2225,6 +2248,9 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 a.ns = ns;
                 a.solid_branch = sb ? 1 : 0;
                 a.all_order2 = sim->all_order2 ? 1 : 0;
+                a.st.ep = plastic ? R.ep[q].p : nullptr;
+                a.mu_ep = plastic ? P.mu_ep.p : nullptr;
+                a.lam_ep = plastic ? P.lY_ep[q].p : nullptr;
                 sim->launches += launch_adjoint_stage(a, sim->tables, sim->kdim, st);
             }
             const float4* yp[kMaxStages];
@@ -2234,6 +2260,12 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                 yv[q] = lY_v[q].p;
             }
             sim->launches += adjoint_step_sum(n, ls_p.p, ls_v.p, S, yp, yv, out_p.p, out_v.p, st);
+            if (plastic) {
+                const float4* ye[kMaxStages];
+                for (int q = 0; q < S; ++q) ye[q] = P.lY_ep[q].p;
+                sim->launches += adjoint_step_sum_all(4 * ns, P.lam_ep.p, S, ye, P.out_ep.p, st);
+                std::swap(P.lam_ep, P.out_ep);
+            }
             sim->launches += adjoint_scatter(n, R.orig.p, out_p.p, out_v.p, lc_p.p, lc_v.p, st);
         }
         if (status == ARP_OK) {

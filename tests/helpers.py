@@ -60,12 +60,15 @@ def _oracle_loss(task):
     distance of their centroid to the target, ("separation", heavy mask) for
     the heavy/light centroid separation, ("points", targets) for the summed
     squared distances to per-particle targets."""
-    sc, steps, stiff, vel, loss = task
+    sc, steps, stiff, vel, loss = task[:5]
+    pos0 = task[5] if len(task) > 5 else None  # a starting state other than the scene's
     from oracle.oracle import Oracle, lib
     lib().orc_set_threads(1)
     o = Oracle(sc, 64)
     if stiff is not None:
         o.set_solid_stiffness(np.ascontiguousarray(stiff, np.float64))
+    if pos0 is not None:
+        o.set_state(pos=np.ascontiguousarray(pos0, np.float64))
     if vel is not None:
         v = np.zeros((sc.n, 4))
         v[:, :3] = vel

@@ -23,13 +23,17 @@ def state_grad(n, gpos):
     return g
 
 
-def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4, eps_vel=1e-4):
+def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4, eps_vel=1e-4, start=None):
     """The GPU gradient along each direction, and the FP64 oracle's central
     difference (L(p + e d) - L(p - e d)) / 2e along the same direction.
-    `loss` is ("tip", ids, target) or ("points", targets)."""
+    `loss` is ("tip", ids, target) or ("points", targets); `start` (particle
+    records) replaces the scene's initial state after creation, keeping the
+    scene's positions as the solids' reference configuration."""
     stiff = sc.meta.get("stiffness")
     sim = FluidSim(sc)
     sim.init()
+    if start is not None:
+        sim.set_particles(start)
     if stiff is not None:
         sim.set_solid_stiffness(stiff)
     sim.tape_begin(every)
@@ -49,16 +53,18 @@ def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1
     after = sim.particles()
     assert before.tobytes() == after.tobytes()  # the forward state is put back
     sim.tape_end()
-    v0 = sc.particles["vel"][:, :3].astype(np.float64)
+    p0 = sc.particles if start is None else start
+    v0 = p0["vel"][:, :3].astype(np.float64)
+    x0 = None if start is None else start["pos"].astype(np.float64)
     s64 = None if stiff is None else stiff.astype(np.float64)
     tasks, adj = [], []
     for d in directions_stiff:
         adj.append(("stiffness", float(np.sum(gs.astype(np.float64) * s64 * d[:, None]))))
-        tasks += [(sc, steps, s64 * (1 + eps_rel * d[:, None]), None, loss),
-                  (sc, steps, s64 * (1 - eps_rel * d[:, None]), None, loss)]
+        tasks += [(sc, steps, s64 * (1 + eps_rel * d[:, None]), v0, loss, x0),
+                  (sc, steps, s64 * (1 - eps_rel * d[:, None]), v0, loss, x0)]
     for d in directions_vel:
         adj.append(("velocity", float(np.sum(g0[:, 4:7].astype(np.float64) * d))))
-        tasks += [(sc, steps, s64, v0 + eps_vel * d, loss), (sc, steps, s64, v0 - eps_vel * d, loss)]
+        tasks += [(sc, steps, s64, v0 + eps_vel * d, loss, x0), (sc, steps, s64, v0 - eps_vel * d, loss, x0)]
     ls = oracle_losses(tasks)
     out = []
     for q, (kind, a) in enumerate(adj):
@@ -145,10 +151,33 @@ def test_strain_order_gradients_match_fp64_finite_differences(order):
     assert report(res, 1e-4) < 1e-4
 
 
-def test_tape_refuses_plastic_materials_and_backward_without_tape():
-    sc = scenes.cantilever_bar(n=(4, 8, 4))
-    sc.materials["plastic"][1] = 1
-    sc.materials["yield_strength"][1] = 1.0
+def test_plastic_flow_gradients_match_fp64_finite_differences():
+    """A 2D block stretched and sheared past its yield strength (the
+    relaxation towards the Johnson-Cook surface, solid.rs:499-517): the plastic
+    strain enters the stress and its own rate, both differentiated, with the
+    plastic strain's adjoint carried across stages, steps and checkpoints."""
+    from test_gpu_solids import deform, solid_block_scene
+    plastic = dict(yield_strength=5e5, work_hardening=1e5, work_hardening_exp=2.0, relaxation_time=1e3)
+    sc = solid_block_scene(n=(12, 4, 1), dim=2, lam=-1e7, mu=-1e8, plastic=plastic, damp=(-500.0, -100.0),
+                           dt=1e-7)
+    rng = np.random.default_rng(7)
+    start = deform(sc.particles, 2, rng, stretch=1.05, shear=0.05)
+    start["vel"][:, :2] = rng.normal(0.0, 0.05, size=(sc.n, 2)).astype(np.float32)
+    sc.meta["stiffness"] = np.tile(np.array([[-1e7, -1e8]], np.float32), (sc.n, 1))
+    target = (start["pos"][:, :3] + rng.normal(0.0, 1e-4, size=(sc.n, 3))).astype(np.float64)
+    target[:, 2] = 0.0
+    ds = [rng.normal(size=sc.n) for _ in range(16)]
+    dv = []
+    for _ in range(16):
+        d = rng.normal(size=(sc.n, 3))
+        d[:, 2] = 0.0
+        dv.append(d)
+    L, res = fd_check(sc, 20, 5, ("points", target), ds, dv, start=start)
+    assert report(res, 1e-4) < 1e-4
+
+
+def test_tape_refuses_verlet_and_backward_without_tape():
+    sc = scenes.cantilever_bar(n=(4, 8, 4), integrator="verlet")
     sim = FluidSim(sc)
     sim.init()
     with pytest.raises(Exception) as e:
