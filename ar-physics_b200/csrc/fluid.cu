@@ -601,7 +601,45 @@ constexpr size_t staged_smem_fixed() {
     return 16 * (size_t)kStageSlots + sizeof(uint32_t) * (size_t)CAP * BLOCK;
 }
 
-template <int DIM, int BLOCK, int CAP>
+// Bulk-copy staging (cp.async.bulk, global -> shared, one copy per window,
+// completion counted on an mbarrier).  Waits are bounded: a block whose
+// copies have not landed after kStageSpins polls sends its tile to the first
+// overflow queue (after waiting, again bounded, for the copies in flight), so
+// results never depend on the staging.
+constexpr uint32_t kStageSpins = 1u << 22;
+__device__ __forceinline__ uint32_t smem_u32(const void* p) {
+    return static_cast<uint32_t>(__cvta_generic_to_shared(p));
+}
+__device__ __forceinline__ void mbar_init(uint64_t* bar, uint32_t count) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;" ::"r"(smem_u32(bar)), "r"(count) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;" ::: "memory");
+}
+__device__ __forceinline__ void mbar_arrive_expect_tx(uint64_t* bar, uint32_t bytes) {
+    asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;" ::"r"(smem_u32(bar)), "r"(bytes)
+                 : "memory");
+}
+__device__ __forceinline__ void bulk_copy_g2s(void* dst, const void* src, uint32_t bytes, uint64_t* bar) {
+    asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];" ::"r"(
+                     smem_u32(dst)),
+                 "l"(src), "r"(bytes), "r"(smem_u32(bar))
+                 : "memory");
+}
+__device__ __forceinline__ bool mbar_try_wait(uint64_t* bar, uint32_t parity) {
+    uint32_t ok;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\tmbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\tselp.u32 %0, 1, 0, p;\n\t}"
+        : "=r"(ok)
+        : "r"(smem_u32(bar)), "r"(parity)
+        : "memory");
+    return ok != 0u;
+}
+__device__ __forceinline__ bool mbar_wait_bounded(uint64_t* bar, uint32_t parity, uint32_t spins) {
+    for (uint32_t k = 0; k < spins; ++k)
+        if (mbar_try_wait(bar, parity)) return true;
+    return false;
+}
+
+template <int DIM, int BLOCK, int CAP, bool BULK>
 __global__ void __launch_bounds__(BLOCK) k_fluid_staged(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
     using SS = StageShape<DIM>;
     static_assert(BLOCK >= SS::NW && BLOCK % 32 == 0, "one thread per window");
@@ -616,8 +654,11 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_staged(FluidArgs a, Tables T, S
     __shared__ int r_y[kMaxOwnRows], r_z[kMaxOwnRows];
     __shared__ uint32_t w_gstart[SS::NW], w_off[SS::NW + 1];
     __shared__ uint32_t s_nrows;
+    __shared__ __align__(8) uint64_t s_bar;
+    __shared__ uint32_t s_landed;
 
     const uint32_t k0 = blockIdx.x * BLOCK;
+    if (BULK && threadIdx.x == 0) mbar_init(&s_bar, 1);  // ordered before its use by the barriers below
     const uint32_t k = k0 + threadIdx.x;
     const uint32_t scene0 = T.mats[__float_as_uint(a.vs[min(k0, a.n - 1u)].w)].scene;
     load_scene_tables(T, scene0, sm, si);
@@ -703,11 +744,36 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_staged(FluidArgs a, Tables T, S
         if (valid) a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
         return;
     }
-    for (uint32_t w = 0; w < nwin; ++w) {
-        const uint32_t o = w_off[w], len = w_off[w + 1] - o, gs = w_gstart[w];
-        for (uint32_t i = threadIdx.x; i < len; i += BLOCK) stg[o + i] = a.xs[gs + i];
+    if (BULK) {
+        // one elected thread issues a bulk copy per non-empty window (16-byte
+        // aligned float4 ranges) and arms the barrier with their bytes
+        if (threadIdx.x == 0) {
+            mbar_arrive_expect_tx(&s_bar, total * 16u);
+            for (uint32_t w = 0; w < nwin; ++w) {
+                const uint32_t o = w_off[w], len = w_off[w + 1] - o;
+                if (len) bulk_copy_g2s(stg + o, a.xs + w_gstart[w], len * 16u, &s_bar);
+            }
+        }
+        const bool landed = mbar_wait_bounded(&s_bar, 0u, kStageSpins);
+        if (threadIdx.x == 0) s_landed = 1u;
+        __syncthreads();
+        if (!landed) atomicAnd(&s_landed, 0u);
+        __syncthreads();
+        if (!s_landed) {
+            // copies still in flight may write the staging area: wait for them
+            // (bounded) before the block leaves, and let the global-memory scan
+            // of the first overflow queue take the tile
+            mbar_wait_bounded(&s_bar, 0u, kStageSpins);
+            if (valid) a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
+            return;
+        }
+    } else {
+        for (uint32_t w = 0; w < nwin; ++w) {
+            const uint32_t o = w_off[w], len = w_off[w + 1] - o, gs = w_gstart[w];
+            for (uint32_t i = threadIdx.x; i < len; i += BLOCK) stg[o + i] = a.xs[gs + i];
+        }
+        __syncthreads();
     }
-    __syncthreads();
     if (!valid) return;
 
     const uint32_t slot = a.perm ? a.perm[k] : k;
@@ -823,15 +889,16 @@ __global__ void k_verlet_kick4(const float4* __restrict__ e, const float4* __res
     out[i] = comb(e[i], axpy(half, k4[i], make_float4(0.f, 0.f, 0.f, 0.f)), false);
 }
 
-template <int DIM, int BLOCK, int CAP>
+template <int DIM, int BLOCK, int CAP, bool BULK>
 int launch_staged(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, cudaStream_t st) {
     const size_t smem = staged_smem_fixed<DIM, BLOCK, CAP>() + sizeof(FluidMat) * T.max_nmat +
                         sizeof(DevInter) * T.max_nmat * T.max_nmat;
     if (smem > 48 * 1024)
-        cudaFuncSetAttribute(k_fluid_staged<DIM, BLOCK, CAP>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+        cudaFuncSetAttribute(k_fluid_staged<DIM, BLOCK, CAP, BULK>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                             (int)smem);
     const uint32_t ntiles = (a.n + BLOCK - 1) / BLOCK;
     if (!a.counters_cleared) cudaMemsetAsync(a.overflow_count, 0, 2 * sizeof(uint32_t), st);
-    k_fluid_staged<DIM, BLOCK, CAP><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
+    k_fluid_staged<DIM, BLOCK, CAP, BULK><<<ntiles, BLOCK, smem, st>>>(a, T, c, b);
     const uint32_t oblocks = std::min<uint32_t>(ntiles * BLOCK / 128u + 1u, 1184u);
     k_fluid_overflow_flush<DIM><<<oblocks, 128, 0, st>>>(a, T, c, b);
     k_fluid_overflow<DIM><<<2u * oblocks, 64, 0, st>>>(a, T, c, b);
@@ -857,7 +924,7 @@ const FluidVariant kFluidVariants[kNumFluidVariants] = {
     {128, 48, 0, 0, 0}, {256, 48, 0, 0, 0}, {128, 48, 1, 0, 0}, {256, 48, 1, 0, 0},
     {128, 96, 0, 0, 0}, {256, 96, 0, 0, 0}, {128, 96, 1, 0, 0}, {256, 96, 1, 0, 0},
     {128, 48, 0, 1, 0}, {128, 48, 1, 1, 0},
-    {128, 48, 0, 0, 1}, {64, 48, 0, 0, 1},
+    {128, 48, 0, 0, 1}, {64, 48, 0, 0, 1}, {128, 48, 0, 0, 2},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -865,11 +932,16 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
     if (a.n == 0) return 0;
     const FluidVariant v = kFluidVariants[variant < 0 || variant >= kNumFluidVariants ? 0 : variant];
     const bool pers = v.persistent != 0;
-    if (v.staged) {
-        if (kdim == 3 && v.block == 128) return launch_staged<3, 128, 48>(a, T, c, b, st);
-        if (kdim == 3 && v.block == 64) return launch_staged<3, 64, 48>(a, T, c, b, st);
-        if (kdim == 2 && v.block == 128) return launch_staged<2, 128, 48>(a, T, c, b, st);
-        if (kdim == 2 && v.block == 64) return launch_staged<2, 64, 48>(a, T, c, b, st);
+    if (v.staged == 1) {  // cooperative loads
+        if (kdim == 3 && v.block == 128) return launch_staged<3, 128, 48, false>(a, T, c, b, st);
+        if (kdim == 3 && v.block == 64) return launch_staged<3, 64, 48, false>(a, T, c, b, st);
+        if (kdim == 2 && v.block == 128) return launch_staged<2, 128, 48, false>(a, T, c, b, st);
+        if (kdim == 2 && v.block == 64) return launch_staged<2, 64, 48, false>(a, T, c, b, st);
+        return 0;
+    }
+    if (v.staged == 2) {  // bulk copies
+        if (kdim == 3 && v.block == 128) return launch_staged<3, 128, 48, true>(a, T, c, b, st);
+        if (kdim == 2 && v.block == 128) return launch_staged<2, 128, 48, true>(a, T, c, b, st);
         return 0;
     }
 #define ARP_FLUID(D, B, C, M)                                               \
