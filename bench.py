@@ -159,6 +159,60 @@ def step_roofline(sc, stages, step_ms, peak):
             "formula": "n*(96*S+96) + n_solid*196*S + n_boundary*16*S, S = stages per step"}
 
 
+def candidate_count(sc):
+    """Candidates the fluid kernel tests per stage: for each mobile particle,
+    the mobile and boundary particles in its search rows (search cells halve
+    the reference cells along x; rows of 5 search cells in x, 3 rows in y
+    and, in 3D, in z), counted on the host from the initial positions."""
+    sub = []
+    for a in range(3):
+        d = np.float32(sc.bounds_dim[a])
+        sub.append(max(1, int(d / np.float32(sc.h))) if d > 0 else 1)
+    sub[0] *= 2
+
+    def cells(p):
+        out = []
+        for a in range(3):
+            if sc.bounds_dim[a] > 0:
+                t = np.clip((p[:, a] - sc.bounds_min[a]) / sc.bounds_dim[a], 0.0, 1.0)
+                out.append(np.minimum((t * sub[a]).astype(np.int64), sub[a] - 1))
+            else:
+                out.append(np.zeros(len(p), np.int64))
+        return out
+
+    grid = np.zeros((sub[2] + 2, sub[1] + 2, sub[0] + 4), np.int64)  # padded by the reach
+    mob = sc.particles["pos"].astype(np.float64)
+    for p in (mob, sc.boundary["pos"].astype(np.float64)):
+        cx, cy, cz = cells(p)
+        np.add.at(grid, (cz + 1, cy + 1, cx + 2), 1)
+    win = np.zeros((sub[2], sub[1], sub[0]), np.int64)
+    for dz in range(3) if sc.dim == 3 else (1,):
+        for dy in range(3):
+            for dx in range(5):
+                win += grid[dz:dz + sub[2], dy:dy + sub[1], dx:dx + sub[0]]
+    cx, cy, cz = cells(mob)
+    per = win[cz, cy, cx]
+    return int(per.sum())
+
+
+def load_issue():
+    """Per-launch instruction figures of the fluid kernel from the committed ncu
+    summary (profiles/ncu_issue.txt): warp instructions, issue-active %, long
+    scoreboard stalls per issue, L1 hit %."""
+    p = os.path.join(ROOT, "profiles", "ncu_issue.txt")
+    out = {}
+    try:
+        for line in open(p):
+            parts = line.split()
+            if len(parts) >= 6 and not line.startswith("#"):
+                out[parts[0]] = {"kernel": parts[1], "warp_instructions": float(parts[2]),
+                                 "issue_active_pct": float(parts[3]), "long_scoreboard_per_issue": float(parts[4]),
+                                 "l1_hit_pct": float(parts[5]), "source": "profiles/ncu_issue.txt"}
+    except OSError:
+        pass
+    return out
+
+
 def pair_rate(sc, stages, fluid_ms_per_step):
     """Fluid pair interactions per second: ordered pairs (i mobile, j mobile or
     boundary, j != i, |x_j - x_i| < h) in the initial state, counted with a
@@ -170,7 +224,9 @@ def pair_rate(sc, stages, fluid_ms_per_step):
     allp = np.concatenate([mob, sc.boundary["pos"][:, :d].astype(np.float64)])
     r = float(sc.h) * (1.0 - 1e-6)  # lattice pairs sit exactly at |r| = h, where W = 0
     pairs = int(cKDTree(mob).count_neighbors(cKDTree(allp), r)) - len(mob)
+    cand = candidate_count(sc)
     return {"per_stage": pairs, "per_particle": pairs / max(sc.n, 1),
+            "candidates_per_stage": cand, "candidates_per_particle": cand / max(sc.n, 1),
             "rate": pairs * stages / (fluid_ms_per_step / 1000.0), "unit": "pair-interactions/s"}
 
 
@@ -564,6 +620,18 @@ def run_ours(args, rank, world, local_rank):
     stages = fl / max(prof["steps"], 1)
     roofline["step"] = step_roofline(sc, stages, total_ms / args.steps, peak)
     roofline["pairs"] = pair_rate(sc, stages, prof["fluid_ms"] / max(prof["steps"], 1))
+    issue = load_issue().get(f"fluid_{args.config}_v{sim.fluid_variant()['variant']}")
+    if issue:
+        # the issue roofline: every warp instruction of a launch issued at one
+        # per scheduler per cycle (148 SMs x 4 schedulers at the sampled clock)
+        mhz = clocks.get("sm_mhz") or 1965.0
+        t_issue = issue["warp_instructions"] / (148 * 4 * mhz * 1e6) * 1e3
+        lanes = issue["warp_instructions"] * 32.0
+        issue.update({"issue_bound_ms": t_issue, "issue_frac": t_issue / fluid_ms,
+                      "lane_instructions_per_particle": lanes / sc.n,
+                      "lane_instructions_per_candidate": lanes / max(roofline["pairs"]["candidates_per_stage"], 1),
+                      "lane_instructions_per_pair": lanes / max(roofline["pairs"]["per_stage"], 1)})
+        roofline["issue"] = issue
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
         "warmup": args.warmup, "ms_per_step": total_ms / args.steps, "higher_is_better": True,

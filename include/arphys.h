@@ -372,8 +372,9 @@ arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* 
  * (cudaGetSymbolAddress) with the device current; make that first call
  * before any stream capture.  All calls share the one array, so calls whose
  * work overlaps on the GPU (different streams or threads without ordering)
- * race and corrupt each other's output.  Sizes beyond the maxima return
- * ARP_ERR_CAPACITY without launching anything. */
+ * race and corrupt each other's output.  Sizes beyond the maxima (a kernel
+ * radius so small against the box that a cell count would not fit in 32 bits
+ * included) return ARP_ERR_CAPACITY without launching anything. */
 arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, const arp_aabb* bounds, float kernel_radius,
                                   uint32_t* cell_start, uint32_t cell_start_capacity, uint32_t* perm,
                                   void* stream);
