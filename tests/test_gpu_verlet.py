@@ -15,7 +15,11 @@ from helpers import load_seeded_scene, rel_err
 pytestmark = pytest.mark.gpu
 
 
-def compare(sc, steps, tol=1e-5, graph=False):
+def compare(sc, steps, tol=1e-5, graph=False, fp32_floor=False):
+    """GPU vs the float oracle within `tol`; with `fp32_floor`, a quantity may
+    instead be as close to the double oracle as twice the float oracle's own
+    distance from it (stiff solids, where float rounding alone moves the
+    velocities by ~1e-4 relative within tens of steps)."""
     sim = FluidSim(sc)
     sim.init()
     if graph:
@@ -30,8 +34,12 @@ def compare(sc, steps, tol=1e-5, graph=False):
     for key in ("den", "pos", "vel"):
         e = rel_err(g[key], r32[key])
         e64 = rel_err(g[key], r64[key])
-        print(f"{sc.name} {key}: vs f32 oracle {e:.2e}, vs f64 oracle {e64:.2e}")
-        assert e < tol, (sc.name, key, e)
+        e_or = rel_err(r32[key], r64[key])
+        print(f"{sc.name} {key}: vs f32 oracle {e:.2e}, vs f64 oracle {e64:.2e} (f32 oracle vs f64 {e_or:.2e})")
+        if fp32_floor:
+            assert e < tol or e64 <= max(tol, 2.0 * e_or), (sc.name, key, e, e64, e_or)
+        else:
+            assert e < tol, (sc.name, key, e)
     return sim
 
 
@@ -82,9 +90,14 @@ def test_verlet_restarts_from_a_new_state():
 @pytest.mark.parametrize("name,steps", [("cloth", 40), ("solid_test_3D", 60), ("spinning_ball", 60),
                                         ("container_buckling", 40)])
 def test_reference_verlet_scenes_match_oracle(name, steps):
+    """The reference's own Verlet scenes are stiff solids (cloth, elastic balls,
+    a buckling container) at small time steps: the float oracle itself is
+    ~1e-4 from the double oracle in velocity after these steps (with RK2 as
+    with Verlet), so the GPU is held to the float oracle's distance from the
+    double one."""
     sc = load_seeded_scene(name)
     assert sc.integrator == "verlet"
-    compare(sc, steps)
+    compare(sc, steps, fp32_floor=True)
 
 
 def test_tape_refuses_verlet():
