@@ -1078,6 +1078,35 @@ __global__ void k_adj_sum_all(uint32_t n, const float4* __restrict__ l, Later L,
     out[k] = p;
 }
 
+// Velocity Verlet.  The weights of a step's one force evaluation f(y*): the
+// closing kick's (dt/2)(lam_rho, lam_v) plus the adjoint of the carried record
+// (the next step's kick reads it); positions are not kicked, so no position part.
+__global__ void k_verlet_mu(uint32_t n, const float4* __restrict__ lsp, const float4* __restrict__ lsv,
+                            const float4* __restrict__ lfp, const float4* __restrict__ lfv, float h,
+                            float4* __restrict__ mp, float4* __restrict__ mv) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 a = lsp[k], b = lsv[k], c = lfp[k], d = lfv[k];
+    mp[k] = make_float4(0.f, 0.f, 0.f, c.w + h * a.w);
+    mv[k] = make_float4(d.x + h * b.x, d.y + h * b.y, d.z + h * b.z, 0.f);
+}
+// The kick-drift's adjoint, per particle (caller order): from lam of
+// y* = (x + dt (v + h a), v + h a, rho + h drho) to lam of (x, v, rho), in
+// place, and the adjoint of the record (a, drho) it read, h = dt/2.
+__global__ void k_verlet_kd_adj(uint32_t n, float4* __restrict__ lp, float4* __restrict__ lv, float h, float dt,
+                                float4* __restrict__ lfp, float4* __restrict__ lfv) {
+    const uint32_t k = blockIdx.x * blockDim.x + threadIdx.x;
+    if (k >= n) return;
+    const float4 p = lp[k];
+    float4 v = lv[k];
+    v.x += dt * p.x;
+    v.y += dt * p.y;
+    v.z += dt * p.z;
+    lv[k] = v;
+    lfp[k] = make_float4(0.f, 0.f, 0.f, h * p.w);
+    lfv[k] = make_float4(h * v.x, h * v.y, h * v.z, 0.f);
+}
+
 __global__ void k_adj_perm(uint32_t n, const uint32_t* __restrict__ orig, const float4* __restrict__ ip,
                            const float4* __restrict__ iv, float4* __restrict__ op, float4* __restrict__ ov,
                            int scatter) {
@@ -1168,6 +1197,20 @@ int adjoint_step_sum_all(uint32_t n, const float4* lam, int stages, const float4
     L.n = stages;
     for (int t = 0; t < stages; ++t) L.pd[t] = lamY[t];
     k_adj_sum_all<<<nblocks(n, 256), 256, 0, st>>>(n, lam, L, out);
+    return 1;
+}
+
+int verlet_adjoint_weights(uint32_t n, const float4* lsp, const float4* lsv, const float4* lfp, const float4* lfv,
+                           float h, float4* mp, float4* mv, cudaStream_t st) {
+    if (n == 0) return 0;
+    k_verlet_mu<<<nblocks(n, 256), 256, 0, st>>>(n, lsp, lsv, lfp, lfv, h, mp, mv);
+    return 1;
+}
+
+int verlet_kick_drift_adjoint(uint32_t n, float4* lp, float4* lv, float h, float dt, float4* lfp, float4* lfv,
+                              cudaStream_t st) {
+    if (n == 0) return 0;
+    k_verlet_kd_adj<<<nblocks(n, 256), 256, 0, st>>>(n, lp, lv, h, dt, lfp, lfv);
     return 1;
 }
 

@@ -419,6 +419,14 @@ int adjoint_stage_weights_all(uint32_t n, float cb, const float4* lam, int nlate
 // out = lam + sum_s lamY[s] for a plain array of `n` float4.
 int adjoint_step_sum_all(uint32_t n, const float4* lam, int stages, const float4* const* lamY, float4* out,
                          cudaStream_t st);
+// Velocity Verlet: the weights of a step's force evaluation,
+// mu = lam_f + (dt/2) P lam (P keeps the density and velocity parts), and the
+// kick-drift's adjoint in place (caller order), writing the adjoint of the
+// carried record it read.  h = dt/2.
+int verlet_adjoint_weights(uint32_t n, const float4* lsp, const float4* lsv, const float4* lfp, const float4* lfv,
+                           float h, float4* mp, float4* mv, cudaStream_t st);
+int verlet_kick_drift_adjoint(uint32_t n, float4* lp, float4* lv, float h, float dt, float4* lfp, float4* lfv,
+                              cudaStream_t st);
 // mu = cb * lam_next + sum_t ca[t] * lamY[t] over the given later stages.
 int adjoint_stage_weights(uint32_t n, float cb, const float4* lam_pd, const float4* lam_vm, int nlater,
                           const float* ca, const float4* const* lamY_pd, const float4* const* lamY_vm,

@@ -159,6 +159,8 @@ struct StepRecord {
 struct Checkpoint {
     DevBuf<float4> pd, vm;
     DevBuf<float4> ep;  // plastic strain (plastic scenes)
+    DevBuf<float4> fpd, fvm, fep;  // velocity Verlet: the carried force record (same storage order as pd)
+    bool fvalid = false;
     DevBuf<uint32_t> orig, sid;
     float time = 0.0f;
 };
@@ -180,6 +182,12 @@ struct AdjointPool {
     DevBuf<double2> gst;
     DevBuf<uint32_t> flags;
     Checkpoint now;
+    // velocity Verlet: the adjoint of the carried force record (caller order;
+    // solid order for the plastic strain's) and the record of the force
+    // evaluation at the tape's start, when the first taped step made one
+    DevBuf<float4> lf_p, lf_v, lf_ep;
+    StepRecord prime;
+    bool prime_recorded = false;
 };
 
 }  // namespace
@@ -288,6 +296,7 @@ struct arp_sim {
         DevBuf<uint8_t> rgb;
     } rbuf;
     StepRecord* rec = nullptr;  // set while a recording step runs
+    StepRecord* rec_prime = nullptr;  // where a recording Verlet step records its force evaluation at y_n
     bool replaying = false;     // steps re-run by the backward pass take no checkpoints
     DevBuf<uint32_t> mat_of_solid, rl_off, rl_nbr;
     DevBuf<float4> rl_gw;
@@ -618,6 +627,12 @@ arp_status save_checkpoint(arp_sim* S) {
     CUDA_TRY(keep(c.orig, (const uint32_t*)S->orig.p, S->n, S->stream));
     CUDA_TRY(keep(c.sid, (const uint32_t*)S->sid.p, S->n, S->stream));
     if (S->any_plastic) CUDA_TRY(keep(c.ep, (const float4*)S->ep.p, 4 * size_t(S->ns), S->stream));
+    c.fvalid = S->verlet() && S->vforce_valid;
+    if (c.fvalid) {
+        CUDA_TRY(keep(c.fpd, (const float4*)S->vforce.pd.p, S->n, S->stream));
+        CUDA_TRY(keep(c.fvm, (const float4*)S->vforce.vm.p, S->n, S->stream));
+        if (S->any_plastic) CUDA_TRY(keep(c.fep, (const float4*)S->ep_force.p, 4 * size_t(S->ns), S->stream));
+    }
     c.time = S->time;
     S->tape->ckpts.push_back(std::move(c));
     return ARP_OK;
@@ -634,6 +649,16 @@ arp_status restore_checkpoint(arp_sim* S, const Checkpoint& c) {
     if (S->any_plastic && S->ns)
         CUDA_TRY(cudaMemcpyAsync(S->ep.p, c.ep.p, 4 * size_t(S->ns) * sizeof(float4), cudaMemcpyDeviceToDevice,
                                  S->stream));
+    if (S->verlet()) {
+        S->vforce_valid = c.fvalid;
+        if (c.fvalid && n) {
+            CUDA_TRY(cudaMemcpyAsync(S->vforce.pd.p, c.fpd.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, S->stream));
+            CUDA_TRY(cudaMemcpyAsync(S->vforce.vm.p, c.fvm.p, n * sizeof(float4), cudaMemcpyDeviceToDevice, S->stream));
+        }
+        if (c.fvalid && S->any_plastic && S->ns)
+            CUDA_TRY(cudaMemcpyAsync(S->ep_force.p, c.fep.p, 4 * size_t(S->ns) * sizeof(float4),
+                                     cudaMemcpyDeviceToDevice, S->stream));
+    }
     S->time = c.time;
     return ARP_OK;
 }
@@ -653,7 +678,16 @@ arp_status do_step(arp_sim* S, bool prime = false) {
         if (S->tape->steps % S->tape->every == 0) ARP_TRY(save_checkpoint(S));
         S->tape->steps++;
     }
-    StepRecord* R = prime ? nullptr : S->rec;
+    if (verlet && !prime && !S->vforce_valid) {
+        // the force evaluation at y_n that the first step after init, a new
+        // state or a tape start makes; a recording step records it too
+        S->rec_prime = S->rec ? &S->adj.prime : nullptr;
+        if (S->rec) S->adj.prime_recorded = true;
+        const arp_status ps = do_step(S, true);
+        S->rec_prime = nullptr;
+        ARP_TRY(ps);
+    }
+    StepRecord* R = prime ? S->rec_prime : S->rec;
     if (!prime) S->time += S->dt_sub;
     const uint32_t* bstart = S->b_start.p;
     uint64_t l0 = S->launches;
@@ -1536,11 +1570,13 @@ arp_status graph_step(arp_sim* S) {
 arp_status arp_sim_step(arp_sim* sim, uint32_t nsteps) {
     ARP_TRY(need_init(sim));
     for (uint32_t i = 0; i < nsteps; ++i) {
-        // velocity Verlet starts from a force evaluation at the current state
-        // (plain launches: it is not part of the step a graph replays)
-        if (sim->verlet() && !sim->vforce_valid) ARP_TRY(do_step(sim, true));
         const bool sampled = sim->prof_on && sim->prof_phase % sim->prof_every == 0;
-        if (sim->use_graph && !sim->tape && !sampled) ARP_TRY(graph_step(sim));
+        const bool graphed = sim->use_graph && !sim->tape && !sampled;
+        // velocity Verlet starts from a force evaluation at the current state:
+        // plain launches before a graphed step (the graph replays only steps
+        // that carry the record); a plain step makes it itself
+        if (graphed && sim->verlet() && !sim->vforce_valid) ARP_TRY(do_step(sim, true));
+        if (graphed) ARP_TRY(graph_step(sim));
         else ARP_TRY(do_step(sim));
     }
     return ARP_OK;
@@ -2097,9 +2133,11 @@ arp_status arp_tape_begin(arp_sim* sim, uint32_t checkpoint_every) {
     ARP_TRY(need_init(sim));
     if (checkpoint_every == 0) return fail(ARP_ERR_INVALID_ARG, "checkpoint interval must be positive");
     if (sim->tab.stages > kMaxStages) return fail(ARP_ERR_UNSUPPORTED, "more than 4 stages");
-    if (sim->verlet()) return fail(ARP_ERR_UNSUPPORTED, "the adjoint differentiates Runge-Kutta steps only");
     sim->drop_graph();
     retire_tape(sim);
+    // velocity Verlet: the tape starts with a force evaluation at the current
+    // state (recorded, so the gradient reaches y_0 through it), as after init
+    if (sim->verlet()) sim->vforce_valid = false;
     sim->tape.reset(new Tape());
     sim->tape->every = checkpoint_every;
     return ARP_OK;
@@ -2134,6 +2172,12 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
     CUDA_TRY(keep(now.orig, (const uint32_t*)sim->orig.p, n, st));
     CUDA_TRY(keep(now.sid, (const uint32_t*)sim->sid.p, n, st));
     if (sim->any_plastic) CUDA_TRY(keep(now.ep, (const float4*)sim->ep.p, 4 * size_t(ns), st));
+    now.fvalid = sim->verlet() && sim->vforce_valid;
+    if (now.fvalid) {
+        CUDA_TRY(keep(now.fpd, (const float4*)sim->vforce.pd.p, n, st));
+        CUDA_TRY(keep(now.fvm, (const float4*)sim->vforce.vm.p, n, st));
+        if (sim->any_plastic) CUDA_TRY(keep(now.fep, (const float4*)sim->ep_force.p, 4 * size_t(ns), st));
+    }
     now.time = sim->time;
     // adjoint buffers: caller order (lc), storage order (ls, out), per stage (lY), stage weights (mu)
     const size_t nn = std::max(n, 1u);
@@ -2169,6 +2213,120 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
         CUDA_TRY(cudaMemcpyAsync(P.io.p, dl_dstate, n * 2 * sizeof(float4), cudaMemcpyHostToDevice, st));
         sim->launches += adjoint_unpack(n, P.io.p, lc_p.p, lc_v.p, st);
     }
+    // lam_Y += J_f(Y)^T mu for stage q of a recorded step
+    auto stage_vjp = [&](const StepRecord& R, int q, const float4* mup, const float4* muv, float4* lyp, float4* lyv,
+                         const float4* muep, float4* lyep) {
+        AdjArgs a{};
+        a.st.pd = R.pd[q].p;
+        a.st.vm = R.vm[q].p;
+        a.st.perm = R.has_perm[q] ? R.perm[q].p : nullptr;
+        a.st.start = R.start[q].p;
+        const bool sb = sim->solid_branch();
+        a.st.F = sb ? R.F[q].p : nullptr;
+        a.st.A = sb ? R.A[q].p : nullptr;
+        a.st.sx = sb ? R.sx[q].p : nullptr;
+        a.st.sv = sb ? R.sv[q].p : nullptr;
+        a.st.sc = sb ? R.sc[q].p : nullptr;
+        a.st.contact_bound = sb ? R.cb[q].p : nullptr;
+        a.sid = R.sid.p;
+        a.slot_of = R.slot_of.p;
+        a.mu_pd = mup;
+        a.mu_vm = muv;
+        a.lam_pd = lyp;
+        a.lam_vm = lyv;
+        a.bxs = sim->b_pd.p;
+        a.bvs = sim->b_vm.p;
+        a.bstart = sim->b_start.p;
+        a.bps = sim->bps.p;
+        a.ref = sim->ref.p;
+        a.L = sim->L.p;
+        a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz};
+        a.stiff = sim->have_stiff ? sim->stiff.p : nullptr;
+        a.lamF = lamF.p;
+        a.lamFd = lamFd.p;
+        a.g_stiff = gst.p;
+        a.flags = flags.p;
+        a.w = P.w.p;
+        a.eq = P.e.p;
+        a.xs = P.xs.p;
+        a.n = n;
+        a.ns = ns;
+        a.solid_branch = sb ? 1 : 0;
+        a.all_order2 = sim->all_order2 ? 1 : 0;
+        a.st.ep = plastic ? R.ep[q].p : nullptr;
+        a.mu_ep = plastic ? muep : nullptr;
+        a.lam_ep = plastic ? lyep : nullptr;
+        sim->launches += launch_adjoint_stage(a, sim->tables, sim->kdim, st);
+    };
+    // Velocity Verlet, one step (reverse): y* = kick-drift(y_n, f_n),
+    // f_{n+1} = f(y*), y_{n+1} = y* + (dt/2) P f_{n+1}.  With lam the state's
+    // adjoint and lf the carried record's (both caller order):
+    //   mu = lf + (dt/2) P lam;  lam* = lam + J_f(y*)^T mu;  then the
+    //   kick-drift's adjoint gives lam_n and lf_n from lam*;  a step that began
+    //   with the force evaluation f_n = f(y_n) adds J_f(y_n)^T lf_n to lam_n.
+    const bool verlet = sim->verlet();
+    const float vh = (float)(sim->tab.b[0] * (double)sim->dt_sub);
+    if (verlet) {
+        for (DevBuf<float4>* b : {&P.lf_p, &P.lf_v}) {
+            CUDA_TRY(fit(*b, nn));
+            CUDA_TRY(cudaMemsetAsync(b->p, 0, nn * sizeof(float4), st));  // the loss reads no force record
+        }
+        if (plastic) {
+            CUDA_TRY(fit(P.lf_ep, ne));
+            CUDA_TRY(cudaMemsetAsync(P.lf_ep.p, 0, ne * sizeof(float4), st));
+        }
+        P.prime_recorded = false;
+    }
+    auto verlet_step_vjp = [&](const StepRecord& R, bool with_prime) -> arp_status {
+        const float one = 1.0f;
+        sim->launches += adjoint_gather(n, R.orig.p, lc_p.p, lc_v.p, ls_p.p, ls_v.p, st);
+        sim->launches += adjoint_gather(n, R.orig.p, P.lf_p.p, P.lf_v.p, out_p.p, out_v.p, st);
+        sim->launches += verlet_adjoint_weights(n, ls_p.p, ls_v.p, out_p.p, out_v.p, vh, mu_p.p, mu_v.p, st);
+        if (plastic) {
+            const float4* lfe[1] = {P.lf_ep.p};
+            sim->launches += adjoint_stage_weights_all(4 * ns, vh, P.lam_ep.p, 1, &one, lfe, P.mu_ep.p, st);
+            CUDA_TRY(cudaMemsetAsync(P.lY_ep[0].p, 0, 4 * size_t(ns) * sizeof(float4), st));
+        }
+        if (n) {
+            CUDA_TRY(cudaMemsetAsync(lY_p[0].p, 0, n * sizeof(float4), st));
+            CUDA_TRY(cudaMemsetAsync(lY_v[0].p, 0, n * sizeof(float4), st));
+        }
+        stage_vjp(R, 0, mu_p.p, mu_v.p, lY_p[0].p, lY_v[0].p, P.mu_ep.p, P.lY_ep[0].p);
+        const float4* yp[1] = {lY_p[0].p};
+        const float4* yv[1] = {lY_v[0].p};
+        sim->launches += adjoint_step_sum(n, ls_p.p, ls_v.p, 1, yp, yv, out_p.p, out_v.p, st);
+        sim->launches += adjoint_scatter(n, R.orig.p, out_p.p, out_v.p, lc_p.p, lc_v.p, st);
+        sim->launches += verlet_kick_drift_adjoint(n, lc_p.p, lc_v.p, vh, sim->dt_sub, P.lf_p.p, P.lf_v.p, st);
+        if (plastic) {
+            const float4* ye[1] = {P.lY_ep[0].p};
+            sim->launches += adjoint_step_sum_all(4 * ns, P.lam_ep.p, 1, ye, P.out_ep.p, st);
+            std::swap(P.lam_ep, P.out_ep);
+            sim->launches += adjoint_stage_weights_all(4 * ns, vh, P.lam_ep.p, 0, nullptr, nullptr, P.lf_ep.p, st);
+        }
+        if (!with_prime) return ARP_OK;
+        // the force evaluation at y_0: lam_0 += J_f(y_0)^T lf_0 (the record's
+        // position part is zero), in the storage order of that evaluation
+        const StepRecord& R0 = P.prime;
+        sim->launches += adjoint_gather(n, R0.orig.p, P.lf_p.p, P.lf_v.p, mu_p.p, mu_v.p, st);
+        if (n) {
+            CUDA_TRY(cudaMemsetAsync(lY_p[0].p, 0, n * sizeof(float4), st));
+            CUDA_TRY(cudaMemsetAsync(lY_v[0].p, 0, n * sizeof(float4), st));
+        }
+        if (plastic) CUDA_TRY(cudaMemsetAsync(P.lY_ep[0].p, 0, 4 * size_t(ns) * sizeof(float4), st));
+        stage_vjp(R0, 0, mu_p.p, mu_v.p, lY_p[0].p, lY_v[0].p, P.lf_ep.p, P.lY_ep[0].p);
+        sim->launches += adjoint_scatter(n, R0.orig.p, lY_p[0].p, lY_v[0].p, out_p.p, out_v.p, st);
+        const float4* op[1] = {out_p.p};
+        const float4* ov[1] = {out_v.p};
+        sim->launches += adjoint_step_sum(n, lc_p.p, lc_v.p, 1, op, ov, ls_p.p, ls_v.p, st);
+        std::swap(P.lc_p, P.ls_p);
+        std::swap(P.lc_v, P.ls_v);
+        if (plastic) {
+            const float4* ye[1] = {P.lY_ep[0].p};
+            sim->launches += adjoint_step_sum_all(4 * ns, P.lam_ep.p, 1, ye, P.out_ep.p, st);
+            std::swap(P.lam_ep, P.out_ep);
+        }
+        return ARP_OK;
+    };
     const uint32_t every = tp.every;
     if (P.recs.size() < every) P.recs.resize(every);
     const uint64_t nseg = (total + every - 1) / every;
@@ -2184,6 +2342,10 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
         }
         for (uint64_t t = t1; t-- > t0 && status == ARP_OK;) {
             const StepRecord& R = P.recs[t - t0];
+            if (verlet) {
+                status = verlet_step_vjp(R, t == 0 && P.prime_recorded);
+                continue;
+            }
             sim->launches += adjoint_gather(n, R.orig.p, lc_p.p, lc_v.p, ls_p.p, ls_v.p, st);
             for (int q = S - 1; q >= 0; --q) {
                 float ca[kMaxStages];
@@ -2211,47 +2373,7 @@ arp_status arp_tape_backward(arp_sim* sim, const float* dl_dstate, float* grad_s
                     cudaMemsetAsync(lY_p[q].p, 0, n * sizeof(float4), st);
                     cudaMemsetAsync(lY_v[q].p, 0, n * sizeof(float4), st);
                 }
-                AdjArgs a{};
-                a.st.pd = R.pd[q].p;
-                a.st.vm = R.vm[q].p;
-                a.st.perm = R.has_perm[q] ? R.perm[q].p : nullptr;
-                a.st.start = R.start[q].p;
-                const bool sb = sim->solid_branch();
-                a.st.F = sb ? R.F[q].p : nullptr;
-                a.st.A = sb ? R.A[q].p : nullptr;
-                a.st.sx = sb ? R.sx[q].p : nullptr;
-                a.st.sv = sb ? R.sv[q].p : nullptr;
-                a.st.sc = sb ? R.sc[q].p : nullptr;
-                a.st.contact_bound = sb ? R.cb[q].p : nullptr;
-                a.sid = R.sid.p;
-                a.slot_of = R.slot_of.p;
-                a.mu_pd = mu_p.p;
-                a.mu_vm = mu_v.p;
-                a.lam_pd = lY_p[q].p;
-                a.lam_vm = lY_v[q].p;
-                a.bxs = sim->b_pd.p;
-                a.bvs = sim->b_vm.p;
-                a.bstart = sim->b_start.p;
-                a.bps = sim->bps.p;
-                a.ref = sim->ref.p;
-                a.L = sim->L.p;
-                a.rl = SolidRefList{sim->rl_off.p, sim->rl_nbr.p, sim->rl_gw.p, sim->rl_nnz};
-                a.stiff = sim->have_stiff ? sim->stiff.p : nullptr;
-                a.lamF = lamF.p;
-                a.lamFd = lamFd.p;
-                a.g_stiff = gst.p;
-                a.flags = flags.p;
-                a.w = P.w.p;
-                a.eq = P.e.p;
-                a.xs = P.xs.p;
-                a.n = n;
-                a.ns = ns;
-                a.solid_branch = sb ? 1 : 0;
-                a.all_order2 = sim->all_order2 ? 1 : 0;
-                a.st.ep = plastic ? R.ep[q].p : nullptr;
-                a.mu_ep = plastic ? P.mu_ep.p : nullptr;
-                a.lam_ep = plastic ? P.lY_ep[q].p : nullptr;
-                sim->launches += launch_adjoint_stage(a, sim->tables, sim->kdim, st);
+                stage_vjp(R, q, mu_p.p, mu_v.p, lY_p[q].p, lY_v[q].p, P.mu_ep.p, P.lY_ep[q].p);
             }
             const float4* yp[kMaxStages];
             const float4* yv[kMaxStages];

@@ -265,13 +265,14 @@ def cpu_baseline(config, steps=5, warmup=1):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20):
+def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=200):
     """256 independent scenes (2,048-65,536 particles each, own h, fluid
     blocks and elastic blocks): stepped as one batch (one set of launches per
     stage) and as a loop over 256 separate simulations, both on one GPU and
     both replaying each step from a CUDA graph.  The batch is timed over the
     configuration's 200 steps with the autotuner's launch shape; every
-    persistent tile-queue shape of the fluid kernel is timed beside it."""
+    persistent tile-queue shape of the fluid kernel is timed beside it over
+    the same 200 steps from the same state."""
     from arphys import FluidSim, scenes
     scs = scenes.batched_scenes()
     parts = int(sum(sc.n + sc.nb for sc in scs))
