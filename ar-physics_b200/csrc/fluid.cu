@@ -813,7 +813,17 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_staged(FluidArgs a, Tables T, S
             const uint32_t w = (uint32_t)rho * SS::NQ + (uint32_t)q;
             const uint32_t jb = a.start[c0], je = a.start[c1];
             const int shift = (int)w_off[w] - (int)w_gstart[w];  // global index -> staging slot
-            for (uint32_t j = jb; j < je; ++j)
+            uint32_t j = jb;
+            for (; j + 3u < je; j += 4u) {  // four shared-memory loads in flight
+                const int i0 = (int)j + shift;
+                const float4 q0 = stg[i0], q1 = stg[i0 + 1], q2 = stg[i0 + 2], q3 = stg[i0 + 3];
+                const bool h0 = hit(q0), h1 = hit(q1), h2 = hit(q2), h3 = hit(q3);
+                if (h0) take(j);
+                if (h1) take(j + 1u);
+                if (h2) take(j + 2u);
+                if (h3) take(j + 3u);
+            }
+            for (; j < je; ++j)
                 if (hit(stg[(int)j + shift])) take(j);
         }
     }

@@ -55,28 +55,44 @@ def gpu_gradients(sc, steps, every, loss, start=None):
     return L, g0, gs
 
 
-def ulp_nudged(sc, start):
-    """The starting state with every position moved by one float32 ulp in a
-    seeded random direction: a trajectory as far from the first as float
-    rounding puts the FP32 forward from the FP64 one."""
-    p = (sc.particles if start is None else start).copy()
-    rng = np.random.default_rng(1234)
-    x = p["pos"][:, :sc.dim]
-    away = np.where(rng.random(x.shape) < 0.5, -np.inf, np.inf).astype(np.float32)
-    p["pos"][:, :sc.dim] = np.nextafter(x, away)
-    return p
+def translated(sc, start, loss, shift=0.0371):
+    """The same problem moved by `shift` along every axis of the scene (its
+    particles, boundary, box and loss target).  In exact arithmetic the
+    trajectory and the gradients are unchanged; in float32 every position is
+    rounded differently at every step, so the spread between the two GPU
+    gradients measures how far float rounding of the forward moves them."""
+    d = sc.dim
+    p = sc.particles.copy()
+    p["pos"][:, :d] += np.float32(shift)
+    b = sc.boundary.copy()
+    if len(b):
+        b["pos"][:, :d] += np.float32(shift)
+    bmin = tuple(float(sc.bounds_min[a]) + (shift if a < d else 0.0) for a in range(4))
+    moved = scenes.Scene(**{**sc.__dict__, "particles": p, "boundary": b, "bounds_min": bmin})
+    st = None
+    if start is not None:
+        st = start.copy()
+        st["pos"][:, :d] += np.float32(shift)
+    off = np.zeros(3)
+    off[:d] = shift
+    if loss[0] == "tip":
+        lo = ("tip", loss[1], np.asarray(loss[2], np.float64) + off)
+    else:
+        lo = ("points", loss[1] + off)
+    return moved, st, lo
 
 
 def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4, eps_vel=1e-4, start=None):
-    """The GPU gradient along each direction, the same from a start nudged by
-    one float32 ulp (the FP32 noise of the gradient itself), and the FP64
+    """The GPU gradient along each direction, the same for the problem
+    translated in space (the FP32 noise of the gradient itself), and the FP64
     oracle's central difference (L(p + e d) - L(p - e d)) / 2e along the same
     direction.  `loss` is ("tip", ids, target) or ("points", targets); `start`
     (particle records) replaces the scene's initial state after creation,
     keeping the scene's positions as the solids' reference configuration."""
     stiff = sc.meta.get("stiffness")
     L, g0, gs = gpu_gradients(sc, steps, every, loss, start)
-    _, g0n, gsn = gpu_gradients(sc, steps, every, loss, ulp_nudged(sc, start))
+    moved, mstart, mloss = translated(sc, start, loss)
+    _, g0n, gsn = gpu_gradients(moved, steps, every, mloss, mstart)
     p0 = sc.particles if start is None else start
     v0 = p0["vel"][:, :3].astype(np.float64)
     x0 = None if start is None else start["pos"].astype(np.float64)
@@ -102,8 +118,8 @@ def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1
 def report(res, tol):
     """Per direction: the relative error |adj - fd| / |fd| against FP64 finite
     differences, and whether it is within `tol` or else within the FP32 noise
-    of the gradient itself (3 x its change under the one-ulp nudge of the
-    start).  The forward runs in float32, as the reference's shaders do; where
+    of the gradient itself (3 x its change when the problem is translated in
+    space, which exact arithmetic leaves unchanged).  The forward runs in float32, as the reference's shaders do; where
     a derivative is small against the gradient's size (random directions
     cancel) or is carried by tiny strains (float positions of order 1 m
     resolve them to ~1e-7), that noise exceeds tol of the derivative.
