@@ -405,32 +405,7 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
             return true;
         }
     } else if (finite3(xi)) {
-        // two-pass lists fill without branches: every candidate is written at
-        // the list's end (slot CAP takes the writes past a full list) and the
-        // count advances by its hit, so lanes do not diverge on hits; a count
-        // above CAP marks the list as overflowed
-        auto put = [&](uint32_t j, bool h) {
-            my[min(cnt, (uint32_t)CAP) * BLOCK] = j;
-            cnt += h ? 1u : 0u;
-        };
         for_search_rows<DIM>(xi, P, [&](uint32_t c0, uint32_t c1) {
-            if (MODE == kTwoPass) {
-                if (cnt > (uint32_t)CAP) return;
-                const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
-                for (uint32_t j = bb; j < be; ++j) put(j | kBoundaryBit, hit(a.bxs[j]));
-                const uint32_t jb = a.start[c0], je = a.start[c1];
-                uint32_t j = jb;
-                for (; j + 3u < je; j += 4u) {  // four loads in flight
-                    const float4 q0 = a.xs[j], q1 = a.xs[j + 1u], q2 = a.xs[j + 2u], q3 = a.xs[j + 3u];
-                    const bool h0 = hit(q0), h1 = hit(q1), h2 = hit(q2), h3 = hit(q3);
-                    put(j, h0);
-                    put(j + 1u, h1);
-                    put(j + 2u, h2);
-                    put(j + 3u, h3);
-                }
-                for (; j < je; ++j) put(j, hit(a.xs[j]));
-                return;
-            }
             if (full) return;
             const uint32_t bb = a.bstart[c0], be = a.bstart[c1];
             for (uint32_t j = bb; j < be; ++j)
@@ -449,7 +424,7 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
                 if (hit(a.xs[j])) take(j);
         });
         if (MODE == kTwoPass) {
-            if (cnt > (uint32_t)CAP) {
+            if (full) {
                 a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
                 return true;
             }
@@ -475,7 +450,7 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const Tables& T, 
                                            const StageBuffers& b) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * (CAP + 1) * BLOCK);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * BLOCK);
     DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
     const uint32_t k0 = blockIdx.x * BLOCK;
     const uint32_t scene0 = T.mats[__float_as_uint(a.vs[min(k0, a.n - 1u)].w)].scene;
@@ -495,7 +470,7 @@ __device__ __forceinline__ void fluid_tiles_persistent(const FluidArgs& a, const
                                                        const StageBuffers& b, uint32_t* tile_counter) {
     extern __shared__ __align__(16) unsigned char smem_raw[];
     uint32_t* lst = reinterpret_cast<uint32_t*>(smem_raw);
-    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * (CAP + 1) * BLOCK);
+    FluidMat* sm = reinterpret_cast<FluidMat*>(smem_raw + sizeof(uint32_t) * CAP * BLOCK);
     DevInter* si = reinterpret_cast<DevInter*>(reinterpret_cast<unsigned char*>(sm) + sizeof(FluidMat) * T.max_nmat);
     __shared__ uint32_t tile_s;
     uint32_t loaded = kInvalid;
@@ -866,7 +841,7 @@ __global__ void __launch_bounds__(BLOCK) k_fluid_staged(FluidArgs a, Tables T, S
 template <int DIM, int BLOCK, int CAP, int MODE>
 void launch_variant(const FluidArgs& a, const Tables& T, const StageCoefs& c, const StageBuffers& b, bool persistent,
                     uint32_t* tile_counter, cudaStream_t st) {
-    const size_t smem = sizeof(uint32_t) * (CAP + 1) * BLOCK + sizeof(FluidMat) * T.max_nmat +
+    const size_t smem = sizeof(uint32_t) * CAP * BLOCK + sizeof(FluidMat) * T.max_nmat +
                         sizeof(DevInter) * T.max_nmat * T.max_nmat;
     if (smem > 48 * 1024) {
         cudaFuncSetAttribute(FluidKernels<DIM, BLOCK, CAP, MODE>::tile, cudaFuncAttributeMaxDynamicSharedMemorySize,

@@ -103,13 +103,13 @@ def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1
     for d in directions_stiff:
         a0 = float(np.sum(gs.astype(np.float64) * s64 * d[:, None]))
         adj.append(("stiffness", a0))
-        nudged.append(max(abs(a0 - float(np.sum(g[1].astype(np.float64) * s64 * d[:, None]))) for g in spread))
+        nudged.append([a0 - float(np.sum(g[1].astype(np.float64) * s64 * d[:, None])) for g in spread])
         tasks += [(sc, steps, s64 * (1 + eps_rel * d[:, None]), v0, loss, x0),
                   (sc, steps, s64 * (1 - eps_rel * d[:, None]), v0, loss, x0)]
     for d in directions_vel:
         a0 = float(np.sum(g0[:, 4:7].astype(np.float64) * d))
         adj.append(("velocity", a0))
-        nudged.append(max(abs(a0 - float(np.sum(g[0][:, 4:7].astype(np.float64) * d))) for g in spread))
+        nudged.append([a0 - float(np.sum(g[0][:, 4:7].astype(np.float64) * d)) for g in spread])
         tasks += [(sc, steps, s64, v0 + eps_vel * d, loss, x0), (sc, steps, s64, v0 - eps_vel * d, loss, x0)]
     ls = oracle_losses(tasks)
     out = []
@@ -122,32 +122,36 @@ def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1
 def report(res, tol):
     """Per direction: the relative error |adj - fd| / |fd| against FP64 finite
     differences, and whether it is within `tol` or else within the FP32 noise
-    of the gradient itself (3 x its largest change when the problem is
-    translated in space by two different shifts, which exact arithmetic
-    leaves unchanged).  The forward runs in float32, as the reference's shaders do; where
-    a derivative is small against the gradient's size (random directions
-    cancel) or is carried by tiny strains (float positions of order 1 m
-    resolve them to ~1e-7), that noise exceeds tol of the derivative.
-    Returns the number of directions meeting neither bound."""
+    of the gradient itself.  The noise is measured: the problem translated in
+    space by two shifts gives the same gradient in exact arithmetic, but every
+    position of the float32 forward rounds differently at every step; with
+    sigma the RMS of those differences over all directions of a kind divided
+    by sqrt 2 (each difference holds two independent roundings), a direction
+    passes within 4 sigma.  The forward runs in float32, as the reference's
+    shaders do: where a derivative is small against the gradient's size
+    (random directions cancel) or is carried by small strains (float positions
+    of order 1 m resolve them to ~1e-7), that noise exceeds tol of the
+    derivative.  Returns the number of directions meeting neither bound."""
     bad = 0
     for kind in ("stiffness", "velocity"):
-        rows = [(a, f, nz) for k, a, f, nz in res if k == kind]
+        rows = [(a, f, sp) for k, a, f, sp in res if k == kind]
         if not rows:
             continue
+        sigma = float(np.sqrt(np.mean([x * x for _, _, sp in rows for x in sp]) / 2.0))
         errs = [abs(a - f) / max(abs(f), 1e-300) for a, f, _ in rows]
         mags = [abs(f) for _, f, _ in rows]
         within = sum(1 for e in errs if e < tol)
-        noise_ok = sum(1 for (a, f, nz), e in zip(rows, errs) if e >= tol and abs(a - f) <= 3.0 * nz)
+        noise_ok = sum(1 for (a, f, _), e in zip(rows, errs) if e >= tol and abs(a - f) <= 4.0 * sigma)
         fails = len(rows) - within - noise_ok
         na = np.array([a for a, _, _ in rows])
         nf = np.array([f for _, f, _ in rows])
         print(f"{kind}: {len(rows)} directions, |fd| {min(mags):.3e} .. {max(mags):.3e}, rel err median "
               f"{np.median(errs):.2e} max {max(errs):.2e}, norm-wise {np.linalg.norm(na - nf) / np.linalg.norm(nf):.2e}; "
-              f"{within} within {tol:.0e}, {noise_ok} within FP32 noise, {fails} neither")
-        for (a, f, nz), e in zip(rows, errs):
+              f"FP32 noise sigma {sigma:.2e}; {within} within {tol:.0e}, {noise_ok} within 4 sigma, {fails} neither")
+        for (a, f, _), e in zip(rows, errs):
             if e >= tol:
                 print(f"  adjoint {a:.6e} fd64 {f:.6e} rel err {e:.2e} |adj - fd| {abs(a - f):.2e} "
-                      f"FP32 noise {nz:.2e}")
+                      f"= {abs(a - f) / sigma:.1f} sigma")
         bad += fails
     return bad
 
@@ -231,11 +235,12 @@ def test_friction_gradients_match_fp64_finite_differences():
             dv.append(d)
         L, res[mu] = fd_check(sc, 20, 5, ("points", target), [], dv)
     assert report(res[5.0], 1e-4) == 0
-    for (_, a1, f1, n1), (_, a0, f0, n0) in zip(res[5.0], res[0.0]):
+    sig = [float(np.sqrt(np.mean([x * x for r in res[m] for x in r[3]]) / 2.0)) for m in (5.0, 0.0)]
+    for (_, a1, f1, _), (_, a0, f0, _) in zip(res[5.0], res[0.0]):
         da, df = a1 - a0, f1 - f0
         err = abs(da - df) / abs(df)
-        print(f"friction part: adjoint {da:.6e} fd64 {df:.6e} rel err {err:.2e} (FP32 noise {n1 + n0:.2e})")
-        assert err < 1e-2 or abs(da - df) <= 3.0 * (n1 + n0)
+        print(f"friction part: adjoint {da:.6e} fd64 {df:.6e} rel err {err:.2e}")
+        assert err < 1e-2 or abs(da - df) <= 4.0 * (sig[0] + sig[1])
 
 
 @pytest.mark.parametrize("order", [0, 1, -2, 3])
