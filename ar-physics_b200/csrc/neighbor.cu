@@ -197,7 +197,9 @@ __device__ __forceinline__ uint32_t reference_cell_occupancy(uint32_t c, const u
     return occ;
 }
 
-constexpr uint32_t kShortRun = 128;  // runs up to this length: insertion sort by their own thread
+constexpr uint32_t kShortRun = 32;    // runs up to this length: insertion sort by their own thread
+constexpr uint32_t kWarpRun = 256;    // up to this length: bitonic sort in shared memory by one warp
+constexpr uint32_t kBlockRun = 4096;  // up to this length: bitonic sort in shared memory by the block
 
 // Block-wide reductions (blockDim.x == kThreads); every thread gets the result.
 template <class Op>
@@ -261,18 +263,75 @@ __device__ void block_sort_run(uint32_t* perm, uint32_t* tmp, uint32_t b, uint32
     __syncthreads();
 }
 
+// Sorts one run perm[b, b + L) (L <= kWarpRun) ascending with one warp: a
+// bitonic network over the run padded to a power of two in `buf` (shared
+// memory, kWarpRun entries of this warp).  The values are distinct slots.
+__device__ void warp_sort_run(uint32_t* perm, uint32_t b, uint32_t L, uint32_t* buf) {
+    const uint32_t lane = threadIdx.x & 31u;
+    uint32_t P = 32u;
+    while (P < L) P <<= 1;
+    for (uint32_t i = lane; i < P; i += 32u) buf[i] = i < L ? perm[b + i] : 0xFFFFFFFFu;
+    __syncwarp();
+    for (uint32_t k = 2u; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0u; j >>= 1) {
+            for (uint32_t i = lane; i < P; i += 32u) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const uint32_t x = buf[i], y = buf[ixj];
+                    if ((x > y) == ((i & k) == 0u)) {
+                        buf[i] = y;
+                        buf[ixj] = x;
+                    }
+                }
+            }
+            __syncwarp();
+        }
+    for (uint32_t i = lane; i < L; i += 32u) perm[b + i] = buf[i];
+    __syncwarp();
+}
+
+// Sorts one run perm[b, b + L) (kWarpRun < L <= kBlockRun) ascending with the
+// whole block: a bitonic network in shared memory (`buf`, kBlockRun entries).
+__device__ void block_bitonic_run(uint32_t* perm, uint32_t b, uint32_t L, uint32_t* buf) {
+    uint32_t P = 2u * kWarpRun;
+    while (P < L) P <<= 1;
+    for (uint32_t i = threadIdx.x; i < P; i += kThreads) buf[i] = i < L ? perm[b + i] : 0xFFFFFFFFu;
+    __syncthreads();
+    for (uint32_t k = 2u; k <= P; k <<= 1)
+        for (uint32_t j = k >> 1; j > 0u; j >>= 1) {
+            for (uint32_t i = threadIdx.x; i < P; i += kThreads) {
+                const uint32_t ixj = i ^ j;
+                if (ixj > i) {
+                    const uint32_t x = buf[i], y = buf[ixj];
+                    if ((x > y) == ((i & k) == 0u)) {
+                        buf[i] = y;
+                        buf[ixj] = x;
+                    }
+                }
+            }
+            __syncthreads();
+        }
+    for (uint32_t i = threadIdx.x; i < L; i += kThreads) perm[b + i] = buf[i];
+    __syncthreads();
+}
+
 // Sort each cell's run ascending, so the order inside a cell never depends
 // on the arrival order of the histogram's atomics: runs of at most kShortRun
-// by an insertion sort on their own thread, longer runs by the whole block
-// (block_sort_run, through the scratch `tmp`, free once the scatter has run).
+// by an insertion sort on their own thread, runs of at most kWarpRun by one
+// warp each (warp_sort_run; the block's warps share its runs), runs of at
+// most kBlockRun by the whole block in shared memory (block_bitonic_run), and
+// longer ones (cells that gather particles outside the box, which are
+// clamped into the edge cells) by the whole block through the scratch `tmp`,
+// free once the scatter has run (block_sort_run).
 // With `stats`, also the occupancy counters of the reference cells.
 __global__ void __launch_bounds__(kThreads) k_sort_runs(const uint32_t* __restrict__ start, uint32_t ncells,
                                                         uint32_t* __restrict__ perm, uint32_t* __restrict__ tmp,
                                                         const uint32_t* __restrict__ boundary_start, DevStats* stats,
                                                         Tables T) {
-    __shared__ uint32_t long_cells[kThreads];
-    __shared__ uint32_t nlong;
-    if (threadIdx.x == 0) nlong = 0;
+    __shared__ uint32_t long_cells[kThreads], mid_cells[kThreads];
+    __shared__ uint32_t nlong, nmid;
+    __shared__ uint32_t wbuf[kBlockRun];  // kThreads / 32 warp buffers of kWarpRun, or one block buffer
+    if (threadIdx.x == 0) nlong = nmid = 0;
     __syncthreads();
     const uint32_t c = blockIdx.x * blockDim.x + threadIdx.x;
     if (c <= ncells) {  // includes the non-finite bucket at index ncells
@@ -283,8 +342,10 @@ __global__ void __launch_bounds__(kThreads) k_sort_runs(const uint32_t* __restri
             if (occ > 0) atomicMax(&stats->max_cell_occupancy, occ);
             if (occ > kBucketSlots) atomicAdd(&stats->overflow_cells, 1u);
         }
-        if (len > kShortRun) {
+        if (len > kWarpRun) {
             long_cells[atomicAdd(&nlong, 1u)] = c;
+        } else if (len > kShortRun) {
+            mid_cells[atomicAdd(&nmid, 1u)] = c;
         } else if (len >= 2) {
             for (uint32_t i = b + 1; i < e; ++i) {
                 uint32_t v = perm[i];
@@ -298,10 +359,18 @@ __global__ void __launch_bounds__(kThreads) k_sort_runs(const uint32_t* __restri
         }
     }
     __syncthreads();
+    const uint32_t nm = nmid, warp = threadIdx.x >> 5;
+    for (uint32_t q = warp; q < nm; q += kThreads / 32) {
+        const uint32_t mc = mid_cells[q];
+        warp_sort_run(perm, start[mc], start[mc + 1] - start[mc], wbuf + warp * kWarpRun);
+    }
+    __syncthreads();  // the warps' buffers are the block buffer below
     const uint32_t cnt = nlong;
     for (uint32_t q = 0; q < cnt; ++q) {
         const uint32_t lc = long_cells[q];
-        block_sort_run(perm, tmp, start[lc], start[lc + 1]);
+        const uint32_t L = start[lc + 1] - start[lc];
+        if (L <= kBlockRun) block_bitonic_run(perm, start[lc], L, wbuf);
+        else block_sort_run(perm, tmp, start[lc], start[lc + 1]);
     }
 }
 
