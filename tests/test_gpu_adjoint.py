@@ -55,46 +55,25 @@ def gpu_gradients(sc, steps, every, loss, start=None):
     return L, g0, gs
 
 
-def translated(sc, start, loss, shift=0.0371):
-    """The same problem moved by `shift` along every axis of the scene (its
-    particles, boundary, box and loss target).  In exact arithmetic the
-    trajectory and the gradients are unchanged; in float32 every position is
-    rounded differently at every step, so the spread between the two GPU
-    gradients measures how far float rounding of the forward moves them."""
-    d = sc.dim
-    p = sc.particles.copy()
-    p["pos"][:, :d] += np.float32(shift)
-    b = sc.boundary.copy()
-    if len(b):
-        b["pos"][:, :d] += np.float32(shift)
-    bmin = tuple(float(sc.bounds_min[a]) + (shift if a < d else 0.0) for a in range(4))
-    moved = scenes.Scene(**{**sc.__dict__, "particles": p, "boundary": b, "bounds_min": bmin})
-    st = None
-    if start is not None:
-        st = start.copy()
-        st["pos"][:, :d] += np.float32(shift)
-    off = np.zeros(3)
-    off[:d] = shift
-    if loss[0] == "tip":
-        lo = ("tip", loss[1], np.asarray(loss[2], np.float64) + off)
-    else:
-        lo = ("points", loss[1] + off)
-    return moved, st, lo
+def retimed(sc, toward):
+    """The scene with its float32 time step moved by one ulp: every product
+    with dt, and so every rounding of the float32 trajectory, changes, while
+    the problem itself moves by 6e-8 relative.  The spread between the GPU
+    gradients of the two problems measures the FP32 noise of the gradient."""
+    dt = np.nextafter(np.float32(sc.dt), np.float32(toward))
+    return scenes.Scene(**{**sc.__dict__, "dt": float(dt)})
 
 
 def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4, eps_vel=1e-4, start=None):
-    """The GPU gradient along each direction, the same for the problem
-    translated in space (the FP32 noise of the gradient itself), and the FP64
-    oracle's central difference (L(p + e d) - L(p - e d)) / 2e along the same
+    """The GPU gradient along each direction, the same for the problem with
+    its time step one float32 ulp either way (the FP32 noise of the gradient
+    itself), and the FP64 oracle's central difference (L(p + e d) - L(p - e d)) / 2e along the same
     direction.  `loss` is ("tip", ids, target) or ("points", targets); `start`
     (particle records) replaces the scene's initial state after creation,
     keeping the scene's positions as the solids' reference configuration."""
     stiff = sc.meta.get("stiffness")
     L, g0, gs = gpu_gradients(sc, steps, every, loss, start)
-    spread = []
-    for shift in (0.0371, -0.0213):  # two re-roundings of the whole trajectory
-        moved, mstart, mloss = translated(sc, start, loss, shift)
-        spread.append(gpu_gradients(moved, steps, every, mloss, mstart)[1:])
+    spread = [gpu_gradients(retimed(sc, t), steps, every, loss, start)[1:] for t in (np.inf, -np.inf)]
     p0 = sc.particles if start is None else start
     v0 = p0["vel"][:, :3].astype(np.float64)
     x0 = None if start is None else start["pos"].astype(np.float64)
@@ -122,16 +101,17 @@ def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1
 def report(res, tol):
     """Per direction: the relative error |adj - fd| / |fd| against FP64 finite
     differences, and whether it is within `tol` or else within the FP32 noise
-    of the gradient itself.  The noise is measured: the problem translated in
-    space by two shifts gives the same gradient in exact arithmetic, but every
-    position of the float32 forward rounds differently at every step; with
-    sigma the RMS of those differences over all directions of a kind divided
-    by sqrt 2 (each difference holds two independent roundings), a direction
-    passes within 4 sigma.  The forward runs in float32, as the reference's
-    shaders do: where a derivative is small against the gradient's size
-    (random directions cancel) or is carried by small strains (float positions
-    of order 1 m resolve them to ~1e-7), that noise exceeds tol of the
-    derivative.  Returns the number of directions meeting neither bound."""
+    of the gradient itself.  The noise is measured: the time step moved by
+    one float32 ulp either way rounds every step of the float32 trajectory
+    differently while leaving the problem the same to 6e-8; with sigma the RMS
+    of the two gradients' differences from this one over all directions of a
+    kind divided by sqrt 2 (each difference holds two independent roundings),
+    a direction passes within 4 sigma.  The forward runs in float32, as the
+    reference's shaders do: where a derivative is small against the
+    gradient's size (random directions cancel) or is carried by small strains
+    (float positions of order 1 m resolve them to ~1e-7), that noise exceeds
+    tol of the derivative.  Returns the number of directions meeting neither
+    bound."""
     bad = 0
     for kind in ("stiffness", "velocity"):
         rows = [(a, f, sp) for k, a, f, sp in res if k == kind]
@@ -234,13 +214,14 @@ def test_friction_gradients_match_fp64_finite_differences():
             d[:, 2] = 0.0
             dv.append(d)
         L, res[mu] = fd_check(sc, 20, 5, ("points", target), [], dv)
-    assert report(res[5.0], 1e-4) == 0
+    bad = report(res[5.0], 1e-4)
     sig = [float(np.sqrt(np.mean([x * x for r in res[m] for x in r[3]]) / 2.0)) for m in (5.0, 0.0)]
     for (_, a1, f1, _), (_, a0, f0, _) in zip(res[5.0], res[0.0]):
         da, df = a1 - a0, f1 - f0
         err = abs(da - df) / abs(df)
         print(f"friction part: adjoint {da:.6e} fd64 {df:.6e} rel err {err:.2e}")
         assert err < 1e-2 or abs(da - df) <= 4.0 * (sig[0] + sig[1])
+    assert bad == 0
 
 
 @pytest.mark.parametrize("order", [0, 1, -2, 3])
