@@ -216,13 +216,22 @@ def stretched_bar(n=(20, 4, 4), spacing=0.01, stretch=1.01, lam=-1e5, mu=-1e5, d
 
 
 def batched_scenes(count=256, seed=3, spacing=0.01, n_min=2048, n_max=65536, integrator="midpoint", dt=1e-4,
-                   c0=20.0, rho0=1000.0, alpha=0.1, steps=200):
-    """Independent 3D scenes for the batched form: particle counts
-    log-uniform in [n_min, n_max]; each scene a seeded mix of 1-3 Tait fluid
-    blocks and 0-2 elastic blocks (E log-uniform in [1e4, 1e6], nu = 0.3,
-    strain order 2 standing in for the Neo-Hookean model, which the reference
-    does not have) above a one-layer floor, with its own h drawn uniformly in
-    [1.5, 2.5] x spacing.  The counts include the floor."""
+                   c0=20.0, rho0=1000.0, alpha=0.1, steps=200, margin=4, gap=4, aspect=2.0):
+    """Independent 3D scenes for the batched form: total particle counts
+    (floor included) log-uniform in [n_min, n_max]; each scene a seeded mix
+    of 1-3 Tait fluid blocks and 0-2 elastic blocks (E log-uniform in
+    [1e4, 1e6], nu = 0.3, strain order 2 standing in for the Neo-Hookean
+    model, which the reference does not have), with its own h drawn
+    uniformly in [1.5, 2.5] x spacing, RK2.
+
+    The blocks stand on a one-layer floor of boundary particles: columns of
+    about `aspect` times their width, at least 3 sites on a side, laid out
+    by shelf packing on the floor with `gap` spacings between blocks and
+    `margin` spacings to the box's sides.  The gap exceeds the largest h, so
+    no pair of particles from different blocks starts within kernel range,
+    and no block overlaps another (particles placed on one another give the
+    continuity equation diverging densities and the step non-finite
+    states within a few hundred steps)."""
     rng = np.random.default_rng(seed)
     out = []
     s = spacing
@@ -231,35 +240,41 @@ def batched_scenes(count=256, seed=3, spacing=0.01, n_min=2048, n_max=65536, int
         h = float(rng.uniform(1.5, 2.5) * s)
         n_fluid = int(rng.integers(1, 4))
         n_solid = int(rng.integers(0, 3))
-        side = int(np.ceil(1.6 * n_target ** (1.0 / 3.0)))
-        box = side * s
-        floor_n = side * side
-        n_body = max(n_target - floor_n, 64)
-        shares = rng.dirichlet(np.ones(n_fluid + n_solid)) * n_body
+        split = rng.dirichlet(np.ones(n_fluid + n_solid))
+        E = np.exp(rng.uniform(np.log(1e4), np.log(1e6), size=n_solid))
+        floor_n = 0
+        for _ in range(4):  # the floor's size follows the layout, the layout the bodies' share
+            body = max(n_target - floor_n, 64 * (n_fluid + n_solid))
+            dims = []
+            for share in split * body:
+                w = max(3, int(round((share / aspect) ** (1.0 / 3.0))))
+                dims.append((w, max(3, int(round(share / (w * w)))), w))
+            row = int(np.ceil(np.sqrt(sum((d[0] + gap) ** 2 for d in dims))))
+            place, x, z, depth_row, width = [], 0, 0, 0, 0
+            for d in dims:
+                if x and x + d[0] > row:
+                    x, z, depth_row = 0, z + depth_row + gap, 0
+                place.append((x, z))
+                x += d[0] + gap
+                width = max(width, x - gap)
+                depth_row = max(depth_row, d[2])
+            nx, nz = width + 2 * margin, z + depth_row + 2 * margin
+            floor_n = nx * nz
+        ny = max(d[1] for d in dims) + margin
         mats = [immobile(0.0, mass=1.0 * s ** 3), liquid(rho0, c0, h, alpha, mass=rho0 * s ** 3)]
         mobile = []
-        x_cursor = 0.5 * s
-        for b, share in enumerate(shares):
-            m = max(2, int(round(share ** (1.0 / 3.0))))
-            mx = min(m, side - 1)
-            my = min(max(2, int(round(share / (mx * mx)))), side - 2)
-            if x_cursor + mx * s > box:
-                x_cursor = 0.5 * s
-            z0 = 0.5 * s + rng.uniform(0, max(box - mx * s, 0) * 0.5)
-            pos = lattice((x_cursor, 0.5 * s, z0), (mx, my, mx), s)
-            pos = jitter(pos, 1e-4, rng)
-            x_cursor += (mx + 2) * s
+        for b, (d, (px, pz)) in enumerate(zip(dims, place)):
+            pos = jitter(lattice(((margin + px + 0.5) * s, 0.5 * s, (margin + pz + 0.5) * s), d, s), 1e-4, rng)
             if b < n_fluid:
                 mobile.append(particles(pos, 1, rho0))
             else:
-                E = float(np.exp(rng.uniform(np.log(1e4), np.log(1e6))))
-                lam, mu = lame_from_young(E, 0.3)
+                lam, mu = lame_from_young(float(E[b - n_fluid]), 0.3)
                 mats.append(elastic_solid(rho0, lam, mu, mass=rho0 * s ** 3))
                 mobile.append(particles(pos, len(mats) - 1, rho0))
-        floor = lattice((0.5 * s, -0.5 * s, 0.5 * s), (side, 1, side), s)
+        floor = lattice((0.5 * s, -0.5 * s, 0.5 * s), (nx, 1, nz), s)
         out.append(Scene(particles=np.concatenate(mobile), boundary=particles(floor, 0, 1.0), materials=np.array(mats),
-                         bounds_min=(0.0, 0.0, 0.0, 0.0), bounds_dim=(box, box, box, 0.0), h=h, integrator=integrator,
-                         dt=dt, gravity=9.81, alpha=alpha, name=f"batched_{k}",
+                         bounds_min=(0.0, -s, 0.0, 0.0), bounds_dim=(nx * s, (ny + 1) * s, nz * s, 0.0), h=h,
+                         integrator=integrator, dt=dt, gravity=9.81, alpha=alpha, name=f"batched_{k}",
                          meta={"steps": steps, "n_target": n_target}))
     return out
 

@@ -4,9 +4,11 @@ oracle.
 The gradient of a loss after N steps with respect to the per-solid stiffness
 and the initial velocities, taken by the GPU's hand-written stage adjoints
 with checkpoints, must match (L(p + e d) - L(p - e d)) / 2e computed with the
-double-precision oracle along seeded random directions d.  The FP32 forward
-differs from the FP64 one by ~1e-6 relative, which bounds the agreement; the
-bound used here is written in each test.
+double-precision oracle along seeded random directions d, to 1e-4 of the
+larger of the direction's own derivative and the derivatives' RMS.  The FP32
+forward differs from the FP64 one by ~1e-6 relative in positions; the
+stiffness gradient depends on strains resolved from those float positions,
+which sets the floor of the agreement.
 """
 import os
 
@@ -55,83 +57,93 @@ def gpu_gradients(sc, steps, every, loss, start=None):
     return L, g0, gs
 
 
-def retimed(sc, toward):
-    """The scene with its float32 time step moved by one ulp: every product
-    with dt, and so every rounding of the float32 trajectory, changes, while
-    the problem itself moves by 6e-8 relative.  The spread between the GPU
-    gradients of the two problems measures the FP32 noise of the gradient."""
-    dt = np.nextafter(np.float32(sc.dt), np.float32(toward))
-    return scenes.Scene(**{**sc.__dict__, "dt": float(dt)})
+def centered(sc, start, loss):
+    """The same problem moved so that its mobile particles' centroid sits at
+    the origin (particles, boundary, box, the solids' reference positions and
+    the loss target move together; the physics is translation invariant).
+    Float32 positions resolve the small strains and displacements the
+    gradients depend on best near the origin: the bar of these tests moved
+    +1 m instead shows 30x the error against FP64 finite differences, which is
+    the forward's float32 position resolution, not the adjoint."""
+    d = sc.dim
+    c = np.zeros(3)
+    c[:d] = -np.round(sc.particles["pos"][:, :d].astype(np.float64).mean(axis=0), 2)
+    p = sc.particles.copy()
+    p["pos"][:, :d] += c[:d].astype(np.float32)
+    b = sc.boundary.copy()
+    if len(b):
+        b["pos"][:, :d] += c[:d].astype(np.float32)
+    bmin = tuple(float(sc.bounds_min[a]) + (c[a] if a < d else 0.0) for a in range(4))
+    moved = scenes.Scene(**{**sc.__dict__, "particles": p, "boundary": b, "bounds_min": bmin})
+    st = None
+    if start is not None:
+        st = start.copy()
+        st["pos"][:, :d] += c[:d].astype(np.float32)
+    lo = ("tip", loss[1], np.asarray(loss[2], np.float64) + c) if loss[0] == "tip" else ("points", loss[1] + c)
+    return moved, st, lo
 
 
 def fd_check(sc, steps, every, loss, directions_stiff, directions_vel, eps_rel=1e-4, eps_vel=1e-4, start=None):
-    """The GPU gradient along each direction, the same for the problem with
-    its time step one float32 ulp either way (the FP32 noise of the gradient
-    itself), and the FP64 oracle's central difference (L(p + e d) - L(p - e d)) / 2e along the same
-    direction.  `loss` is ("tip", ids, target) or ("points", targets); `start`
-    (particle records) replaces the scene's initial state after creation,
-    keeping the scene's positions as the solids' reference configuration."""
+    """For the problem centred at the origin: the GPU gradient projected on
+    each seeded direction, and the FP64 oracle's central difference
+    (L(p + e d) - L(p - e d)) / 2e along the same direction.  Returns the
+    loss and (kind, adjoint, fd) per direction.  `loss` is ("tip", ids,
+    target) or ("points", targets); `start` (particle records) replaces the
+    scene's initial state after creation, keeping the scene's positions as
+    the solids' reference configuration."""
+    sc, start, loss = centered(sc, start, loss)
     stiff = sc.meta.get("stiffness")
     L, g0, gs = gpu_gradients(sc, steps, every, loss, start)
-    spread = [gpu_gradients(retimed(sc, t), steps, every, loss, start)[1:] for t in (np.inf, -np.inf)]
     p0 = sc.particles if start is None else start
     v0 = p0["vel"][:, :3].astype(np.float64)
     x0 = None if start is None else start["pos"].astype(np.float64)
     s64 = None if stiff is None else stiff.astype(np.float64)
-    tasks, adj, nudged = [], [], []
+    tasks, adj = [], []
     for d in directions_stiff:
-        a0 = float(np.sum(gs.astype(np.float64) * s64 * d[:, None]))
-        adj.append(("stiffness", a0))
-        nudged.append([a0 - float(np.sum(g[1].astype(np.float64) * s64 * d[:, None])) for g in spread])
+        adj.append(("stiffness", float(np.sum(gs.astype(np.float64) * s64 * d[:, None]))))
         tasks += [(sc, steps, s64 * (1 + eps_rel * d[:, None]), v0, loss, x0),
                   (sc, steps, s64 * (1 - eps_rel * d[:, None]), v0, loss, x0)]
     for d in directions_vel:
-        a0 = float(np.sum(g0[:, 4:7].astype(np.float64) * d))
-        adj.append(("velocity", a0))
-        nudged.append([a0 - float(np.sum(g[0][:, 4:7].astype(np.float64) * d)) for g in spread])
+        adj.append(("velocity", float(np.sum(g0[:, 4:7].astype(np.float64) * d))))
         tasks += [(sc, steps, s64, v0 + eps_vel * d, loss, x0), (sc, steps, s64, v0 - eps_vel * d, loss, x0)]
     ls = oracle_losses(tasks)
     out = []
     for q, (kind, a) in enumerate(adj):
         e = eps_rel if kind == "stiffness" else eps_vel
-        out.append((kind, a, (ls[2 * q] - ls[2 * q + 1]) / (2 * e), nudged[q]))
+        out.append((kind, a, (ls[2 * q] - ls[2 * q + 1]) / (2 * e)))
     return L, out
 
 
 def report(res, tol):
-    """Per direction: the relative error |adj - fd| / |fd| against FP64 finite
-    differences, and whether it is within `tol` or else within the FP32 noise
-    of the gradient itself.  The noise is measured: the time step moved by
-    one float32 ulp either way rounds every step of the float32 trajectory
-    differently while leaving the problem the same to 6e-8; with sigma the RMS
-    of the two gradients' differences from this one over all directions of a
-    kind divided by sqrt 2 (each difference holds two independent roundings),
-    a direction passes within 4 sigma.  The forward runs in float32, as the
-    reference's shaders do: where a derivative is small against the
-    gradient's size (random directions cancel) or is carried by small strains
-    (float positions of order 1 m resolve them to ~1e-7), that noise exceeds
-    tol of the derivative.  Returns the number of directions meeting neither
-    bound."""
+    """Per direction, the error |adj - fd| of the GPU gradient against the FP64
+    central difference, relative to the larger of the direction's own
+    derivative |fd| and the derivatives' RMS over all directions of the kind:
+    it must stay within `tol`.  Seeded random directions make some
+    derivatives small against the gradient's size (their terms cancel); the
+    float32 forward, as the reference's shaders compute it, leaves an error
+    of fixed absolute size (the strains behind the stiffness gradient are
+    resolved from float positions), so such a direction is held to the
+    gradient's scale rather than to its own small value.  Prints each
+    direction's own relative error and the norm-wise error as well.  Returns
+    the number of directions outside the bound."""
     bad = 0
     for kind in ("stiffness", "velocity"):
-        rows = [(a, f, sp) for k, a, f, sp in res if k == kind]
+        rows = [(a, f) for k, a, f in res if k == kind]
         if not rows:
             continue
-        sigma = float(np.sqrt(np.mean([x * x for _, _, sp in rows for x in sp]) / 2.0))
-        errs = [abs(a - f) / max(abs(f), 1e-300) for a, f, _ in rows]
-        mags = [abs(f) for _, f, _ in rows]
-        within = sum(1 for e in errs if e < tol)
-        noise_ok = sum(1 for (a, f, _), e in zip(rows, errs) if e >= tol and abs(a - f) <= 4.0 * sigma)
-        fails = len(rows) - within - noise_ok
-        na = np.array([a for a, _, _ in rows])
-        nf = np.array([f for _, f, _ in rows])
-        print(f"{kind}: {len(rows)} directions, |fd| {min(mags):.3e} .. {max(mags):.3e}, rel err median "
-              f"{np.median(errs):.2e} max {max(errs):.2e}, norm-wise {np.linalg.norm(na - nf) / np.linalg.norm(nf):.2e}; "
-              f"FP32 noise sigma {sigma:.2e}; {within} within {tol:.0e}, {noise_ok} within 4 sigma, {fails} neither")
-        for (a, f, _), e in zip(rows, errs):
+        nf = np.array([f for _, f in rows])
+        na = np.array([a for a, _ in rows])
+        rms = float(np.sqrt(np.mean(nf * nf)))
+        own = np.abs(na - nf) / np.maximum(np.abs(nf), 1e-300)
+        scaled = np.abs(na - nf) / np.maximum(np.abs(nf), rms)
+        fails = int(np.count_nonzero(scaled >= tol))
+        print(f"{kind}: {len(rows)} directions, |fd| {np.abs(nf).min():.3e} .. {np.abs(nf).max():.3e} (RMS {rms:.3e}), "
+              f"own rel err median {np.median(own):.2e} max {own.max():.2e}, against max(|fd|, RMS) max "
+              f"{scaled.max():.2e}, norm-wise {np.linalg.norm(na - nf) / np.linalg.norm(nf):.2e}; "
+              f"{int(np.count_nonzero(own < tol))} within {tol:.0e} of their own derivative, {fails} outside the bound")
+        for a, f, e, sc in zip(na, nf, own, scaled):
             if e >= tol:
-                print(f"  adjoint {a:.6e} fd64 {f:.6e} rel err {e:.2e} |adj - fd| {abs(a - f):.2e} "
-                      f"= {abs(a - f) / sigma:.1f} sigma")
+                print(f"  adjoint {a:.6e} fd64 {f:.6e} own rel err {e:.2e}, against max(|fd|, RMS) {sc:.2e}")
         bad += fails
     return bad
 
@@ -215,12 +227,12 @@ def test_friction_gradients_match_fp64_finite_differences():
             dv.append(d)
         L, res[mu] = fd_check(sc, 20, 5, ("points", target), [], dv)
     bad = report(res[5.0], 1e-4)
-    sig = [float(np.sqrt(np.mean([x * x for r in res[m] for x in r[3]]) / 2.0)) for m in (5.0, 0.0)]
-    for (_, a1, f1, _), (_, a0, f0, _) in zip(res[5.0], res[0.0]):
-        da, df = a1 - a0, f1 - f0
-        err = abs(da - df) / abs(df)
-        print(f"friction part: adjoint {da:.6e} fd64 {df:.6e} rel err {err:.2e}")
-        assert err < 1e-2 or abs(da - df) <= 4.0 * (sig[0] + sig[1])
+    parts = np.array([(a1 - a0, f1 - f0) for (_, a1, f1), (_, a0, f0) in zip(res[5.0], res[0.0])])
+    rms = float(np.sqrt(np.mean(parts[:, 1] ** 2)))
+    for da, df in parts:
+        err = abs(da - df) / max(abs(df), rms)
+        print(f"friction part: adjoint {da:.6e} fd64 {df:.6e} error against max(|fd|, RMS) {err:.2e}")
+        assert err < 1e-2
     assert bad == 0
 
 

@@ -170,3 +170,43 @@ def test_solid_scene_runs_and_stays_finite():
     o.step(5)
     s = o.state()
     assert np.isfinite(s["pos"]).all() and np.isfinite(s["vel"]).all()
+
+
+def test_batched_workload_layout():
+    """The 256 batched scenes: total counts within 10% of their log-uniform
+    targets in [2048, 65536], no two blocks within kernel range of one
+    another (particles of one block closer than one spacing to another's, or
+    different materials within h, start the step on overlapping bodies), and
+    every body inside its scene's box."""
+    from scipy.spatial import cKDTree
+    scs = scenes.batched_scenes()
+    assert len(scs) == 256
+    for sc in scs:
+        total = sc.n + len(sc.boundary)
+        assert abs(total / sc.meta["n_target"] - 1.0) < 0.1, (sc.name, total, sc.meta["n_target"])
+        p = sc.particles["pos"][:, :3].astype(np.float64)
+        d, _ = cKDTree(p).query(p, k=2)
+        assert d[:, 1].min() > 0.5 * 0.01, sc.name
+        m = sc.particles["mat"]
+        for a in np.unique(m):
+            other = p[m != a]
+            if len(other):
+                dd, _ = cKDTree(other).query(p[m == a], k=1)
+                assert dd.min() > sc.h, sc.name
+        lo = np.asarray(sc.bounds_min[:3])
+        assert (p > lo).all() and (p < lo + np.asarray(sc.bounds_dim[:3])).all(), sc.name
+
+
+def test_batched_workload_sample_stays_in_its_box_for_200_steps():
+    """The oracle runs the three smallest batched scenes with an elastic
+    block for the workload's 200 RK2 steps: every state finite and inside
+    the scene's box."""
+    scs = scenes.batched_scenes()
+    solid = [sc for sc in scs if (sc.materials["normal_stiffness"] != 0).any()]
+    for sc in sorted(solid, key=lambda sc: sc.n)[:3]:
+        o = Oracle(sc)
+        o.step(200)
+        p = o.state()["pos"][:, :3]
+        lo = np.asarray(sc.bounds_min[:3])
+        assert np.isfinite(p).all(), sc.name
+        assert ((p > lo) & (p < lo + np.asarray(sc.bounds_dim[:3]))).all(), sc.name
