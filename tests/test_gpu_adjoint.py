@@ -315,14 +315,26 @@ def test_batched_gradients_equal_per_scene_gradients():
 @pytest.mark.slow
 @pytest.mark.skipif(not os.environ.get("ARP_SLOW_TESTS"), reason="full-size FP64 differences: set ARP_SLOW_TESTS=1")
 def test_differentiation_workload_full_size_gradients_match_fp64_finite_differences():
-    """The differentiation workload at its full size (16 x 16 x 256 bar, 65,024
-    elastic particles, seeded initial velocities) over 20 RK2 steps (a
-    reduced-step horizon: each FP64 oracle run of the full 400 steps takes
-    minutes on one core), 4 seeded directions each for the per-particle
-    stiffness and the initial velocities, within 1e-4."""
+    """The differentiation workload as benchmarked (16 x 16 x 256 bar, 65,024
+    elastic particles, seeded initial velocities, 400 RK2 steps, checkpoints
+    every 20), 4 seeded directions each for the per-particle stiffness and
+    the initial velocities.  Sixteen FP64 oracle runs of the full 400 steps
+    take about 20 minutes of host time, hence the marker; the 32-direction
+    checks at 1e-4 run on the reduced bar above.
+
+    Measured on a B200: norm-wise 9.5e-5 (stiffness) and 6.9e-5 (velocity);
+    per direction against max(|fd|, RMS) at most 9.7e-5 and 1.01e-4.  The
+    agreement sits at the float32 forward's own resolution here: the bar is
+    2.56 m tall, so even centred its tip positions are resolved to 1.2e-7 m,
+    1e-4 of the few millimetres the tip moves in 400 steps.  The bound
+    asserted is 1e-4 norm-wise and 1.5e-4 per direction."""
     sc = scenes.cantilever_bar(v_sigma=0.05)
     rng = np.random.default_rng(404)
     ds = [rng.normal(size=sc.n) for _ in range(4)]
     dv = [rng.normal(size=(sc.n, 3)) for _ in range(4)]
-    L, res = fd_check(sc, 20, 20, ("tip", sc.meta["tip"], sc.meta["target"]), ds, dv)
-    assert report(res, 1e-4) == 0
+    L, res = fd_check(sc, 400, 20, ("tip", sc.meta["tip"], sc.meta["target"]), ds, dv)
+    assert report(res, 1.5e-4) == 0
+    for kind in ("stiffness", "velocity"):
+        a = np.array([x for k, x, _ in res if k == kind])
+        f = np.array([x for k, _, x in res if k == kind])
+        assert np.linalg.norm(a - f) / np.linalg.norm(f) < 1e-4, kind
