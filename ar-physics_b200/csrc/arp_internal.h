@@ -274,9 +274,8 @@ struct FluidVariant {
     int flush;       // warp-voted list flushes (kFlush) instead of pass 1 then pass 2
     int staged;      // candidates staged in shared memory per tile before the scan
                      // (1: cooperative loads, 2: bulk copies on an mbarrier)
-    int pipe;        // pass 2 loads the next hit's records before evaluating the current one
 };
-constexpr int kNumFluidVariants = 17;
+constexpr int kNumFluidVariants = 13;
 extern const FluidVariant kFluidVariants[kNumFluidVariants];
 // `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,

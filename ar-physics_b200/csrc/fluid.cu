@@ -304,41 +304,7 @@ enum FluidMode {
                    // kDirect (second overflow queue)
     kDirect = 2,   // every hit evaluated during the scan (a row above even the
                    // second queue's list)
-    kTwoPassPipe = 3,  // kTwoPass with pass 2 software-pipelined: the records
-                       // of hit e + 1 are loaded before hit e is evaluated
-    kFlushPipe = 4,    // kFlush with the same pipelined list evaluation
 };
-__host__ __device__ constexpr bool is_flush(int mode) { return mode == kFlush || mode == kFlushPipe; }
-__host__ __device__ constexpr bool is_pipe(int mode) { return mode == kTwoPassPipe || mode == kFlushPipe; }
-
-// The neighbor records one hit reads (position and density, velocity and
-// material, p / rho^2), from the mobile or the boundary arrays.
-struct HitRec {
-    float4 x, v;
-    float pt;
-};
-__device__ __forceinline__ HitRec load_hit(uint32_t j, const FluidArgs& a) {
-    const bool bnd = (j & kBoundaryBit) != 0u;
-    const uint32_t jj = j & ~kBoundaryBit;
-    const float4* X = bnd ? a.bxs : a.xs;
-    const float4* V = bnd ? a.bvs : a.vs;
-    const float* PT = bnd ? a.bps : a.ps;
-    return HitRec{X[jj], V[jj], PT[jj]};
-}
-// eval_hit on records already loaded.
-template <int DIM>
-__device__ __forceinline__ void eval_rec(uint32_t j, const HitRec& h, const Self& s, const FluidArgs& a,
-                                         const PairK& K, Acc& acc) {
-    const uint32_t mat2 = __float_as_uint(h.v.w);
-    if (j & kBoundaryBit) {
-        bool elastic2 = false;
-        if (a.any_stiff_immobile && s.mt[mat2].stiff)
-            elastic2 = a.sid_of_boundary_index[a.borig[j & ~kBoundaryBit]] != kInvalid;
-        pair<DIM, true>(s, h.x, h.v, h.pt, mat2, elastic2, K, acc);
-    } else {
-        pair<DIM, false>(s, h.x, h.v, h.pt, mat2, s.mt[mat2].stiff != 0u, K, acc);
-    }
-}
 
 // Fluid forces and the stage update of sorted particle k.  `lst` is the
 // thread's column of the hit list ([CAP][BLOCK]); `sm`/`si` hold the
@@ -377,7 +343,6 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
         return r2 < K.h2;
     };
     constexpr bool DIRECT = MODE == kDirect;
-    constexpr bool TWO = MODE == kTwoPass || MODE == kTwoPassPipe;
     auto take = [&](uint32_t j) {
         if (DIRECT) {
             if (j != k) eval_hit<DIM>(j, s, a, K, acc);
@@ -389,27 +354,13 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
     };
     // pass 2 over the hits collected so far, in candidate order
     auto flush = [&]() {
-        if constexpr (is_pipe(MODE)) {
-            if (cnt) {
-                uint32_t j = my[0];
-                HitRec h = load_hit(j, a);
-                for (uint32_t e = 1; e <= cnt; ++e) {
-                    const uint32_t jn = my[min(e, cnt - 1u) * BLOCK];
-                    const HitRec hn = load_hit(jn, a);
-                    if (j != k) eval_rec<DIM>(j, h, s, a, K, acc);
-                    j = jn;
-                    h = hn;
-                }
-            }
-        } else {
-            for (uint32_t e = 0; e < cnt; ++e) {
-                const uint32_t j = my[e * BLOCK];
-                if (j != k) eval_hit<DIM>(j, s, a, K, acc);
-            }
+        for (uint32_t e = 0; e < cnt; ++e) {
+            const uint32_t j = my[e * BLOCK];
+            if (j != k) eval_hit<DIM>(j, s, a, K, acc);
         }
         cnt = 0;
     };
-    if (is_flush(MODE)) {
+    if (MODE == kFlush) {
         // The search rows (x-rows of the search cells within reach, see
         // for_search_rows) in a fixed order and number for every lane, rows
         // outside the grid (and every row of a non-finite particle) empty, so
@@ -472,7 +423,7 @@ __device__ __forceinline__ bool fluid_particle(uint32_t k, const FluidArgs& a, c
             for (; j < je; ++j)
                 if (hit(a.xs[j])) take(j);
         });
-        if (TWO) {
+        if (MODE == kTwoPass) {
             if (full) {
                 a.overflow[atomicAdd(a.overflow_count, 1u)] = k;
                 return true;
@@ -506,7 +457,7 @@ __device__ __forceinline__ void fluid_tile(const FluidArgs& a, const Tables& T, 
     load_scene_tables(T, scene0, sm, si);
     __syncthreads();
     const uint32_t k = k0 + threadIdx.x;
-    const unsigned wmask = is_flush(MODE) ? __ballot_sync(0xFFFFFFFFu, k < a.n) : 0u;  // lanes with a particle
+    const unsigned wmask = MODE == kFlush ? __ballot_sync(0xFFFFFFFFu, k < a.n) : 0u;  // lanes with a particle
     if (k < a.n) fluid_particle<DIM, BLOCK, CAP, MODE>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, wmask);
 }
 
@@ -537,7 +488,7 @@ __device__ __forceinline__ void fluid_tiles_persistent(const FluidArgs& a, const
         }
         __syncthreads();
         const uint32_t k = k0 + threadIdx.x;
-        const unsigned wmask = is_flush(MODE) ? __ballot_sync(0xFFFFFFFFu, k < a.n) : 0u;  // lanes with a particle
+        const unsigned wmask = MODE == kFlush ? __ballot_sync(0xFFFFFFFFu, k < a.n) : 0u;  // lanes with a particle
         if (k < a.n) fluid_particle<DIM, BLOCK, CAP, MODE>(k, a, T, c, b, lst + threadIdx.x, sm, si, scene0, wmask);
         __syncthreads();
     }
@@ -546,24 +497,6 @@ __device__ __forceinline__ void fluid_tiles_persistent(const FluidArgs& a, const
 template <int DIM, int BLOCK, int CAP>
 __global__ void __launch_bounds__(BLOCK) k_fluid(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
     fluid_tile<DIM, BLOCK, CAP, kTwoPass>(a, T, c, b);
-}
-template <int DIM, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK) k_fluid_pipe(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
-    fluid_tile<DIM, BLOCK, CAP, kTwoPassPipe>(a, T, c, b);
-}
-template <int DIM, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK) k_fluid_pipe_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
-                                                                 uint32_t* tile_counter) {
-    fluid_tiles_persistent<DIM, BLOCK, CAP, kTwoPassPipe>(a, T, c, b, tile_counter);
-}
-template <int DIM, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK) k_fluid_flush_pipe(FluidArgs a, Tables T, StageCoefs c, StageBuffers b) {
-    fluid_tile<DIM, BLOCK, CAP, kFlushPipe>(a, T, c, b);
-}
-template <int DIM, int BLOCK, int CAP>
-__global__ void __launch_bounds__(BLOCK) k_fluid_flush_pipe_persistent(FluidArgs a, Tables T, StageCoefs c,
-                                                                       StageBuffers b, uint32_t* tile_counter) {
-    fluid_tiles_persistent<DIM, BLOCK, CAP, kFlushPipe>(a, T, c, b, tile_counter);
 }
 template <int DIM, int BLOCK, int CAP>
 __global__ void __launch_bounds__(BLOCK) k_fluid_persistent(FluidArgs a, Tables T, StageCoefs c, StageBuffers b,
@@ -586,14 +519,10 @@ template <int DIM, int BLOCK, int CAP, int MODE>
 struct FluidKernels {
     static constexpr auto tile_kernel() {
         if constexpr (MODE == kFlush) return k_fluid_flush<DIM, BLOCK, CAP>;
-        else if constexpr (MODE == kTwoPassPipe) return k_fluid_pipe<DIM, BLOCK, CAP>;
-        else if constexpr (MODE == kFlushPipe) return k_fluid_flush_pipe<DIM, BLOCK, CAP>;
         else return k_fluid<DIM, BLOCK, CAP>;
     }
     static constexpr auto persistent_kernel() {
         if constexpr (MODE == kFlush) return k_fluid_flush_persistent<DIM, BLOCK, CAP>;
-        else if constexpr (MODE == kTwoPassPipe) return k_fluid_pipe_persistent<DIM, BLOCK, CAP>;
-        else if constexpr (MODE == kFlushPipe) return k_fluid_flush_pipe_persistent<DIM, BLOCK, CAP>;
         else return k_fluid_persistent<DIM, BLOCK, CAP>;
     }
     static constexpr auto tile = tile_kernel();
@@ -1002,11 +931,10 @@ int verlet_kick4(const float4* e, const float4* k4, uint32_t count, float half, 
 }
 
 const FluidVariant kFluidVariants[kNumFluidVariants] = {
-    {128, 48, 0, 0, 0, 0}, {256, 48, 0, 0, 0, 0}, {128, 48, 1, 0, 0, 0}, {256, 48, 1, 0, 0, 0},
-    {128, 96, 0, 0, 0, 0}, {256, 96, 0, 0, 0, 0}, {128, 96, 1, 0, 0, 0}, {256, 96, 1, 0, 0, 0},
-    {128, 48, 0, 1, 0, 0}, {128, 48, 1, 1, 0, 0},
-    {128, 48, 0, 0, 1, 0}, {64, 48, 0, 0, 1, 0}, {128, 48, 0, 0, 2, 0},
-    {128, 48, 0, 0, 0, 1}, {128, 48, 1, 0, 0, 1}, {128, 48, 0, 1, 0, 1}, {128, 48, 1, 1, 0, 1},
+    {128, 48, 0, 0, 0}, {256, 48, 0, 0, 0}, {128, 48, 1, 0, 0}, {256, 48, 1, 0, 0},
+    {128, 96, 0, 0, 0}, {256, 96, 0, 0, 0}, {128, 96, 1, 0, 0}, {256, 96, 1, 0, 0},
+    {128, 48, 0, 1, 0}, {128, 48, 1, 1, 0},
+    {128, 48, 0, 0, 1}, {64, 48, 0, 0, 1}, {128, 48, 0, 0, 2},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -1026,18 +954,14 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
         if (kdim == 2 && v.block == 128) return launch_staged<2, 128, 48, true>(a, T, c, b, st);
         return 0;
     }
-    const int mode = v.flush ? (v.pipe ? kFlushPipe : kFlush) : (v.pipe ? kTwoPassPipe : kTwoPass);
 #define ARP_FLUID(D, B, C, M)                                               \
-    if (kdim == D && v.block == B && v.cap == C && mode == M && !v.staged) {  \
+    if (kdim == D && v.block == B && v.cap == C && v.flush == M && !v.staged) {  \
         launch_variant<D, B, C, M>(a, T, c, b, pers, tile_counter, st);     \
         return 3; /* the tile kernel and the two overflow kernels */       \
     }
-    ARP_FLUID(3, 128, 48, kTwoPass) ARP_FLUID(3, 256, 48, kTwoPass) ARP_FLUID(3, 128, 96, kTwoPass)
-    ARP_FLUID(3, 256, 96, kTwoPass) ARP_FLUID(2, 128, 48, kTwoPass) ARP_FLUID(2, 256, 48, kTwoPass)
-    ARP_FLUID(2, 128, 96, kTwoPass) ARP_FLUID(2, 256, 96, kTwoPass)
-    ARP_FLUID(3, 128, 48, kFlush) ARP_FLUID(2, 128, 48, kFlush)
-    ARP_FLUID(3, 128, 48, kTwoPassPipe) ARP_FLUID(2, 128, 48, kTwoPassPipe)
-    ARP_FLUID(3, 128, 48, kFlushPipe) ARP_FLUID(2, 128, 48, kFlushPipe)
+    ARP_FLUID(3, 128, 48, 0) ARP_FLUID(3, 256, 48, 0) ARP_FLUID(3, 128, 96, 0) ARP_FLUID(3, 256, 96, 0)
+    ARP_FLUID(2, 128, 48, 0) ARP_FLUID(2, 256, 48, 0) ARP_FLUID(2, 128, 96, 0) ARP_FLUID(2, 256, 96, 0)
+    ARP_FLUID(3, 128, 48, 1) ARP_FLUID(2, 128, 48, 1)
 #undef ARP_FLUID
     return 0;
 }
