@@ -173,6 +173,8 @@ def load_library():
         "arp_sim_get_materials": [c_sim, ctypes.c_void_p, ctypes.c_uint32],
         "arp_sim_get_interactions": [c_sim, ctypes.c_void_p, ctypes.c_uint32],
         "arp_sim_set_particles": [c_sim, ctypes.c_void_p, ctypes.c_uint32],
+        "arp_sim_set_particles_async": [c_sim, ctypes.c_void_p, ctypes.c_uint32],
+        "arp_sim_get_particles_async": [c_sim, ctypes.c_void_p, ctypes.c_uint32],
         "arp_sim_device_state": [c_sim, ctypes.POINTER(ArpDeviceView)],
         "arp_sim_add_particles": [c_sim, ctypes.c_void_p, ctypes.c_uint32, ctypes.c_void_p, ctypes.c_void_p,
                                   ctypes.POINTER(ctypes.c_int)],

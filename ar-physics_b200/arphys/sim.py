@@ -145,6 +145,22 @@ class FluidSim:
         p = np.ascontiguousarray(p, dtype=PARTICLE_DTYPE)
         check(self._L.arp_sim_set_particles(self._h, ptr(p), len(p)))
 
+    def set_particles_async(self, p):
+        """arp_sim_set_particles_async: `p` (a contiguous Particle record
+        array, page-locked for a truly asynchronous copy) must stay unchanged
+        until synchronize()."""
+        if p.dtype != PARTICLE_DTYPE or not p.flags["C_CONTIGUOUS"]:
+            raise ValueError("set_particles_async needs a contiguous Particle record array")
+        check(self._L.arp_sim_set_particles_async(self._h, ptr(p), len(p)))
+
+    def particles_async(self, out):
+        """arp_sim_get_particles_async: `out` (a contiguous Particle record
+        array) holds the records after synchronize()."""
+        if out.dtype != PARTICLE_DTYPE or not out.flags["C_CONTIGUOUS"]:
+            raise ValueError("particles_async needs a contiguous Particle record array")
+        check(self._L.arp_sim_get_particles_async(self._h, ptr(out), len(out)))
+        return out
+
     def add_particles(self, p, material, offset=None):
         """FluidSim::add_particles (mod.rs:180-206); returns True when a
         material entry was appended."""
@@ -205,6 +221,8 @@ class FluidSim:
         check(self._L.arp_sim_set_stream(self._h, ctypes.c_void_p(stream_handle)))
 
     def synchronize(self):
+        """Waits for the handle's device work and asynchronous copies and
+        raises the record-check errors of asynchronous sets."""
         check(self._L.arp_sim_synchronize(self._h))
 
     def profile_enable(self, on=True, every=1):

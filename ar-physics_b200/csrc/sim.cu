@@ -338,8 +338,38 @@ struct arp_sim {
     double acc_ms[3] = {0, 0, 0};  // neighbor, solid, fluid
     uint64_t prof_steps = 0, prof_stages = 0, prof_launches = 0, prof_l[3] = {0, 0, 0};
 
+    // Asynchronous host exchange (arp_sim_set_particles_async /
+    // arp_sim_get_particles_async): records cross PCIe on two copy streams of
+    // their own through two device staging slots each way, so that the copy
+    // of the next state in, the step on the handle's stream and the copy of
+    // the last result out run at the same time.  Events order each slot's
+    // reuse; record checks accumulate in a sticky flag that
+    // arp_sim_synchronize reports.
+    struct HostIO {
+        cudaStream_t copy_in = nullptr, copy_out = nullptr;
+        DevBuf<arp_particle> in_rec[2], out_rec[2];
+        cudaEvent_t in_copied[2] = {}, in_used[2] = {}, out_ready[2] = {}, out_copied[2] = {};
+        int in_slot = 0, out_slot = 0;
+        uint32_t cap = 0;  // records per staging slot
+        DevBuf<uint32_t> flag;
+        bool ready = false;
+    } io;
+    void release_io() {
+        if (!io.ready) return;
+        if (io.copy_in) cudaStreamSynchronize(io.copy_in);
+        if (io.copy_out) cudaStreamSynchronize(io.copy_out);
+        for (int q = 0; q < 2; ++q)
+            for (cudaEvent_t e : {io.in_copied[q], io.in_used[q], io.out_ready[q], io.out_copied[q]})
+                if (e) cudaEventDestroy(e);
+        if (io.copy_in) cudaStreamDestroy(io.copy_in);
+        if (io.copy_out) cudaStreamDestroy(io.copy_out);
+        io.ready = false;
+    }
+
     ~arp_sim() {
         drop_graph();
+        if (stream) cudaStreamSynchronize(stream);
+        release_io();
         for (auto& m : marks)
             for (auto e : m.e) ev_free.push_back(e);
         for (auto e : ev_free) cudaEventDestroy(e);
@@ -1729,6 +1759,98 @@ arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t 
     return ARP_OK;
 }
 
+namespace {
+// Streams, events, staging slots and the sticky flag of the asynchronous
+// exchange, made on first use.
+arp_status ensure_io(arp_sim* S) {
+    auto& io = S->io;
+    if (io.ready && io.cap >= S->n) return ARP_OK;
+    if (!io.ready) {
+        CUDA_TRY(cudaStreamCreateWithFlags(&io.copy_in, cudaStreamNonBlocking));
+        CUDA_TRY(cudaStreamCreateWithFlags(&io.copy_out, cudaStreamNonBlocking));
+        for (int q = 0; q < 2; ++q)
+            for (cudaEvent_t* e : {&io.in_copied[q], &io.in_used[q], &io.out_ready[q], &io.out_copied[q]})
+                CUDA_TRY(cudaEventCreateWithFlags(e, cudaEventDisableTiming));
+        CUDA_TRY(io.flag.alloc(1));
+        CUDA_TRY(cudaMemsetAsync(io.flag.p, 0, sizeof(uint32_t), S->stream));
+        io.ready = true;
+    }
+    // (re)size the slots: particles were added since they were made
+    CUDA_TRY(cudaStreamSynchronize(io.copy_in));
+    CUDA_TRY(cudaStreamSynchronize(io.copy_out));
+    CUDA_TRY(cudaStreamSynchronize(S->stream));
+    for (int q = 0; q < 2; ++q) {
+        CUDA_TRY(io.in_rec[q].alloc(S->n));
+        CUDA_TRY(io.out_rec[q].alloc(S->n));
+    }
+    io.cap = S->n;
+    return ARP_OK;
+}
+}  // namespace
+
+arp_status arp_sim_set_particles_async(arp_sim* sim, const arp_particle* in, uint32_t n) {
+    ARP_TRY(need_init(sim));
+    if (sim->tape && sim->tape->steps) return fail(ARP_ERR_INVALID_ARG, "a tape is recording steps");
+    if (!in && n) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (n != sim->n) return fail(ARP_ERR_INVALID_ARG, "particle count differs from the handle's");
+    if (!n) return ARP_OK;
+    ARP_TRY(ensure_io(sim));
+    auto& io = sim->io;
+    const int q = io.in_slot;
+    io.in_slot ^= 1;
+    cudaStream_t st = sim->stream;
+    // the slot's previous records have been converted before they are overwritten
+    CUDA_TRY(cudaStreamWaitEvent(io.copy_in, io.in_used[q], 0));
+    CUDA_TRY(cudaMemcpyAsync(io.in_rec[q].p, in, n * sizeof(arp_particle), cudaMemcpyHostToDevice, io.copy_in));
+    CUDA_TRY(cudaEventRecord(io.in_copied[q], io.copy_in));
+    CUDA_TRY(cudaStreamWaitEvent(st, io.in_copied[q], 0));
+    // the conversion takes materials and solid ids from the handle's own
+    // tables, so a record that fails the check cannot reach outside them
+    sim->launches += check_records(io.in_rec[q].p, n, sim->mat_of_caller_d.p, sim->d_mats.p, sim->pos_w,
+                                   io.flag.p, st);
+    sim->launches += records_to_soa(io.in_rec[q].p, n, sim->sid_of_caller_d.p, sim->mat_of_caller_d.p,
+                                    sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, st);
+    CUDA_TRY(cudaEventRecord(io.in_used[q], st));
+    sim->vforce_valid = false;  // a new state: velocity Verlet evaluates its forces again
+    return check_launch("set_particles_async");
+}
+
+arp_status arp_sim_get_particles_async(arp_sim* sim, arp_particle* out, uint32_t cap) {
+    ARP_TRY(need_init(sim));
+    if (!out && sim->n) return fail(ARP_ERR_INVALID_ARG, "null argument");
+    if (cap < sim->n) return fail(ARP_ERR_CAPACITY, "output holds fewer records than n_particles");
+    const uint32_t n = sim->n;
+    if (!n) return ARP_OK;
+    ARP_TRY(ensure_io(sim));
+    auto& io = sim->io;
+    const int q = io.out_slot;
+    io.out_slot ^= 1;
+    cudaStream_t st = sim->stream;
+    // the slot's previous records have left for the host before they are overwritten
+    CUDA_TRY(cudaStreamWaitEvent(st, io.out_copied[q], 0));
+    sim->launches += soa_to_records(sim->Y.pd.p, sim->Y.vm.p, sim->orig.p, sim->sid.p, n, sim->pos_w, sim->d_mats.p,
+                                    io.out_rec[q].p, st);
+    CUDA_TRY(cudaEventRecord(io.out_ready[q], st));
+    CUDA_TRY(cudaStreamWaitEvent(io.copy_out, io.out_ready[q], 0));
+    CUDA_TRY(cudaMemcpyAsync(out, io.out_rec[q].p, n * sizeof(arp_particle), cudaMemcpyDeviceToHost, io.copy_out));
+    CUDA_TRY(cudaEventRecord(io.out_copied[q], io.copy_out));
+    return check_launch("get_particles_async");
+}
+
+arp_status arp_sim_synchronize(arp_sim* sim) {
+    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
+    if (sim->io.ready) CUDA_TRY(cudaStreamSynchronize(sim->io.copy_in));
+    if (sim->stream) CUDA_TRY(cudaStreamSynchronize(sim->stream));
+    if (!sim->io.ready) return check_launch("synchronize");
+    CUDA_TRY(cudaStreamSynchronize(sim->io.copy_out));
+    uint32_t flag = 0;
+    CUDA_TRY(cudaMemcpy(&flag, sim->io.flag.p, sizeof(uint32_t), cudaMemcpyDeviceToHost));
+    if (flag) CUDA_TRY(cudaMemset(sim->io.flag.p, 0, sizeof(uint32_t)));
+    if (flag & 1u) return fail(ARP_ERR_INVALID_ARG, "material of a particle changed (asynchronous set)");
+    if (flag & 2u) return fail(ARP_ERR_UNSUPPORTED, "w components must keep their values (asynchronous set)");
+    return check_launch("synchronize");
+}
+
 arp_status arp_sim_device_state(arp_sim* sim, arp_device_view* out) {
     ARP_TRY(need_init(sim));
     if (!out) return fail(ARP_ERR_INVALID_ARG, "null argument");
@@ -1947,12 +2069,6 @@ arp_status arp_sim_set_stream(arp_sim* sim, void* stream) {
     sim->stream = stream ? (cudaStream_t)stream : sim->own_stream;
     if (sim->graph_stream != sim->stream) sim->drop_graph();
     return ARP_OK;
-}
-
-arp_status arp_sim_synchronize(arp_sim* sim) {
-    if (!sim) return fail(ARP_ERR_INVALID_ARG, "sim is null");
-    CUDA_TRY(cudaStreamSynchronize(sim->stream));
-    return check_launch("synchronize");
 }
 
 arp_status arp_sim_profile_enable(arp_sim* sim, int enable) {

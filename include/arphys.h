@@ -19,7 +19,9 @@
  *   - each handle owns a CUDA stream (or uses the one given by
  *     `arp_sim_set_stream`); device work of a call is ordered on that stream.
  *   - host buffers passed in are only read during the call; host buffers
- *     passed out are written before the call returns.
+ *     passed out are written before the call returns -- except for the two
+ *     `_async` exchange calls, whose buffers belong to the library until the
+ *     next `arp_sim_synchronize`.
  */
 #ifndef ARPHYS_H
 #define ARPHYS_H
@@ -313,6 +315,24 @@ arp_status arp_sim_get_interactions(const arp_sim* sim, arp_interaction* out, ui
 /* Replace the mobile state (den, pos, vel) of all particles, caller order;
  * mat and solid_id of the input must match the handle's. */
 arp_status arp_sim_set_particles(arp_sim* sim, const arp_particle* in, uint32_t n);
+/* Asynchronous forms of arp_sim_set_particles / arp_sim_get_particles (no
+ * counterpart in the reference, whose particles() hands out GL buffers): the
+ * records cross PCIe on copy streams of the handle's own through two device
+ * staging slots each way, ordered with the steps on the handle's stream by
+ * events, so that the copy of the next state in, a step and the copy of the
+ * last result out overlap.  Both return before their copies finish: `in`
+ * must stay unchanged and `out` is valid only after arp_sim_synchronize.
+ * Page-locked host memory lets the copies run truly asynchronously.  The
+ * record checks of arp_sim_set_particles run on the device and are
+ * reported by the next arp_sim_synchronize (ARP_ERR_INVALID_ARG for a
+ * changed material, ARP_ERR_UNSUPPORTED for a changed w component); the
+ * state they replaced takes materials and solid ids from the handle's own
+ * tables either way. */
+arp_status arp_sim_set_particles_async(arp_sim* sim, const arp_particle* in, uint32_t n);
+arp_status arp_sim_get_particles_async(arp_sim* sim, arp_particle* out, uint32_t cap);
+/* Wait for the handle's device work and asynchronous copies; reports the
+ * checks of asynchronous sets since the last call. */
+arp_status arp_sim_synchronize(arp_sim* sim);
 arp_status arp_sim_device_state(arp_sim* sim, arp_device_view* out);
 
 /* FluidSim::add_particles, src/soft_body/mod.rs:180-206 with
@@ -384,7 +404,7 @@ arp_status arp_grid_build_noalloc(const void* pos_den, uint32_t n, const arp_aab
 /* Use a caller-owned CUDA stream (cudaStream_t passed as void*); NULL returns
  * to the handle's own stream. */
 arp_status arp_sim_set_stream(arp_sim* sim, void* stream);
-arp_status arp_sim_synchronize(arp_sim* sim);
+/* (arp_sim_synchronize is declared with the asynchronous exchange above.) */
 /* Per-segment timing (grid build, solid, fluid) with CUDA events between the
  * launches of a step.  enable = 0 stops it; enable = N >= 1 records the events
  * on one step in every N (1: every step; each event costs the step a few

@@ -78,6 +78,9 @@ def test_null_handle_calls_fail_cleanly(lib):
     t = ctypes.c_float()
     assert lib.arp_sim_time(None, ctypes.byref(t)) == 1
     assert lib.arp_sim_step(None, 1) == 1
+    assert lib.arp_sim_set_particles_async(None, None, 0) == 1
+    assert lib.arp_sim_get_particles_async(None, None, 0) == 1
+    assert lib.arp_sim_synchronize(None) == 1
     assert lib.arp_sim_destroy(None) == 0
 
 
