@@ -1,6 +1,9 @@
-"""Seeded scenes of the reference's example files that use velocity Verlet
-(the reference's default integrator, examples/test_mods/config.rs:451), saved
-as fixtures for the GPU tests, which run where the reference tree is absent.
+"""Seeded scenes of the reference's shipped example files, saved as fixtures
+for the GPU tests, which run where the reference tree is absent: every
+example that loads.  model_import_test names an STL model
+(examples/models/gear3.stl) that the reference does not ship, so it loads
+in neither program.  STL paths in the files are relative to the reference's
+root, as the demo runs from there.
 
 Each scene file is parsed and seeded by this library's own loader
 (arp_scene_file_load, checked bit for bit against the restatement in
@@ -21,7 +24,10 @@ sys.path.insert(0, os.path.join(ROOT, "ar-physics_b200"))
 
 from arphys import scenes  # noqa: E402
 
-NAMES = ("cloth", "solid_test_3D", "spinning_ball", "container_buckling")
+NAMES = ("car", "cloth", "container_buckling", "esophagus", "flow_over_cylinder_2d", "flow_over_cylinder_3d",
+         "ink_drop", "interactivity_test", "liquid_solid_test", "metal_bar", "plastic_test", "raindrop",
+         "raindrop_real_time", "rayleigh_taylor", "rope", "siphon", "solid_test", "solid_test_3D", "spinning_ball",
+         "stomach", "wave_3d", "wave_3d_real_time")
 OUT = os.path.join(HERE, "scenes_seeded")
 
 
@@ -30,6 +36,8 @@ def main():
     if not src:
         sys.exit("set ARP_REFERENCE_EXAMPLES to the reference's examples directory")
     os.makedirs(OUT, exist_ok=True)
+    src = os.path.abspath(src)
+    os.chdir(os.path.dirname(src))  # STL paths are relative to the reference's root
     for name in NAMES:
         sc = scenes.load_toml(os.path.join(src, name + ".toml"))
         np.savez_compressed(

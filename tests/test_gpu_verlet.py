@@ -10,37 +10,9 @@ import pytest
 
 from arphys import FluidSim, scenes
 from oracle.oracle import Oracle
-from helpers import load_seeded_scene, rel_err
+from helpers import compare_with_oracle as compare, load_seeded_scene, rel_err
 
 pytestmark = pytest.mark.gpu
-
-
-def compare(sc, steps, tol=1e-5, graph=False, fp32_floor=False):
-    """GPU vs the float oracle within `tol`; with `fp32_floor`, a quantity may
-    instead be as close to the double oracle as twice the float oracle's own
-    distance from it (stiff solids, where float rounding alone moves the
-    velocities by ~1e-4 relative within tens of steps)."""
-    sim = FluidSim(sc)
-    sim.init()
-    if graph:
-        sim.set_graph(True)
-    sim.step(steps)
-    g = sim.particles()
-    o32, o64 = Oracle(sc, 32), Oracle(sc, 64)
-    o32.step(steps)
-    o64.step(steps)
-    r32, r64 = o32.state(), o64.state()
-    assert abs(sim.time() - o32.time) < 1e-6
-    for key in ("den", "pos", "vel"):
-        e = rel_err(g[key], r32[key])
-        e64 = rel_err(g[key], r64[key])
-        e_or = rel_err(r32[key], r64[key])
-        print(f"{sc.name} {key}: vs f32 oracle {e:.2e}, vs f64 oracle {e64:.2e} (f32 oracle vs f64 {e_or:.2e})")
-        if fp32_floor:
-            assert e < tol or e64 <= max(tol, 2.0 * e_or), (sc.name, key, e, e64, e_or)
-        else:
-            assert e < tol, (sc.name, key, e)
-    return sim
 
 
 def test_verlet_dam_break_matches_oracle():

@@ -105,6 +105,23 @@ def test_reference_example_scene_matches_the_oracle(path, monkeypatch):
     assert_same_scene(scenes.load_toml(path), orc)
 
 
+@pytest.mark.skipif(not REFERENCE_EXAMPLES, reason="the reference's example scenes are not mounted")
+def test_seeded_fixtures_are_the_loaders_output(monkeypatch):
+    """tests/golden/scenes_seeded holds what the loader seeds from the
+    reference's shipped scenes (the GPU tests step them where the reference
+    tree is absent); each fixture is the loader's output bit for bit."""
+    from helpers import load_seeded_scene
+    names = sorted(os.path.basename(p)[:-4] for p in glob.glob(os.path.join(HERE, "golden", "scenes_seeded", "*.npz")))
+    assert len(names) == 22
+    monkeypatch.chdir(os.path.dirname(os.path.abspath(_EXAMPLES_DIR)))
+    for name in names:
+        fresh = scenes.load_toml(os.path.join(_EXAMPLES_DIR, name + ".toml"))
+        fix = load_seeded_scene(name)
+        for key in ("particles", "boundary", "materials", "interactions"):
+            assert getattr(fresh, key).tobytes() == getattr(fix, key).tobytes(), (name, key)
+        assert (fresh.h, fresh.dt, fresh.integrator, fresh.subticks) == (fix.h, fix.dt, fix.integrator, fix.subticks)
+
+
 def _write_stl(path, tris, ascii=False):
     """Triangles (F x 3 x 3) with outward normals from the winding."""
     tris = np.asarray(tris, np.float32)
