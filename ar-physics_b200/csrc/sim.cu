@@ -1886,6 +1886,11 @@ arp_status arp_sim_add_particles(arp_sim* sim, const arp_particle* p, uint32_t n
     if (!material || (n && !p)) return fail(ARP_ERR_INVALID_ARG, "null argument");
     if (n == 0) return ARP_OK;  // particles.rs:548: nothing added, no material
     if (sim->scenes.size() != 1) return fail(ARP_ERR_UNSUPPORTED, "add_particles on a batch of scenes");
+    // asynchronous copies in flight finish before the state is rebuilt
+    if (sim->io.ready) {
+        CUDA_TRY(cudaStreamSynchronize(sim->io.copy_in));
+        CUDA_TRY(cudaStreamSynchronize(sim->io.copy_out));
+    }
     if (material->immobile)
         return fail(ARP_ERR_UNSUPPORTED, "added particles join the mobile set; an immobile material is not supported");
     if (sim->tape) return fail(ARP_ERR_UNSUPPORTED, "add_particles while a tape records");

@@ -76,3 +76,38 @@ def test_async_set_reports_a_changed_material_at_synchronize():
     ref.set_particles(good)
     ref.step(1)
     assert out.tobytes() == ref.particles().tobytes()
+
+
+def test_async_exchange_follows_added_particles():
+    """The staging slots grow with the particle count: after add_particles
+    the asynchronous calls move the new count of records, matching the
+    synchronous calls on a twin handle."""
+    import os
+    path = os.path.join(os.path.dirname(os.path.abspath(__file__)), "golden", "scenes", "csg_2d.toml")
+    sc = scenes.load_toml(path)
+    click = sc.meta["on_click"][0]
+    offset = np.array([0.1, -0.05, 0.0, 0.0], np.float32)
+    a, b = FluidSim.from_toml(path), FluidSim.from_toml(path)
+    a.init()
+    b.init()
+    p0 = a.particles()
+    out = np.zeros_like(p0)
+    b.set_particles_async(p0)
+    b.step(1)
+    b.particles_async(out)
+    b.synchronize()
+    a.set_particles(p0)
+    a.step(1)
+    assert a.particles().tobytes() == out.tobytes()
+    a.add_particles(click["particles"], click["material"], offset)
+    b.add_particles(click["particles"], click["material"], offset)
+    p1 = a.particles()
+    assert len(p1) > len(p0)
+    out1 = np.zeros_like(p1)
+    b.set_particles_async(p1)
+    b.step(2)
+    b.particles_async(out1)
+    b.synchronize()
+    a.set_particles(p1)
+    a.step(2)
+    assert a.particles().tobytes() == out1.tobytes()
