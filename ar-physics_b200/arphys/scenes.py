@@ -279,6 +279,23 @@ def batched_scenes(count=256, seed=3, spacing=0.01, n_min=2048, n_max=65536, int
     return out
 
 
+def partition_scenes(sizes, world):
+    """Scene-parallel sharding of a batch over `world` ranks: each scene goes,
+    largest first, to the rank with the least work so far (ties to the lower
+    rank).  Scenes are independent, so ranks step their shares with no
+    exchange.  Returns, per rank, the indices of its scenes in ascending
+    order."""
+    if world < 1:
+        raise ValueError("world must be at least 1")
+    load = [0] * world
+    share = [[] for _ in range(world)]
+    for k in sorted(range(len(sizes)), key=lambda k: (-int(sizes[k]), k)):
+        r = min(range(world), key=lambda q: (load[q], q))
+        share[r].append(k)
+        load[r] += int(sizes[k])
+    return [sorted(x) for x in share]
+
+
 def load_toml(path):
     """A scene file in the reference's TOML schema (examples/test_mods/config.rs)
     parsed and seeded by the library (arp_scene_file_load), copied into a

@@ -265,17 +265,22 @@ def cpu_baseline(config, steps=5, warmup=1):
     return json.loads(r.stdout.strip().splitlines()[-1])
 
 
-def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=200):
+def run_batched(torch, stream, rank=0, world=1, steps_batch=200, rounds_loop=10, steps_variant=200):
     """256 independent scenes (2,048-65,536 particles each, own h, fluid
     blocks and elastic blocks): stepped as one batch (one set of launches per
     stage) and as a loop over 256 separate simulations, both on one GPU and
     both replaying each step from a CUDA graph.  The batch is timed over the
     configuration's 200 steps with the autotuner's launch shape; every
     persistent tile-queue shape of the fluid kernel is timed beside it over
-    the same 200 steps from the same state."""
+    the same 200 steps from the same state.  With N ranks the scenes are
+    sharded (scenes.partition_scenes, by particle count) and each rank steps
+    its share; every time is the slowest rank's, and rates count all 256
+    scenes."""
     from arphys import FluidSim, scenes
-    scs = scenes.batched_scenes()
-    parts = int(sum(sc.n + sc.nb for sc in scs))
+    everything = scenes.batched_scenes()
+    mine = scenes.partition_scenes([sc.n + sc.nb for sc in everything], world)[rank]
+    scs = [everything[k] for k in mine]
+    parts_all = int(sum(sc.n + sc.nb for sc in everything))
     batch = FluidSim.batch(scs)
     batch.init()
     batch.set_stream(stream.cuda_stream)
@@ -289,7 +294,7 @@ def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20
     batch.step(steps_batch)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_batch = e0.elapsed_time(e1) / 1000.0
+    t_batch = max_over_ranks(e0.elapsed_time(e1) / 1000.0, "cuda")
     variant = batch.fluid_variant()
     # the persistent (scene, cell-tile) work-queue shapes, same state, same steps each
     shapes = {}
@@ -305,7 +310,7 @@ def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20
         batch.step(steps_variant)
         e1.record(stream)
         torch.cuda.synchronize()
-        shapes[str(v)] = dict(vi, ms_per_step=e0.elapsed_time(e1) / steps_variant)
+        shapes[str(v)] = dict(vi, ms_per_step=max_over_ranks(e0.elapsed_time(e1), "cuda") / steps_variant)
     batch.set_fluid_variant(variant["variant"])
     best_pers = min(shapes, key=lambda k: shapes[k]["ms_per_step"]) if shapes else None
     # where a batch step goes: a few more steps, untimed, with the library's
@@ -334,13 +339,14 @@ def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20
             sim.step(1)
     e1.record(stream)
     torch.cuda.synchronize()
-    t_loop = e0.elapsed_time(e1) / 1000.0
+    t_loop = max_over_ranks(e0.elapsed_time(e1) / 1000.0, "cuda")
     for sim in sims:
         sim.close()
-    batched = len(scs) * steps_batch / t_batch
-    loop = len(scs) * rounds_loop / t_loop
-    return {"scenes": len(scs), "particles": parts, "integrator": "rk2", "steps": steps_batch,
-            "scene_steps_per_s": batched, "particle_steps_per_s": parts * steps_batch / t_batch,
+    batched = len(everything) * steps_batch / t_batch
+    loop = len(everything) * rounds_loop / t_loop
+    return {"scenes": len(everything), "particles": parts_all, "integrator": "rk2", "steps": steps_batch,
+            "sharding": f"scene-parallel x{world} (largest scene first to the least-loaded rank)",
+            "scene_steps_per_s": batched, "particle_steps_per_s": parts_all * steps_batch / t_batch,
             "ms_per_step": t_batch * 1000.0 / steps_batch,
             "per_scene_loop_scene_steps_per_s": loop, "speedup_vs_per_scene_loop": batched / loop,
             "fluid_launch_shape": variant, "persistent_shapes": shapes, "best_persistent_shape": best_pers,
@@ -348,7 +354,7 @@ def run_batched(torch, stream, steps_batch=200, rounds_loop=10, steps_variant=20
             "solids": int(sum(sc.n_solids() for sc in scs)),
             "note": ("no L2 flush: the batch's state (~%d MB) is larger than L2; both the batch and the "
                      "per-scene loop (%d rounds of one step per simulation) replay CUDA graphs"
-                     % (parts * 32 * 4 // (1 << 20), rounds_loop))}
+                     % (parts_all * 32 * 4 // (1 << 20), rounds_loop))}
 
 
 def _time_adjoint(torch, stream, sim, steps, every, loss_grad, stiff=None):
@@ -671,12 +677,16 @@ def run_ours(args, rank, world, local_rank):
         "e2e": e2e, "roofline": roofline, "clocks": clocks, "gpu_launches": launches,
     }
     line["fluid_launch_shape"] = sim.fluid_variant()
+    # every rank takes part in the batched form (scene-parallel, collectives
+    # for its max-over-ranks times) before rank 0 alone runs the rest
+    if not args.no_batched:
+        batched = run_batched(torch, stream, rank, world)
+        if rank == 0:
+            line["batched"] = batched
     if rank == 0 and not args.no_render:
         line["render"] = run_render(torch, sim, sc)
     if rank == 0 and not args.no_adjoint:
         line["adjoint"] = run_adjoint(torch, stream)
-    if rank == 0 and not args.no_batched:
-        line["batched"] = run_batched(torch, stream)
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         line["cpu_baseline"] = cpu_baseline(args.config)
     if rank == 0:
