@@ -257,9 +257,10 @@ def oracle_sample(config, steps, warmup, max_seconds=60.0):
                       f"run here", "seconds": dt, "steps": done}
 
 
-def cpu_baseline(config, steps=5, warmup=1):
+def cpu_baseline(config, steps=20, warmup=1):
     """oracle_sample in a fresh interpreter (this process has loaded torch,
-    whose OpenMP runtime would otherwise be the one the oracle runs on)."""
+    whose OpenMP runtime would otherwise be the one the oracle runs on): 20
+    full steps of the workload, about 13 s of host time on 16 cores."""
     r = subprocess.run([sys.executable, os.path.abspath(__file__), "--oracle-sample", config, str(steps),
                         str(warmup)], capture_output=True, text=True, check=True)
     return json.loads(r.stdout.strip().splitlines()[-1])
