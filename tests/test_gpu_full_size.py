@@ -4,7 +4,9 @@
     workload): neighbor grid bit-exact against the oracle's serial
     fill_buckets (neighbor_list.rs:37-143), state within 1e-5 of the float
     oracle after 3 RK2 steps, with the FP64 error printed;
-  * the 256 batched scenes (2,048-65,536 particles each) stepped as one batch;
+  * the 256 batched scenes (2,048-65,536 particles each) stepped as one batch,
+    against the oracle for 3 steps and finite and inside their boxes over
+    the workload's 200 steps;
   * eight full-size Rayleigh-Taylor scenes (the first eight of the 64 of the
     batched differentiation workload, 8,192-131,072 particles each): forward
     parity, the batch's gradient equal to each scene's own, and FP64 finite
@@ -90,6 +92,27 @@ def test_batched_workload_all_256_scenes_match_the_oracle():
             worst[key] = max(worst[key], e)
             assert e < TOL, (k, key, e)
     print("256 scenes, worst per quantity:", {k: f"{v:.2e}" for k, v in worst.items()})
+
+
+def test_batched_workload_stays_finite_and_in_its_boxes_over_200_steps():
+    """The batched workload over its 200 steps, as the benchmark times it
+    (one batch, graph replay): every scene finite and inside its box, so the
+    timed steps are the physics the workload describes."""
+    scs = scenes.batched_scenes()
+    batch = FluidSim.batch(scs)
+    batch.init()
+    batch.set_graph(True)
+    batch.step(200)
+    pb = batch.particles()
+    bad = []
+    for k, sc in enumerate(scs):
+        first, n = batch.scene_range(k)[:2]
+        p = pb["pos"][first:first + n, :3].astype(np.float64)
+        lo = np.asarray(sc.bounds_min[:3], np.float64)
+        hi = lo + np.asarray(sc.bounds_dim[:3], np.float64)
+        if not (np.isfinite(p).all() and (p > lo).all() and (p < hi).all()):
+            bad.append(k)
+    assert not bad, bad
 
 
 @pytest.fixture(scope="module")
