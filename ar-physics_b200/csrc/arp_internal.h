@@ -275,7 +275,7 @@ struct FluidVariant {
     int staged;      // candidates staged in shared memory per tile before the scan
                      // (1: cooperative loads, 2: bulk copies on an mbarrier)
 };
-constexpr int kNumFluidVariants = 16;
+constexpr int kNumFluidVariants = 15;
 extern const FluidVariant kFluidVariants[kNumFluidVariants];
 // `tile_counter` (one uint32 on the device) is used by persistent variants.
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,

@@ -935,7 +935,7 @@ const FluidVariant kFluidVariants[kNumFluidVariants] = {
     {128, 96, 0, 0, 0}, {256, 96, 0, 0, 0}, {128, 96, 1, 0, 0}, {256, 96, 1, 0, 0},
     {128, 48, 0, 1, 0}, {128, 48, 1, 1, 0},
     {128, 48, 0, 0, 1}, {64, 48, 0, 0, 1}, {128, 48, 0, 0, 2},
-    {128, 40, 0, 0, 0}, {128, 40, 0, 1, 0}, {128, 32, 0, 1, 0},
+    {128, 40, 0, 1, 0}, {128, 32, 0, 1, 0},
 };
 
 int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs& c, const StageBuffers& b,
@@ -963,8 +963,7 @@ int launch_fluid(const FluidArgs& a, const Tables& T, int kdim, const StageCoefs
     ARP_FLUID(3, 128, 48, 0) ARP_FLUID(3, 256, 48, 0) ARP_FLUID(3, 128, 96, 0) ARP_FLUID(3, 256, 96, 0)
     ARP_FLUID(2, 128, 48, 0) ARP_FLUID(2, 256, 48, 0) ARP_FLUID(2, 128, 96, 0) ARP_FLUID(2, 256, 96, 0)
     ARP_FLUID(3, 128, 48, 1) ARP_FLUID(2, 128, 48, 1)
-    ARP_FLUID(3, 128, 40, 0) ARP_FLUID(3, 128, 40, 1) ARP_FLUID(3, 128, 32, 1)
-    ARP_FLUID(2, 128, 40, 0) ARP_FLUID(2, 128, 40, 1) ARP_FLUID(2, 128, 32, 1)
+    ARP_FLUID(3, 128, 40, 1) ARP_FLUID(3, 128, 32, 1) ARP_FLUID(2, 128, 40, 1) ARP_FLUID(2, 128, 32, 1)
 #undef ARP_FLUID
     return 0;
 }
