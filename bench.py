@@ -417,6 +417,7 @@ def _time_adjoint(torch, stream, sim, steps, every, loss_grad, stiff=None):
             "forward_taped_ms": t_tape,
             "backward_ms": t_mean, "backward_ms_each": t_bwd, "adjoint_fwd_ratio": t_mean / t_fwd, "loss": L,
             "grad_v0_norm": float(np.linalg.norm(g0[:, 4:7])), "grad_stiffness_norm": float(np.linalg.norm(gs)),
+            "fluid_launch_shape": sim.fluid_variant(),  # the autotuner's pick on the initial state
             "timing": "forwards: CUDA events on the library stream (forward_ms: steps replayed from CUDA graphs, "
                       "the ratio's denominator; taped: plain launches); backward: host wall clock around the call "
                       "(it synchronizes), including dL/dy upload and gradient download"}
