@@ -587,6 +587,14 @@ struct CullGrid {
     float lo[3] = {0, 0, 0}, inv[3] = {0, 0, 0};
     int n[3] = {1, 1, 1};
     std::vector<uint32_t> start, items;
+    // cell of the scaled coordinate t = (p - lo) * inv along an axis of n
+    // cells, clamped to [0, n - 1] in float before the conversion (a NaN or a
+    // point far outside the grid would not fit in an int)
+    static int axis_cell(float t, int n) {
+        if (!(t >= 1.0f)) return 0;
+        if (t >= (float)n) return n - 1;
+        return std::min(n - 1, (int)t);
+    }
     void build(const float mn[3], const float mx[3], int dims, size_t count,
                const std::function<void(size_t, float*, float*)>& box) {
         const int g = std::max(1, std::min(dims == 2 ? 512 : 96, (int)std::cbrt((double)count) * (dims == 2 ? 4 : 2)));
@@ -600,8 +608,8 @@ struct CullGrid {
         std::vector<uint32_t> cnt(cells + 1, 0);
         auto range = [&](const float* b0, const float* b1, int* c0, int* c1) {
             for (int a = 0; a < 3; ++a) {
-                c0[a] = std::max(0, std::min(n[a] - 1, (int)std::floor((b0[a] - lo[a]) * inv[a])));
-                c1[a] = std::max(0, std::min(n[a] - 1, (int)std::floor((b1[a] - lo[a]) * inv[a])));
+                c0[a] = axis_cell((b0[a] - lo[a]) * inv[a], n[a]);
+                c1[a] = axis_cell((b1[a] - lo[a]) * inv[a], n[a]);
             }
         };
         for (int pass = 0; pass < 2; ++pass) {
@@ -630,7 +638,7 @@ struct CullGrid {
     std::pair<const uint32_t*, const uint32_t*> query(const float* p) const {
         size_t c = 0, mul = 1;
         for (int a = 0; a < 3; ++a) {
-            const int i = std::max(0, std::min(n[a] - 1, (int)std::floor((p[a] - lo[a]) * inv[a])));
+            const int i = axis_cell((p[a] - lo[a]) * inv[a], n[a]);
             c += (size_t)i * mul;
             mul *= (size_t)n[a];
         }
