@@ -1,0 +1,42 @@
+"""The Rust binding written out in INTEGRATION.md (the declarations a user of
+the reference adds to call this library from `src/soft_body/mod.rs`) declares
+every function of include/arphys.h with the same number of parameters."""
+import os
+import re
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _arity(args):
+    args = args.strip()
+    if args in ("", "void"):
+        return 0
+    return len([a for a in args.split(",") if a.strip()])
+
+
+def header_functions():
+    text = open(os.path.join(ROOT, "include", "arphys.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"\b(arp_[a-z0-9_]+)\s*\(([^;{}]*?)\)\s*;", text):
+        out[m.group(1)] = _arity(m.group(2))
+    return out
+
+
+def rust_functions():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    out = {}
+    for m in re.finditer(r"pub fn (arp_[a-z0-9_]+)\(([^)]*)\)", text):
+        out[m.group(1)] = _arity(m.group(2))
+    return out
+
+
+def test_rust_binding_declares_every_header_function():
+    h, r = header_functions(), rust_functions()
+    assert len(h) > 40
+    missing = sorted(set(h) - set(r))
+    assert not missing, f"functions of include/arphys.h without a Rust declaration: {missing}"
+    extra = sorted(set(r) - set(h))
+    assert not extra, f"Rust declarations with no function in include/arphys.h: {extra}"
+    wrong = {f: (h[f], r[f]) for f in h if h[f] != r[f]}
+    assert not wrong, f"parameter counts differ (header, Rust): {wrong}"
