@@ -103,3 +103,52 @@ def test_scene_with_a_grid_too_large_to_index_is_rejected(lib):
     sc.h = 1e-12
     code, _, msg = _create(lib, sc)
     assert code == 6 and "2^30" in msg
+
+
+@pytest.mark.parametrize("h", [0.0, -0.02, float("nan"), float("inf")])
+def test_kernel_radius_must_be_positive_and_finite(lib, h):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.h = h
+    code, _, msg = _create(lib, sc)
+    assert code == 1 and "kernel_radius" in msg
+
+
+def test_non_finite_timestep_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.dt = float("nan")
+    code, _, msg = _create(lib, sc)
+    assert code == 1 and "timestep" in msg
+
+
+def test_unknown_integrator_id_is_rejected(lib):
+    s, keep = scene_struct(scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2)))
+    s.integrator = 99
+    h = ctypes.c_void_p()
+    assert lib.arp_sim_create(ctypes.byref(s), ctypes.byref(h)) == 1
+    assert b"integrator" in lib.arp_last_error()
+
+
+def test_box_without_extent_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.bounds_dim = (0.0, 0.0, 0.0, 0.0)
+    code, _, msg = _create(lib, sc)
+    assert code == 1 and "extent" in msg
+
+
+def test_velocity_with_a_w_component_is_rejected(lib):
+    sc = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    sc.particles["vel"][2, 3] = 1.0
+    code, _, msg = _create(lib, sc)
+    assert code == 6 and "w component" in msg
+
+
+def test_batch_scenes_must_share_the_time_step(lib):
+    a = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    b = scenes.dam_break_2d(nx=4, ny=4, box=(0.2, 0.2))
+    b.dt = a.dt * 2
+    sa, ka = scene_struct(a)
+    sb, kb = scene_struct(b)
+    arr = (ArpScene * 2)(sa, sb)
+    h = ctypes.c_void_p()
+    assert lib.arp_sim_create_batch(arr, 2, ctypes.byref(h)) == 6
+    assert b"share integrator" in lib.arp_last_error()
