@@ -377,8 +377,8 @@ arp_status arp_sim_boundary_cells(arp_sim* sim, uint32_t* cell_start, uint32_t* 
  * for `n` caller-owned device positions without allocating any memory, for
  * callers that cannot call cudaMalloc on this path: code running inside a
  * host framework that owns the device allocator (a caching allocator or an
- * engine's pre-reserved heap), a real-time loop that forbids allocation after
- * start-up, or work being recorded into a CUDA graph.
+ * engine's pre-reserved heap), or a real-time loop that forbids allocation
+ * after start-up.
  *   pos_den     device float4[n] (x, y, z used; 16-byte aligned), n <= 1048576
  *   cell_start  device uint32[n_cells + 2], n_cells = prod_a max(1, floor(dim_a / h))
  *               <= 4194302: entries c..c+1 bound the slots of cell c, the last

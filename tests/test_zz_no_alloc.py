@@ -1,9 +1,8 @@
 """The allocation-free grid build, called through the C ABI.
 
 arp_grid_build_noalloc serves callers that cannot call cudaMalloc on this
-path (a host framework that owns the device allocator, a real-time loop that
-forbids allocation after start-up, work recorded into a CUDA graph): they
-pass device inputs and outputs they already own, and the call keeps its
+path (a host framework that owns the device allocator, or a real-time loop
+that forbids allocation after start-up): they pass device inputs and outputs they already own, and the call keeps its
 scratch in a fixed device array inside the library.  Its output must equal
 the grid that the handle-based entry point (arp_sim_neighbors) reports for
 the same positions, bit for bit, on consecutive calls that reuse the shared
