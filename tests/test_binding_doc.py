@@ -1,6 +1,7 @@
-"""The Rust binding written out in INTEGRATION.md (the declarations a user of
-the reference adds to call this library from `src/soft_body/mod.rs`) declares
-every function of include/arphys.h with the same number of parameters."""
+"""The Rust binding the integration guide at the repository root writes out
+(the declarations a user of the reference adds to call this library from
+`src/soft_body/mod.rs`) declares every function of include/arphys.h with the
+same number of parameters."""
 import os
 import re
 
