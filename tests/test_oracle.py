@@ -4,7 +4,8 @@ The reference ships no golden vectors, so the oracle is pinned by analytic
 known-answer tests: kernel normalisation and gradient, the correction matrix
 identity on a lattice, the sign of the elastic force on a stretched bar,
 momentum balance of the pair terms, brute-force neighbor sets, and exact
-integration of free fall by the Runge-Kutta tableaus.
+integration of free fall by the Runge-Kutta tableaus, and the order of
+accuracy of every integrator on a smooth two-particle collision.
 """
 import numpy as np
 import pytest
@@ -210,3 +211,53 @@ def test_batched_workload_sample_stays_in_its_box_for_200_steps():
         lo = np.asarray(sc.bounds_min[:3])
         assert np.isfinite(p).all(), sc.name
         assert ((p > lo) & (p < lo + np.asarray(sc.bounds_dim[:3]))).all(), sc.name
+
+
+def _pair_collision(integ, n, horizon=2.0 ** -6):
+    """Two fluid particles 0.5 h apart moving towards each other (pressure,
+    continuity, viscosity and artificial viscosity all active, every pair term
+    smooth while they stay inside h), stepped to `horizon` in n steps of a time
+    step that float32 represents exactly, in the FP64 oracle; returns the
+    final positions, velocities and densities."""
+    mats = np.array([scenes.liquid(1000.0, 20.0, 0.02, 0.0, mass=0.1)])
+    p = np.zeros(2, dtype=PARTICLE_DTYPE)
+    p["den"] = 1000.0
+    p["pos"][0, :2] = (0.49, 0.5)
+    p["pos"][1, :2] = (0.5, 0.503)
+    p["vel"][0, :2] = (0.3, 0.1)
+    p["vel"][1, :2] = (-0.2, -0.05)
+    sc = scenes.Scene(particles=p, boundary=np.zeros(0, PARTICLE_DTYPE), materials=mats,
+                      bounds_min=(0, 0, 0, 0), bounds_dim=(1, 1, 0, 0), h=0.02, integrator=integ,
+                      dt=horizon / n, gravity=0.0)
+    o = Oracle(sc, precision=64)
+    o.step(n)
+    assert o.time == horizon
+    s = o.state()
+    return np.concatenate([s["pos"][:, :2].ravel(), s["vel"][:, :2].ravel(), s["den"]])
+
+
+@pytest.fixture(scope="module")
+def collision_reference():
+    return _pair_collision("rk4", 4096)
+
+
+@pytest.mark.parametrize("integ,order", [("euler", 1), ("midpoint", 2), ("heun2", 2), ("ralston", 2),
+                                         ("rk3", 3), ("heun3", 3), ("rk4", 4), ("rk_3_8", 4)])
+def test_runge_kutta_tableaus_converge_at_their_order(integ, order, collision_reference):
+    """Halving the time step divides the error of an order-p tableau by 2^p:
+    the restated tableaus are the textbook ones (the reference's integrator
+    crate is not vendored)."""
+    errs = [np.abs(_pair_collision(integ, n) - collision_reference).max() for n in (16, 32, 64)]
+    observed = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert all(abs(o - order) < 0.25 for o in observed), (errs, observed)
+
+
+def test_velocity_verlet_converges_at_first_order_on_sph_states(collision_reference):
+    """Velocity Verlet kicks density like velocity, so the force evaluation
+    after the drift sees a half-updated density (and the density rate a
+    half-kicked velocity): on an SPH state the scheme converges at first
+    order, positions included, not at the second order it has for forces of
+    position alone."""
+    errs = [np.abs(_pair_collision("verlet", n) - collision_reference).max() for n in (128, 256, 512)]
+    observed = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
+    assert all(abs(o - 1.0) < 0.2 for o in observed), (errs, observed)
