@@ -4,8 +4,10 @@ The reference ships no golden vectors, so the oracle is pinned by analytic
 known-answer tests: kernel normalisation and gradient, the correction matrix
 identity on a lattice, the sign of the elastic force on a stretched bar,
 momentum balance of the pair terms, brute-force neighbor sets, and exact
-integration of free fall by the Runge-Kutta tableaus, and the order of
-accuracy of every integrator on a smooth two-particle collision.
+integration of free fall by the Runge-Kutta tableaus, the order of
+accuracy of every integrator on a smooth two-particle collision, and the
+symmetries of the step (translation, Galilean boost, rotation) on a scene of
+fluid, an elastic block and a wall.
 """
 import numpy as np
 import pytest
@@ -261,3 +263,95 @@ def test_velocity_verlet_converges_at_first_order_on_sph_states(collision_refere
     errs = [np.abs(_pair_collision("verlet", n) - collision_reference).max() for n in (128, 256, 512)]
     observed = [np.log2(errs[i] / errs[i + 1]) for i in range(2)]
     assert all(abs(o - 1.0) < 0.2 for o in observed), (errs, observed)
+
+
+_Q = 2.0 ** -20  # positions and velocities on this grid shift and rotate exactly in float32
+
+
+def _fluid_block_wall(gravity=9.81, walls=True, seed=7):
+    """2D: a 10 x 10 jittered fluid block (Tait, viscosity, artificial
+    viscosity), a 6 x 6 elastic block moving into it, seeded velocities, and a
+    three-row wall under both, every coordinate a multiple of 2^-20."""
+    rng = np.random.default_rng(seed)
+    s, h = 0.01, 0.02
+
+    def q(a):
+        return np.round(a / _Q) * _Q
+    fluid = q(scenes.jitter(scenes.lattice((0.105, 0.035), (10, 10), s), 1e-3, rng))
+    solid = q(scenes.jitter(scenes.lattice((0.225, 0.035), (6, 6), s), 1e-3, rng))
+    fv = q(rng.normal(0, 0.3, size=fluid.shape))
+    sv = q(rng.normal(0, 0.3, size=solid.shape))
+    sv[:, 0] -= 0.5
+    lam, mu = scenes.lame_from_young(1e5, 0.3)
+    mats = np.array([scenes.immobile(0.0, mass=s * s), scenes.liquid(1000.0, 20.0, h, 0.1, visc=1e-3, mass=0.1),
+                     scenes.elastic_solid(1000.0, lam, mu, mass=0.1)])
+    p = np.concatenate([scenes.particles(fluid, 1, 1000.0, fv), scenes.particles(solid, 2, 1000.0, sv)])
+    wall = q(scenes.lattice((0.005, 0.005), (40, 3), s)) if walls else np.zeros((0, 2))
+    return scenes.Scene(particles=p, boundary=scenes.particles(wall, 0, 1.0), materials=mats,
+                        bounds_min=(0, 0, 0, 0), bounds_dim=(0.4, 0.3, 0, 0), h=h, integrator="rk2", dt=1e-4,
+                        gravity=gravity, alpha=0.1)
+
+
+def _run64(sc, steps=20):
+    o = Oracle(sc, precision=64)
+    o.step(steps)
+    return o.state()
+
+
+def _rel(a, b):
+    return np.abs(a - b).max() / np.abs(b).max()
+
+
+def test_step_is_invariant_under_translation():
+    """Moving every particle and the box by the same vector moves the result
+    by it: the pair terms see only differences, and the grid moves along."""
+    a = _fluid_block_wall()
+    b = _fluid_block_wall()
+    d = np.array([0.5, 0.25])
+    b.particles["pos"][:, :2] += d
+    b.boundary["pos"][:, :2] += d
+    b.bounds_min = (0.5, 0.25, 0.0, 0.0)
+    sa, sb = _run64(a), _run64(b)
+    assert _rel(sb["pos"][:, :2] - d, sa["pos"][:, :2]) < 1e-13
+    assert _rel(sb["vel"], sa["vel"]) < 1e-13
+    assert _rel(sb["den"], sa["den"]) < 1e-13
+
+
+def test_step_is_galilean_invariant_with_solids_drifting_at_twice_their_velocity():
+    """Adding one velocity u to every particle (no walls: they would not move
+    with it) leaves densities and relative velocities unchanged.  Fluid
+    particles end u t further on, elastic ones 2 u t: the fluid and the solid
+    derivative records both carry dx/dt = v and the two are summed (the
+    reference's shaders/mod.rs:79 with fluid.rs:247 and solid.rs:494)."""
+    a = _fluid_block_wall(walls=False)
+    b = _fluid_block_wall(walls=False)
+    u = np.array([0.25, -0.125])
+    b.particles["vel"][:, :2] += u
+    sa, sb = _run64(a, 20), _run64(b, 20)
+    t = 20 * float(np.float32(1e-4))
+    solid = (b.particles["mat"] == 2)[:, None]
+    shift = np.where(solid, 2.0, 1.0) * u * t
+    assert _rel(sb["pos"][:, :2] - shift, sa["pos"][:, :2]) < 1e-13
+    assert _rel(sb["vel"][:, :2] - u, sa["vel"][:, :2]) < 1e-13
+    assert _rel(sb["den"], sa["den"]) < 1e-13
+
+
+def test_step_is_invariant_under_a_quarter_turn():
+    """Without gravity, turning every position and velocity (and the box) by
+    90 degrees turns the result: the pair terms and the solid's strain and
+    stress are isotropic."""
+    def turn(v):
+        return np.stack([-v[:, 1], v[:, 0]], axis=1)
+    a = _fluid_block_wall(gravity=0.0)
+    b = _fluid_block_wall(gravity=0.0)
+    for arr in (b.particles, b.boundary):
+        arr["pos"][:, :2] = turn(arr["pos"][:, :2].astype(np.float64))
+        arr["vel"][:, :2] = turn(arr["vel"][:, :2].astype(np.float64))
+    b.bounds_min = (-0.3, 0.0, 0.0, 0.0)
+    b.bounds_dim = (0.3, 0.4, 0.0, 0.0)
+    sa, sb = _run64(a), _run64(b)
+    assert _rel(sb["pos"][:, :2], turn(sa["pos"][:, :2])) < 1e-13
+    assert _rel(sb["vel"][:, :2], turn(sa["vel"][:, :2])) < 1e-13
+    assert _rel(sb["den"], sa["den"]) < 1e-13
+    moved = np.abs(sa["pos"][:, :2] - a.particles["pos"][:, :2]).max()
+    assert moved > 1e-3  # the scene does move over the 20 steps
