@@ -98,6 +98,10 @@ struct Tableau {
     double b[4];
 };
 
+// The integrators the reference names (examples/test.rs:165-180), whose
+// tableaus live in the un-vendored numerical-integration 0.0.1 crate: the
+// textbook explicit Runge-Kutta tableaus, coefficients in double (rounded to
+// float where the step multiplies them by dt).
 static bool make_tableau(int id, Tableau& t) {
     std::memset(&t, 0, sizeof(t));
     switch (id) {
@@ -138,6 +142,7 @@ template <class T> static T norm_const(uint32_t n, T h) {
     return (pi * pi * pi) / (T(6) * volume_nball<T>(n + 6, h));
 }
 
+// kernel.rs:81-89: poly6 gradient and value, zero from |r| >= h on
 template <class T> static inline vec4<T> grad_w(const vec4<T>& r, T h, T k) {
     T diff = std::max(h * h - dot(r, r), T(0));
     return (T(-6) * k * diff * diff) * r;
@@ -964,6 +969,9 @@ public:
         fcarry = std::move(f);
     }
 
+    // One integrator step of y' = f(y) (mod.rs:252-265 through the crate's
+    // step_with_vel): stage states y0 + sum_j (a_sj dt) k_j, the result
+    // y0 + sum_j (b_j dt) k_j, sums in stage order.
     void step() {
         if (verlet) {
             step_verlet();
