@@ -357,12 +357,14 @@ def test_step_is_invariant_under_a_quarter_turn():
     assert moved > 1e-3  # the scene does move over the 20 steps
 
 
-@pytest.mark.parametrize("order", [2, 0, 1, -2, 3])
-def test_3d_step_commutes_with_a_cyclic_permutation_of_the_axes(order):
+@pytest.mark.parametrize("order,plastic", [(2, False), (0, False), (1, False), (-2, False), (3, False),
+                                           (2, True)])
+def test_3d_step_commutes_with_a_cyclic_permutation_of_the_axes(order, plastic):
     """3D, without gravity: relabelling the axes (x, y, z) -> (z, x, y) for
     every position, velocity and the box relabels the result; the fluid pair
-    terms and the solid's Seth-Hill strain of each order (log series,
-    Denman-Beavers square root, inverse) are isotropic."""
+    terms, the solid's Seth-Hill strain of each order (log series,
+    Denman-Beavers square root, inverse) and Johnson-Cook plastic flow are
+    isotropic."""
     rng = np.random.default_rng(9)
     s, h = 0.01, 0.02
 
@@ -375,7 +377,9 @@ def test_3d_step_commutes_with_a_cyclic_permutation_of_the_axes(order):
     sv[:, 0] -= 0.5
     lam, mu = scenes.lame_from_young(1e5, 0.3)
     mats = np.array([scenes.immobile(0.0, mass=s ** 3), scenes.liquid(1000.0, 20.0, h, 0.1, visc=1e-3, mass=1e-3),
-                     scenes.elastic_solid(1000.0, lam, mu, mass=1e-3, strain_order=order)])
+                     scenes.elastic_solid(1000.0, lam, mu, mass=1e-3, strain_order=order,
+                                          plastic=dict(yield_strength=1e3, work_hardening=1e2, work_hardening_exp=2.0,
+                                                       relaxation_time=1e3) if plastic else None)])
     wall = q(scenes.lattice((0.005, 0.005, 0.005), (30, 2, 30), s))
 
     def make():
@@ -397,3 +401,5 @@ def test_3d_step_commutes_with_a_cyclic_permutation_of_the_axes(order):
     assert _rel(sb["den"], sa["den"]) < 1e-13
     solids = a.particles["mat"] == 2
     assert np.abs(sa["vel"][solids, :3] - a.particles["vel"][solids, :3]).max() > 1e-3  # the solid is loaded
+    if plastic:
+        assert np.abs(sa["plastic"]).max() > 0  # and yields
