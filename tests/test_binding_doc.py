@@ -24,12 +24,13 @@ def header_functions():
     return out
 
 
-def rust_functions():
+def rust_declarations():
     text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
-    out = {}
-    for m in re.finditer(r"pub fn (arp_[a-z0-9_]+)\(([^)]*)\)", text):
-        out[m.group(1)] = _arity(m.group(2))
-    return out
+    return [(m.group(1), _arity(m.group(2))) for m in re.finditer(r"pub fn (arp_[a-z0-9_]+)\(([^)]*)\)", text)]
+
+
+def rust_functions():
+    return dict(rust_declarations())
 
 
 def test_rust_binding_declares_every_header_function():
@@ -41,3 +42,10 @@ def test_rust_binding_declares_every_header_function():
     assert not extra, f"Rust declarations with no function in include/arphys.h: {extra}"
     wrong = {f: (h[f], r[f]) for f in h if h[f] != r[f]}
     assert not wrong, f"parameter counts differ (header, Rust): {wrong}"
+
+
+def test_rust_binding_declares_each_function_once():
+    """One crate may not declare an extern function twice."""
+    names = [n for n, _ in rust_declarations()]
+    dup = sorted({n for n in names if names.count(n) > 1})
+    assert not dup, f"declared more than once: {dup}"
