@@ -49,3 +49,29 @@ def test_rust_binding_declares_each_function_once():
     names = [n for n, _ in rust_declarations()]
     dup = sorted({n for n in names if names.count(n) > 1})
     assert not dup, f"declared more than once: {dup}"
+
+
+def _header_structs():
+    text = open(os.path.join(ROOT, "include", "arphys.h")).read()
+    text = re.sub(r"/\*.*?\*/", "", text, flags=re.S)
+    out = {}
+    for m in re.finditer(r"typedef struct (arp_\w+)\s*\{(.*?)\}\s*\1\s*;", text, flags=re.S):
+        decls = [d.strip() for d in m.group(2).split(";") if d.strip()]
+        out[m.group(1)] = sum(len(d.split(",")) for d in decls)  # `uint32_t mat, solid_id;` is two fields
+    return out
+
+
+def _rust_structs():
+    text = open(os.path.join(ROOT, "INTEGRATION.md")).read()
+    return {m.group(1): len(re.findall(r"\bpub\s+\w+\s*:", m.group(2)))
+            for m in re.finditer(r"pub struct (arp_\w+)\s*\{(.*?)\}", text, flags=re.S)}
+
+
+def test_rust_records_have_the_header_fields():
+    """Every record of the header has a #[repr(C)] twin in the binding with the
+    same number of fields (the field types follow the header line by line)."""
+    h, r = _header_structs(), _rust_structs()
+    assert len(h) >= 10
+    assert sorted(h) == sorted(r), (sorted(set(h) ^ set(r)))
+    wrong = {k: (h[k], r[k]) for k in h if h[k] != r[k]}
+    assert not wrong, f"field counts differ (header, Rust): {wrong}"
