@@ -271,7 +271,9 @@ _Q = 2.0 ** -20  # positions and velocities on this grid shift and rotate exactl
 def _fluid_block_wall(gravity=9.81, walls=True, seed=7):
     """2D: a 10 x 10 jittered fluid block (Tait, viscosity, artificial
     viscosity), a 6 x 6 elastic block moving into it, seeded velocities, and a
-    three-row wall under both, every coordinate a multiple of 2^-20."""
+    three-row wall with Coulomb friction 5 under both (friction acts on the
+    pairs of the wall with the fluid and the solid), every coordinate a
+    multiple of 2^-20."""
     rng = np.random.default_rng(seed)
     s, h = 0.01, 0.02
 
@@ -283,7 +285,7 @@ def _fluid_block_wall(gravity=9.81, walls=True, seed=7):
     sv = q(rng.normal(0, 0.3, size=solid.shape))
     sv[:, 0] -= 0.5
     lam, mu = scenes.lame_from_young(1e5, 0.3)
-    mats = np.array([scenes.immobile(0.0, mass=s * s), scenes.liquid(1000.0, 20.0, h, 0.1, visc=1e-3, mass=0.1),
+    mats = np.array([scenes.immobile(5.0, mass=s * s), scenes.liquid(1000.0, 20.0, h, 0.1, visc=1e-3, mass=0.1),
                      scenes.elastic_solid(1000.0, lam, mu, mass=0.1)])
     p = np.concatenate([scenes.particles(fluid, 1, 1000.0, fv), scenes.particles(solid, 2, 1000.0, sv)])
     wall = q(scenes.lattice((0.005, 0.005), (40, 3), s)) if walls else np.zeros((0, 2))
